@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark of the pattern-evaluator fitting path on B200.
+
+Workload (one step): the 20M-row, 8-pattern fit — 20,000,000 random-play
+positions with empty counts uniform in 20..40, patterns edge+2X, 3x3 corner,
+2x5 corner, main diagonal, rows 2/3/4 and the 7-square diagonal, each under
+the 8 board symmetries (expanded layout: 166,212 columns, 64 entries per
+row, 1.28e9 entries), seeded synthetic targets.  A step is FitWeights on
+device-resident positions and targets: indexing, CSR and transposed-copy
+build, Jacobi, and mixed-precision Jacobi-PCG to a relative normal-equation
+residual of 1e-8.  The metric is the time of that step (lower is better);
+the plain FP64 GPU path on the same system is reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs under torchrun, one rank per GPU, each rank fitting its own
+independently seeded replica (the fits are independent; no collective on
+the data path).  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "time to rel. residual 1e-8: mixed/batched vs plain FP64 GPU; SpMV HBM GB/s"
+PATTERNS_8 = [0x42FF, 0x070707, 0x1F1F, 0x8040201008040201, 0xFF00, 0xFF0000, 0xFF000000, 0x0080402010080402]
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--rows", type=int, default=20_000_000)
+    ap.add_argument("--min-empties", type=int, default=20)
+    ap.add_argument("--max-empties", type=int, default=40)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-sample-rows", type=int, default=200_000,
+                    help="rows of the bounded sample the CPU baseline runs")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    return ap.parse_args(argv)
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, flags in rows for i, f in enumerate(flags) if f.lower() == "active"})
+        busy = [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------- ours
+
+def run_ours(args) -> dict | None:
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    import cassandra_b200 as cb
+    from cassandra_b200 import _lib as L
+
+    lib = cb.load()
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    seed = args.seed + 7919 * rank
+    R = args.rows
+
+    # Inputs, resident in HBM before the timed region (positions 320 MB > L2).
+    pos = cb.generate_positions(seed, R, args.min_empties, args.max_empties)
+    g = cb.GroupIndexer(PATTERNS_8, "expanded")
+    cols, K = g.index_space_size, g.nnz_per_row
+    a0 = cb.MatrixCSR.from_positions(g, pos)
+    b = cb.generate_targets(a0, seed)
+    torch.cuda.synchronize()
+    nnz = R * K
+
+    # ---- roofline of the two sparse products (FP32, as in the mixed solver)
+    def time_kernel(fn, n=10):
+        for _ in range(2):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / n * 1e-3
+
+    x32 = torch.randn(cols, dtype=torch.float32, device="cuda")
+    y32 = torch.randn(R, dtype=torch.float32, device="cuda")
+    yo = torch.empty(R, dtype=torch.float32, device="cuda")
+    xo = torch.empty(cols, dtype=torch.float32, device="cuda")
+    t_spmv = time_kernel(lambda: L.check(lib.cas_spmv(a0.handle, L.CAS_F32, C.c_void_p(x32.data_ptr()),
+                                                      C.c_void_p(yo.data_ptr()), sp)))
+    t_spmv_t = time_kernel(lambda: L.check(lib.cas_spmv_t(a0.handle, L.CAS_F32, C.c_void_p(y32.data_ptr()),
+                                                          C.c_void_p(xo.data_ptr()), sp)))
+    units = int(np.ceil(nnz / 2048)) + cols  # upper bound of A'y work units
+    bytes_spmv = 4 * nnz + 4 * R + 4 * cols
+    bytes_spmv_t = 4 * nnz + 4 * R + 4 * cols + 8 * (cols + 1)
+    del x32, y32, yo, xo
+    del a0
+    torch.cuda.synchronize()
+
+    opts_mixed = cb.solve_opts("pcg", "mixed", args.tol, 20000, 50, 50)
+    opts_plain = cb.solve_opts("pcg", "fp64", args.tol, 20000, 50, 50)
+    w = torch.empty(cols, dtype=torch.float64, device="cuda")
+
+    def fit(opts):
+        rep = L.SolveReport()
+        st = lib.cas_fit_weights_device(g.handle, C.c_void_p(pos.data_ptr()), C.c_void_p(b.data_ptr()), R,
+                                        C.byref(opts), C.c_void_p(w.data_ptr()), C.byref(rep), sp)
+        if st != L.CAS_OK:
+            L.check(st)
+        return rep
+
+    for _ in range(args.warmup):
+        fit(opts_mixed)
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.cas_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    reps = [fit(opts_mixed) for _ in range(args.steps)]
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    launches = lib.cas_kernel_launches() - launches0
+    clk = clocks.stop()
+    elapsed = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        dist.barrier()
+        t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    per_step = elapsed / args.steps
+
+    # plain FP64 GPU path on the same system (the comparison the metric names)
+    plain = None if args.no_plain else fit(opts_plain)
+    mixed = reps[-1]
+
+    # ---- end to end through the public C ABI with host buffers
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
+    pos_h = torch.empty((R, 2), dtype=torch.int64, pin_memory=True)
+    pos_h.copy_(pos)
+    sc_h = torch.empty(R, dtype=torch.float32, pin_memory=True)
+    sc_h.copy_(b.float())
+    w_h = torch.empty(cols, dtype=torch.float32, pin_memory=True)
+    masks = np.asarray(PATTERNS_8, np.uint64)
+    e2e_times = []
+    for _ in range(e2e_steps):
+        rep = L.SolveReport()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = lib.cas_fit_weights(masks.ctypes.data_as(C.c_void_p), len(masks), L.CAS_INDEX_EXPANDED,
+                                 C.c_void_p(pos_h.data_ptr()), C.c_void_p(sc_h.data_ptr()), R, C.byref(opts_mixed),
+                                 C.c_void_p(w_h.data_ptr()), C.byref(rep))
+        e2e_times.append(time.perf_counter() - t0)
+        L.check(st)
+    e2e_val = statistics.mean(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_val], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = float(t.item())
+
+    peak, peak_kind = measured_peaks()
+    kernels = {
+        "spmv_f32": {"seconds": t_spmv, "bytes": bytes_spmv, "gbs": bytes_spmv / t_spmv / 1e9},
+        "spmv_t_f32": {"seconds": t_spmv_t, "bytes": bytes_spmv_t, "gbs": bytes_spmv_t / t_spmv_t / 1e9},
+    }
+    dom = max(kernels, key=lambda k: kernels[k]["seconds"])
+    ach = kernels[dom]["gbs"]
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, seed, mixed.iterations)
+
+    result = {
+        "metric": METRIC,
+        "value": per_step,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 products / f64 scalars",
+        "data": "synthetic (seeded random-play positions, seeded targets)",
+        "config": {
+            "workload": f"8-pattern expanded fit, {R} rows, empties {args.min_empties}..{args.max_empties}, "
+                        f"mixed Jacobi-PCG to rel. normal-eq. residual {args.tol:g}",
+            "rows": R, "cols": cols, "nnz_per_row": K, "nnz": nnz, "method": "pcg", "precision": "mixed",
+            "refine_every": 50, "tol": args.tol,
+            "l2": "inputs larger than L2 (positions 320 MB, CSR 5.1 GB)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        },
+        "breakdown": {
+            "build_s": mixed.setup_seconds, "solve_s": mixed.seconds, "iterations": mixed.iterations,
+            "refinements": mixed.refinements, "rel_residual": mixed.rel_residual,
+        },
+        "plain_fp64": None if plain is None else {
+            "step_s": plain.setup_seconds + plain.seconds, "solve_s": plain.seconds, "iterations": plain.iterations,
+            "rel_residual": plain.rel_residual,
+            "solve_speedup_mixed_vs_plain": plain.seconds / mixed.seconds if mixed.seconds else None,
+        },
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": ach / peak, "peak_kind": peak_kind, "traffic": None},
+        "kernels": kernels,
+        "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": int(pos_h.numel() * 8 + sc_h.numel() * 4),
+                "d2h_bytes_per_step": int(w_h.numel() * 4), "steps": e2e_steps},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result if rank == 0 else None
+
+
+# ---------------------------------------------------------------- CPU reference
+
+def _reference_sample(rows: int, seed: int, min_e: int, max_e: int) -> dict:
+    """One bounded sample of the workload on the host cores with the
+    reference's own code: its A_Indexer recipe over FastIndex/Flipped* for the
+    expanded layout, then its Math/ PCG retyped to FP64, run to 1e-8."""
+    import oracle
+    import cassandra_b200 as cb
+
+    ref, ref64 = oracle.ref_lib(), oracle.ref64_lib()
+    ref.ref_expanded_index.restype = None
+    ref.ref_expanded_index.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p]
+    pos = cb.generate_positions_host(seed, 0, rows, min_e, max_e)  # seeded input generation (not timed)
+    m = np.asarray(PATTERNS_8, np.uint64)
+    idx = np.empty((rows, 64), np.uint32)
+    t0 = time.perf_counter()
+    ref.ref_expanded_index(m.ctypes.data_as(C.c_void_p), len(m), pos.ctypes.data_as(C.c_void_p), rows,
+                           idx.ctypes.data_as(C.c_void_p))
+    t_index = time.perf_counter() - t0
+    cols = int(sum(3 ** bin(x).count("1") for x in PATTERNS_8))
+    rng = np.random.default_rng(seed)
+    wst = rng.normal(0, 0.5, cols)
+    b = np.clip(2 * np.rint((wst[idx].sum(axis=1) + rng.normal(0, 4, rows)) / 2), -64, 64)
+    x = np.empty(cols)
+    rel, sec = np.zeros(1), np.zeros(1)
+    it = ref64.ref64_pcg(64, rows, cols, idx.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p), 20000, 1e-8,
+                         10, x.ctypes.data_as(C.c_void_p), rel.ctypes.data_as(C.c_void_p),
+                         sec.ctypes.data_as(C.c_void_p))
+    return {"index_s": t_index, "solve_s": float(sec[0]), "iterations": int(it), "rel_residual": float(rel[0])}
+
+
+def cpu_baseline(args, seed: int, gpu_iterations: int | None = None) -> dict | None:
+    try:
+        import oracle
+
+        if not oracle.ref_available():
+            return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+                    "sample": "unavailable: oracle/_ref not built"}
+    except Exception as e:  # pragma: no cover
+        return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference", "sample": f"error {e}"}
+    n = args.cpu_sample_rows
+    s = _reference_sample(n, seed, args.min_empties, args.max_empties)
+    scale = args.rows / n
+    value = (s["index_s"] + s["solve_s"]) * scale
+    return {"value": value, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"{n} of {args.rows} rows; reference A_Indexer recipe (FastIndex/Flipped*) + reference "
+                      f"Math/ PCG retyped to FP64 run to 1e-8 ({s['iterations']} iterations, rel {s['rel_residual']:.2e}"
+                      f", index {s['index_s']:.3f} s, solve {s['solve_s']:.2f} s), time scaled by rows x{scale:g}; "
+                      f"OMP threads = {os.environ.get('OMP_NUM_THREADS', os.cpu_count())}"}
+
+
+def run_reference(args) -> dict | None:
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return None
+    import oracle
+
+    if not oracle.ref_available():
+        return {"impl": "reference", "metric": METRIC,
+                "unavailable": "oracle/_ref (reference sources compiled here) is missing"}
+    times, last = [], None
+    n = args.cpu_sample_rows
+    for i in range(args.warmup + args.steps):
+        s = _reference_sample(n, args.seed, args.min_empties, args.max_empties)
+        if i >= args.warmup:
+            times.append((s["index_s"] + s["solve_s"]) * args.rows / n)
+            last = s
+    value = statistics.mean(times)
+    cb = {"value": value, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+          "sample": f"each step: {n} of {args.rows} rows, reference indexing + FP64 PCG to 1e-8 "
+                    f"({last['iterations']} iterations), time scaled by rows x{args.rows / n:g}"}
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random-play positions, seeded targets)",
+        "config": {"workload": f"8-pattern expanded fit, {args.rows} rows, empties {args.min_empties}.."
+                               f"{args.max_empties}, FP64 Jacobi-PCG to rel. normal-eq. residual {args.tol:g}",
+                   "rows": args.rows},
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main(argv=None) -> int:
+    args = parse_args(argv)
+    res = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

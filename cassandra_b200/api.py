@@ -1,0 +1,353 @@
+"""Python mirror of the reference's fitting API over the C ABI.
+
+Names follow the reference: ``GroupIndexer`` (Pattern/Indexer.h:29-40),
+``MatrixCSR`` with ``A @ x`` / ``x @ A`` (Math/MatrixCSR.h:11-33),
+``jacobi_preconditioner_of_ata`` (Math/MatrixCSR.h:30), the iterative solvers
+``PCG``, ``CG`` and ``LSQR`` with ``iterate`` / ``residuum`` / ``x`` / ``error``
+(Math/Solver.h:9-182), and ``fit_weights`` (PatternFit/PatternFit.cpp:7-39).
+
+Device data is exchanged as CUDA torch tensors (PyTorch is used only for
+device memory and the current stream); host data as numpy arrays.  Size
+errors raise ``SizeMismatch`` like the reference's ``runtime_error("Size
+mismatch.")``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+_REF_MODES = {"reference": L.CAS_INDEX_REFERENCE, "expanded": L.CAS_INDEX_EXPANDED}
+
+
+def _stream() -> C.c_void_p:
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t: torch.Tensor | None) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr() if t is not None else 0)
+
+
+def _require_cuda(t: torch.Tensor, name: str) -> None:
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+class GroupIndexer:
+    """GroupIndexer(std::vector<uint64_t>) (Pattern/Indexer.cpp:382-392).
+
+    mode="reference" is bit-exact with the reference; mode="expanded" uses
+    3^k columns and all 8 symmetry instances for every mask."""
+
+    def __init__(self, masks, mode: str = "reference"):
+        self._lib = L.load()
+        m = np.ascontiguousarray(masks, dtype=np.uint64)
+        if m.ndim != 1 or len(m) == 0:
+            raise ValueError("masks must be a non-empty 1-D sequence")
+        self.masks = m
+        self.mode = mode
+        h = C.c_void_p()
+        L.check(self._lib.cas_patterns_create(m.ctypes.data_as(C.c_void_p), len(m), _REF_MODES[mode], C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.cas_patterns_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @property
+    def index_space_size(self) -> int:
+        return int(self._lib.cas_patterns_cols(self._h))
+
+    @property
+    def nnz_per_row(self) -> int:
+        return int(self._lib.cas_patterns_nnz_per_row(self._h))
+
+    def variations(self) -> np.ndarray:
+        out = np.empty(self.nnz_per_row, dtype=np.uint64)
+        L.check(self._lib.cas_patterns_variations(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def indexer(self, i: int) -> dict:
+        sp, order, space, off = C.c_uint64(), C.c_int(), C.c_int64(), C.c_int64()
+        L.check(self._lib.cas_patterns_indexer(self._h, i, C.byref(sp), C.byref(order), C.byref(space),
+                                               C.byref(off)))
+        return {"pattern": sp.value, "order": order.value, "space": space.value, "offset": off.value}
+
+    def indices(self, positions: torch.Tensor) -> torch.Tensor:
+        """positions: CUDA int64 [n, 2] (P, O) -> int32 [n, K] (uint32 bit patterns)."""
+        _require_cuda(positions, "positions")
+        n = positions.shape[0]
+        out = torch.empty((n, self.nnz_per_row), dtype=torch.int32, device=positions.device)
+        L.check(self._lib.cas_index(self._h, _ptr(positions), n, _ptr(out), _stream()))
+        return out
+
+
+class MatrixCSR:
+    """Device-resident MatrixCSR with implicit 1.0 entries and its transposed copy."""
+
+    def __init__(self, handle: C.c_void_p, keep=None):
+        self._lib = L.load()
+        self._h = handle
+        self._keep = keep
+
+    @classmethod
+    def from_positions(cls, indexer: GroupIndexer, positions: torch.Tensor) -> "MatrixCSR":
+        _require_cuda(positions, "positions")
+        lib = L.load()
+        h = C.c_void_p()
+        L.check(lib.cas_csr_from_positions(indexer.handle, _ptr(positions), positions.shape[0], _stream(), C.byref(h)))
+        return cls(h, keep=indexer)
+
+    @classmethod
+    def from_indices(cls, indices: torch.Tensor, cols: int) -> "MatrixCSR":
+        """indices: CUDA int32 [rows, K] (column indices, copied)."""
+        _require_cuda(indices, "indices")
+        lib = L.load()
+        h = C.c_void_p()
+        L.check(lib.cas_csr_from_indices(_ptr(indices), indices.shape[1], indices.shape[0], cols, _stream(),
+                                         C.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            torch.cuda.current_stream().synchronize()
+            self._lib.cas_csr_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def rows(self) -> int:
+        return int(self._lib.cas_csr_rows(self._h))
+
+    def cols(self) -> int:
+        return int(self._lib.cas_csr_cols(self._h))
+
+    @property
+    def nnz_per_row(self) -> int:
+        return int(self._lib.cas_csr_nnz_per_row(self._h))
+
+    def indices(self) -> torch.Tensor:
+        """Copy of the row-major column indices (int32 [rows, K])."""
+        src = self._lib.cas_csr_indices(self._h)
+        return _device_view(src, (self.rows(), self.nnz_per_row), "<i4").clone()
+
+    def transposed(self) -> tuple[torch.Tensor, torch.Tensor]:
+        """Copies of (col_ptr int64 [cols+1], row_idx int32 [nnz]) of the transposed copy."""
+        cp, ri = C.c_void_p(), C.c_void_p()
+        L.check(self._lib.cas_csr_transposed(self._h, C.byref(cp), C.byref(ri)))
+        col_ptr = _device_view(cp.value, (self.cols() + 1,), "<i8").clone()
+        row_idx = _device_view(ri.value, (self.rows() * self.nnz_per_row,), "<i4").clone()
+        return col_ptr, row_idx
+
+    def _dtype(self, t: torch.Tensor) -> int:
+        if t.dtype == torch.float32:
+            return L.CAS_F32
+        if t.dtype == torch.float64:
+            return L.CAS_F64
+        raise TypeError("vectors must be float32 or float64")
+
+    def matvec(self, x: torch.Tensor) -> torch.Tensor:
+        """A x (operator*(const MatrixCSR&, const Vector&))."""
+        _require_cuda(x, "x")
+        if x.numel() != self.cols():
+            raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+        y = torch.empty(self.rows(), dtype=x.dtype, device=x.device)
+        L.check(self._lib.cas_spmv(self._h, self._dtype(x), _ptr(x), _ptr(y), _stream()))
+        return y
+
+    def rmatvec(self, y: torch.Tensor) -> torch.Tensor:
+        """A' y, i.e. the reference's y * A (operator*(const Vector&, const MatrixCSR&))."""
+        _require_cuda(y, "y")
+        if y.numel() != self.rows():
+            raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+        x = torch.empty(self.cols(), dtype=y.dtype, device=y.device)
+        L.check(self._lib.cas_spmv_t(self._h, self._dtype(y), _ptr(y), _ptr(x), _stream()))
+        return x
+
+    def __matmul__(self, x: torch.Tensor) -> torch.Tensor:
+        return self.matvec(x)
+
+    def __rmatmul__(self, y: torch.Tensor) -> torch.Tensor:
+        return self.rmatvec(y)
+
+
+class _CudaArray:
+    """Borrowed view of library-owned device memory (CUDA array interface v3)."""
+
+    def __init__(self, ptr: int, shape: tuple, typestr: str):
+        self.__cuda_array_interface__ = {"data": (int(ptr or 0), True), "shape": tuple(shape), "typestr": typestr,
+                                         "version": 3, "strides": None}
+
+
+def _device_view(ptr: int, shape: tuple, typestr: str) -> torch.Tensor:
+    if int(np.prod(shape)) == 0:
+        return torch.empty(shape, dtype={"<i4": torch.int32, "<i8": torch.int64}[typestr], device="cuda")
+    return torch.as_tensor(_CudaArray(ptr, shape, typestr), device="cuda")
+
+
+def jacobi_preconditioner_of_ata(a: MatrixCSR, dtype=torch.float64) -> torch.Tensor:
+    """1 / diag(A'A) (Math/MatrixCSR.cpp:21-47); empty columns give inf."""
+    out = torch.empty(a.cols(), dtype=dtype, device="cuda")
+    L.check(a._lib.cas_jacobi(a.handle, L.CAS_F32 if dtype == torch.float32 else L.CAS_F64, _ptr(out), _stream()))
+    return out
+
+
+def solve_opts(method: str = "pcg", precision: str = "fp64", tol: float = 1e-8, max_iterations: int = 20000,
+               refine_every: int = 50, check_every: int = 50, jacobi: bool = True) -> L.SolveOpts:
+    o = L.SolveOpts()
+    L.load().cas_solve_opts_default(C.byref(o))
+    o.method = {"pcg": L.CAS_PCG, "lsqr": L.CAS_LSQR, "cg": L.CAS_CG}[method]
+    o.precision = {"fp64": L.CAS_PLAIN_FP64, "mixed": L.CAS_MIXED}[precision]
+    o.tol = tol
+    o.max_iterations = max_iterations
+    o.refine_every = refine_every
+    o.check_every = check_every
+    o.jacobi = int(jacobi)
+    return o
+
+
+class _Solver:
+    """IterativeSolver (Math/Solver.h:9-16) over a device-resident system."""
+
+    method = "pcg"
+
+    def __init__(self, a: MatrixCSR, b: torch.Tensor, x0: torch.Tensor | None = None, precision: str = "fp64",
+                 tol: float = 0.0, max_iterations: int = 1 << 30, refine_every: int = 50, check_every: int = 50,
+                 jacobi: bool = True):
+        _require_cuda(b, "b")
+        if b.dtype != torch.float64:
+            b = b.double()
+        if b.numel() != a.rows():
+            raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+        if x0 is not None:
+            x0 = x0.double().contiguous()
+            if x0.numel() != a.cols():
+                raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+        self._lib = L.load()
+        self.a = a
+        self.b = b.contiguous()
+        self.opts = solve_opts(self.method, precision, tol, max_iterations, refine_every, check_every, jacobi)
+        h = C.c_void_p()
+        L.check(self._lib.cas_solver_create(a.handle, C.byref(self.opts), _ptr(self.b), _ptr(x0), _stream(),
+                                            C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.cas_solver_destroy(h)
+            self._h = None
+
+    def iterate(self, n: int = 1) -> None:
+        L.check(self._lib.cas_solver_iterate(self._h, n))
+
+    def residuum(self) -> float:
+        v = C.c_double()
+        L.check(self._lib.cas_solver_residuum(self._h, C.byref(v)))
+        return v.value
+
+    def x(self) -> torch.Tensor:
+        out = torch.empty(self.a.cols(), dtype=torch.float64, device="cuda")
+        L.check(self._lib.cas_solver_x(self._h, _ptr(out)))
+        return out
+
+    def rel_residual(self) -> float:
+        v = C.c_double()
+        L.check(self._lib.cas_solver_rel_residual(self._h, C.byref(v)))
+        return v.value
+
+    def iterations(self) -> int:
+        return int(self._lib.cas_solver_iterations(self._h))
+
+    def run(self) -> dict:
+        rep = L.SolveReport()
+        st = self._lib.cas_solver_run(self._h, C.byref(rep))
+        if st not in (L.CAS_OK, L.CAS_ERR_NOT_CONVERGED):
+            L.check(st)
+        d = rep.as_dict()
+        d["converged"] = st == L.CAS_OK
+        return d
+
+
+class PCG(_Solver):
+    """PCG(transposed(A) * A, DiagonalPreconditioner(Jacobi), x0, transposed(A) * b)."""
+
+    method = "pcg"
+
+
+class CG(_Solver):
+    """CG on A'A x = A'b (Math/Solver.h:40-76)."""
+
+    method = "cg"
+
+
+class LSQR(_Solver):
+    """LSQR(A, x0, b) (Math/Solver.h:128-182)."""
+
+    method = "lsqr"
+
+
+def fit_weights(masks, positions: np.ndarray, scores: np.ndarray, mode: str = "reference", method: str = "pcg",
+                precision: str = "fp64", tol: float = 1e-8, max_iterations: int = 20000,
+                refine_every: int = 50, check_every: int = 50) -> tuple[np.ndarray, dict]:
+    """FitWeights with host buffers in and out (PatternFit/PatternFit.cpp:7-39).
+
+    tol <= 0 runs exactly max_iterations iterations, as the reference's
+    FitWeights(pattern, positions, iterations) does."""
+    lib = L.load()
+    m = np.ascontiguousarray(masks, dtype=np.uint64)
+    pos = np.ascontiguousarray(positions, dtype=np.uint64).reshape(-1, 2)
+    sc = np.ascontiguousarray(scores, dtype=np.float32)
+    if len(sc) != len(pos):
+        raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+    h = C.c_void_p()
+    L.check(lib.cas_patterns_create(m.ctypes.data_as(C.c_void_p), len(m), _REF_MODES[mode], C.byref(h)))
+    cols = int(lib.cas_patterns_cols(h))
+    lib.cas_patterns_destroy(h)
+    w = np.empty(cols, dtype=np.float32)
+    o = solve_opts(method, precision, tol, max_iterations, refine_every, check_every)
+    rep = L.SolveReport()
+    st = lib.cas_fit_weights(m.ctypes.data_as(C.c_void_p), len(m), _REF_MODES[mode], pos.ctypes.data_as(C.c_void_p),
+                             sc.ctypes.data_as(C.c_void_p), len(pos), C.byref(o), w.ctypes.data_as(C.c_void_p),
+                             C.byref(rep))
+    if st not in (L.CAS_OK, L.CAS_ERR_NOT_CONVERGED):
+        L.check(st)
+    d = rep.as_dict()
+    d["converged"] = st == L.CAS_OK
+    return w, d
+
+
+def generate_positions(seed: int, n: int, min_empties: int, max_empties: int, device="cuda") -> torch.Tensor:
+    """Seeded random-play positions as CUDA int64 [n, 2]."""
+    out = torch.empty((n, 2), dtype=torch.int64, device=device)
+    L.check(L.load().cas_generate_positions(seed, n, min_empties, max_empties, _ptr(out), _stream()))
+    return out
+
+
+def generate_positions_host(seed: int, first: int, n: int, min_empties: int, max_empties: int) -> np.ndarray:
+    out = np.empty((n, 2), dtype=np.uint64)
+    L.check(L.load().cas_generate_positions_host(seed, first, n, min_empties, max_empties,
+                                                 out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+def generate_targets(a: MatrixCSR, seed: int, w_sigma: float = 0.5, noise_sigma: float = 4.0,
+                     return_true_weights: bool = False):
+    b = torch.empty(a.rows(), dtype=torch.float64, device="cuda")
+    w = torch.empty(a.cols(), dtype=torch.float64, device="cuda") if return_true_weights else None
+    L.check(L.load().cas_generate_targets(a.handle, seed, w_sigma, noise_sigma, _ptr(b), _ptr(w), _stream()))
+    return (b, w) if return_true_weights else b

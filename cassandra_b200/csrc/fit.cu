@@ -1,0 +1,219 @@
+// FitWeights (PatternFit/PatternFit.cpp:7-39) end to end on the device, and
+// the seeded synthetic data generator.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "board.cuh"
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace cas {
+namespace {
+
+__global__ void generate_positions_kernel(uint64_t seed, int64_t n, int min_e, int max_e, ulonglong2* __restrict__ out,
+                                          unsigned int* __restrict__ failures)
+{
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        uint64_t p, o;
+        if (!random_play_position(seed, static_cast<uint64_t>(i), min_e, max_e, p, o)) atomicAdd(failures, 1u);
+        out[i] = make_ulonglong2(p, o);
+    }
+}
+
+// w*_c ~ N(0, sigma^2) by Box-Muller on the counter stream (seed, c).
+__global__ void true_weights_kernel(uint64_t seed, int64_t cols, double sigma, double* __restrict__ w)
+{
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cols;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        Stream rng(seed ^ 0x5EED0F3EC7ED1ULL, static_cast<uint64_t>(c));
+        const double u1 = rng.unit(), u2 = rng.unit();
+        w[c] = sigma * sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+    }
+}
+
+// b_r = clamp(2 rint((A w*)_r + e_r) / 2), -64, 64), e_r ~ N(0, noise^2).
+__global__ void targets_kernel(const uint32_t* __restrict__ idx, int64_t rows, int k, const double* __restrict__ w,
+                               uint64_t seed, double noise, double* __restrict__ b)
+{
+    for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < rows;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double acc = 0;
+        for (int j = 0; j < k; j++) acc += w[idx[r * k + j]];
+        Stream rng(seed ^ 0xB0A5EDD15EA5EULL, static_cast<uint64_t>(r));
+        const double u1 = rng.unit(), u2 = rng.unit();
+        const double e = noise * sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+        b[r] = fmin(64.0, fmax(-64.0, 2.0 * rint((acc + e) * 0.5)));
+    }
+}
+
+__global__ void f32_to_f64_kernel(const float* __restrict__ in, int64_t n, double* __restrict__ out)
+{
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        out[i] = static_cast<double>(in[i]);
+}
+
+__global__ void f64_to_f32_kernel(const double* __restrict__ in, int64_t n, float* __restrict__ out)
+{
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        out[i] = static_cast<float>(in[i]);
+}
+
+unsigned grid(int64_t n)
+{
+    return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sm_count() * 16LL)));
+}
+
+}  // namespace
+}  // namespace cas
+
+using namespace cas;
+
+extern "C" {
+
+CAS_API cas_status cas_generate_positions(uint64_t seed, int64_t n, int min_empties, int max_empties,
+                                          uint64_t* d_out, void* stream)
+{
+    CAS_REQUIRE(n >= 0 && (n == 0 || d_out), CAS_ERR_INVALID_ARGUMENT, "cas_generate_positions: bad argument");
+    CAS_REQUIRE(0 <= min_empties && min_empties <= max_empties && max_empties <= 60, CAS_ERR_INVALID_ARGUMENT,
+                "cas_generate_positions: empty counts must satisfy 0 <= min <= max <= 60");
+    CAS_REQUIRE((reinterpret_cast<uintptr_t>(d_out) & 15) == 0, CAS_ERR_INVALID_ARGUMENT,
+                "cas_generate_positions: output must be 16-byte aligned");
+    CAS_TRY(require_device());
+    if (n == 0) return CAS_OK;
+    auto s = static_cast<cudaStream_t>(stream);
+    unsigned int* fails = nullptr;
+    CAS_CUDA(cudaMallocAsync(&fails, sizeof(unsigned int), s));
+    CAS_CUDA(cudaMemsetAsync(fails, 0, sizeof(unsigned int), s));
+    { generate_positions_kernel<<<grid(n), 256, 0, s>>>(seed, n, min_empties, max_empties,
+                                                      reinterpret_cast<ulonglong2*>(d_out), fails); cas::count_launch(); }
+    CAS_CHECK_LAUNCH();
+    unsigned int h = 0;
+    CAS_CUDA(cudaMemcpyAsync(&h, fails, sizeof h, cudaMemcpyDeviceToHost, s));
+    CAS_CUDA(cudaStreamSynchronize(s));
+    cudaFreeAsync(fails, s);
+    CAS_REQUIRE(h == 0, CAS_ERR_INVALID_ARGUMENT, "cas_generate_positions: target empty count unreachable");
+    return CAS_OK;
+}
+
+CAS_API cas_status cas_generate_positions_host(uint64_t seed, int64_t first, int64_t n, int min_empties,
+                                               int max_empties, uint64_t* h_out)
+{
+    CAS_REQUIRE(n >= 0 && first >= 0 && (n == 0 || h_out), CAS_ERR_INVALID_ARGUMENT,
+                "cas_generate_positions_host: bad argument");
+    CAS_REQUIRE(0 <= min_empties && min_empties <= max_empties && max_empties <= 60, CAS_ERR_INVALID_ARGUMENT,
+                "cas_generate_positions_host: empty counts must satisfy 0 <= min <= max <= 60");
+    bool ok = true;
+#pragma omp parallel for schedule(static) reduction(&& : ok)
+    for (int64_t i = 0; i < n; i++) {
+        uint64_t p, o;
+        ok = random_play_position(seed, static_cast<uint64_t>(first + i), min_empties, max_empties, p, o) && ok;
+        h_out[2 * i] = p;
+        h_out[2 * i + 1] = o;
+    }
+    CAS_REQUIRE(ok, CAS_ERR_INVALID_ARGUMENT, "cas_generate_positions_host: target empty count unreachable");
+    return CAS_OK;
+}
+
+CAS_API cas_status cas_generate_targets(const cas_csr* a, uint64_t seed, double w_sigma, double noise_sigma,
+                                        double* d_b, double* d_w_true, void* stream)
+{
+    CAS_REQUIRE(a && (d_b || a->rows == 0), CAS_ERR_INVALID_ARGUMENT, "cas_generate_targets: bad argument");
+    auto s = static_cast<cudaStream_t>(stream);
+    double* w = d_w_true;
+    if (!w) CAS_CUDA(cudaMallocAsync(&w, sizeof(double) * std::max<int64_t>(a->cols, 1), s));
+    { true_weights_kernel<<<grid(a->cols), 256, 0, s>>>(seed, a->cols, w_sigma, w); cas::count_launch(); }
+    CAS_CHECK_LAUNCH();
+    if (a->rows) {
+        { targets_kernel<<<grid(a->rows), 256, 0, s>>>(a->idx, a->rows, a->k, w, seed, noise_sigma, d_b); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+    }
+    if (!d_w_true) cudaFreeAsync(w, s);
+    return CAS_OK;
+}
+
+CAS_API cas_status cas_fit_weights_device(const cas_patterns* p, const uint64_t* d_positions, const double* d_scores,
+                                          int64_t rows, const cas_solve_opts* o, double* d_weights,
+                                          cas_solve_report* rep, void* stream)
+{
+    CAS_REQUIRE(p && o && d_weights, CAS_ERR_INVALID_ARGUMENT, "cas_fit_weights_device: null argument");
+    CAS_REQUIRE(rows >= 0 && (rows == 0 || (d_positions && d_scores)), CAS_ERR_INVALID_ARGUMENT,
+                "cas_fit_weights_device: bad rows or buffers");
+    auto s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0, e1;
+    CAS_CUDA(cudaEventCreate(&e0));
+    CAS_CUDA(cudaEventCreate(&e1));
+    CAS_CUDA(cudaEventRecord(e0, s));
+    cas_csr* a = nullptr;
+    cas_status st = cas_csr_from_positions(p, d_positions, rows, stream, &a);
+    if (st != CAS_OK) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return st;
+    }
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float setup_ms = 0;
+    cudaEventElapsedTime(&setup_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st = cas_solve(a, o, d_scores, d_weights, rep, stream);
+    if (rep) rep->setup_seconds = setup_ms * 1e-3;
+    cas_csr_destroy(a);
+    return st;
+}
+
+CAS_API cas_status cas_fit_weights(const uint64_t* masks, int n_masks, cas_index_mode mode,
+                                   const uint64_t* h_positions, const float* h_scores, int64_t rows,
+                                   const cas_solve_opts* o, float* h_weights, cas_solve_report* rep)
+{
+    CAS_REQUIRE(masks && o && h_weights && rows >= 0, CAS_ERR_INVALID_ARGUMENT, "cas_fit_weights: bad argument");
+    CAS_REQUIRE(rows == 0 || (h_positions && h_scores), CAS_ERR_INVALID_ARGUMENT, "cas_fit_weights: null input");
+    CAS_TRY(require_device());
+    cas_patterns* p = nullptr;
+    CAS_TRY(cas_patterns_create(masks, n_masks, mode, &p));
+    const int64_t cols = cas_patterns_cols(p);
+    cudaStream_t s = nullptr;
+    CAS_CUDA(cudaStreamCreate(&s));
+    uint64_t* d_pos = nullptr;
+    float* d_s32 = nullptr;
+    double *d_s = nullptr, *d_w = nullptr;
+    float* d_w32 = nullptr;
+    cas_status st = CAS_OK;
+    auto fail = [&](cudaError_t e) {
+        set_error(std::string("cas_fit_weights: ") + cudaGetErrorString(e));
+        st = e == cudaErrorMemoryAllocation ? CAS_ERR_OUT_OF_MEMORY : CAS_ERR_CUDA;
+    };
+    cudaError_t e = cudaMalloc(&d_pos, 16 * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_s32, sizeof(float) * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_s, sizeof(double) * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_w, sizeof(double) * std::max<int64_t>(cols, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_w32, sizeof(float) * std::max<int64_t>(cols, 1));
+    if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_pos, h_positions, 16 * rows, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_s32, h_scores, sizeof(float) * rows, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) fail(e);
+    if (st == CAS_OK) {
+        { f32_to_f64_kernel<<<grid(rows), 256, 0, s>>>(d_s32, rows, d_s); cas::count_launch(); }
+        st = cas_fit_weights_device(p, d_pos, d_s, rows, o, d_w, rep, s);
+    }
+    if (st == CAS_OK || st == CAS_ERR_NOT_CONVERGED) {
+        { f64_to_f32_kernel<<<grid(cols), 256, 0, s>>>(d_w, cols, d_w32); cas::count_launch(); }
+        e = cudaMemcpyAsync(h_weights, d_w32, sizeof(float) * cols, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) fail(e);
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(d_pos);
+    cudaFree(d_s32);
+    cudaFree(d_s);
+    cudaFree(d_w);
+    cudaFree(d_w32);
+    cudaStreamDestroy(s);
+    cas_patterns_destroy(p);
+    return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,953 @@
+// Iterative solvers on the device: Jacobi-PCG on the normal equations
+// (Math/Solver.h:78-117, driven as in PatternFit/PatternFit.cpp:29-32), CG
+// (P = I, Math/Solver.h:40-76) and LSQR (Math/Solver.h:128-182).
+//
+// All solver state and every scalar (alpha, beta, r.z, norms) lives on the
+// device, so an iteration is a fixed sequence of kernel launches with no
+// host round trip; `check_every` iterations are captured once as a CUDA graph
+// and replayed.  After convergence every kernel returns at entry (device
+// flag), so the tail of a chunk costs only launch latency.
+//
+// Precision modes:
+//   CAS_PLAIN_FP64  FP64 vectors, FP64 sparse products, plain FP64 sums.
+//   CAS_MIXED       FP32 gather vectors (p for A p, q = A p for A' q) — exact
+//                   for A's 0/1 entries up to the rounding of the vectors —
+//                   FP64 accumulation inside the products, FP64 compensated
+//                   (Neumaier) dots and norms, and every refine_every
+//                   iterations the true normal-equation residual
+//                   A'(b - A x) recomputed in FP64 and substituted for the
+//                   recursive one (residual replacement, search direction
+//                   kept).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace cas {
+
+namespace {
+
+constexpr int kVecThreads = 256;
+constexpr int kRedThreads = 1024;
+
+// Device scalar slots.
+enum Slot {
+    kRz = 0,      // r.z
+    kPap = 1,     // p.A'A p = ||A p||^2
+    kAlpha = 2,
+    kBeta = 3,
+    kRr = 4,      // r.r (Residuum of PCG)
+    kBn2 = 5,     // ||A'b||^2
+    kRes = 6,     // sqrt(rr / bn2), recursive
+    kTol = 7,
+    // LSQR
+    kLAlpha = 8, kLBeta = 9, kPhiBar = 10, kRhoBar = 11, kPhiRho = 12, kThetaRho = 13, kInvBeta = 14,
+    kArNorm = 15,  // |phi_bar * alpha * c| estimate of ||A'r||
+    kTrue = 16,    // ||A'(b - A x)||^2 of the last true-residual evaluation
+    kSlots = 17
+};
+enum Flag { kDone = 0, kStatus = 1, kIter = 2, kRefine = 3, kFlags = 4 };
+
+struct Dev {
+    double* scal;
+    int* flags;
+};
+
+__device__ __forceinline__ bool finished(const int* flags) { return *(volatile const int*)flags != 0; }
+
+// Sum of n (s, c) partial pairs in a fixed order by one block.
+template <bool COMP>
+__device__ double reduce_partials(const double* part, int n, double* smem)
+{
+    Comp acc;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        if (COMP) {
+            acc.add(part[2 * i]);
+            acc.add(part[2 * i + 1]);
+        } else {
+            acc.s += part[2 * i];
+        }
+    }
+    if (COMP) return block_sum_comp<kRedThreads>(acc, smem).value();
+    return block_sum<kRedThreads>(acc.s, smem);
+}
+
+template <bool COMP>
+__device__ void write_partial(double* part, Comp v, double* smem)
+{
+    if (COMP) {
+        Comp r = block_sum_comp<kVecThreads>(v, smem);
+        if (threadIdx.x == 0) {
+            part[2 * blockIdx.x] = r.s;
+            part[2 * blockIdx.x + 1] = r.c;
+        }
+    } else {
+        double r = block_sum<kVecThreads>(v.s, smem);
+        if (threadIdx.x == 0) {
+            part[2 * blockIdx.x] = r;
+            part[2 * blockIdx.x + 1] = 0;
+        }
+    }
+}
+
+template <bool COMP>
+__device__ __forceinline__ void acc_add(Comp& c, double x)
+{
+    if (COMP)
+        c.add(x);
+    else
+        c.s += x;
+}
+
+// ---------------------------------------------------------------------------
+// Products with fused reductions.
+// ---------------------------------------------------------------------------
+
+// q = A p (+ optionally q -= coef * q_old for LSQR), partial ||q||^2.
+// mode 0: q = A p.  mode 1 (LSQR): q = A p - scal[coef_slot] * q (in place).
+// mode 2 (residual): q = b - A p, FP64 (b given).
+template <typename T, typename Q, bool COMP, int MODE>
+__global__ void __launch_bounds__(kVecThreads) spmv_norm_kernel(const uint32_t* __restrict__ idx, int64_t rows, int k,
+                                                                 const T* __restrict__ p, Q* __restrict__ q,
+                                                                 const double* __restrict__ b,
+                                                                 double* __restrict__ part, Dev dv, int coef_slot,
+                                                                 int force)
+{
+    __shared__ double smem[64];
+    if (!force && finished(dv.flags)) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+    const double coef = MODE == 1 ? dv.scal[coef_slot] : 0.0;
+    Comp mine;
+    for (int64_t r = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows;
+         r += warps) {
+        const uint32_t* row = idx + r * k;
+        double acc = 0;
+        for (int j = lane; j < k; j += 32) acc += static_cast<double>(__ldg(p + __ldg(row + j)));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+            if (MODE == 1) acc -= coef * static_cast<double>(q[r]);
+            if (MODE == 2) acc = b[r] - acc;
+            q[r] = static_cast<Q>(acc);
+            const double qq = static_cast<double>(static_cast<Q>(acc));
+            acc_add<COMP>(mine, qq * qq);
+        }
+    }
+    write_partial<COMP>(part, mine, smem);
+}
+
+// Partial sums of A' q per work unit (deterministic, FP64 accumulation).
+template <typename Q>
+__global__ void __launch_bounds__(kVecThreads) spmv_t_units_flag_kernel(CsrView a, const Q* __restrict__ q,
+                                                                        double* __restrict__ partial, Dev dv,
+                                                                        int ignore_flag)
+{
+    if (!ignore_flag && finished(dv.flags)) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t u = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); u < a.units;
+         u += warps) {
+        const int32_t c = a.unit_col[u];
+        const int64_t begin = a.col_ptr[c] + static_cast<int64_t>(u - a.unit_ptr[c]) * kUnit;
+        const int64_t end = min(a.col_ptr[c + 1], begin + kUnit);
+        double acc = 0;
+        for (int64_t e = begin + lane; e < end; e += 32) acc += static_cast<double>(__ldg(q + __ldg(a.row_idx + e)));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) partial[u] = acc;
+    }
+}
+
+__device__ __forceinline__ double unit_sum(const CsrView& a, const double* partial, int64_t c)
+{
+    double acc = 0;
+    for (uint32_t u = a.unit_ptr[c]; u < a.unit_ptr[c + 1]; u++) acc += partial[u];
+    return acc;
+}
+
+// ---------------------------------------------------------------------------
+// PCG vector steps.
+// ---------------------------------------------------------------------------
+
+// alpha = rz / pAp (single block).  Breakdown when pAp <= 0 with rz > 0.
+template <bool COMP>
+__global__ void __launch_bounds__(kRedThreads) pcg_alpha_kernel(const double* __restrict__ part, int n, Dev dv)
+{
+    __shared__ double smem[64];
+    if (finished(dv.flags)) return;
+    const double pap = reduce_partials<COMP>(part, n, smem);
+    if (threadIdx.x == 0) {
+        const double rz = dv.scal[kRz];
+        dv.scal[kPap] = pap;
+        if (!(pap > 0) || !isfinite(pap)) {
+            dv.scal[kAlpha] = 0;
+            if (rz != 0) dv.flags[kStatus] = CAS_ERR_BREAKDOWN;
+            dv.flags[kDone] = 1;
+        } else {
+            dv.scal[kAlpha] = rz / pap;
+        }
+    }
+}
+
+// s = A'A p (from unit partials); x += alpha p; r -= alpha s; z = d r;
+// partials of r.z and r.r.
+template <bool COMP>
+__global__ void __launch_bounds__(kVecThreads) pcg_update_kernel(CsrView a, const double* __restrict__ partial,
+                                                                 double* __restrict__ x, double* __restrict__ r,
+                                                                 double* __restrict__ z, const double* __restrict__ p,
+                                                                 const double* __restrict__ d,
+                                                                 double* __restrict__ part_rz,
+                                                                 double* __restrict__ part_rr, Dev dv)
+{
+    __shared__ double smem[64];
+    if (finished(dv.flags)) return;
+    const double alpha = dv.scal[kAlpha];
+    Comp rz, rr;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < a.cols;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double s = unit_sum(a, partial, c);
+        x[c] += alpha * p[c];
+        const double rc = r[c] - alpha * s;
+        const double zc = d[c] * rc;
+        r[c] = rc;
+        z[c] = zc;
+        acc_add<COMP>(rz, rc * zc);
+        acc_add<COMP>(rr, rc * rc);
+    }
+    write_partial<COMP>(part_rz, rz, smem);
+    write_partial<COMP>(part_rr, rr, smem);
+}
+
+// rz_new, rr -> beta, residual, convergence (single block).
+// replace != 0: residual-replacement step; r.z is replaced but beta and the
+// iteration count are left alone.
+template <bool COMP>
+__global__ void __launch_bounds__(kRedThreads) pcg_beta_kernel(const double* __restrict__ part_rz,
+                                                               const double* __restrict__ part_rr, int n, Dev dv,
+                                                               int replace, int force)
+{
+    __shared__ double smem[64];
+    if (!force && finished(dv.flags)) return;
+    const double rz_new = reduce_partials<COMP>(part_rz, n, smem);
+    const double rr = reduce_partials<COMP>(part_rr, n, smem);
+    if (threadIdx.x == 0) {
+        const double rz = dv.scal[kRz];
+        const double bn2 = dv.scal[kBn2];
+        const double res = bn2 > 0 ? sqrt(rr / bn2) : sqrt(rr);
+        if (!replace) {
+            dv.scal[kBeta] = rz != 0 ? rz_new / rz : 0.0;
+            dv.flags[kIter] += 1;
+        } else {
+            dv.flags[kRefine] += 1;
+        }
+        dv.scal[kRz] = rz_new;
+        dv.scal[kRr] = rr;
+        dv.scal[kRes] = res;
+        if (!isfinite(rz_new) || !isfinite(rr)) {
+            dv.flags[kStatus] = CAS_ERR_BREAKDOWN;
+            dv.flags[kDone] = 1;
+        } else if (dv.scal[kTol] > 0 && res <= dv.scal[kTol]) {
+            dv.flags[kDone] = 1;
+        }
+    }
+}
+
+// p = z + beta p (and the FP32 gather copy).
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) pcg_direction_kernel(int64_t n, const double* __restrict__ z,
+                                                                    double* __restrict__ p, T* __restrict__ pg,
+                                                                    Dev dv)
+{
+    if (finished(dv.flags)) return;
+    const double beta = dv.scal[kBeta];
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double v = z[c] + beta * p[c];
+        p[c] = v;
+        if (pg) pg[c] = static_cast<T>(v);
+    }
+}
+
+// r = A'(b - A x) from unit partials; z = d r; partials of r.z and r.r.
+// Also initialises p = z (init != 0) and ||A'b||^2 (bn != 0, x = 0).
+template <bool COMP, typename T>
+__global__ void __launch_bounds__(kVecThreads) pcg_residual_kernel(CsrView a, const double* __restrict__ partial,
+                                                                   double* __restrict__ r, double* __restrict__ z,
+                                                                   double* __restrict__ p, T* __restrict__ pg,
+                                                                   const double* __restrict__ d,
+                                                                   double* __restrict__ part_rz,
+                                                                   double* __restrict__ part_rr, int init, Dev dv,
+                                                                   int force)
+{
+    __shared__ double smem[64];
+    if (!force && finished(dv.flags)) return;
+    Comp rz, rr;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < a.cols;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double rc = unit_sum(a, partial, c);
+        const double zc = d[c] * rc;
+        r[c] = rc;
+        z[c] = zc;
+        if (init) {
+            p[c] = zc;
+            if (pg) pg[c] = static_cast<T>(zc);
+        }
+        acc_add<COMP>(rz, rc * zc);
+        acc_add<COMP>(rr, rc * rc);
+    }
+    write_partial<COMP>(part_rz, rz, smem);
+    write_partial<COMP>(part_rr, rr, smem);
+}
+
+// DiagonalPreconditioner (Math/Solver.h:25-38): d = 1/diag(A'A), entries that
+// are not normal (inf from an empty column) become 1.  jacobi == 0: d = 1.
+__global__ void precond_kernel(const uint64_t* __restrict__ diag, int64_t n, int jacobi, double* __restrict__ d)
+{
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double v = 1.0;
+        if (jacobi) {
+            v = 1.0 / static_cast<double>(diag[c]);
+            if (!(isfinite(v) && fabs(v) >= 2.2250738585072014e-308)) v = 1.0;  // not std::isnormal
+        }
+        d[c] = v;
+    }
+}
+
+template <typename T>
+__global__ void cast_kernel(int64_t n, const double* __restrict__ in, T* __restrict__ out)
+{
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        out[c] = static_cast<T>(in[c]);
+}
+
+// ||v||^2 partials of a vector (used for ||A'b||^2 and ||A'r||^2).
+template <bool COMP>
+__global__ void __launch_bounds__(kVecThreads) norm_units_kernel(CsrView a, const double* __restrict__ partial,
+                                                                 double* __restrict__ out, double* __restrict__ part)
+{
+    __shared__ double smem[64];
+    Comp acc;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < a.cols;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double v = unit_sum(a, partial, c);
+        if (out) out[c] = v;
+        acc_add<COMP>(acc, v * v);
+    }
+    write_partial<COMP>(part, acc, smem);
+}
+
+template <bool COMP>
+__global__ void __launch_bounds__(kRedThreads) store_sum_kernel(const double* __restrict__ part, int n,
+                                                                double* __restrict__ dst)
+{
+    __shared__ double smem[64];
+    const double v = reduce_partials<COMP>(part, n, smem);
+    if (threadIdx.x == 0) *dst = v;
+}
+
+// ---------------------------------------------------------------------------
+// LSQR steps (Math/Solver.h:139-177) with deferred normalisation: u and v
+// are stored unnormalised (u_hat, v_hat) next to their scale 1/beta, 1/alpha
+// held as device scalars, so no separate scaling pass is needed.
+// ---------------------------------------------------------------------------
+
+// v_hat = (1/beta) A' u_hat - beta v  (v = v_hat_prev / alpha_prev);
+// partial ||v_hat||^2.  init: v_hat = (1/beta) A' u_hat.
+template <bool COMP, typename T>
+__global__ void __launch_bounds__(kVecThreads) lsqr_v_kernel(CsrView a, const double* __restrict__ partial,
+                                                             double* __restrict__ v, double* __restrict__ part,
+                                                             Dev dv, int init)
+{
+    __shared__ double smem[64];
+    if (!init && finished(dv.flags)) return;
+    const double inv_beta = dv.scal[kInvBeta];
+    const double beta = dv.scal[kLBeta];
+    const double inv_alpha_prev = dv.scal[kLAlpha] != 0 ? 1.0 / dv.scal[kLAlpha] : 0.0;
+    Comp acc;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < a.cols;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double val = inv_beta * unit_sum(a, partial, c);
+        if (!init) val -= beta * (v[c] * inv_alpha_prev);
+        v[c] = val;
+        acc_add<COMP>(acc, val * val);
+    }
+    write_partial<COMP>(part, acc, smem);
+}
+
+// beta = ||u_hat|| (u_hat = A v - alpha u, alpha u = alpha/beta_prev u_hat_prev
+// folded into the SpMV's coefficient slot).  Single block.
+template <bool COMP>
+__global__ void __launch_bounds__(kRedThreads) lsqr_beta_kernel(const double* __restrict__ part, int n, Dev dv,
+                                                                int init)
+{
+    __shared__ double smem[64];
+    if (!init && finished(dv.flags)) return;
+    const double s = reduce_partials<COMP>(part, n, smem);
+    if (threadIdx.x == 0) {
+        const double beta = sqrt(s);
+        dv.scal[kLBeta] = beta;
+        dv.scal[kInvBeta] = beta > 0 ? 1.0 / beta : 0.0;
+        if (init) dv.scal[kPhiBar] = beta;  // phi_bar = beta (Math/Solver.h:149)
+    }
+}
+
+// alpha = ||v_hat||; Givens step; scalars for the x/w update.  Single block.
+template <bool COMP>
+__global__ void __launch_bounds__(kRedThreads) lsqr_alpha_kernel(const double* __restrict__ part, int n, Dev dv,
+                                                                 int init)
+{
+    __shared__ double smem[64];
+    if (!init && finished(dv.flags)) return;
+    const double s = reduce_partials<COMP>(part, n, smem);
+    if (threadIdx.x == 0) {
+        const double alpha = sqrt(s);
+        if (init) {
+            dv.scal[kLAlpha] = alpha;
+            dv.scal[kRhoBar] = alpha;  // rho_bar = alpha (Math/Solver.h:150)
+            dv.scal[kArNorm] = alpha * dv.scal[kLBeta];
+            return;
+        }
+        const double beta = dv.scal[kLBeta];
+        const double rho_bar = dv.scal[kRhoBar], phi_bar = dv.scal[kPhiBar];
+        const double rho = sqrt(rho_bar * rho_bar + beta * beta);
+        if (!(rho > 0) || !isfinite(rho)) {
+            dv.scal[kPhiRho] = 0;
+            dv.scal[kThetaRho] = 0;
+            dv.flags[kDone] = 1;
+            if (!isfinite(rho)) dv.flags[kStatus] = CAS_ERR_BREAKDOWN;
+            return;
+        }
+        const double c = rho_bar / rho, sn = beta / rho;
+        const double theta = sn * alpha;
+        const double phi = c * phi_bar;
+        dv.scal[kRhoBar] = -c * alpha;
+        dv.scal[kPhiBar] = sn * phi_bar;
+        dv.scal[kPhiRho] = phi / rho;
+        dv.scal[kThetaRho] = theta / rho;
+        dv.scal[kLAlpha] = alpha;
+        // ||A'r_k|| = phi_bar_{k+1} * alpha_{k+1} * |c_k| (Paige & Saunders 1982)
+        const double arn = fabs(sn * phi_bar * alpha * c);
+        dv.scal[kArNorm] = arn;
+        dv.flags[kIter] += 1;
+        const double bn2 = dv.scal[kBn2];
+        const double res = bn2 > 0 ? arn / sqrt(bn2) : arn;
+        dv.scal[kRes] = res;
+        if (dv.scal[kTol] > 0 && res <= dv.scal[kTol]) dv.flags[kDone] = 1;
+    }
+}
+
+// x += (phi/rho) w; w = v - (theta/rho) w; gather copy vg = v (normalised).
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) lsqr_xw_kernel(int64_t n, double* __restrict__ x,
+                                                              double* __restrict__ w, const double* __restrict__ v,
+                                                              T* __restrict__ vg, Dev dv, int init)
+{
+    if (!init && finished(dv.flags)) return;
+    const double inv_alpha = dv.scal[kLAlpha] != 0 ? 1.0 / dv.scal[kLAlpha] : 0.0;
+    const double phi_rho = dv.scal[kPhiRho], theta_rho = dv.scal[kThetaRho];
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double vn = v[c] * inv_alpha;
+        if (init) {
+            w[c] = vn;
+        } else {
+            x[c] += phi_rho * w[c];
+            w[c] = vn - theta_rho * w[c];
+        }
+        vg[c] = static_cast<T>(vn);
+    }
+}
+
+// coefficient of the u recursion: alpha / beta_prev (u_hat holds beta_prev u).
+__global__ void lsqr_coef_kernel(Dev dv, int slot)
+{
+    if (finished(dv.flags)) return;
+    dv.scal[slot] = dv.scal[kLAlpha] * dv.scal[kInvBeta];
+}
+
+unsigned vec_grid(int64_t n)
+{
+    const int64_t want = (n + kVecThreads - 1) / kVecThreads;
+    return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(sm_count()) * 4)));
+}
+unsigned row_grid(int64_t rows)
+{
+    const int64_t want = (rows + 7) / 8;
+    return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(sm_count()) * 16)));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Solver object.
+// ---------------------------------------------------------------------------
+struct SolverImpl {
+    const cas_csr* A = nullptr;
+    CsrView a;
+    cas_solve_opts o{};
+    cudaStream_t s = nullptr;
+    int device = 0;
+    bool mixed = false;
+    int64_t C = 0, R = 0;
+    // C-length FP64 vectors
+    double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *d = nullptr, *w = nullptr, *v = nullptr;
+    float* pg32 = nullptr;   // FP32 gather copy (mixed)
+    // R-length
+    void* q = nullptr;        // A p: float (mixed) or double (plain)
+    double* q64 = nullptr;    // FP64 residual b - A x (refinement / true residual)
+    const double* b = nullptr;
+    double* b_own = nullptr;
+    double* partial = nullptr;  // unit partials
+    double *part_q = nullptr, *part_a = nullptr, *part_b = nullptr;
+    int n_row_blocks = 0, n_vec_blocks = 0;
+    double* scal = nullptr;
+    int* flags = nullptr;
+    double* host_scal = nullptr;  // pinned mirror
+    int* host_flags = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_len = 0;
+    int graph_phase = -1;
+    long long graph_kernels = 0;
+    int launched = 0;  // iterations issued (including no-op tail)
+    bool own_stream = false;  // graphs cannot be captured on the legacy default stream
+    Dev dv() const { return Dev{scal, flags}; }
+
+    ~SolverImpl()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (own_stream) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+        for (void* ptr : {(void*)x, (void*)r, (void*)z, (void*)p, (void*)d, (void*)w, (void*)v, (void*)pg32, q,
+                          (void*)q64, (void*)b_own, (void*)partial, (void*)part_q, (void*)part_a, (void*)part_b,
+                          (void*)scal, (void*)flags})
+            cudaFree(ptr);
+        cudaFreeHost(host_scal);
+        cudaFreeHost(host_flags);
+    }
+
+    template <bool COMP, typename T>
+    cas_status issue_pcg_iteration()
+    {
+        const Dev D = dv();
+        const T* pgather = std::is_same<T, float>::value ? reinterpret_cast<const T*>(pg32) : reinterpret_cast<const T*>(p);
+        { spmv_norm_kernel<T, T, COMP, 0><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, pgather,
+                                                                           static_cast<T*>(q), nullptr, part_q, D, 0, 0); cas::count_launch(); }
+        { spmv_t_units_flag_kernel<T><<<row_grid(a.units), kVecThreads, 0, s>>>(a, static_cast<const T*>(q), partial, D, 0); cas::count_launch(); }
+        { pcg_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_row_blocks, D); cas::count_launch(); }
+        { pcg_update_kernel<COMP><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, x, r, z, p, d, part_a, part_b, D); cas::count_launch(); }
+        { pcg_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, part_b, n_vec_blocks, D, 0, 0); cas::count_launch(); }
+        { pcg_direction_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(
+            C, z, p, std::is_same<T, float>::value ? reinterpret_cast<T*>(pg32) : nullptr, D); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+        return CAS_OK;
+    }
+
+    // Residual replacement: r = A'(b - A x) in FP64, z = d r, r.z, r.r.
+    // Inside a graph chunk (force == false) it is skipped once converged.
+    template <bool COMP>
+    cas_status issue_pcg_refine(bool init, bool force)
+    {
+        const Dev D = dv();
+        const int f = force ? 1 : 0;
+        { spmv_norm_kernel<double, double, COMP, 2><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, x, q64, b,
+                                                                                    part_q, D, 0, f); cas::count_launch(); }
+        { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, q64, partial, D, f); cas::count_launch(); }
+        if (mixed)
+            { pcg_residual_kernel<COMP, float><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, r, z, p, pg32, d, part_a,
+                                                                                part_b, init ? 1 : 0, D, f); cas::count_launch(); }
+        else
+            { pcg_residual_kernel<COMP, double><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, r, z, p, nullptr, d,
+                                                                                 part_a, part_b, init ? 1 : 0, D, f); cas::count_launch(); }
+        { pcg_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, part_b, n_vec_blocks, D, 1, f); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+        return CAS_OK;
+    }
+
+    template <bool COMP, typename T>
+    cas_status issue_lsqr_iteration()
+    {
+        const Dev D = dv();
+        T* vg = reinterpret_cast<T*>(std::is_same<T, float>::value ? (void*)pg32 : (void*)p);
+        // u_hat = A v - (alpha / beta_prev) u_hat_prev
+        { lsqr_coef_kernel<<<1, 1, 0, s>>>(D, kPap); cas::count_launch(); }
+        { spmv_norm_kernel<T, T, COMP, 1><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, vg, static_cast<T*>(q),
+                                                                           nullptr, part_q, D, kPap, 0); cas::count_launch(); }
+        { lsqr_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_row_blocks, D, 0); cas::count_launch(); }
+        // v_hat = (1/beta) A' u_hat - beta v
+        { spmv_t_units_flag_kernel<T><<<row_grid(a.units), kVecThreads, 0, s>>>(a, static_cast<const T*>(q), partial, D, 0); cas::count_launch(); }
+        { lsqr_v_kernel<COMP, T><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, v, part_a, D, 0); cas::count_launch(); }
+        { lsqr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 0); cas::count_launch(); }
+        { lsqr_xw_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, vg, D, 0); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+        return CAS_OK;
+    }
+
+    cas_status issue_iteration(int global_index)
+    {
+        const bool lsqr = o.method == CAS_LSQR;
+        if (lsqr) {
+            if (mixed) CAS_TRY((issue_lsqr_iteration<true, float>()));
+            else CAS_TRY((issue_lsqr_iteration<false, double>()));
+            return CAS_OK;
+        }
+        if (mixed) CAS_TRY((issue_pcg_iteration<true, float>()));
+        else CAS_TRY((issue_pcg_iteration<false, double>()));
+        if (mixed && o.refine_every > 0 && (global_index + 1) % o.refine_every == 0) CAS_TRY(issue_pcg_refine<true>(false, false));
+        return CAS_OK;
+    }
+
+    // Issues n iterations starting at global index `first`, through a cached
+    // CUDA graph when the chunk shape allows.
+    cas_status issue_chunk(int first, int n)
+    {
+        const int period = (mixed && o.method != CAS_LSQR && o.refine_every > 0) ? o.refine_every : 1;
+        const int phase = first % period;
+        if (n > 1) {
+            if (!graph || graph_len != n || graph_phase != phase) {
+                if (graph) {
+                    cudaGraphExecDestroy(graph);
+                    graph = nullptr;
+                }
+                cudaGraph_t g = nullptr;
+                CAS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                cas_status st = CAS_OK;
+                const long long before = launch_count();
+                for (int i = 0; i < n && st == CAS_OK; i++) st = issue_iteration(first + i);
+                graph_kernels = launch_count() - before;
+                count_launch(-graph_kernels);  // captured, not launched
+                cudaError_t e = cudaStreamEndCapture(s, &g);
+                if (st != CAS_OK) {
+                    if (g) cudaGraphDestroy(g);
+                    return st;
+                }
+                CAS_CUDA(e);
+                e = cudaGraphInstantiate(&graph, g, 0);
+                cudaGraphDestroy(g);
+                CAS_CUDA(e);
+                graph_len = n;
+                graph_phase = phase;
+            }
+            CAS_CUDA(cudaGraphLaunch(graph, s));
+            count_launch(graph_kernels);
+        } else {
+            for (int i = 0; i < n; i++) CAS_TRY(issue_iteration(first + i));
+        }
+        launched += n;
+        return CAS_OK;
+    }
+
+    cas_status read_state()
+    {
+        CAS_CUDA(cudaMemcpyAsync(host_scal, scal, sizeof(double) * kSlots, cudaMemcpyDeviceToHost, s));
+        CAS_CUDA(cudaMemcpyAsync(host_flags, flags, sizeof(int) * kFlags, cudaMemcpyDeviceToHost, s));
+        CAS_CUDA(cudaStreamSynchronize(s));
+        return CAS_OK;
+    }
+
+    // ||A'(b - A x)|| / ||A'b|| in FP64 (does not touch solver state).
+    cas_status true_residual(double* out)
+    {
+        const Dev D = dv();
+        { spmv_norm_kernel<double, double, false, 2><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, x, q64, b,
+                                                                                     part_q, D, 0, 1); cas::count_launch(); }
+        { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, q64, partial, D, 1); cas::count_launch(); }
+        { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, nullptr, part_a); cas::count_launch(); }
+        { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kTrue); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+        double h[kSlots];
+        CAS_CUDA(cudaMemcpyAsync(h, scal, sizeof(double) * kSlots, cudaMemcpyDeviceToHost, s));
+        CAS_CUDA(cudaStreamSynchronize(s));
+        const double num = h[kTrue];
+        const double bn2 = h[kBn2];
+        *out = bn2 > 0 ? std::sqrt(num / bn2) : std::sqrt(num);
+        return CAS_OK;
+    }
+
+    cas_status init(const double* x0)
+    {
+        C = a.cols;
+        R = a.rows;
+        mixed = o.precision == CAS_MIXED;
+        n_row_blocks = static_cast<int>(row_grid(R));
+        n_vec_blocks = static_cast<int>(vec_grid(C));
+        const size_t cb = sizeof(double) * std::max<int64_t>(C, 1), rb8 = sizeof(double) * std::max<int64_t>(R, 1);
+        for (double** ptr : {&x, &r, &z, &p, &d, &w, &v}) CAS_CUDA(cudaMalloc(ptr, cb));
+        if (mixed) CAS_CUDA(cudaMalloc(&pg32, sizeof(float) * std::max<int64_t>(C, 1)));
+        CAS_CUDA(cudaMalloc(&q, mixed ? sizeof(float) * std::max<int64_t>(R, 1) : rb8));
+        CAS_CUDA(cudaMalloc(&q64, rb8));
+        CAS_CUDA(cudaMalloc(&partial, sizeof(double) * std::max<int64_t>(a.units, 1)));
+        CAS_CUDA(cudaMalloc(&part_q, sizeof(double) * 2 * n_row_blocks));
+        CAS_CUDA(cudaMalloc(&part_a, sizeof(double) * 2 * std::max(n_vec_blocks, n_row_blocks)));
+        CAS_CUDA(cudaMalloc(&part_b, sizeof(double) * 2 * n_vec_blocks));
+        CAS_CUDA(cudaMalloc(&scal, sizeof(double) * kSlots));
+        CAS_CUDA(cudaMalloc(&flags, sizeof(int) * kFlags));
+        CAS_CUDA(cudaMallocHost(&host_scal, sizeof(double) * kSlots));
+        CAS_CUDA(cudaMallocHost(&host_flags, sizeof(int) * kFlags));
+        CAS_CUDA(cudaMemsetAsync(scal, 0, sizeof(double) * kSlots, s));
+        CAS_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * kFlags, s));
+        const double tol = o.tol;
+        CAS_CUDA(cudaMemcpyAsync(scal + kTol, &tol, sizeof tol, cudaMemcpyHostToDevice, s));
+        if (x0)
+            CAS_CUDA(cudaMemcpyAsync(x, x0, cb, cudaMemcpyDeviceToDevice, s));
+        else
+            CAS_CUDA(cudaMemsetAsync(x, 0, cb, s));
+        CAS_CUDA(cudaMemsetAsync(w, 0, cb, s));
+        CAS_CUDA(cudaMemsetAsync(v, 0, cb, s));
+        { precond_kernel<<<vec_grid(C), kVecThreads, 0, s>>>(a.diag_int, C, (o.method == CAS_PCG && o.jacobi) ? 1 : 0, d); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+        const Dev D = dv();
+
+        // ||A'b||^2 (denominator of the relative residual)
+        { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, b, partial, D, 1); cas::count_launch(); }
+        { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, nullptr, part_a); cas::count_launch(); }
+        { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kBn2); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+
+        if (o.method == CAS_LSQR) {
+            // beta u = b - A x0 ; alpha v = A'u ; w = v ; phi_bar = beta ; rho_bar = alpha
+            if (mixed) {
+                { spmv_norm_kernel<double, float, true, 2><<<n_row_blocks, kVecThreads, 0, s>>>(
+                    a.idx, R, a.k, x, static_cast<float*>(q), b, part_q, D, 0, 1); cas::count_launch(); }
+            } else {
+                { spmv_norm_kernel<double, double, false, 2><<<n_row_blocks, kVecThreads, 0, s>>>(
+                    a.idx, R, a.k, x, static_cast<double*>(q), b, part_q, D, 0, 1); cas::count_launch(); }
+            }
+            if (mixed) {
+                { lsqr_beta_kernel<true><<<1, kRedThreads, 0, s>>>(part_q, n_row_blocks, D, 1); cas::count_launch(); }
+                { spmv_t_units_flag_kernel<float><<<row_grid(a.units), kVecThreads, 0, s>>>(a, static_cast<float*>(q),
+                                                                                         partial, D, 1); cas::count_launch(); }
+                { lsqr_v_kernel<true, float><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, v, part_a, D, 1); cas::count_launch(); }
+                { lsqr_alpha_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 1); cas::count_launch(); }
+                { lsqr_xw_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, pg32, D, 1); cas::count_launch(); }
+            } else {
+                { lsqr_beta_kernel<false><<<1, kRedThreads, 0, s>>>(part_q, n_row_blocks, D, 1); cas::count_launch(); }
+                { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, static_cast<double*>(q),
+                                                                                          partial, D, 1); cas::count_launch(); }
+                { lsqr_v_kernel<false, double><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, v, part_a, D, 1); cas::count_launch(); }
+                { lsqr_alpha_kernel<false><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 1); cas::count_launch(); }
+                { lsqr_xw_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, p, D, 1); cas::count_launch(); }
+            }
+            CAS_CHECK_LAUNCH();
+        } else {
+            if (mixed) CAS_TRY(issue_pcg_refine<true>(true, true));
+            else CAS_TRY(issue_pcg_refine<false>(true, true));
+        }
+        CAS_TRY(read_state());
+        // the initial residual replacement counted as a refinement; reset
+        int zero = 0;
+        CAS_CUDA(cudaMemcpyAsync(flags + kRefine, &zero, sizeof zero, cudaMemcpyHostToDevice, s));
+        if (host_flags[kStatus] != 0) {
+            set_error("solver setup: non-finite right-hand side");
+            return static_cast<cas_status>(host_flags[kStatus]);
+        }
+        return CAS_OK;
+    }
+};
+
+}  // namespace cas
+
+using namespace cas;
+
+struct cas_solver {
+    SolverImpl impl;
+};
+
+namespace {
+cas_status validate_opts(const cas_solve_opts* o)
+{
+    CAS_REQUIRE(o, CAS_ERR_INVALID_ARGUMENT, "null solver options");
+    CAS_REQUIRE(o->method == CAS_PCG || o->method == CAS_LSQR || o->method == CAS_CG, CAS_ERR_INVALID_ARGUMENT,
+                "unknown solver method");
+    CAS_REQUIRE(o->precision == CAS_PLAIN_FP64 || o->precision == CAS_MIXED, CAS_ERR_INVALID_ARGUMENT,
+                "unknown precision mode");
+    CAS_REQUIRE(o->max_iterations >= 0 && o->check_every >= 0 && o->refine_every >= 0, CAS_ERR_INVALID_ARGUMENT,
+                "negative iteration counts in solver options");
+    return CAS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+CAS_API void cas_solve_opts_default(cas_solve_opts* o)
+{
+    if (!o) return;
+    o->method = CAS_PCG;
+    o->precision = CAS_PLAIN_FP64;
+    o->tol = 1e-8;
+    o->max_iterations = 20000;
+    o->refine_every = 50;
+    o->check_every = 50;
+    o->jacobi = 1;
+}
+
+CAS_API cas_status cas_solver_create(const cas_csr* a, const cas_solve_opts* o, const double* d_b,
+                                     const double* d_x0, void* stream, cas_solver** out)
+{
+    CAS_REQUIRE(a && out, CAS_ERR_INVALID_ARGUMENT, "cas_solver_create: null argument");
+    CAS_REQUIRE(d_b || a->rows == 0, CAS_ERR_INVALID_ARGUMENT, "cas_solver_create: null right-hand side");
+    CAS_TRY(validate_opts(o));
+    *out = nullptr;
+    CAS_TRY(require_device());
+    auto* sv = new (std::nothrow) cas_solver;
+    CAS_REQUIRE(sv, CAS_ERR_OUT_OF_MEMORY, "cas_solver_create: out of host memory");
+    SolverImpl& m = sv->impl;
+    m.A = a;
+    m.a = a->view();
+    m.o = *o;
+    m.s = static_cast<cudaStream_t>(stream);
+    if (m.s == nullptr) {
+        // a blocking stream orders itself with the legacy default stream
+        if (cudaStreamCreate(&m.s) != cudaSuccess) {
+            delete sv;
+            set_error("cas_solver_create: cannot create a stream");
+            return CAS_ERR_CUDA;
+        }
+        m.own_stream = true;
+    }
+    m.b = d_b;
+    cudaGetDevice(&m.device);
+    cas_status st = m.init(d_x0);
+    if (st != CAS_OK) {
+        delete sv;
+        return st;
+    }
+    *out = sv;
+    return CAS_OK;
+}
+
+CAS_API void cas_solver_destroy(cas_solver* s) { delete s; }
+
+CAS_API cas_status cas_solver_iterate(cas_solver* sv, int n)
+{
+    CAS_REQUIRE(sv && n >= 0, CAS_ERR_INVALID_ARGUMENT, "cas_solver_iterate: bad argument");
+    SolverImpl& m = sv->impl;
+    const int chunk = m.o.check_every > 0 ? m.o.check_every : n;
+    int done = 0;
+    while (done < n) {
+        const int c = std::min(chunk, n - done);
+        CAS_TRY(m.issue_chunk(m.launched, c));
+        done += c;
+    }
+    CAS_TRY(m.read_state());
+    return m.host_flags[kStatus] != 0 ? static_cast<cas_status>(m.host_flags[kStatus]) : CAS_OK;
+}
+
+CAS_API cas_status cas_solver_residuum(cas_solver* sv, double* h_out)
+{
+    CAS_REQUIRE(sv && h_out, CAS_ERR_INVALID_ARGUMENT, "cas_solver_residuum: null argument");
+    CAS_TRY(sv->impl.read_state());
+    *h_out = sv->impl.o.method == CAS_LSQR ? sv->impl.host_scal[kPhiBar] : sv->impl.host_scal[kRr];
+    return CAS_OK;
+}
+
+CAS_API cas_status cas_solver_x(cas_solver* sv, double* d_out)
+{
+    CAS_REQUIRE(sv && (d_out || sv->impl.C == 0), CAS_ERR_INVALID_ARGUMENT, "cas_solver_x: null argument");
+    SolverImpl& m = sv->impl;
+    if (m.C) CAS_CUDA(cudaMemcpyAsync(d_out, m.x, sizeof(double) * m.C, cudaMemcpyDeviceToDevice, m.s));
+    return CAS_OK;
+}
+
+CAS_API cas_status cas_solver_rel_residual(cas_solver* sv, double* h_out)
+{
+    CAS_REQUIRE(sv && h_out, CAS_ERR_INVALID_ARGUMENT, "cas_solver_rel_residual: null argument");
+    return sv->impl.true_residual(h_out);
+}
+
+CAS_API int cas_solver_iterations(const cas_solver* sv)
+{
+    if (!sv) return -1;
+    auto& m = const_cast<cas_solver*>(sv)->impl;
+    if (m.read_state() != CAS_OK) return -1;
+    return m.host_flags[kIter];
+}
+
+CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
+{
+    CAS_REQUIRE(sv, CAS_ERR_INVALID_ARGUMENT, "cas_solver_run: null solver");
+    SolverImpl& m = sv->impl;
+    const int chunk = m.o.check_every > 0 ? m.o.check_every : 50;
+    cudaEvent_t e0, e1;
+    CAS_CUDA(cudaEventCreate(&e0));
+    CAS_CUDA(cudaEventCreate(&e1));
+    CAS_CUDA(cudaEventRecord(e0, m.s));
+    cas_status st = CAS_OK;
+    double rel = 0;
+    int extra_checks = 0;
+    while (true) {
+        CAS_TRY(m.read_state());
+        const int it = m.host_flags[kIter];
+        if (m.host_flags[kStatus] != 0) {
+            st = static_cast<cas_status>(m.host_flags[kStatus]);
+            break;
+        }
+        if (m.host_flags[kDone]) {
+            // verify with the true FP64 residual
+            CAS_TRY(m.true_residual(&rel));
+            if (m.o.tol <= 0 || rel <= m.o.tol || it >= m.o.max_iterations || extra_checks > 20) break;
+            // recursive residual drifted: replace it and continue
+            extra_checks++;
+            int zero = 0;
+            CAS_CUDA(cudaMemcpyAsync(m.flags + kDone, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
+            if (m.o.method == CAS_LSQR) {
+                // LSQR has no residual to replace: tighten the recursive target
+                double t = m.host_scal[kTol] * 0.5;
+                CAS_CUDA(cudaMemcpyAsync(m.scal + kTol, &t, sizeof t, cudaMemcpyHostToDevice, m.s));
+            } else if (m.mixed) {
+                CAS_TRY(m.issue_pcg_refine<true>(false, true));
+            } else {
+                CAS_TRY(m.issue_pcg_refine<false>(false, true));
+            }
+            continue;
+        }
+        if (it >= m.o.max_iterations) {
+            CAS_TRY(m.true_residual(&rel));
+            if (m.o.tol > 0 && rel > m.o.tol) st = CAS_ERR_NOT_CONVERGED;
+            break;
+        }
+        const int n = std::min(chunk, m.o.max_iterations - it);
+        CAS_TRY(m.issue_chunk(m.launched, n));
+    }
+    CAS_CUDA(cudaEventRecord(e1, m.s));
+    CAS_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CAS_TRY(m.read_state());
+    if (rep) {
+        rep->iterations = m.host_flags[kIter];
+        rep->refinements = m.host_flags[kRefine];
+        rep->rel_residual = rel;
+        rep->residuum = m.o.method == CAS_LSQR ? m.host_scal[kPhiBar] : m.host_scal[kRr];
+        rep->seconds = ms * 1e-3;
+        rep->setup_seconds = 0;
+    }
+    if (st == CAS_ERR_NOT_CONVERGED) set_error("solver did not reach the tolerance within max_iterations");
+    if (st == CAS_ERR_BREAKDOWN) set_error("solver breakdown (p'A'Ap <= 0 or non-finite scalar)");
+    return st;
+}
+
+CAS_API cas_status cas_solve(const cas_csr* a, const cas_solve_opts* o, const double* d_b, double* d_x,
+                             cas_solve_report* rep, void* stream)
+{
+    cas_solver* sv = nullptr;
+    CAS_TRY(cas_solver_create(a, o, d_b, nullptr, stream, &sv));
+    cas_status st = cas_solver_run(sv, rep);
+    if (st == CAS_OK || st == CAS_ERR_NOT_CONVERGED) {
+        cas_status s2 = cas_solver_x(sv, d_x);
+        if (s2 != CAS_OK) st = s2;
+        cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    }
+    cas_solver_destroy(sv);
+    return st;
+}
+
+}  // extern "C"

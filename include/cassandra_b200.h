@@ -1,0 +1,243 @@
+/*
+ * cassandra_b200 — C ABI of the B200 pattern-evaluator fitting path.
+ *
+ * The path: batches of Reversi positions -> ternary pattern indices under the
+ * board symmetries (Pattern/Indexer.cpp) -> a fixed-width CSR matrix with
+ * implicit 1.0 entries (Math/MatrixCSR.h) and a sort-built transposed copy ->
+ * Jacobi-PCG on the normal equations and LSQR (Math/Solver.h), as driven by
+ * FitWeights (PatternFit/PatternFit.cpp:7-39).
+ *
+ * Conventions
+ *  - Every entry point returns a cas_status; CAS_OK is 0.  A failing call
+ *    leaves a message retrievable with cas_last_error() on the same thread.
+ *    No C++ exception crosses this boundary.
+ *  - Pointers prefixed d_ are device pointers (CUDA global memory of the
+ *    current device); h_ are host pointers.  Both are borrowed for the call
+ *    (device pointers until the stream work completes).
+ *  - `stream` is a cudaStream_t passed as void*; NULL means the legacy
+ *    default stream.  Calls on one handle must be serialised by the caller.
+ *  - Positions are 16-byte records {uint64 P, uint64 O}: P = discs of the
+ *    side to move, O = opponent, bit 63 = A1 ... bit 0 = H8
+ *    (Board/Position.h:11-33, Board/Field.h:7-18).
+ *  - Handles own their device memory; destroy functions accept NULL.
+ *  - There is no CPU fallback: without a usable CUDA device the compute
+ *    entry points return CAS_ERR_NO_DEVICE.
+ */
+#ifndef CASSANDRA_B200_H
+#define CASSANDRA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CAS_API __attribute__((visibility("default")))
+
+typedef enum cas_status {
+    CAS_OK = 0,
+    CAS_ERR_SIZE_MISMATCH = 1,    /* "Size mismatch." (Math/MatrixCSR.cpp:51-52, Math/Solver.h:91-93) */
+    CAS_ERR_INVALID_ARGUMENT = 2, /* null pointer, negative size, bad enum */
+    CAS_ERR_PATTERN = 3,          /* mask unusable (empty, >16 squares, index space > 2^32) */
+    CAS_ERR_CUDA = 4,             /* CUDA runtime error (message has the details) */
+    CAS_ERR_OUT_OF_MEMORY = 5,
+    CAS_ERR_NO_DEVICE = 6,        /* no usable CUDA device */
+    CAS_ERR_BREAKDOWN = 7,        /* solver breakdown: p'A'Ap <= 0, or a non-finite scalar */
+    CAS_ERR_NOT_CONVERGED = 8,    /* tolerance not reached within max_iterations */
+    CAS_ERR_TIMEOUT = 9           /* a bounded device-side wait gave up */
+} cas_status;
+
+/* Name of a status code ("CAS_OK", ...).  Never NULL. */
+CAS_API const char* cas_status_name(cas_status s);
+
+/* Copies the calling thread's last error message (NUL-terminated, truncated
+ * to cap) and returns its full length. */
+CAS_API size_t cas_last_error(char* buf, size_t cap);
+
+/* ABI version: major * 10000 + minor * 100 + patch. */
+CAS_API int cas_version(void);
+
+/* Number of kernels this library has launched in this process (kernels of a
+ * replayed CUDA graph count at every replay).  Used to report launches. */
+CAS_API long long cas_kernel_launches(void);
+
+/* ------------------------------------------------------------------------ */
+/* Pattern sets: GroupIndexer (Pattern/Indexer.h:29-40)                      */
+/* ------------------------------------------------------------------------ */
+
+typedef enum cas_index_mode {
+    /* Bit-exact with GroupIndexer::InsertIndices (Pattern/Indexer.cpp:413-422):
+     * each mask goes through CreateIndexer (:319-365) and is collapsed by its
+     * symmetry stabiliser. */
+    CAS_INDEX_REFERENCE = 0,
+    /* The A_Indexer recipe (Pattern/Indexer.cpp:31-41) for every mask: 8
+     * instances (id, C, D, H, V, H.C, H.D, H.V), 3^k columns per mask, column
+     * offsets the running sum of 3^k. */
+    CAS_INDEX_EXPANDED = 1
+} cas_index_mode;
+
+typedef struct cas_patterns cas_patterns;
+
+/* Replaces GroupIndexer(std::vector<uint64_t>) (Pattern/Indexer.cpp:382-392).
+ * Masks use the repo's bit order (bit 0 = H8). */
+CAS_API cas_status cas_patterns_create(const uint64_t* masks, int n, cas_index_mode mode, cas_patterns** out);
+CAS_API void cas_patterns_destroy(cas_patterns* p);
+/* GroupIndexer::index_space_size (Pattern/Indexer.h:33). */
+CAS_API int64_t cas_patterns_cols(const cas_patterns* p);
+/* Variations().size(): entries per CSR row (PatternFit/PatternFit.cpp:14). */
+CAS_API int cas_patterns_nnz_per_row(const cas_patterns* p);
+/* GroupIndexer::Variations() (Pattern/Indexer.cpp:394-403): writes
+ * nnz_per_row masks. */
+CAS_API cas_status cas_patterns_variations(const cas_patterns* p, uint64_t* h_out);
+/* Per-mask indexer facts for mask i: the pattern CreateIndexer stores
+ * (Pattern/Indexer.cpp:353-360 may flip it), symmetry_group_order,
+ * index_space_size and the column offset of its block. */
+CAS_API cas_status cas_patterns_indexer(const cas_patterns* p, int i, uint64_t* stored_pattern, int* order,
+                                        int64_t* space, int64_t* offset);
+
+/* Indexer kernel: writes nnz_per_row uint32 column indices per position,
+ * row-major, exactly as GroupIndexer::InsertIndices fills MatrixCSR::Row(i)
+ * (PatternFit/PatternFit.cpp:18-21). */
+CAS_API cas_status cas_index(const cas_patterns* p, const uint64_t* d_positions, int64_t n, uint32_t* d_out,
+                             void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Matrices: MatrixCSR (Math/MatrixCSR.h:11-33)                              */
+/* ------------------------------------------------------------------------ */
+
+typedef enum cas_dtype { CAS_F32 = 0, CAS_F64 = 1 } cas_dtype;
+
+typedef struct cas_csr cas_csr;
+
+/* Index d_positions and build the device-resident CSR plus its transposed
+ * copy and the column statistics (replaces PatternFit/PatternFit.cpp:12-21). */
+CAS_API cas_status cas_csr_from_positions(const cas_patterns* p, const uint64_t* d_positions, int64_t rows,
+                                          void* stream, cas_csr** out);
+/* Build from existing row-major indices (MatrixCSR(K, rows, cols) filled via
+ * Row(i), Math/MatrixCSR.cpp:5-19).  The indices are copied. */
+CAS_API cas_status cas_csr_from_indices(const uint32_t* d_indices, int nnz_per_row, int64_t rows, int64_t cols,
+                                        void* stream, cas_csr** out);
+CAS_API void cas_csr_destroy(cas_csr* a);
+CAS_API int64_t cas_csr_rows(const cas_csr* a);
+CAS_API int64_t cas_csr_cols(const cas_csr* a);
+CAS_API int cas_csr_nnz_per_row(const cas_csr* a);
+/* Device pointer to the rows * nnz_per_row row-major column indices. */
+CAS_API const uint32_t* cas_csr_indices(const cas_csr* a);
+/* Device pointers to the transposed copy: col_ptr (cols + 1 int64) and the
+ * row index of every entry, sorted by (column, row). */
+CAS_API cas_status cas_csr_transposed(const cas_csr* a, const int64_t** d_col_ptr, const uint32_t** d_row_idx);
+
+/* y = A x (operator*(const MatrixCSR&, const Vector&), Math/MatrixCSR.cpp:49-65).
+ * x has cols entries, y rows entries, both of dtype. */
+CAS_API cas_status cas_spmv(const cas_csr* a, cas_dtype dtype, const void* d_x, void* d_y, void* stream);
+/* x = A' y (operator*(const Vector&, const MatrixCSR&), Math/MatrixCSR.cpp:67-87),
+ * computed over the transposed copy: deterministic, no atomics. */
+CAS_API cas_status cas_spmv_t(const cas_csr* a, cas_dtype dtype, const void* d_y, void* d_x, void* stream);
+/* 1 / diag(A'A) with a duplicate of multiplicity m counting m^2
+ * (JacobiPreconditionerOfATA, Math/MatrixCSR.cpp:21-47); empty columns give inf. */
+CAS_API cas_status cas_jacobi(const cas_csr* a, cas_dtype dtype, void* d_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Solvers: PCG, LSQR, CG (Math/Solver.h)                                    */
+/* ------------------------------------------------------------------------ */
+
+typedef enum cas_method {
+    CAS_PCG = 0,  /* Jacobi-PCG on A'A x = A'b (Math/Solver.h:78-117 as FitWeights calls it) */
+    CAS_LSQR = 1, /* LSQR on min ||Ax - b|| (Math/Solver.h:128-182) */
+    CAS_CG = 2    /* PCG with the identity preconditioner (Math/Solver.h:40-76) */
+} cas_method;
+
+typedef enum cas_precision {
+    /* FP64 vectors, FP64 products: the plain method. */
+    CAS_PLAIN_FP64 = 0,
+    /* FP32 sparse products and FP32 gather vectors (exact for the 0/1 entries
+     * of A); FP64 accumulation, FP64 compensated dots/norms/scalars; the true
+     * FP64 residual is recomputed every refine_every iterations. */
+    CAS_MIXED = 1
+} cas_precision;
+
+typedef struct cas_solve_opts {
+    cas_method method;
+    cas_precision precision;
+    double tol;         /* stop when ||A'(b-Ax)|| / ||A'b|| <= tol; <= 0: run max_iterations */
+    int max_iterations;
+    int refine_every;   /* CAS_MIXED: iterations between true-residual replacements (50) */
+    int check_every;    /* iterations per host-side convergence check (graph chunk) */
+    int jacobi;         /* PCG: 1 = Jacobi preconditioner (FitWeights), 0 = none */
+} cas_solve_opts;
+
+typedef struct cas_solve_report {
+    int iterations;          /* iterations performed */
+    int refinements;         /* true-residual recomputations performed */
+    double rel_residual;     /* final ||A'(b-Ax)|| / ||A'b||, recomputed in FP64 */
+    double residuum;         /* IterativeSolver::Residuum(): PCG r.r, LSQR phi_bar */
+    double seconds;          /* device time of the solve (CUDA events) */
+    double setup_seconds;    /* device time of indexing/CSR build (fit calls only) */
+} cas_solve_report;
+
+/* tol 1e-8, max_iterations 20000, refine_every 50, check_every 50, jacobi 1, PCG, FP64. */
+CAS_API void cas_solve_opts_default(cas_solve_opts* o);
+
+typedef struct cas_solver cas_solver;
+
+/* Stateful solver mirroring IterativeSolver (Math/Solver.h:9-16).  For PCG
+ * the system is A'A x = A'b with b the rows-length target vector, exactly
+ * PCG(transposed(A) * A, P, x0, transposed(A) * b) of PatternFit.cpp:31.
+ * d_x0 may be NULL (x0 = 0).  A must outlive the solver. */
+CAS_API cas_status cas_solver_create(const cas_csr* a, const cas_solve_opts* o, const double* d_b,
+                                     const double* d_x0, void* stream, cas_solver** out);
+CAS_API void cas_solver_destroy(cas_solver* s);
+/* IterativeSolver::Iterate(n). */
+CAS_API cas_status cas_solver_iterate(cas_solver* s, int n);
+/* IterativeSolver::Residuum(): PCG r.r of the recursive residual, LSQR phi_bar. */
+CAS_API cas_status cas_solver_residuum(cas_solver* s, double* h_out);
+/* IterativeSolver::X(): cols doubles into device memory. */
+CAS_API cas_status cas_solver_x(cas_solver* s, double* d_out);
+/* ||A'(b - Ax)|| / ||A'b|| of the current iterate, in FP64. */
+CAS_API cas_status cas_solver_rel_residual(cas_solver* s, double* h_out);
+/* Iterate until opts.tol or opts.max_iterations; fills the report. */
+CAS_API cas_status cas_solver_run(cas_solver* s, cas_solve_report* rep);
+CAS_API int cas_solver_iterations(const cas_solver* s);
+
+/* One-shot solve: create, run, copy x, destroy. */
+CAS_API cas_status cas_solve(const cas_csr* a, const cas_solve_opts* o, const double* d_b, double* d_x,
+                             cas_solve_report* rep, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* FitWeights (PatternFit/PatternFit.cpp:7-39)                               */
+/* ------------------------------------------------------------------------ */
+
+/* Host buffers in, host weights out (cols floats); every step (upload,
+ * indexing, CSR build, Jacobi, solve, download) runs on the device. */
+CAS_API cas_status cas_fit_weights(const uint64_t* masks, int n_masks, cas_index_mode mode,
+                                   const uint64_t* h_positions, const float* h_scores, int64_t rows,
+                                   const cas_solve_opts* o, float* h_weights, cas_solve_report* rep);
+/* Device-resident variant: scores and weights are FP64 device vectors. */
+CAS_API cas_status cas_fit_weights_device(const cas_patterns* p, const uint64_t* d_positions, const double* d_scores,
+                                          int64_t rows, const cas_solve_opts* o, double* d_weights,
+                                          cas_solve_report* rep, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic data (seeded, deterministic, identical on host and device)      */
+/* ------------------------------------------------------------------------ */
+
+/* Positions reached by uniform random legal play from the start position
+ * (RandomPlayer semantics, Game/Player.cpp:3-16; passes are played, games
+ * that end before the target are discarded and replayed).  The empty count
+ * of position i is drawn uniformly from [min_empties, max_empties]. */
+CAS_API cas_status cas_generate_positions(uint64_t seed, int64_t n, int min_empties, int max_empties,
+                                          uint64_t* d_out, void* stream);
+/* Same generator on the host CPU (for fixtures and cross-checks). */
+CAS_API cas_status cas_generate_positions_host(uint64_t seed, int64_t first, int64_t n, int min_empties,
+                                               int max_empties, uint64_t* h_out);
+/* Targets b = clamp(2*rint((A w* + e)/2), -64, 64) with w* ~ N(0, w_sigma^2)
+ * per column and e ~ N(0, noise_sigma^2) per row, seeded.  Optionally
+ * returns w* (cols doubles, may be NULL). */
+CAS_API cas_status cas_generate_targets(const cas_csr* a, uint64_t seed, double w_sigma, double noise_sigma,
+                                        double* d_b, double* d_w_true, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CASSANDRA_B200_H */

@@ -1,0 +1,437 @@
+/*
+ * Parity oracle (test infrastructure only; see oracle.h).  Each function cites
+ * the reference lines it restates.  Everything is scalar, FP64 and written
+ * for clarity, not speed.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ---- Board symmetries (Board/BitBoard.cpp:4-84), square by square -------- */
+
+static int square_after(int which, int b)
+{
+    int x = b & 7, y = b >> 3;
+    switch (which) {
+        case 0: return (7 - x) * 8 + (7 - y); /* codiagonal */
+        case 1: return x * 8 + y;             /* diagonal */
+        case 2: return y * 8 + (7 - x);       /* horizontal */
+        default: return (7 - y) * 8 + x;      /* vertical */
+    }
+}
+
+uint64_t or_flip(int which, uint64_t b)
+{
+    uint64_t r = 0;
+    for (int s = 0; s < 64; s++)
+        if ((b >> s) & 1) r |= 1ULL << square_after(which, s);
+    return r;
+}
+
+typedef struct {
+    uint64_t p, o;
+} pos_t;
+
+static pos_t flip_pos(int which, pos_t a)
+{
+    pos_t r = {or_flip(which, a.p), or_flip(which, a.o)};
+    return r;
+}
+#define FC(x) flip_pos(0, x)
+#define FD(x) flip_pos(1, x)
+#define FH(x) flip_pos(2, x)
+#define FV(x) flip_pos(3, x)
+
+/* ---- FastIndex (Pattern/Helpers.cpp:5-47): PExt then the SumPow3 table ---- */
+
+static uint64_t pext(uint64_t src, uint64_t mask)
+{
+    uint64_t r = 0;
+    int i = 0;
+    for (; mask; mask &= mask - 1, i++)
+        if (src & mask & (0 - mask)) r |= 1ULL << i;
+    return r;
+}
+
+static uint32_t sum_pow3(uint64_t bits)
+{
+    uint32_t sum = 0, w = 1;
+    for (; bits; bits >>= 1, w *= 3)
+        if (bits & 1) sum += w;
+    return sum;
+}
+
+uint32_t or_fast_index(uint64_t p, uint64_t o, uint64_t mask)
+{
+    return sum_pow3(pext(p, mask)) + 2 * sum_pow3(pext(o, mask));
+}
+
+static uint32_t fi(pos_t a, uint64_t mask) { return or_fast_index(a.p, a.o, mask); }
+
+static int popcount64(uint64_t x)
+{
+    int n = 0;
+    for (; x; x &= x - 1) n++;
+    return n;
+}
+
+static int pown3(int e)
+{
+    int r = 1;
+    while (e-- > 0) r *= 3;
+    return r;
+}
+
+/* ---- Indexers (Pattern/Indexer.cpp:17-365) ------------------------------- */
+
+enum { K_A, K_V, K_D, K_VH, K_DC, K_VHDC };
+
+typedef struct {
+    int kind;
+    uint64_t pattern;
+    int order;
+    int64_t space;
+    uint32_t half_size, diag_size;
+    uint32_t* dense;
+} indexer_t;
+
+static const uint64_t V_HALF = 0x00000000FFFFFFFFULL;
+static const uint64_t D_HALF = 0x0080C0E0F0F8FCFEULL;
+static const uint64_t D_DIAG = 0x8040201008040201ULL;
+
+static uint64_t pdep(uint64_t src, uint64_t mask)
+{
+    uint64_t r = 0;
+    for (int i = 0; mask; mask &= mask - 1, i++)
+        if ((src >> i) & 1) r |= mask & (0 - mask);
+    return r;
+}
+
+/* Dense orbit tables: Configurations order (Pattern/Helpers.cpp:81-102). */
+static void build_dense(indexer_t* ix)
+{
+    uint64_t m = ix->pattern;
+    int64_t n = pown3(popcount64(m));
+    ix->dense = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    for (int64_t i = 0; i < n; i++) ix->dense[i] = 0xFFFFFFFFu;
+    uint64_t size = 1ULL << popcount64(m);
+    uint32_t index = 0;
+    for (uint64_t p = 0; p < size; p++)
+        for (uint64_t o = 0; o < size; o++) {
+            if (p & o) continue;
+            pos_t c = {pdep(p, m), pdep(o, m)};
+            if (ix->dense[fi(c, m)] != 0xFFFFFFFFu) continue;
+            pos_t v[8];
+            int nv;
+            if (ix->kind == K_VH) { /* :165-174 */
+                v[0] = c; v[1] = FV(c); v[2] = FH(c); v[3] = FH(FV(c)); nv = 4;
+            } else if (ix->kind == K_DC) { /* :219-228 */
+                v[0] = c; v[1] = FD(c); v[2] = FC(c); v[3] = FC(FD(c)); nv = 4;
+            } else { /* :273-290 */
+                v[0] = c; v[1] = FC(c); v[2] = FD(c); v[3] = FH(c); v[4] = FV(c);
+                v[5] = FC(FH(c)); v[6] = FD(FH(c)); v[7] = FV(FH(c)); nv = 8;
+            }
+            for (int i = 0; i < nv; i++) ix->dense[fi(v[i], m)] = index;
+            index++;
+        }
+    ix->space = index;
+}
+
+static void make_indexer(uint64_t p, int mode, indexer_t* ix)
+{
+    memset(ix, 0, sizeof *ix);
+    ix->pattern = p;
+    if (mode == 1) {
+        ix->kind = K_A;
+        ix->order = 8;
+        ix->space = pown3(popcount64(p));
+        return;
+    }
+    /* CreateIndexer (:319-365) */
+    int v = or_flip(3, p) == p, h = or_flip(2, p) == p, d = or_flip(1, p) == p, c = or_flip(0, p) == p;
+    if (v && h && d && c) {
+        ix->kind = K_VHDC; ix->order = 1; build_dense(ix);
+    } else if (v && h) {
+        ix->kind = K_VH; ix->order = 2; build_dense(ix);
+    } else if (d && c) {
+        ix->kind = K_DC; ix->order = 2; build_dense(ix);
+    } else if (v || h) {
+        ix->kind = K_V; ix->order = 4;
+        if (!v) ix->pattern = or_flip(1, p);
+        ix->half_size = (uint32_t)pown3(popcount64(ix->pattern & V_HALF));
+        ix->space = (int64_t)ix->half_size * (ix->half_size + 1) / 2;
+    } else if (d || c) {
+        ix->kind = K_D; ix->order = 4;
+        if (!d) ix->pattern = or_flip(3, p);
+        ix->half_size = (uint32_t)pown3(popcount64(ix->pattern & D_HALF));
+        ix->diag_size = (uint32_t)pown3(popcount64(ix->pattern & D_DIAG));
+        ix->space = (int64_t)ix->diag_size * ix->half_size * (ix->half_size + 1) / 2;
+    } else {
+        ix->kind = K_A; ix->order = 8; ix->space = pown3(popcount64(p));
+    }
+}
+
+static uint32_t index_of(const indexer_t* ix, pos_t a)
+{
+    uint64_t m = ix->pattern;
+    switch (ix->kind) {
+        case K_A: return fi(a, m); /* :27-30 */
+        case K_V: { /* :74-81 */
+            uint32_t mn = fi(a, m & V_HALF), mx = fi(FV(a), m & V_HALF);
+            if (mn > mx) { uint32_t t = mn; mn = mx; mx = t; }
+            return mn * ix->half_size + mx - (mn * (mn + 1) / 2);
+        }
+        case K_D: { /* :118-126 */
+            uint32_t dd = fi(a, m & D_DIAG);
+            uint32_t mn = fi(a, m & D_HALF), mx = fi(FD(a), m & D_HALF);
+            if (mn > mx) { uint32_t t = mn; mn = mx; mx = t; }
+            return (mn * ix->half_size + mx - (mn * (mn + 1) / 2)) * ix->diag_size + dd;
+        }
+        default: return ix->dense[fi(a, m)];
+    }
+}
+
+static int insert_indices(const indexer_t* ix, pos_t a, uint32_t* loc, uint32_t off)
+{
+    switch (ix->kind) {
+        case K_A: /* :32-41 */
+            loc[0] = off + index_of(ix, a);
+            loc[1] = off + index_of(ix, FC(a));
+            loc[2] = off + index_of(ix, FD(a));
+            loc[3] = off + index_of(ix, FH(a));
+            loc[4] = off + index_of(ix, FV(a));
+            loc[5] = off + index_of(ix, FH(FC(a)));
+            loc[6] = off + index_of(ix, FH(FD(a)));
+            loc[7] = off + index_of(ix, FH(FV(a)));
+            return 8;
+        case K_V: /* :83-89 */
+            loc[0] = off + index_of(ix, a);
+            loc[1] = off + index_of(ix, FC(a));
+            loc[2] = off + index_of(ix, FD(a));
+            loc[3] = off + index_of(ix, FH(a));
+            return 4;
+        case K_D: /* :128-134 */
+            loc[0] = off + index_of(ix, a);
+            loc[1] = off + index_of(ix, FC(a));
+            loc[2] = off + index_of(ix, FH(a));
+            loc[3] = off + index_of(ix, FV(a));
+            return 4;
+        case K_VH: /* :187-191 */
+            loc[0] = off + index_of(ix, a);
+            loc[1] = off + index_of(ix, FD(a));
+            return 2;
+        case K_DC: /* :241-245 */
+            loc[0] = off + index_of(ix, a);
+            loc[1] = off + index_of(ix, FV(a));
+            return 2;
+        default: /* :306-309 */
+            loc[0] = off + index_of(ix, a);
+            return 1;
+    }
+}
+
+int or_group_info(const uint64_t* masks, int n, int mode, int64_t* cols, int* k)
+{
+    int64_t c = 0;
+    int kk = 0;
+    for (int i = 0; i < n; i++) {
+        if (masks[i] == 0 || popcount64(masks[i]) > 16) return -1;
+        indexer_t ix;
+        make_indexer(masks[i], mode, &ix);
+        c += ix.space;
+        kk += ix.order;
+        free(ix.dense);
+    }
+    *cols = c;
+    *k = kk;
+    return 0;
+}
+
+int or_group_index(const uint64_t* masks, int n, int mode, const uint64_t* po, int64_t rows, uint32_t* out)
+{
+    indexer_t* ix = (indexer_t*)calloc((size_t)n, sizeof(indexer_t));
+    int k = 0;
+    for (int i = 0; i < n; i++) {
+        if (masks[i] == 0 || popcount64(masks[i]) > 16) {
+            free(ix);
+            return -1;
+        }
+        make_indexer(masks[i], mode, &ix[i]);
+        k += ix[i].order;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < rows; r++) {
+        pos_t a = {po[2 * r], po[2 * r + 1]};
+        uint32_t* loc = out + r * k;
+        uint32_t off = 0; /* GroupIndexer::InsertIndices (:413-422) */
+        for (int i = 0; i < n; i++) {
+            loc += insert_indices(&ix[i], a, loc, off);
+            off += (uint32_t)ix[i].space;
+        }
+    }
+    for (int i = 0; i < n; i++) free(ix[i].dense);
+    free(ix);
+    return 0;
+}
+
+/* ---- MatrixCSR products (Math/MatrixCSR.cpp:21-87), FP64 ----------------- */
+
+void or_spmv(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* x, double* y)
+{
+    (void)cols;
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < rows; r++) {
+        double s = 0;
+        for (int j = 0; j < k; j++) s += x[idx[r * k + j]];
+        y[r] = s;
+    }
+}
+
+void or_spmv_t(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* y, double* x)
+{
+    memset(x, 0, sizeof(double) * (size_t)cols);
+    for (int64_t r = 0; r < rows; r++)
+        for (int j = 0; j < k; j++) x[idx[r * k + j]] += y[r];
+}
+
+static int cmp_u32(const void* a, const void* b)
+{
+    uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
+    return x < y ? -1 : x > y;
+}
+
+void or_jacobi(int k, int64_t rows, int64_t cols, const uint32_t* idx, double* d)
+{
+    double* diag = (double*)calloc((size_t)cols, sizeof(double));
+    uint32_t* row = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)k);
+    for (int64_t r = 0; r < rows; r++) {
+        memcpy(row, idx + r * k, sizeof(uint32_t) * (size_t)k);
+        qsort(row, (size_t)k, sizeof(uint32_t), cmp_u32);
+        for (int i = 0, j; i < k; i = j) { /* duplicates count m^2 (:34-40) */
+            j = i + 1;
+            while (j < k && row[i] == row[j]) j++;
+            diag[row[i]] += (double)(j - i) * (j - i);
+        }
+    }
+    for (int64_t c = 0; c < cols; c++) d[c] = 1.0 / diag[c]; /* inv() (Math/Vector.cpp:117-124) */
+    free(row);
+    free(diag);
+}
+
+static double dot(const double* a, const double* b, int64_t n)
+{
+    double s = 0;
+    for (int64_t i = 0; i < n; i++) s += a[i] * b[i];
+    return s;
+}
+
+double or_normal_residual(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, const double* x)
+{
+    double* ax = (double*)malloc(sizeof(double) * (size_t)(rows ? rows : 1));
+    double* g = (double*)malloc(sizeof(double) * (size_t)(cols ? cols : 1));
+    or_spmv_t(k, rows, cols, idx, b, g);
+    double bn = sqrt(dot(g, g, cols));
+    or_spmv(k, rows, cols, idx, x, ax);
+    for (int64_t r = 0; r < rows; r++) ax[r] = b[r] - ax[r];
+    or_spmv_t(k, rows, cols, idx, ax, g);
+    double rn = sqrt(dot(g, g, cols));
+    free(ax);
+    free(g);
+    return bn > 0 ? rn / bn : rn;
+}
+
+/* A'A v through the two products (TwoMatrix, Math/MatrixProxy.h:63-67). */
+static void normal_apply(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* v, double* tmp,
+                         double* out)
+{
+    or_spmv(k, rows, cols, idx, v, tmp);
+    or_spmv_t(k, rows, cols, idx, tmp, out);
+}
+
+int or_pcg(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int jacobi, int iterations,
+           double tol, int check_every, double* x, double* residuum)
+{
+    size_t cb = sizeof(double) * (size_t)(cols ? cols : 1);
+    double *P = malloc(cb), *r = malloc(cb), *z = malloc(cb), *p = malloc(cb), *Ap = malloc(cb);
+    double* tmp = malloc(sizeof(double) * (size_t)(rows ? rows : 1));
+    /* DiagonalPreconditioner(JacobiPreconditionerOfATA(A)) (Math/Solver.h:25-38) */
+    if (jacobi) {
+        or_jacobi(k, rows, cols, idx, P);
+        for (int64_t c = 0; c < cols; c++)
+            if (!isnormal(P[c])) P[c] = 1;
+    } else {
+        for (int64_t c = 0; c < cols; c++) P[c] = 1;
+    }
+    /* PCG(transposed(A) * A, P, 0, transposed(A) * b) (PatternFit/PatternFit.cpp:31, Math/Solver.h:88-97) */
+    memset(x, 0, cb);
+    or_spmv_t(k, rows, cols, idx, b, r); /* r = b' - A'A x0 with x0 = 0 */
+    for (int64_t c = 0; c < cols; c++) p[c] = z[c] = P[c] * r[c];
+    int it = 0;
+    if (check_every <= 0) check_every = 1;
+    for (; it < iterations;) { /* Iterate (:99-112) */
+        double rz_old = dot(r, z, cols);
+        normal_apply(k, rows, cols, idx, p, tmp, Ap);
+        double pap = dot(p, Ap, cols);
+        if (pap == 0) break;
+        double alpha = rz_old / pap;
+        for (int64_t c = 0; c < cols; c++) x[c] += alpha * p[c];
+        for (int64_t c = 0; c < cols; c++) r[c] -= alpha * Ap[c];
+        for (int64_t c = 0; c < cols; c++) z[c] = P[c] * r[c];
+        double beta = dot(r, z, cols) / rz_old;
+        for (int64_t c = 0; c < cols; c++) p[c] = z[c] + beta * p[c];
+        it++;
+        if (tol > 0 && it % check_every == 0 && or_normal_residual(k, rows, cols, idx, b, x) <= tol) break;
+    }
+    *residuum = dot(r, r, cols); /* Residuum (:114) */
+    free(P); free(r); free(z); free(p); free(Ap); free(tmp);
+    return it;
+}
+
+/* decompose (Math/Solver.h:119-126) */
+static double decompose(double* v, int64_t n)
+{
+    double len = sqrt(dot(v, v, n));
+    if (len == 0) return 0;
+    for (int64_t i = 0; i < n; i++) v[i] /= len;
+    return len;
+}
+
+int or_lsqr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int iterations, double tol,
+            int check_every, double* x, double* residuum)
+{
+    size_t cb = sizeof(double) * (size_t)(cols ? cols : 1), rb = sizeof(double) * (size_t)(rows ? rows : 1);
+    double *u = malloc(rb), *tu = malloc(rb), *v = malloc(cb), *tv = malloc(cb), *w = malloc(cb);
+    memset(x, 0, cb);
+    memcpy(u, b, rb); /* (:139-151) */
+    double beta = decompose(u, rows);
+    or_spmv_t(k, rows, cols, idx, u, v);
+    double alpha = decompose(v, cols);
+    memcpy(w, v, cb);
+    double phi_bar = beta, rho_bar = alpha;
+    int it = 0;
+    if (check_every <= 0) check_every = 1;
+    for (; it < iterations;) { /* Iterate (:153-177) */
+        or_spmv(k, rows, cols, idx, v, tu);
+        for (int64_t i = 0; i < rows; i++) u[i] = tu[i] - alpha * u[i];
+        beta = decompose(u, rows);
+        or_spmv_t(k, rows, cols, idx, u, tv);
+        for (int64_t i = 0; i < cols; i++) v[i] = tv[i] - beta * v[i];
+        alpha = decompose(v, cols);
+        double rho = sqrt(rho_bar * rho_bar + beta * beta);
+        if (rho == 0) break;
+        double c = rho_bar / rho, s = beta / rho;
+        double theta = s * alpha;
+        rho_bar = -c * alpha;
+        double phi = c * phi_bar;
+        phi_bar = s * phi_bar;
+        for (int64_t i = 0; i < cols; i++) x[i] += (phi / rho) * w[i];
+        for (int64_t i = 0; i < cols; i++) w[i] = v[i] - (theta / rho) * w[i];
+        it++;
+        if (tol > 0 && it % check_every == 0 && or_normal_residual(k, rows, cols, idx, b, x) <= tol) break;
+    }
+    *residuum = phi_bar; /* Residuum (:179) */
+    free(u); free(tu); free(v); free(tv); free(w);
+    return it;
+}

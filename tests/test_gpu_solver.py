@@ -1,0 +1,114 @@
+"""PCG / CG / LSQR on the device against the FP64 oracle and the reference."""
+import numpy as np
+import pytest
+import torch
+
+import cassandra_b200 as cb
+from tests.golden.make_golden import SET5, SET8
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(rows, masks=SET5, mode="reference", seed=11, lo=20, hi=40):
+    pos = cb.generate_positions(seed, rows, lo, hi)
+    g = cb.GroupIndexer(masks, mode)
+    a = cb.MatrixCSR.from_positions(g, pos)
+    b = cb.generate_targets(a, seed)
+    idx = a.indices().cpu().numpy().view(np.uint32)
+    return a, b, idx, g.index_space_size, pos
+
+
+def test_pcg_iterates_match_oracle(cuda, orc):
+    a, b, idx, cols, _ = _system(4000)
+    bh = b.cpu().numpy()
+    s = cb.PCG(a, b, check_every=5)
+    s.iterate(10)
+    want, res, it = orc.pcg(idx, cols, bh, 10)
+    got = s.x().cpu().numpy()
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-10 * np.abs(want).max())
+    np.testing.assert_allclose(s.residuum(), res, rtol=1e-8)
+    assert s.iterations() == 10
+
+
+def test_cg_iterates_match_oracle(cuda, orc):
+    a, b, idx, cols, _ = _system(3000, seed=4)
+    s = cb.CG(a, b, check_every=3)
+    s.iterate(8)
+    want, res, _ = orc.pcg(idx, cols, b.cpu().numpy(), 8, jacobi=False)
+    np.testing.assert_allclose(s.x().cpu().numpy(), want, rtol=0, atol=1e-10 * np.abs(want).max())
+
+
+def test_lsqr_iterates_match_oracle(cuda, orc):
+    a, b, idx, cols, _ = _system(3000, seed=5)
+    bh = b.cpu().numpy()
+    s = cb.LSQR(a, b, check_every=5)
+    s.iterate(5)
+    want, res, _ = orc.lsqr(idx, cols, bh, 5)
+    np.testing.assert_allclose(s.x().cpu().numpy(), want, rtol=0, atol=1e-9 * np.abs(want).max())
+    np.testing.assert_allclose(s.residuum(), res, rtol=1e-9)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("mode", ["reference", "expanded"])
+def test_pcg_reaches_tolerance(cuda, orc, precision, mode):
+    a, b, idx, cols, _ = _system(20_000, SET8, mode, seed=21)
+    s = cb.PCG(a, b, precision=precision, tol=1e-8, max_iterations=5000)
+    rep = s.run()
+    assert rep["converged"], rep
+    assert rep["rel_residual"] <= 1e-8
+    x = s.x().cpu().numpy()
+    bh = b.cpu().numpy()
+    # independent FP64 check on the host
+    assert orc.normal_residual(idx, cols, bh, x) <= 1.5e-8
+    # same least-squares fit as the oracle's FP64 PCG run to the same tolerance
+    want, _, _ = orc.pcg(idx, cols, bh, 5000, tol=1e-8, check_every=10)
+    pred, pw = orc.spmv(idx, cols, x), orc.spmv(idx, cols, want)
+    np.testing.assert_allclose(pred, pw, rtol=0, atol=1e-5 * np.abs(pw).max())
+
+
+def test_lsqr_reaches_tolerance(cuda, orc):
+    a, b, idx, cols, _ = _system(3000, SET5, seed=8)
+    s = cb.LSQR(a, b, tol=1e-8, max_iterations=50_000, check_every=100)
+    rep = s.run()
+    assert rep["converged"], rep
+    assert orc.normal_residual(idx, cols, b.cpu().numpy(), s.x().cpu().numpy()) <= 1.5e-8
+
+
+def test_fit_weights_host_api_matches_reference_fitweights(cuda, ref):
+    """cas_fit_weights with the reference's FitWeights(pattern, pos, 10): same
+    10 Jacobi-PCG steps; the reference runs them in FP32."""
+    import ctypes as C
+
+    pos = cb.generate_positions_host(17, 0, 5000, 20, 40)
+    rng = np.random.default_rng(17)
+    scores = (2 * rng.integers(-16, 17, len(pos))).astype(np.float32)
+    w, rep = cb.fit_weights(SET5, pos, scores, mode="reference", tol=0, max_iterations=10, check_every=10)
+    assert rep["iterations"] == 10
+    m = np.asarray(SET5, np.uint64)
+    cols = np.zeros(1, np.int64)
+    lib = ref.ref_lib()
+    k = lib.ref_group_info(m.ctypes.data_as(C.c_void_p), len(m), cols.ctypes.data_as(C.c_void_p), None)
+    idx = np.empty((len(pos), k), np.uint32)
+    lib.ref_group_index(m.ctypes.data_as(C.c_void_p), len(m), pos.ctypes.data_as(C.c_void_p), len(pos),
+                        idx.ctypes.data_as(C.c_void_p))
+    want = np.empty(int(cols[0]), np.float32)
+    res = C.c_float()
+    lib.ref_pcg(k, len(pos), int(cols[0]), idx.ctypes.data_as(C.c_void_p), scores.ctypes.data_as(C.c_void_p), 10,
+                want.ctypes.data_as(C.c_void_p), C.byref(res))
+    np.testing.assert_allclose(w, want, rtol=0, atol=2e-4 * np.abs(want).max())
+
+
+def test_solver_size_mismatch(cuda):
+    a, b, idx, cols, _ = _system(100)
+    with pytest.raises(cb.SizeMismatch):
+        cb.PCG(a, b[:-1])
+    with pytest.raises(cb.SizeMismatch):
+        cb.PCG(a, b, x0=torch.zeros(cols + 1, dtype=torch.float64, device="cuda"))
+
+
+def test_zero_rhs_converges_immediately(cuda):
+    a, b, idx, cols, _ = _system(500)
+    s = cb.PCG(a, torch.zeros_like(b), tol=1e-8)
+    rep = s.run()
+    assert rep["converged"] and rep["iterations"] == 0
+    assert torch.count_nonzero(s.x()) == 0
