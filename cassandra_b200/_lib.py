@@ -106,6 +106,7 @@ SIGNATURES: dict[str, tuple] = {
     "cas_jacobi": (C.c_int, [_VP, C.c_int, _VP, _VP]),
     "cas_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
     "cas_solver_create": (C.c_int, [_VP, C.POINTER(SolveOpts), _VP, _VP, _VP, _PP]),
+    "cas_solver_create_normal": (C.c_int, [_VP, C.POINTER(SolveOpts), _VP, _VP, _VP, _PP]),
     "cas_solver_destroy": (None, [_VP]),
     "cas_solver_iterate": (C.c_int, [_VP, C.c_int]),
     "cas_solver_residuum": (C.c_int, [_VP, C.POINTER(C.c_double)]),

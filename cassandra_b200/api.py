@@ -189,7 +189,7 @@ class _CudaArray:
     """Borrowed view of library-owned device memory (CUDA array interface v3)."""
 
     def __init__(self, ptr: int, shape: tuple, typestr: str):
-        self.__cuda_array_interface__ = {"data": (int(ptr or 0), True), "shape": tuple(shape), "typestr": typestr,
+        self.__cuda_array_interface__ = {"data": (int(ptr or 0), False), "shape": tuple(shape), "typestr": typestr,
                                          "version": 3, "strides": None}
 
 

@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(kVecThreads) spmv_norm_kernel(const uint32_t* 
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) {
             if (MODE == 1) acc -= coef * static_cast<double>(q[r]);
-            if (MODE == 2) acc = b[r] - acc;
+            if (MODE == 2) acc = (b ? b[r] : 0.0) - acc;
             q[r] = static_cast<Q>(acc);
             const double qq = static_cast<double>(static_cast<Q>(acc));
             acc_add<COMP>(mine, qq * qq);
@@ -280,14 +280,14 @@ __global__ void __launch_bounds__(kVecThreads) pcg_residual_kernel(CsrView a, co
                                                                    const double* __restrict__ d,
                                                                    double* __restrict__ part_rz,
                                                                    double* __restrict__ part_rr, int init, Dev dv,
-                                                                   int force)
+                                                                   int force, const double* __restrict__ bn)
 {
     __shared__ double smem[64];
     if (!force && finished(dv.flags)) return;
     Comp rz, rr;
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < a.cols;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const double rc = unit_sum(a, partial, c);
+        const double rc = (bn ? bn[c] : 0.0) + unit_sum(a, partial, c);
         const double zc = d[c] * rc;
         r[c] = rc;
         z[c] = zc;
@@ -325,16 +325,18 @@ __global__ void cast_kernel(int64_t n, const double* __restrict__ in, T* __restr
         out[c] = static_cast<T>(in[c]);
 }
 
-// ||v||^2 partials of a vector (used for ||A'b||^2 and ||A'r||^2).
+// ||v||^2 partials of v = bn + (A' q from unit partials); partial may be
+// null (v = bn), bn may be null (v = A' q).  Used for ||A'b||^2 and ||A'r||^2.
 template <bool COMP>
 __global__ void __launch_bounds__(kVecThreads) norm_units_kernel(CsrView a, const double* __restrict__ partial,
-                                                                 double* __restrict__ out, double* __restrict__ part)
+                                                                 double* __restrict__ out, double* __restrict__ part,
+                                                                 const double* __restrict__ bn)
 {
     __shared__ double smem[64];
     Comp acc;
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < a.cols;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const double v = unit_sum(a, partial, c);
+        const double v = (bn ? bn[c] : 0.0) + (partial ? unit_sum(a, partial, c) : 0.0);
         if (out) out[c] = v;
         acc_add<COMP>(acc, v * v);
     }
@@ -500,7 +502,8 @@ struct SolverImpl {
     // R-length
     void* q = nullptr;        // A p: float (mixed) or double (plain)
     double* q64 = nullptr;    // FP64 residual b - A x (refinement / true residual)
-    const double* b = nullptr;
+    const double* b = nullptr;   // rows-length targets (null with a normal RHS)
+    const double* bn = nullptr;  // cols-length normal-equation RHS A'b (PCG/CG only)
     double* b_own = nullptr;
     double* partial = nullptr;  // unit partials
     double *part_q = nullptr, *part_a = nullptr, *part_b = nullptr;
@@ -561,10 +564,10 @@ struct SolverImpl {
         { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, q64, partial, D, f); cas::count_launch(); }
         if (mixed)
             { pcg_residual_kernel<COMP, float><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, r, z, p, pg32, d, part_a,
-                                                                                part_b, init ? 1 : 0, D, f); cas::count_launch(); }
+                                                                                part_b, init ? 1 : 0, D, f, bn); cas::count_launch(); }
         else
             { pcg_residual_kernel<COMP, double><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, r, z, p, nullptr, d,
-                                                                                 part_a, part_b, init ? 1 : 0, D, f); cas::count_launch(); }
+                                                                                 part_a, part_b, init ? 1 : 0, D, f, bn); cas::count_launch(); }
         { pcg_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, part_b, n_vec_blocks, D, 1, f); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
@@ -658,7 +661,7 @@ struct SolverImpl {
         { spmv_norm_kernel<double, double, false, 2><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, x, q64, b,
                                                                                      part_q, D, 0, 1); cas::count_launch(); }
         { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, q64, partial, D, 1); cas::count_launch(); }
-        { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, nullptr, part_a); cas::count_launch(); }
+        { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, nullptr, part_a, bn); cas::count_launch(); }
         { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kTrue); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         double h[kSlots];
@@ -705,8 +708,12 @@ struct SolverImpl {
         const Dev D = dv();
 
         // ||A'b||^2 (denominator of the relative residual)
-        { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, b, partial, D, 1); cas::count_launch(); }
-        { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, nullptr, part_a); cas::count_launch(); }
+        if (bn) {
+            { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(a, nullptr, nullptr, part_a, bn); cas::count_launch(); }
+        } else {
+            { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, b, partial, D, 1); cas::count_launch(); }
+            { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, nullptr, part_a, nullptr); cas::count_launch(); }
+        }
         { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kBn2); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
 
@@ -787,11 +794,12 @@ CAS_API void cas_solve_opts_default(cas_solve_opts* o)
     o->jacobi = 1;
 }
 
-CAS_API cas_status cas_solver_create(const cas_csr* a, const cas_solve_opts* o, const double* d_b,
-                                     const double* d_x0, void* stream, cas_solver** out)
+}  // extern "C"
+
+namespace {
+cas_status create_solver(const cas_csr* a, const cas_solve_opts* o, const double* d_b, const double* d_bn,
+                         const double* d_x0, void* stream, cas_solver** out)
 {
-    CAS_REQUIRE(a && out, CAS_ERR_INVALID_ARGUMENT, "cas_solver_create: null argument");
-    CAS_REQUIRE(d_b || a->rows == 0, CAS_ERR_INVALID_ARGUMENT, "cas_solver_create: null right-hand side");
     CAS_TRY(validate_opts(o));
     *out = nullptr;
     CAS_TRY(require_device());
@@ -812,6 +820,16 @@ CAS_API cas_status cas_solver_create(const cas_csr* a, const cas_solve_opts* o, 
         m.own_stream = true;
     }
     m.b = d_b;
+    if (d_bn) {
+        // the normal-equation right-hand side is copied (cols doubles)
+        if (cudaMalloc(&m.b_own, sizeof(double) * std::max<int64_t>(a->cols, 1)) != cudaSuccess ||
+            cudaMemcpyAsync(m.b_own, d_bn, sizeof(double) * a->cols, cudaMemcpyDeviceToDevice, m.s) != cudaSuccess) {
+            delete sv;
+            set_error("cas_solver_create_normal: cannot copy the right-hand side");
+            return CAS_ERR_CUDA;
+        }
+        m.bn = m.b_own;
+    }
     cudaGetDevice(&m.device);
     cas_status st = m.init(d_x0);
     if (st != CAS_OK) {
@@ -820,6 +838,28 @@ CAS_API cas_status cas_solver_create(const cas_csr* a, const cas_solve_opts* o, 
     }
     *out = sv;
     return CAS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+CAS_API cas_status cas_solver_create(const cas_csr* a, const cas_solve_opts* o, const double* d_b,
+                                     const double* d_x0, void* stream, cas_solver** out)
+{
+    CAS_REQUIRE(a && out, CAS_ERR_INVALID_ARGUMENT, "cas_solver_create: null argument");
+    CAS_REQUIRE(d_b || a->rows == 0, CAS_ERR_INVALID_ARGUMENT, "cas_solver_create: null right-hand side");
+    return create_solver(a, o, d_b, nullptr, d_x0, stream, out);
+}
+
+CAS_API cas_status cas_solver_create_normal(const cas_csr* a, const cas_solve_opts* o, const double* d_normal_b,
+                                            const double* d_x0, void* stream, cas_solver** out)
+{
+    CAS_REQUIRE(a && out, CAS_ERR_INVALID_ARGUMENT, "cas_solver_create_normal: null argument");
+    CAS_REQUIRE(d_normal_b || a->cols == 0, CAS_ERR_INVALID_ARGUMENT,
+                "cas_solver_create_normal: null right-hand side");
+    CAS_REQUIRE(o && o->method != CAS_LSQR, CAS_ERR_INVALID_ARGUMENT,
+                "cas_solver_create_normal: LSQR needs the rows-length right-hand side");
+    return create_solver(a, o, nullptr, d_normal_b, d_x0, stream, out);
 }
 
 CAS_API void cas_solver_destroy(cas_solver* s) { delete s; }

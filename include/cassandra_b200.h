@@ -187,6 +187,12 @@ typedef struct cas_solver cas_solver;
  * d_x0 may be NULL (x0 = 0).  A must outlive the solver. */
 CAS_API cas_status cas_solver_create(const cas_csr* a, const cas_solve_opts* o, const double* d_b,
                                      const double* d_x0, void* stream, cas_solver** out);
+/* The same solver given the normal-equation right-hand side b' = A'b (cols
+ * doubles, copied) instead of b: PCG(transposed(A) * A, P, x0, b') exactly as
+ * the reference's caller writes it (PatternFit/PatternFit.cpp:31).  PCG and CG
+ * only; residuals are then b' - A'A x. */
+CAS_API cas_status cas_solver_create_normal(const cas_csr* a, const cas_solve_opts* o, const double* d_normal_b,
+                                            const double* d_x0, void* stream, cas_solver** out);
 CAS_API void cas_solver_destroy(cas_solver* s);
 /* IterativeSolver::Iterate(n). */
 CAS_API cas_status cas_solver_iterate(cas_solver* s, int n);
