@@ -34,6 +34,8 @@ CAS_LSQR = 1
 CAS_CG = 2
 CAS_PLAIN_FP64 = 0
 CAS_MIXED = 1
+CAS_LAYOUT_ROWS = 1
+CAS_LAYOUT_BLOCKED = 2
 
 
 class SolveOpts(C.Structure):
@@ -94,6 +96,8 @@ SIGNATURES: dict[str, tuple] = {
                                        C.POINTER(_I64)]),
     "cas_index": (C.c_int, [_VP, _VP, _I64, _VP, _VP]),
     "cas_csr_from_positions": (C.c_int, [_VP, _VP, _I64, _VP, _PP]),
+    "cas_csr_from_positions_layout": (C.c_int, [_VP, _VP, _I64, C.c_int, _VP, _PP]),
+    "cas_csr_layouts": (C.c_int, [_VP]),
     "cas_csr_from_indices": (C.c_int, [_VP, C.c_int, _I64, _I64, _VP, _PP]),
     "cas_csr_destroy": (None, [_VP]),
     "cas_csr_rows": (_I64, [_VP]),

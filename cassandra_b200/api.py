@@ -102,12 +102,23 @@ class MatrixCSR:
         self._keep = keep
 
     @classmethod
-    def from_positions(cls, indexer: GroupIndexer, positions: torch.Tensor) -> "MatrixCSR":
+    def from_positions(cls, indexer: GroupIndexer, positions: torch.Tensor, layouts: str | None = None) -> "MatrixCSR":
+        """layouts: None (both where possible), "rows", "blocked" or "rows+blocked"."""
         _require_cuda(positions, "positions")
         lib = L.load()
         h = C.c_void_p()
-        L.check(lib.cas_csr_from_positions(indexer.handle, _ptr(positions), positions.shape[0], _stream(), C.byref(h)))
+        if layouts is None:
+            L.check(lib.cas_csr_from_positions(indexer.handle, _ptr(positions), positions.shape[0], _stream(),
+                                               C.byref(h)))
+        else:
+            mask = sum({"rows": L.CAS_LAYOUT_ROWS, "blocked": L.CAS_LAYOUT_BLOCKED}[x] for x in layouts.split("+"))
+            L.check(lib.cas_csr_from_positions_layout(indexer.handle, _ptr(positions), positions.shape[0], mask,
+                                                      _stream(), C.byref(h)))
         return cls(h, keep=indexer)
+
+    def layouts(self) -> set[str]:
+        m = int(self._lib.cas_csr_layouts(self._h))
+        return {n for n, bit in (("rows", L.CAS_LAYOUT_ROWS), ("blocked", L.CAS_LAYOUT_BLOCKED)) if m & bit}
 
     @classmethod
     def from_indices(cls, indices: torch.Tensor, cols: int) -> "MatrixCSR":

@@ -7,6 +7,7 @@
 
 #include "common.cuh"
 #include "internal.cuh"
+#include "indexer.cuh"
 #include "patterns.h"
 
 namespace cas {
@@ -59,37 +60,6 @@ cas_status require_device()
 // position, so each CSR row is written as contiguous 128-byte segments.
 // The slot recipes live in shared memory.
 // ---------------------------------------------------------------------------
-
-__device__ __forceinline__ uint32_t digits(const uint8_t* sq, int n, uint32_t plo, uint32_t phi, uint32_t olo,
-                                           uint32_t ohi)
-{
-    uint32_t idx = 0;
-    for (int i = n - 1; i >= 0; i--) {
-        const int t = sq[i];
-        const uint32_t pw = t < 32 ? plo : phi, ow = t < 32 ? olo : ohi;
-        const int sh = t & 31;
-        idx = idx * 3 + ((pw >> sh) & 1u) + (((ow >> sh) & 1u) << 1);
-    }
-    return idx;
-}
-
-__device__ __forceinline__ uint32_t eval_slot(const Instance& in, const uint32_t* __restrict__ tables, uint32_t plo,
-                                              uint32_t phi, uint32_t olo, uint32_t ohi)
-{
-    uint32_t r;
-    if (in.kind == kDirect) {
-        r = digits(in.sq[0], in.n0, plo, phi, olo, ohi);
-    } else if (in.kind == kTable) {
-        r = __ldg(tables + in.table_offset + digits(in.sq[0], in.n0, plo, phi, olo, ohi));
-    } else {
-        uint32_t a = digits(in.sq[0], in.n0, plo, phi, olo, ohi);
-        uint32_t b = digits(in.sq[1], in.n1, plo, phi, olo, ohi);
-        const uint32_t lo = min(a, b), hi = max(a, b);
-        r = lo * in.half_size + hi - (lo * (lo + 1) / 2);
-        if (in.kind == kDiagPair) r = r * in.diag_size + digits(in.sq[2], in.n2, plo, phi, olo, ohi);
-    }
-    return in.offset + r;
-}
 
 __global__ void __launch_bounds__(256) index_kernel(const Instance* __restrict__ g_inst, int k,
                                                     const uint32_t* __restrict__ tables,

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "fast.cuh"
 #include "internal.cuh"
 
 namespace cas {
@@ -391,8 +392,10 @@ cas_status build_structure(cas_csr* a, cudaStream_t s)
     CAS_REQUIRE(a->rows < 0xFFFFFFFFLL, CAS_ERR_INVALID_ARGUMENT, "rows must fit uint32");
     const int64_t cols = a->cols;
     CAS_CUDA(cudaMalloc(&a->col_ptr, sizeof(int64_t) * (cols + 1)));
-    CAS_CUDA(cudaMalloc(&a->diag_int, sizeof(uint64_t) * std::max<int64_t>(cols, 1)));
-    CAS_CUDA(cudaMemsetAsync(a->diag_int, 0, sizeof(uint64_t) * std::max<int64_t>(cols, 1), s));
+    if (!a->diag_int) {
+        CAS_CUDA(cudaMalloc(&a->diag_int, sizeof(uint64_t) * std::max<int64_t>(cols, 1)));
+        CAS_CUDA(cudaMemsetAsync(a->diag_int, 0, sizeof(uint64_t) * std::max<int64_t>(cols, 1), s));
+    }
 
     if (nnz > 0) {
         unsigned int* bad = nullptr;
@@ -468,6 +471,10 @@ void free_csr(cas_csr* a)
     cudaFree(a->unit_ptr);
     cudaFree(a->diag_int);
     cudaFree(a->unit_partial);
+    if (a->fast) {
+        fast_free(*a->fast);
+        delete a->fast;
+    }
     cudaSetDevice(cur);
     delete a;
 }
@@ -493,13 +500,19 @@ cas_status finish_create(cas_csr* a, cudaStream_t s, cas_csr** out)
 
 extern "C" {
 
-CAS_API cas_status cas_csr_from_positions(const cas_patterns* p, const uint64_t* d_positions, int64_t rows,
-                                          void* stream, cas_csr** out)
+CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const uint64_t* d_positions, int64_t rows,
+                                                 int layouts, void* stream, cas_csr** out)
 {
     CAS_REQUIRE(p && out && rows >= 0, CAS_ERR_INVALID_ARGUMENT, "cas_csr_from_positions: bad argument");
     CAS_REQUIRE(rows == 0 || d_positions, CAS_ERR_INVALID_ARGUMENT, "cas_csr_from_positions: null positions");
     CAS_REQUIRE((reinterpret_cast<uintptr_t>(d_positions) & 15) == 0, CAS_ERR_INVALID_ARGUMENT,
                 "cas_csr_from_positions: position records must be 16-byte aligned");
+    CAS_REQUIRE(layouts > 0 && (layouts & ~(CAS_LAYOUT_ROWS | CAS_LAYOUT_BLOCKED)) == 0, CAS_ERR_INVALID_ARGUMENT,
+                "cas_csr_from_positions: layouts must be a non-empty mask of cas_layout");
+    CAS_REQUIRE(!(layouts & CAS_LAYOUT_BLOCKED) || fast_supported(pattern_set(p)), CAS_ERR_INVALID_ARGUMENT,
+                "cas_csr_from_positions: the blocked layout needs index spaces <= 65536 per pattern");
+    CAS_REQUIRE(rows * static_cast<int64_t>(cas_patterns_nnz_per_row(p)) < 0xFFFFFFFFLL, CAS_ERR_INVALID_ARGUMENT,
+                "cas_csr_from_positions: 2^32 or more entries are not supported");
     *out = nullptr;
     const DevicePatterns* dp = nullptr;
     CAS_TRY(patterns_on_device(p, &dp));
@@ -509,19 +522,58 @@ CAS_API cas_status cas_csr_from_positions(const cas_patterns* p, const uint64_t*
     a->rows = rows;
     a->cols = dp->cols;
     a->k = dp->k;
-    cudaError_t e = cudaMalloc(&a->idx, sizeof(uint32_t) * std::max<int64_t>(rows * a->k, 1));
+    a->layouts = layouts;
+    cudaError_t e = cudaMalloc(&a->diag_int, sizeof(uint64_t) * std::max<int64_t>(a->cols, 1));
+    if (e == cudaSuccess) e = cudaMemsetAsync(a->diag_int, 0, sizeof(uint64_t) * std::max<int64_t>(a->cols, 1), s);
     if (e != cudaSuccess) {
         free_csr(a);
-        set_error("cas_csr_from_positions: cannot allocate the index array");
+        set_error("cas_csr_from_positions: cannot allocate the column statistics");
         return CAS_ERR_OUT_OF_MEMORY;
     }
-    cas_status st = launch_index(*dp, d_positions, rows, a->idx, s);
-    if (st != CAS_OK) {
-        free_csr(a);
-        return st;
+    cas_status st = CAS_OK;
+    if (layouts & CAS_LAYOUT_BLOCKED) {
+        a->fast = new FastLayout;
+        // diag(A'A) comes from the blocked copy unless the row layout builds it
+        st = fast_build(*dp, pattern_set(p), d_positions, rows, (layouts & CAS_LAYOUT_ROWS) ? nullptr : a->diag_int,
+                        *a->fast, s);
+        if (st != CAS_OK) {
+            free_csr(a);
+            return st;
+        }
     }
-    return finish_create(a, s, out);
+    if (layouts & CAS_LAYOUT_ROWS) {
+        e = cudaMalloc(&a->idx, sizeof(uint32_t) * std::max<int64_t>(rows * a->k, 1));
+        if (e != cudaSuccess) {
+            free_csr(a);
+            set_error("cas_csr_from_positions: cannot allocate the index array");
+            return CAS_ERR_OUT_OF_MEMORY;
+        }
+        st = launch_index(*dp, d_positions, rows, a->idx, s);
+        if (st != CAS_OK) {
+            free_csr(a);
+            return st;
+        }
+        return finish_create(a, s, out);
+    }
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        free_csr(a);
+        set_error(std::string("CSR build: ") + cudaGetErrorString(e));
+        return CAS_ERR_CUDA;
+    }
+    *out = a;
+    return CAS_OK;
 }
+
+CAS_API cas_status cas_csr_from_positions(const cas_patterns* p, const uint64_t* d_positions, int64_t rows,
+                                          void* stream, cas_csr** out)
+{
+    CAS_REQUIRE(p, CAS_ERR_INVALID_ARGUMENT, "cas_csr_from_positions: null pattern set");
+    const int layouts = CAS_LAYOUT_ROWS | (fast_supported(pattern_set(p)) ? CAS_LAYOUT_BLOCKED : 0);
+    return cas_csr_from_positions_layout(p, d_positions, rows, layouts, stream, out);
+}
+
+CAS_API int cas_csr_layouts(const cas_csr* a) { return a ? a->layouts : 0; }
 
 CAS_API cas_status cas_csr_from_indices(const uint32_t* d_indices, int nnz_per_row, int64_t rows, int64_t cols,
                                         void* stream, cas_csr** out)
@@ -538,6 +590,7 @@ CAS_API cas_status cas_csr_from_indices(const uint32_t* d_indices, int nnz_per_r
     a->rows = rows;
     a->cols = cols;
     a->k = nnz_per_row;
+    a->layouts = CAS_LAYOUT_ROWS;
     const size_t bytes = sizeof(uint32_t) * rows * nnz_per_row;
     cudaError_t e = cudaMalloc(&a->idx, std::max<size_t>(bytes, 4));
     if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(a->idx, d_indices, bytes, cudaMemcpyDefault, s);
@@ -568,6 +621,13 @@ CAS_API cas_status cas_spmv(const cas_csr* a, cas_dtype dtype, const void* d_x, 
     CAS_REQUIRE(a, CAS_ERR_INVALID_ARGUMENT, "cas_spmv: null handle");
     CAS_REQUIRE((d_x || a->cols == 0) && (d_y || a->rows == 0), CAS_ERR_INVALID_ARGUMENT, "cas_spmv: null vector");
     auto s = static_cast<cudaStream_t>(stream);
+    if (a->fast && (dtype == CAS_F32 || dtype == CAS_F64)) {
+        if (dtype == CAS_F32)
+            return fast_spmv<float, float>(*a->fast, static_cast<const float*>(d_x), static_cast<float*>(d_y), nullptr,
+                                           nullptr, nullptr, nullptr, 0, s, nullptr);
+        return fast_spmv<double, double>(*a->fast, static_cast<const double*>(d_x), static_cast<double*>(d_y), nullptr,
+                                         nullptr, nullptr, nullptr, 0, s, nullptr);
+    }
     if (dtype == CAS_F32) return spmv<float>(a->view(), static_cast<const float*>(d_x), static_cast<float*>(d_y), s);
     if (dtype == CAS_F64)
         return spmv<double>(a->view(), static_cast<const double*>(d_x), static_cast<double*>(d_y), s);
@@ -580,6 +640,10 @@ CAS_API cas_status cas_spmv_t(const cas_csr* a, cas_dtype dtype, const void* d_y
     CAS_REQUIRE(a, CAS_ERR_INVALID_ARGUMENT, "cas_spmv_t: null handle");
     CAS_REQUIRE((d_y || a->rows == 0) && (d_x || a->cols == 0), CAS_ERR_INVALID_ARGUMENT, "cas_spmv_t: null vector");
     auto s = static_cast<cudaStream_t>(stream);
+    if (a->fast && dtype == CAS_F32)
+        return fast_spmv_t<float>(*a->fast, static_cast<const float*>(d_y), static_cast<float*>(d_x), s);
+    if (a->fast && dtype == CAS_F64)
+        return fast_spmv_t<double>(*a->fast, static_cast<const double*>(d_y), static_cast<double*>(d_x), s);
     if (dtype == CAS_F32)
         return spmv_t<float>(a->view(), static_cast<const float*>(d_y), a->unit_partial, static_cast<float*>(d_x), s);
     if (dtype == CAS_F64)

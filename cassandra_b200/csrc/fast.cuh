@@ -1,0 +1,142 @@
+// The blocked layout of a pattern CSR and its products (fast.cu).
+//
+// Rows are cut into blocks of kBlockRows.  Inside a block the entries of each
+// pattern (indexer) are stored together:
+//
+//   A16  uint16  [block][pattern][row][slot]   local column of every entry
+//   G32  uint32  [block][pattern][entry]       (local column << 16) | row in
+//                                              block, sorted by column then
+//                                              row (the transposed copy)
+//
+// so that a CTA touches one pattern's columns at a time.  A x stages that
+// pattern's slice of x in shared memory and gathers from there; A'y stages
+// the block's slice of y in shared memory and reduces the column-sorted
+// entries of one column chunk into a shared-memory accumulator.  Local
+// columns must fit 16 bits (index space per pattern <= 65536).
+#pragma once
+#include <cstdint>
+
+#include "internal.cuh"
+
+namespace cas {
+
+constexpr int kBlockRows = 16384;        // rows per block (and per A'y tile)
+constexpr int kFastThreads = 1024;       // threads of the product kernels
+constexpr int kRowsPerThread = kBlockRows / kFastThreads;
+constexpr int kChunkCols = 8192;         // column chunk of the A'y accumulators
+constexpr int kMaxFastPatterns = 32;
+constexpr int kTable32 = 57344;          // x entries staged per pattern, FP32
+constexpr int kTable64 = 28672;          // x entries staged per pattern, FP64
+
+// Per-pattern geometry, passed to kernels by value.
+struct FastGeometry {
+    int npat = 0;
+    int k = 0;                           // entries per row (sum of slots)
+    int64_t rows = 0, cols = 0;
+    int64_t nblocks = 0;
+    int slot0[kMaxFastPatterns];
+    int slots[kMaxFastPatterns];
+    int64_t off[kMaxFastPatterns];       // global column offset
+    int space[kMaxFastPatterns];         // columns of the pattern
+    int chunk0[kMaxFastPatterns];        // first global chunk of the pattern
+    int nchunks = 0;
+
+    __host__ __device__ int64_t block_rows(int64_t b) const
+    {
+        const int64_t r = rows - b * kBlockRows;
+        return r < kBlockRows ? r : kBlockRows;
+    }
+    // Rows of a block rounded up to 8 so that every segment is 16-byte aligned.
+    __host__ __device__ int64_t padded_rows(int64_t b) const { return (block_rows(b) + 7) & ~int64_t(7); }
+    // Element offset of (block, pattern) in A16 / G32.
+    __host__ __device__ int64_t seg(int64_t b, int p) const
+    {
+        return b * int64_t(kBlockRows) * k + padded_rows(b) * slot0[p];
+    }
+    __host__ __device__ int64_t seg_len(int64_t b, int p) const { return block_rows(b) * slots[p]; }
+    __host__ __device__ int64_t total_elems() const
+    {
+        return nblocks == 0 ? 0 : (nblocks - 1) * int64_t(kBlockRows) * k + padded_rows(nblocks - 1) * k;
+    }
+};
+
+// Work list of one A'y variant: a "super-chunk" is up to `per_sc` consecutive
+// chunks of one pattern; an item is (super-chunk, block range).  Every item
+// writes the partial sums of its super-chunk's columns; a column's value is
+// the sum of its super-chunk's items in item order.
+struct FastTranspose {
+    int per_sc = 1;        // chunks per super-chunk
+    int nsc = 0;
+    int nitems = 0;
+    int sc_base[kMaxFastPatterns + 1];  // first super-chunk of each pattern
+    int* item_sc = nullptr;             // [nitems]
+    int* item_b0 = nullptr;             // [nitems]
+    int* item_b1 = nullptr;             // [nitems]
+    int64_t* item_part = nullptr;       // [nitems] offset of the item's partials
+    int* sc_item0 = nullptr;            // [nsc + 1] first item of each super-chunk
+    void* partial = nullptr;            // float or double partials
+};
+
+struct FastLayout {
+    FastGeometry g;
+    uint16_t* a16 = nullptr;
+    uint32_t* g32 = nullptr;
+    uint32_t* chunk_start = nullptr;   // [nblocks][nchunks] absolute index in G32
+    FastTranspose t32, t64;
+};
+
+// Device view used by the column reductions of the solver.
+struct FastCols {
+    FastGeometry g;
+    int per_sc;
+    const int* sc_item0;
+    const int64_t* item_part;
+    int sc_base[kMaxFastPatterns + 1];
+};
+
+// Builds the blocked layout from positions (indexes them itself).  Returns
+// CAS_ERR_INVALID_ARGUMENT without touching `out` if the pattern set does
+// not fit the layout (a pattern wider than 16-bit columns, too many patterns
+// or a slot count other than 1, 2, 4, 8).
+cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint64_t* d_pos, int64_t rows,
+                      uint64_t* diag_int, FastLayout& out, cudaStream_t s);
+bool fast_supported(const PatternSet& ps);
+void fast_free(FastLayout& f);
+
+// y = A x on the blocked layout; also writes per-CTA partials of ||y||^2
+// (part may be null).  mode 0: y = A x; 1: y = A x - coef * y (coef read
+// from *coef); 2: y = b - A x (b may be null: y = -A x).
+template <typename T, typename Y>
+cas_status fast_spmv(const FastLayout& f, const T* x, Y* y, const double* b, const double* coef, double* part,
+                     int* done_flag, int mode, cudaStream_t s, int* n_parts);
+
+// Partials of A' y on the blocked layout (FP32: float partials, FP64:
+// double partials); columns are summed by fast_col_sum().
+template <typename T>
+cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag, cudaStream_t s);
+
+template <typename T>
+FastCols fast_cols(const FastLayout& f);
+
+template <typename T>
+__device__ __forceinline__ double fast_col_sum(const FastCols& fc, const T* partial, int64_t c)
+{
+    int p = 0;
+    while (p + 1 < fc.g.npat && fc.g.off[p + 1] <= c) p++;
+    const int local = static_cast<int>(c - fc.g.off[p]);
+    const int width = kChunkCols * fc.per_sc;
+    const int sc = fc.sc_base[p] + local / width;
+    const int lc = local - (local / width) * width;
+    double acc = 0;
+    for (int it = fc.sc_item0[sc]; it < fc.sc_item0[sc + 1]; it++) acc += static_cast<double>(partial[fc.item_part[it] + lc]);
+    return acc;
+}
+
+// Jacobi diagonal from G32 (integer, deterministic).
+cas_status fast_diag(const FastLayout& f, uint64_t* diag, cudaStream_t s);
+
+// Full A'y into a dense vector (standalone product).
+template <typename T>
+cas_status fast_spmv_t(const FastLayout& f, const T* y, T* x, cudaStream_t s);
+
+}  // namespace cas

@@ -6,6 +6,7 @@
 
 #include "board.cuh"
 #include "common.cuh"
+#include "fast.cuh"
 #include "internal.cuh"
 
 namespace cas {
@@ -147,8 +148,12 @@ CAS_API cas_status cas_fit_weights_device(const cas_patterns* p, const uint64_t*
     CAS_CUDA(cudaEventCreate(&e0));
     CAS_CUDA(cudaEventCreate(&e1));
     CAS_CUDA(cudaEventRecord(e0, s));
+    // The mixed solver runs on the blocked layout, the plain FP64 path on the
+    // reference's row layout; only the layout the solve uses is built.
+    int layouts = CAS_LAYOUT_ROWS;
+    if (o->precision == CAS_MIXED && fast_supported(pattern_set(p))) layouts = CAS_LAYOUT_BLOCKED;
     cas_csr* a = nullptr;
-    cas_status st = cas_csr_from_positions(p, d_positions, rows, stream, &a);
+    cas_status st = cas_csr_from_positions_layout(p, d_positions, rows, layouts, stream, &a);
     if (st != CAS_OK) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);

@@ -40,8 +40,14 @@ struct CsrView {
 
 }  // namespace cas
 
+namespace cas {
+struct FastLayout;
+}
+
 struct cas_csr {
     int device = -1;
+    int layouts = 0;                 // CAS_LAYOUT_* bits present
+    cas::FastLayout* fast = nullptr;  // blocked layout (fast.cuh), or null
     int64_t rows = 0, cols = 0;
     int k = 0;
     uint32_t* idx = nullptr;

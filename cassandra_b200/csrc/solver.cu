@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "fast.cuh"
 #include "internal.cuh"
 
 namespace cas {
@@ -168,6 +169,25 @@ __device__ __forceinline__ double unit_sum(const CsrView& a, const double* parti
     return acc;
 }
 
+// Column c of the last A'q product, whichever layout computed it:
+// kind 0 sums the rows layout's work-unit partials, kind 1/2 the blocked
+// layout's FP32/FP64 item partials; kind -1 means "no product" (0).
+struct ColSum {
+    int kind = -1;
+    CsrView a;
+    const double* unit_partial = nullptr;
+    FastCols fc;
+    const float* p32 = nullptr;
+    const double* p64 = nullptr;
+    __device__ __forceinline__ double operator()(int64_t c) const
+    {
+        if (kind == 1) return fast_col_sum<float>(fc, p32, c);
+        if (kind == 2) return fast_col_sum<double>(fc, p64, c);
+        if (kind == 0) return unit_sum(a, unit_partial, c);
+        return 0.0;
+    }
+};
+
 // ---------------------------------------------------------------------------
 // PCG vector steps.
 // ---------------------------------------------------------------------------
@@ -195,7 +215,7 @@ __global__ void __launch_bounds__(kRedThreads) pcg_alpha_kernel(const double* __
 // s = A'A p (from unit partials); x += alpha p; r -= alpha s; z = d r;
 // partials of r.z and r.r.
 template <bool COMP>
-__global__ void __launch_bounds__(kVecThreads) pcg_update_kernel(CsrView a, const double* __restrict__ partial,
+__global__ void __launch_bounds__(kVecThreads) pcg_update_kernel(ColSum cs,
                                                                  double* __restrict__ x, double* __restrict__ r,
                                                                  double* __restrict__ z, const double* __restrict__ p,
                                                                  const double* __restrict__ d,
@@ -206,9 +226,9 @@ __global__ void __launch_bounds__(kVecThreads) pcg_update_kernel(CsrView a, cons
     if (finished(dv.flags)) return;
     const double alpha = dv.scal[kAlpha];
     Comp rz, rr;
-    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < a.cols;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cs.a.cols;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const double s = unit_sum(a, partial, c);
+        const double s = cs(c);
         x[c] += alpha * p[c];
         const double rc = r[c] - alpha * s;
         const double zc = d[c] * rc;
@@ -274,7 +294,7 @@ __global__ void __launch_bounds__(kVecThreads) pcg_direction_kernel(int64_t n, c
 // r = A'(b - A x) from unit partials; z = d r; partials of r.z and r.r.
 // Also initialises p = z (init != 0) and ||A'b||^2 (bn != 0, x = 0).
 template <bool COMP, typename T>
-__global__ void __launch_bounds__(kVecThreads) pcg_residual_kernel(CsrView a, const double* __restrict__ partial,
+__global__ void __launch_bounds__(kVecThreads) pcg_residual_kernel(ColSum cs,
                                                                    double* __restrict__ r, double* __restrict__ z,
                                                                    double* __restrict__ p, T* __restrict__ pg,
                                                                    const double* __restrict__ d,
@@ -285,9 +305,9 @@ __global__ void __launch_bounds__(kVecThreads) pcg_residual_kernel(CsrView a, co
     __shared__ double smem[64];
     if (!force && finished(dv.flags)) return;
     Comp rz, rr;
-    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < a.cols;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cs.a.cols;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const double rc = (bn ? bn[c] : 0.0) + unit_sum(a, partial, c);
+        const double rc = (bn ? bn[c] : 0.0) + cs(c);
         const double zc = d[c] * rc;
         r[c] = rc;
         z[c] = zc;
@@ -328,15 +348,15 @@ __global__ void cast_kernel(int64_t n, const double* __restrict__ in, T* __restr
 // ||v||^2 partials of v = bn + (A' q from unit partials); partial may be
 // null (v = bn), bn may be null (v = A' q).  Used for ||A'b||^2 and ||A'r||^2.
 template <bool COMP>
-__global__ void __launch_bounds__(kVecThreads) norm_units_kernel(CsrView a, const double* __restrict__ partial,
+__global__ void __launch_bounds__(kVecThreads) norm_units_kernel(ColSum cs,
                                                                  double* __restrict__ out, double* __restrict__ part,
                                                                  const double* __restrict__ bn)
 {
     __shared__ double smem[64];
     Comp acc;
-    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < a.cols;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cs.a.cols;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const double v = (bn ? bn[c] : 0.0) + (partial ? unit_sum(a, partial, c) : 0.0);
+        const double v = (bn ? bn[c] : 0.0) + cs(c);
         if (out) out[c] = v;
         acc_add<COMP>(acc, v * v);
     }
@@ -361,7 +381,7 @@ __global__ void __launch_bounds__(kRedThreads) store_sum_kernel(const double* __
 // v_hat = (1/beta) A' u_hat - beta v  (v = v_hat_prev / alpha_prev);
 // partial ||v_hat||^2.  init: v_hat = (1/beta) A' u_hat.
 template <bool COMP, typename T>
-__global__ void __launch_bounds__(kVecThreads) lsqr_v_kernel(CsrView a, const double* __restrict__ partial,
+__global__ void __launch_bounds__(kVecThreads) lsqr_v_kernel(ColSum cs,
                                                              double* __restrict__ v, double* __restrict__ part,
                                                              Dev dv, int init)
 {
@@ -371,9 +391,9 @@ __global__ void __launch_bounds__(kVecThreads) lsqr_v_kernel(CsrView a, const do
     const double beta = dv.scal[kLBeta];
     const double inv_alpha_prev = dv.scal[kLAlpha] != 0 ? 1.0 / dv.scal[kLAlpha] : 0.0;
     Comp acc;
-    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < a.cols;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cs.a.cols;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        double val = inv_beta * unit_sum(a, partial, c);
+        double val = inv_beta * cs(c);
         if (!init) val -= beta * (v[c] * inv_alpha_prev);
         v[c] = val;
         acc_add<COMP>(acc, val * val);
@@ -491,10 +511,13 @@ unsigned row_grid(int64_t rows)
 struct SolverImpl {
     const cas_csr* A = nullptr;
     CsrView a;
+    const FastLayout* fast = nullptr;
     cas_solve_opts o{};
     cudaStream_t s = nullptr;
     int device = 0;
     bool mixed = false;
+    bool fast32 = false;  // FP32 products on the blocked layout
+    bool fast64 = false;  // FP64 products on the blocked layout
     int64_t C = 0, R = 0;
     // C-length FP64 vectors
     double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *d = nullptr, *w = nullptr, *v = nullptr;
@@ -505,9 +528,9 @@ struct SolverImpl {
     const double* b = nullptr;   // rows-length targets (null with a normal RHS)
     const double* bn = nullptr;  // cols-length normal-equation RHS A'b (PCG/CG only)
     double* b_own = nullptr;
-    double* partial = nullptr;  // unit partials
+    double* partial = nullptr;  // unit partials of the rows layout
     double *part_q = nullptr, *part_a = nullptr, *part_b = nullptr;
-    int n_row_blocks = 0, n_vec_blocks = 0;
+    int n_row_blocks = 0, n_vec_blocks = 0, n_q_parts = 0;
     double* scal = nullptr;
     int* flags = nullptr;
     double* host_scal = nullptr;  // pinned mirror
@@ -535,16 +558,72 @@ struct SolverImpl {
         cudaFreeHost(host_flags);
     }
 
+    // Column sums of the last A'q of precision T.
+    template <typename T>
+    ColSum colsum() const
+    {
+        ColSum cs;
+        cs.a = a;
+        const bool use_fast = sizeof(T) == 4 ? fast32 : fast64;
+        if (use_fast) {
+            cs.kind = sizeof(T) == 4 ? 1 : 2;
+            cs.fc = fast_cols<T>(*fast);
+            cs.p32 = static_cast<const float*>(fast->t32.partial);
+            cs.p64 = static_cast<const double*>(fast->t64.partial);
+        } else {
+            cs.kind = 0;
+            cs.unit_partial = partial;
+        }
+        return cs;
+    }
+
+    // q = A g (mode 0), A g - scal[coef_slot] q (1), rhs - A g (2), with
+    // partials of ||q||^2 in part_q (count in n_q_parts).  `gate` lets the
+    // kernels return at entry once the solver has converged.
+    template <bool COMP, typename G, typename Q>
+    cas_status product(const G* g, Q* qq, int mode, const double* rhs, int coef_slot, bool gate)
+    {
+        const bool use_fast = sizeof(G) == 4 ? fast32 : fast64;
+        if (use_fast) {
+            return fast_spmv<G, Q>(*fast, g, qq, rhs, scal + coef_slot, part_q, gate ? flags : nullptr, mode, s,
+                                   &n_q_parts);
+        }
+        n_q_parts = n_row_blocks;
+        const Dev D = dv();
+        const int force = gate ? 0 : 1;
+        if (mode == 0)
+            { spmv_norm_kernel<G, Q, COMP, 0><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, g, qq, rhs, part_q, D,
+                                                                               coef_slot, force); cas::count_launch(); }
+        else if (mode == 1)
+            { spmv_norm_kernel<G, Q, COMP, 1><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, g, qq, rhs, part_q, D,
+                                                                               coef_slot, force); cas::count_launch(); }
+        else
+            { spmv_norm_kernel<G, Q, COMP, 2><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, g, qq, rhs, part_q, D,
+                                                                               coef_slot, force); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+        return CAS_OK;
+    }
+
+    // Partials of A' q (summed later through colsum<Q>()).
+    template <typename Q>
+    cas_status product_t(const Q* qq, bool gate)
+    {
+        const bool use_fast = sizeof(Q) == 4 ? fast32 : fast64;
+        if (use_fast) return fast_spmv_t_partials<Q>(*fast, qq, gate ? flags : nullptr, s);
+        { spmv_t_units_flag_kernel<Q><<<row_grid(a.units), kVecThreads, 0, s>>>(a, qq, partial, dv(), gate ? 0 : 1); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+        return CAS_OK;
+    }
+
     template <bool COMP, typename T>
     cas_status issue_pcg_iteration()
     {
         const Dev D = dv();
         const T* pgather = std::is_same<T, float>::value ? reinterpret_cast<const T*>(pg32) : reinterpret_cast<const T*>(p);
-        { spmv_norm_kernel<T, T, COMP, 0><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, pgather,
-                                                                           static_cast<T*>(q), nullptr, part_q, D, 0, 0); cas::count_launch(); }
-        { spmv_t_units_flag_kernel<T><<<row_grid(a.units), kVecThreads, 0, s>>>(a, static_cast<const T*>(q), partial, D, 0); cas::count_launch(); }
-        { pcg_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_row_blocks, D); cas::count_launch(); }
-        { pcg_update_kernel<COMP><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, x, r, z, p, d, part_a, part_b, D); cas::count_launch(); }
+        CAS_TRY((product<COMP, T, T>(pgather, static_cast<T*>(q), 0, nullptr, 0, true)));
+        CAS_TRY(product_t<T>(static_cast<const T*>(q), true));
+        { pcg_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D); cas::count_launch(); }
+        { pcg_update_kernel<COMP><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<T>(), x, r, z, p, d, part_a, part_b, D); cas::count_launch(); }
         { pcg_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, part_b, n_vec_blocks, D, 0, 0); cas::count_launch(); }
         { pcg_direction_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(
             C, z, p, std::is_same<T, float>::value ? reinterpret_cast<T*>(pg32) : nullptr, D); cas::count_launch(); }
@@ -552,22 +631,24 @@ struct SolverImpl {
         return CAS_OK;
     }
 
-    // Residual replacement: r = A'(b - A x) in FP64, z = d r, r.z, r.r.
-    // Inside a graph chunk (force == false) it is skipped once converged.
+    // Residual replacement: r = A'(b - A x) (or b' - A'A x) in FP64, z = d r,
+    // r.z, r.r.  Inside a graph chunk (force == false) it is skipped once
+    // converged.
     template <bool COMP>
     cas_status issue_pcg_refine(bool init, bool force)
     {
         const Dev D = dv();
         const int f = force ? 1 : 0;
-        { spmv_norm_kernel<double, double, COMP, 2><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, x, q64, b,
-                                                                                    part_q, D, 0, f); cas::count_launch(); }
-        { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, q64, partial, D, f); cas::count_launch(); }
+        CAS_TRY((product<COMP, double, double>(x, q64, 2, b, 0, !force)));
+        CAS_TRY(product_t<double>(q64, !force));
         if (mixed)
-            { pcg_residual_kernel<COMP, float><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, r, z, p, pg32, d, part_a,
-                                                                                part_b, init ? 1 : 0, D, f, bn); cas::count_launch(); }
+            { pcg_residual_kernel<COMP, float><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), r, z, p, pg32, d,
+                                                                                part_a, part_b, init ? 1 : 0, D, f,
+                                                                                bn); cas::count_launch(); }
         else
-            { pcg_residual_kernel<COMP, double><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, r, z, p, nullptr, d,
-                                                                                 part_a, part_b, init ? 1 : 0, D, f, bn); cas::count_launch(); }
+            { pcg_residual_kernel<COMP, double><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), r, z, p, nullptr, d,
+                                                                                 part_a, part_b, init ? 1 : 0, D, f,
+                                                                                 bn); cas::count_launch(); }
         { pcg_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, part_b, n_vec_blocks, D, 1, f); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
@@ -580,12 +661,11 @@ struct SolverImpl {
         T* vg = reinterpret_cast<T*>(std::is_same<T, float>::value ? (void*)pg32 : (void*)p);
         // u_hat = A v - (alpha / beta_prev) u_hat_prev
         { lsqr_coef_kernel<<<1, 1, 0, s>>>(D, kPap); cas::count_launch(); }
-        { spmv_norm_kernel<T, T, COMP, 1><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, vg, static_cast<T*>(q),
-                                                                           nullptr, part_q, D, kPap, 0); cas::count_launch(); }
-        { lsqr_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_row_blocks, D, 0); cas::count_launch(); }
+        CAS_TRY((product<COMP, T, T>(vg, static_cast<T*>(q), 1, nullptr, kPap, true)));
+        { lsqr_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, 0); cas::count_launch(); }
         // v_hat = (1/beta) A' u_hat - beta v
-        { spmv_t_units_flag_kernel<T><<<row_grid(a.units), kVecThreads, 0, s>>>(a, static_cast<const T*>(q), partial, D, 0); cas::count_launch(); }
-        { lsqr_v_kernel<COMP, T><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, v, part_a, D, 0); cas::count_launch(); }
+        CAS_TRY(product_t<T>(static_cast<const T*>(q), true));
+        { lsqr_v_kernel<COMP, T><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<T>(), v, part_a, D, 0); cas::count_launch(); }
         { lsqr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 0); cas::count_launch(); }
         { lsqr_xw_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, vg, D, 0); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
@@ -657,11 +737,9 @@ struct SolverImpl {
     // ||A'(b - A x)|| / ||A'b|| in FP64 (does not touch solver state).
     cas_status true_residual(double* out)
     {
-        const Dev D = dv();
-        { spmv_norm_kernel<double, double, false, 2><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, x, q64, b,
-                                                                                     part_q, D, 0, 1); cas::count_launch(); }
-        { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, q64, partial, D, 1); cas::count_launch(); }
-        { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, nullptr, part_a, bn); cas::count_launch(); }
+        CAS_TRY((product<true, double, double>(x, q64, 2, b, 0, false)));
+        CAS_TRY(product_t<double>(q64, false));
+        { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), nullptr, part_a, bn); cas::count_launch(); }
         { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kTrue); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         double h[kSlots];
@@ -678,16 +756,21 @@ struct SolverImpl {
         C = a.cols;
         R = a.rows;
         mixed = o.precision == CAS_MIXED;
+        fast = A->fast;
+        const bool rows_layout = (A->layouts & CAS_LAYOUT_ROWS) != 0;
+        fast32 = fast && (mixed || !rows_layout);
+        fast64 = fast && (mixed || !rows_layout);
         n_row_blocks = static_cast<int>(row_grid(R));
         n_vec_blocks = static_cast<int>(vec_grid(C));
+        const int q_parts = std::max(n_row_blocks, sm_count());
         const size_t cb = sizeof(double) * std::max<int64_t>(C, 1), rb8 = sizeof(double) * std::max<int64_t>(R, 1);
         for (double** ptr : {&x, &r, &z, &p, &d, &w, &v}) CAS_CUDA(cudaMalloc(ptr, cb));
         if (mixed) CAS_CUDA(cudaMalloc(&pg32, sizeof(float) * std::max<int64_t>(C, 1)));
         CAS_CUDA(cudaMalloc(&q, mixed ? sizeof(float) * std::max<int64_t>(R, 1) : rb8));
         CAS_CUDA(cudaMalloc(&q64, rb8));
-        CAS_CUDA(cudaMalloc(&partial, sizeof(double) * std::max<int64_t>(a.units, 1)));
-        CAS_CUDA(cudaMalloc(&part_q, sizeof(double) * 2 * n_row_blocks));
-        CAS_CUDA(cudaMalloc(&part_a, sizeof(double) * 2 * std::max(n_vec_blocks, n_row_blocks)));
+        if (rows_layout) CAS_CUDA(cudaMalloc(&partial, sizeof(double) * std::max<int64_t>(a.units, 1)));
+        CAS_CUDA(cudaMalloc(&part_q, sizeof(double) * 2 * q_parts));
+        CAS_CUDA(cudaMalloc(&part_a, sizeof(double) * 2 * std::max(n_vec_blocks, q_parts)));
         CAS_CUDA(cudaMalloc(&part_b, sizeof(double) * 2 * n_vec_blocks));
         CAS_CUDA(cudaMalloc(&scal, sizeof(double) * kSlots));
         CAS_CUDA(cudaMalloc(&flags, sizeof(int) * kFlags));
@@ -709,10 +792,12 @@ struct SolverImpl {
 
         // ||A'b||^2 (denominator of the relative residual)
         if (bn) {
-            { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(a, nullptr, nullptr, part_a, bn); cas::count_launch(); }
+            ColSum none;
+            none.a = a;
+            { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(none, nullptr, part_a, bn); cas::count_launch(); }
         } else {
-            { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, b, partial, D, 1); cas::count_launch(); }
-            { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, nullptr, part_a, nullptr); cas::count_launch(); }
+            CAS_TRY(product_t<double>(b, false));
+            { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), nullptr, part_a, nullptr); cas::count_launch(); }
         }
         { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kBn2); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
@@ -720,24 +805,17 @@ struct SolverImpl {
         if (o.method == CAS_LSQR) {
             // beta u = b - A x0 ; alpha v = A'u ; w = v ; phi_bar = beta ; rho_bar = alpha
             if (mixed) {
-                { spmv_norm_kernel<double, float, true, 2><<<n_row_blocks, kVecThreads, 0, s>>>(
-                    a.idx, R, a.k, x, static_cast<float*>(q), b, part_q, D, 0, 1); cas::count_launch(); }
-            } else {
-                { spmv_norm_kernel<double, double, false, 2><<<n_row_blocks, kVecThreads, 0, s>>>(
-                    a.idx, R, a.k, x, static_cast<double*>(q), b, part_q, D, 0, 1); cas::count_launch(); }
-            }
-            if (mixed) {
-                { lsqr_beta_kernel<true><<<1, kRedThreads, 0, s>>>(part_q, n_row_blocks, D, 1); cas::count_launch(); }
-                { spmv_t_units_flag_kernel<float><<<row_grid(a.units), kVecThreads, 0, s>>>(a, static_cast<float*>(q),
-                                                                                         partial, D, 1); cas::count_launch(); }
-                { lsqr_v_kernel<true, float><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, v, part_a, D, 1); cas::count_launch(); }
+                CAS_TRY((product<true, double, float>(x, static_cast<float*>(q), 2, b, 0, false)));
+                { lsqr_beta_kernel<true><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, 1); cas::count_launch(); }
+                CAS_TRY(product_t<float>(static_cast<const float*>(q), false));
+                { lsqr_v_kernel<true, float><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<float>(), v, part_a, D, 1); cas::count_launch(); }
                 { lsqr_alpha_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 1); cas::count_launch(); }
                 { lsqr_xw_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, pg32, D, 1); cas::count_launch(); }
             } else {
-                { lsqr_beta_kernel<false><<<1, kRedThreads, 0, s>>>(part_q, n_row_blocks, D, 1); cas::count_launch(); }
-                { spmv_t_units_flag_kernel<double><<<row_grid(a.units), kVecThreads, 0, s>>>(a, static_cast<double*>(q),
-                                                                                          partial, D, 1); cas::count_launch(); }
-                { lsqr_v_kernel<false, double><<<n_vec_blocks, kVecThreads, 0, s>>>(a, partial, v, part_a, D, 1); cas::count_launch(); }
+                CAS_TRY((product<false, double, double>(x, static_cast<double*>(q), 2, b, 0, false)));
+                { lsqr_beta_kernel<false><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, 1); cas::count_launch(); }
+                CAS_TRY(product_t<double>(static_cast<const double*>(q), false));
+                { lsqr_v_kernel<false, double><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), v, part_a, D, 1); cas::count_launch(); }
                 { lsqr_alpha_kernel<false><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 1); cas::count_launch(); }
                 { lsqr_xw_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, p, D, 1); cas::count_launch(); }
             }

@@ -111,9 +111,25 @@ typedef enum cas_dtype { CAS_F32 = 0, CAS_F64 = 1 } cas_dtype;
 typedef struct cas_csr cas_csr;
 
 /* Index d_positions and build the device-resident CSR plus its transposed
- * copy and the column statistics (replaces PatternFit/PatternFit.cpp:12-21). */
+ * copy and the column statistics (replaces PatternFit/PatternFit.cpp:12-21).
+ * Builds both layouts below (BLOCKED only when the pattern set fits it). */
 CAS_API cas_status cas_csr_from_positions(const cas_patterns* p, const uint64_t* d_positions, int64_t rows,
                                           void* stream, cas_csr** out);
+/* Device layouts of a CSR.  ROWS is the reference's row-major structure
+ * (uint32 indices, rows * nnz_per_row) plus its transposed copy sorted by
+ * (column, row).  BLOCKED stores each pattern's entries per 16384-row block
+ * as 16-bit local columns, plus a per-block column-sorted copy; its products
+ * stage their gather vectors in shared memory (the fast path of the mixed
+ * solver).  BLOCKED needs every pattern's index space <= 65536. */
+typedef enum cas_layout { CAS_LAYOUT_ROWS = 1, CAS_LAYOUT_BLOCKED = 2 } cas_layout;
+
+/* As cas_csr_from_positions, building only the layouts in `layouts` (a mask
+ * of cas_layout).  Products use BLOCKED when present. */
+CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const uint64_t* d_positions, int64_t rows,
+                                                 int layouts, void* stream, cas_csr** out);
+/* Mask of the layouts a CSR holds. */
+CAS_API int cas_csr_layouts(const cas_csr* a);
+
 /* Build from existing row-major indices (MatrixCSR(K, rows, cols) filled via
  * Row(i), Math/MatrixCSR.cpp:5-19).  The indices are copied. */
 CAS_API cas_status cas_csr_from_indices(const uint32_t* d_indices, int nnz_per_row, int64_t rows, int64_t cols,
@@ -122,7 +138,8 @@ CAS_API void cas_csr_destroy(cas_csr* a);
 CAS_API int64_t cas_csr_rows(const cas_csr* a);
 CAS_API int64_t cas_csr_cols(const cas_csr* a);
 CAS_API int cas_csr_nnz_per_row(const cas_csr* a);
-/* Device pointer to the rows * nnz_per_row row-major column indices. */
+/* Device pointer to the rows * nnz_per_row row-major column indices (NULL
+ * when the CSR has no ROWS layout). */
 CAS_API const uint32_t* cas_csr_indices(const cas_csr* a);
 /* Device pointers to the transposed copy: col_ptr (cols + 1 int64) and the
  * row index of every entry, sorted by (column, row). */

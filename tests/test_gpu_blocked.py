@@ -1,0 +1,122 @@
+"""The blocked layout (16-bit pattern-local columns per 16384-row block and a
+per-block column-sorted copy): products and solvers against the oracle and
+against the rows layout, on block-boundary sizes and both index modes."""
+import numpy as np
+import pytest
+import torch
+
+import cassandra_b200 as cb
+from tests.golden.make_golden import FIXTURES, SET5, SET8
+
+pytestmark = pytest.mark.gpu
+
+ROWS = [1, 7, 16383, 16384, 16385, 50_001]
+
+
+def _build(rows, masks, mode, layouts, seed=3):
+    pos = cb.generate_positions(seed, rows, 10, 50)
+    g = cb.GroupIndexer(masks, mode)
+    return cb.MatrixCSR.from_positions(g, pos, layouts), pos, g
+
+
+@pytest.mark.parametrize("rows", ROWS)
+@pytest.mark.parametrize("masks,mode", [(SET8, "expanded"), (SET5, "reference"), (list(FIXTURES.values()), "reference")])
+def test_blocked_products_match_oracle(cuda, orc, rows, masks, mode):
+    a, pos, g = _build(rows, masks, mode, "blocked")
+    assert a.layouts() == {"blocked"}
+    cols = g.index_space_size
+    idx = orc.group_index(masks, 0 if mode == "reference" else 1, pos.cpu().numpy().view(np.uint64))
+    rng = np.random.default_rng(rows)
+    x = rng.standard_normal(cols)
+    y = rng.standard_normal(rows)
+    np.testing.assert_allclose((a @ torch.from_numpy(x).cuda()).cpu().numpy(), orc.spmv(idx, cols, x), rtol=1e-12,
+                               atol=1e-11)
+    np.testing.assert_allclose((torch.from_numpy(y).cuda() @ a).cpu().numpy(), orc.spmv_t(idx, cols, y), rtol=1e-11,
+                               atol=1e-10)
+    # FP32: exact for integer-valued vectors
+    xi = rng.integers(-50, 50, cols).astype(np.float32)
+    yi = rng.integers(-50, 50, rows).astype(np.float32)
+    np.testing.assert_array_equal((a @ torch.from_numpy(xi).cuda()).cpu().numpy(),
+                                  orc.spmv(idx, cols, xi.astype(np.float64)).astype(np.float32))
+    np.testing.assert_array_equal((torch.from_numpy(yi).cuda() @ a).cpu().numpy(),
+                                  orc.spmv_t(idx, cols, yi.astype(np.float64)).astype(np.float32))
+    # FP32, general values: within FP32 accumulation error
+    x32 = x.astype(np.float32)
+    got = (a @ torch.from_numpy(x32).cuda()).cpu().numpy().astype(np.float64)
+    want = orc.spmv(idx, cols, x32.astype(np.float64))
+    assert np.abs(got - want).max() <= 64 * 2 ** -23 * np.abs(want).max() + 1e-6
+    with np.errstate(divide="ignore"):
+        np.testing.assert_array_equal(cb.jacobi_preconditioner_of_ata(a).cpu().numpy(), orc.jacobi(idx, cols))
+
+
+def test_blocked_and_rows_layouts_agree(cuda):
+    both, pos, g = _build(40_000, SET8, "expanded", "rows+blocked")
+    rows_only = cb.MatrixCSR.from_positions(g, pos, "rows")
+    assert both.layouts() == {"rows", "blocked"}
+    np.testing.assert_array_equal(both.indices().cpu().numpy(), rows_only.indices().cpu().numpy())
+    y = torch.randn(40_000, dtype=torch.float64, device="cuda")
+    np.testing.assert_allclose((y @ both).cpu().numpy(), (y @ rows_only).cpu().numpy(), rtol=1e-11, atol=1e-10)
+    np.testing.assert_array_equal(cb.jacobi_preconditioner_of_ata(both).cpu().numpy(),
+                                  cb.jacobi_preconditioner_of_ata(rows_only).cpu().numpy())
+
+
+def test_blocked_transpose_is_deterministic(cuda):
+    a, pos, g = _build(120_000, SET8, "expanded", "blocked")
+    for dt in (torch.float32, torch.float64):
+        y = torch.randn(120_000, dtype=dt, device="cuda")
+        r1 = (y @ a).cpu().numpy()
+        r2 = (y @ a).cpu().numpy()
+        assert r1.tobytes() == r2.tobytes()
+
+
+def test_blocked_rejects_wide_patterns(cuda):
+    pos = cb.generate_positions(1, 100, 10, 50)
+    g = cb.GroupIndexer([0xFFF], "expanded")  # 12 squares: 531441 columns > 65536
+    with pytest.raises(cb.CasError):
+        cb.MatrixCSR.from_positions(g, pos, "blocked")
+    a = cb.MatrixCSR.from_positions(g, pos)  # default falls back to the rows layout
+    assert a.layouts() == {"rows"}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("method", ["pcg", "lsqr"])
+def test_solvers_on_blocked_layout(cuda, orc, precision, method):
+    rows = 3000 if method == "lsqr" else 40_000
+    a, pos, g = _build(rows, SET5 if method == "lsqr" else SET8, "reference" if method == "lsqr" else "expanded",
+                       "blocked", seed=9)
+    b = cb.generate_targets(a, 9)
+    masks = SET5 if method == "lsqr" else SET8
+    idx = orc.group_index(masks, 0 if method == "lsqr" else 1, pos.cpu().numpy().view(np.uint64))
+    cols = g.index_space_size
+    cls = cb.PCG if method == "pcg" else cb.LSQR
+    s = cls(a, b, precision=precision, tol=1e-8, max_iterations=60_000, check_every=100)
+    rep = s.run()
+    assert rep["converged"], rep
+    assert orc.normal_residual(idx, cols, b.cpu().numpy(), s.x().cpu().numpy()) <= 1.5e-8
+
+
+def test_pcg_iterates_on_blocked_match_oracle(cuda, orc):
+    a, pos, g = _build(30_000, SET8, "expanded", "blocked", seed=4)
+    b = cb.generate_targets(a, 4)
+    idx = orc.group_index(SET8, 1, pos.cpu().numpy().view(np.uint64))
+    s = cb.PCG(a, b, check_every=5)  # plain FP64 on the blocked layout
+    s.iterate(10)
+    want, res, _ = orc.pcg(idx, g.index_space_size, b.cpu().numpy(), 10)
+    np.testing.assert_allclose(s.x().cpu().numpy(), want, rtol=0, atol=1e-10 * np.abs(want).max())
+
+
+def test_mixed_solution_matches_plain(cuda):
+    """Mixed precision on the blocked layout and plain FP64 on the rows layout
+    reach the same least-squares fit (same predictions) at 1e-8."""
+    pos = cb.generate_positions(12, 60_000, 20, 40)
+    g = cb.GroupIndexer(SET8, "expanded")
+    fast = cb.MatrixCSR.from_positions(g, pos, "blocked")
+    plain = cb.MatrixCSR.from_positions(g, pos, "rows")
+    b = cb.generate_targets(plain, 12)
+    m = cb.PCG(fast, b, precision="mixed", tol=1e-8)
+    p = cb.PCG(plain, b, precision="fp64", tol=1e-8)
+    rm, rp = m.run(), p.run()
+    assert rm["converged"] and rp["converged"]
+    pm = (plain @ m.x()).cpu().numpy()
+    pp = (plain @ p.x()).cpu().numpy()
+    np.testing.assert_allclose(pm, pp, rtol=0, atol=1e-5 * np.abs(pp).max())
