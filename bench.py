@@ -51,7 +51,7 @@ def parse_args(argv=None):
     ap.add_argument("--max-empties", type=int, default=40)
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--cpu-sample-rows", type=int, default=200_000,
+    ap.add_argument("--cpu-sample-rows", type=int, default=5_000_000,
                     help="rows of the bounded sample the CPU baseline runs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
@@ -236,6 +236,7 @@ def run_ours(args) -> dict | None:
 
     # ---- end to end through the public C ABI with host buffers
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
+    e2e_val = None
     pos_h = torch.empty((R, 2), dtype=torch.int64, pin_memory=True)
     pos_h.copy_(pos)
     sc_h = torch.empty(R, dtype=torch.float32, pin_memory=True)
@@ -252,8 +253,8 @@ def run_ours(args) -> dict | None:
                                  C.c_void_p(w_h.data_ptr()), C.byref(rep))
         e2e_times.append(time.perf_counter() - t0)
         L.check(st)
-    e2e_val = statistics.mean(e2e_times)
-    if world > 1:
+    e2e_val = statistics.mean(e2e_times) if e2e_times else None
+    if world > 1 and e2e_val is not None:
         t = torch.tensor([e2e_val], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_val = float(t.item())
@@ -314,33 +315,48 @@ def run_ours(args) -> dict | None:
 
 # ---------------------------------------------------------------- CPU reference
 
-def _reference_sample(rows: int, seed: int, min_e: int, max_e: int) -> dict:
-    """One bounded sample of the workload on the host cores with the
+class ReferenceSample:
+    """A bounded sample of the workload for the host cores, run with the
     reference's own code: its A_Indexer recipe over FastIndex/Flipped* for the
-    expanded layout, then its Math/ PCG retyped to FP64, run to 1e-8."""
-    import oracle
-    import cassandra_b200 as cb
+    expanded layout (oracle/ref/ref_driver.cpp) and its Math/ PCG retyped to
+    FP64 (oracle/ref/ref64_driver.cpp), to a relative normal-equation residual
+    of 1e-8.  Inputs (positions, targets) are prepared once, untimed."""
 
-    ref, ref64 = oracle.ref_lib(), oracle.ref64_lib()
-    ref.ref_expanded_index.restype = None
-    ref.ref_expanded_index.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p]
-    pos = cb.generate_positions_host(seed, 0, rows, min_e, max_e)  # seeded input generation (not timed)
-    m = np.asarray(PATTERNS_8, np.uint64)
-    idx = np.empty((rows, 64), np.uint32)
-    t0 = time.perf_counter()
-    ref.ref_expanded_index(m.ctypes.data_as(C.c_void_p), len(m), pos.ctypes.data_as(C.c_void_p), rows,
-                           idx.ctypes.data_as(C.c_void_p))
-    t_index = time.perf_counter() - t0
-    cols = int(sum(3 ** bin(x).count("1") for x in PATTERNS_8))
-    rng = np.random.default_rng(seed)
-    wst = rng.normal(0, 0.5, cols)
-    b = np.clip(2 * np.rint((wst[idx].sum(axis=1) + rng.normal(0, 4, rows)) / 2), -64, 64)
-    x = np.empty(cols)
-    rel, sec = np.zeros(1), np.zeros(1)
-    it = ref64.ref64_pcg(64, rows, cols, idx.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p), 20000, 1e-8,
-                         10, x.ctypes.data_as(C.c_void_p), rel.ctypes.data_as(C.c_void_p),
-                         sec.ctypes.data_as(C.c_void_p))
-    return {"index_s": t_index, "solve_s": float(sec[0]), "iterations": int(it), "rel_residual": float(rel[0])}
+    def __init__(self, rows: int, seed: int, min_e: int, max_e: int):
+        import oracle
+        import cassandra_b200 as cb
+
+        self.ref, self.ref64 = oracle.ref_lib(), oracle.ref64_lib()
+        self.ref.ref_expanded_index.restype = None
+        self.ref.ref_expanded_index.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p]
+        self.rows = rows
+        self.masks = np.asarray(PATTERNS_8, np.uint64)
+        self.cols = int(sum(3 ** bin(x).count("1") for x in PATTERNS_8))
+        self.pos = cb.generate_positions_host(seed, 0, rows, min_e, max_e)  # same positions as the GPU arm
+        self.idx = np.empty((rows, 64), np.uint32)
+        self._index()
+        rng = np.random.default_rng(seed)
+        wst = rng.normal(0, 0.5, self.cols)
+        aw = np.empty(rows)
+        self.ref64.ref64_spmv(64, rows, self.cols, self.idx.ctypes.data_as(C.c_void_p),
+                              wst.ctypes.data_as(C.c_void_p), aw.ctypes.data_as(C.c_void_p))
+        self.b = np.clip(2 * np.rint((aw + rng.normal(0, 4, rows)) / 2), -64, 64)
+
+    def _index(self) -> float:
+        t0 = time.perf_counter()
+        self.ref.ref_expanded_index(self.masks.ctypes.data_as(C.c_void_p), len(self.masks),
+                                    self.pos.ctypes.data_as(C.c_void_p), self.rows,
+                                    self.idx.ctypes.data_as(C.c_void_p))
+        return time.perf_counter() - t0
+
+    def run(self) -> dict:
+        t_index = self._index()
+        x = np.empty(self.cols)
+        rel, sec = np.zeros(1), np.zeros(1)
+        it = self.ref64.ref64_pcg(64, self.rows, self.cols, self.idx.ctypes.data_as(C.c_void_p),
+                                  self.b.ctypes.data_as(C.c_void_p), 20000, 1e-8, 10, x.ctypes.data_as(C.c_void_p),
+                                  rel.ctypes.data_as(C.c_void_p), sec.ctypes.data_as(C.c_void_p))
+        return {"index_s": t_index, "solve_s": float(sec[0]), "iterations": int(it), "rel_residual": float(rel[0])}
 
 
 def cpu_baseline(args, seed: int, gpu_iterations: int | None = None) -> dict | None:
@@ -352,15 +368,16 @@ def cpu_baseline(args, seed: int, gpu_iterations: int | None = None) -> dict | N
                     "sample": "unavailable: oracle/_ref not built"}
     except Exception as e:  # pragma: no cover
         return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference", "sample": f"error {e}"}
-    n = args.cpu_sample_rows
-    s = _reference_sample(n, seed, args.min_empties, args.max_empties)
+    n = min(args.cpu_sample_rows, args.rows)
+    s = ReferenceSample(n, seed, args.min_empties, args.max_empties).run()
     scale = args.rows / n
     value = (s["index_s"] + s["solve_s"]) * scale
     return {"value": value, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
-            "sample": f"{n} of {args.rows} rows; reference A_Indexer recipe (FastIndex/Flipped*) + reference "
-                      f"Math/ PCG retyped to FP64 run to 1e-8 ({s['iterations']} iterations, rel {s['rel_residual']:.2e}"
-                      f", index {s['index_s']:.3f} s, solve {s['solve_s']:.2f} s), time scaled by rows x{scale:g}; "
-                      f"OMP threads = {os.environ.get('OMP_NUM_THREADS', os.cpu_count())}"}
+            "sample": f"{n} of {args.rows} rows (same generator and seed); reference A_Indexer recipe "
+                      f"(FastIndex/Flipped*) + reference Math/ PCG retyped to FP64, run to 1e-8 "
+                      f"({s['iterations']} iterations, rel {s['rel_residual']:.2e}, index {s['index_s']:.3f} s, "
+                      f"solve {s['solve_s']:.2f} s), time scaled by rows x{scale:g}; "
+                      f"OpenMP threads {os.environ.get('OMP_NUM_THREADS', os.cpu_count())}"}
 
 
 def run_reference(args) -> dict | None:
@@ -373,9 +390,10 @@ def run_reference(args) -> dict | None:
         return {"impl": "reference", "metric": METRIC,
                 "unavailable": "oracle/_ref (reference sources compiled here) is missing"}
     times, last = [], None
-    n = args.cpu_sample_rows
+    n = min(args.cpu_sample_rows, args.rows)
+    sample = ReferenceSample(n, args.seed, args.min_empties, args.max_empties)
     for i in range(args.warmup + args.steps):
-        s = _reference_sample(n, args.seed, args.min_empties, args.max_empties)
+        s = sample.run()
         if i >= args.warmup:
             times.append((s["index_s"] + s["solve_s"]) * args.rows / n)
             last = s

@@ -98,6 +98,9 @@ SIGNATURES: dict[str, tuple] = {
     "cas_csr_from_positions": (C.c_int, [_VP, _VP, _I64, _VP, _PP]),
     "cas_csr_from_positions_layout": (C.c_int, [_VP, _VP, _I64, C.c_int, _VP, _PP]),
     "cas_csr_layouts": (C.c_int, [_VP]),
+    "cas_block_rows": (_I64, []),
+    "cas_eval_forward": (C.c_int, [_VP, _I64, _I64, _VP, _VP, _VP]),
+    "cas_eval_backward": (C.c_int, [_VP, _I64, _I64, _VP, _VP, _VP]),
     "cas_csr_from_indices": (C.c_int, [_VP, C.c_int, _I64, _I64, _VP, _PP]),
     "cas_csr_destroy": (None, [_VP]),
     "cas_csr_rows": (_I64, [_VP]),

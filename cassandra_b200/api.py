@@ -154,12 +154,16 @@ class MatrixCSR:
     def indices(self) -> torch.Tensor:
         """Copy of the row-major column indices (int32 [rows, K])."""
         src = self._lib.cas_csr_indices(self._h)
+        if not src and self.rows() > 0:
+            raise ValueError("this CSR has no rows layout (built with layouts='blocked')")
         return _device_view(src, (self.rows(), self.nnz_per_row), "<i4").clone()
 
     def transposed(self) -> tuple[torch.Tensor, torch.Tensor]:
         """Copies of (col_ptr int64 [cols+1], row_idx int32 [nnz]) of the transposed copy."""
         cp, ri = C.c_void_p(), C.c_void_p()
         L.check(self._lib.cas_csr_transposed(self._h, C.byref(cp), C.byref(ri)))
+        if not cp.value:
+            raise ValueError("this CSR has no rows layout (built with layouts='blocked')")
         col_ptr = _device_view(cp.value, (self.cols() + 1,), "<i8").clone()
         row_idx = _device_view(ri.value, (self.rows() * self.nnz_per_row,), "<i4").clone()
         return col_ptr, row_idx

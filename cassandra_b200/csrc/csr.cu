@@ -575,6 +575,31 @@ CAS_API cas_status cas_csr_from_positions(const cas_patterns* p, const uint64_t*
 
 CAS_API int cas_csr_layouts(const cas_csr* a) { return a ? a->layouts : 0; }
 
+CAS_API int64_t cas_block_rows(void) { return kBlockRows; }
+
+CAS_API cas_status cas_eval_forward(const cas_csr* a, int64_t row0, int64_t row1, const float* d_w, float* d_score,
+                                    void* stream)
+{
+    CAS_REQUIRE(a && a->fast, CAS_ERR_INVALID_ARGUMENT, "cas_eval_forward: the CSR needs the blocked layout");
+    CAS_REQUIRE(0 <= row0 && row0 <= row1 && row1 <= a->rows, CAS_ERR_SIZE_MISMATCH,
+                "cas_eval_forward: row range outside the matrix");
+    CAS_REQUIRE(row1 == row0 || (d_w && d_score), CAS_ERR_INVALID_ARGUMENT, "cas_eval_forward: null buffer");
+    return fast_eval_forward(*a->fast, row0, row1, d_w, d_score, static_cast<cudaStream_t>(stream));
+}
+
+CAS_API cas_status cas_eval_backward(const cas_csr* a, int64_t row0, int64_t row1, const float* d_g, float* d_grad,
+                                     void* stream)
+{
+    CAS_REQUIRE(a && a->fast, CAS_ERR_INVALID_ARGUMENT, "cas_eval_backward: the CSR needs the blocked layout");
+    CAS_REQUIRE(0 <= row0 && row0 <= row1 && row1 <= a->rows, CAS_ERR_SIZE_MISMATCH,
+                "cas_eval_backward: row range outside the matrix");
+    CAS_REQUIRE(row0 % kBlockRows == 0 && (row1 % kBlockRows == 0 || row1 == a->rows), CAS_ERR_INVALID_ARGUMENT,
+                "cas_eval_backward: the row range must start and end on block boundaries (cas_block_rows())");
+    CAS_REQUIRE(d_grad && (row1 == row0 || d_g), CAS_ERR_INVALID_ARGUMENT, "cas_eval_backward: null buffer");
+    const int64_t b0 = row0 / kBlockRows, b1 = (row1 + kBlockRows - 1) / kBlockRows;
+    return fast_eval_backward(*a->fast, b0, b1, d_g, d_grad, static_cast<cudaStream_t>(stream));
+}
+
 CAS_API cas_status cas_csr_from_indices(const uint32_t* d_indices, int nnz_per_row, int64_t rows, int64_t cols,
                                         void* stream, cas_csr** out)
 {

@@ -27,7 +27,7 @@ namespace {
 
 constexpr int kSortThreads = 1024;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kItemsPerThread = 8;  // A'y entries per thread and round
+constexpr int kItemsPerThread = 16;  // A'y entries per thread and round (a multiple of 8)
 
 unsigned fgrid(int64_t work, int per)
 {
@@ -351,65 +351,73 @@ struct SegSmem {
 };
 
 // Segmented reduction of one round of column-sorted entries into acc.
-// Each thread owns kItemsPerThread consecutive entries [e_first, e_first+8)
-// of [e_lo, e_hi); runs of equal columns are summed and added to acc[col]
-// exactly once, in an order fixed by the data, so the result is bitwise
-// reproducible.  `carry` holds the open run carried in from the previous
-// round (its column is the column of entry round_start - 1).
+// Each thread owns kItemsPerThread consecutive entries of [e_lo, e_hi); runs
+// of equal columns are summed and added to acc[col] exactly once, in an
+// order fixed by the data, so the result is bitwise reproducible:
+//   1. each thread sums its runs; runs wholly inside the thread are added to
+//      acc directly (no other thread touches that column in this tile);
+//   2. the partial runs at thread boundaries are combined by a segmented
+//      scan: shuffles inside each warp, then warp 0 scans the 32 warp
+//      aggregates; the chain entering the round (an open run of the previous
+//      round) is ss.carry;
+//   3. the thread where a boundary run ends adds the combined sum.
+// round_start is a multiple of 4 entries, so every thread reads its
+// entries with 16-byte loads.
 template <typename T>
 __device__ void seg_round(const uint32_t* __restrict__ g32, int64_t round_start, int64_t e_lo, int64_t e_hi,
                           uint32_t c0, const T* __restrict__ ytile, T* __restrict__ acc, SegSmem<T>& ss)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t e_first = round_start + static_cast<int64_t>(threadIdx.x) * kItemsPerThread;
-    uint32_t ent[kItemsPerThread];
-    // round_start is a multiple of 4 entries: two aligned 16-byte loads
-    if (e_first + kItemsPerThread <= e_hi && e_first >= e_lo) {
-        const uint4 u0 = *reinterpret_cast<const uint4*>(g32 + e_first);
-        const uint4 u1 = *reinterpret_cast<const uint4*>(g32 + e_first + 4);
-        ent[0] = u0.x, ent[1] = u0.y, ent[2] = u0.z, ent[3] = u0.w;
-        ent[4] = u1.x, ent[5] = u1.y, ent[6] = u1.z, ent[7] = u1.w;
-    } else {
-#pragma unroll
-        for (int i = 0; i < kItemsPerThread; i++) {
-            const int64_t e = e_first + i;
-            ent[i] = (e >= e_lo && e < e_hi) ? g32[e] : 0xFFFFFFFFu;
-        }
-    }
-    // local pass
     int hc = -1, tc = -1;
     T hs = 0, sum = 0;
     bool single = true, any = false;
 #pragma unroll
-    for (int i = 0; i < kItemsPerThread; i++) {
-        const int64_t e = e_first + i;
-        if (e < e_lo || e >= e_hi) continue;
-        const int col = static_cast<int>((ent[i] >> 16) - c0);
-        const T v = ytile[ent[i] & 0xFFFFu];
-        if (!any) {
-            any = true;
-            hc = tc = col;
-            sum = v;
-        } else if (col == tc) {
-            sum += v;
+    for (int half = 0; half < kItemsPerThread / 8; half++) {
+        const int64_t e8 = e_first + half * 8;
+        uint32_t ent[8];
+        if (e8 + 8 <= e_hi && e8 >= e_lo) {
+            const uint4 u0 = *reinterpret_cast<const uint4*>(g32 + e8);
+            const uint4 u1 = *reinterpret_cast<const uint4*>(g32 + e8 + 4);
+            ent[0] = u0.x, ent[1] = u0.y, ent[2] = u0.z, ent[3] = u0.w;
+            ent[4] = u1.x, ent[5] = u1.y, ent[6] = u1.z, ent[7] = u1.w;
         } else {
-            if (single) {
-                hs = sum;  // head run closes
-                single = false;
-            } else {
-                acc[tc] += sum;  // interior run: only this thread touches tc
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int64_t e = e8 + i;
+                ent[i] = (e >= e_lo && e < e_hi) ? g32[e] : 0xFFFFFFFFu;
             }
-            tc = col;
-            sum = v;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int64_t e = e8 + i;
+            if (e < e_lo || e >= e_hi) continue;
+            const int col = static_cast<int>((ent[i] >> 16) - c0);
+            const T v = ytile[ent[i] & 0xFFFFu];
+            if (!any) {
+                any = true;
+                hc = tc = col;
+                sum = v;
+            } else if (col == tc) {
+                sum += v;
+            } else {
+                if (single) {
+                    hs = sum;  // the head run closes inside this thread
+                    single = false;
+                } else {
+                    acc[tc] += sum;  // interior run: only this thread touches tc
+                }
+                tc = col;
+                sum = v;
+            }
         }
     }
     const T ts = sum;
     if (single) hs = sum;
     // neighbours: does my head continue the previous entry's run, does my
     // tail continue into the next entry?
-    int64_t first_valid = e_first < e_lo ? e_lo : e_first;
-    int64_t last_valid = e_first + kItemsPerThread - 1;
-    if (last_valid >= e_hi) last_valid = e_hi - 1;
+    const int64_t first_valid = e_first < e_lo ? e_lo : e_first;
+    const int64_t last_valid = min(e_first + kItemsPerThread - 1, e_hi - 1);
     bool cont_prev = false, cont_next = false;
     if (any) {
         if (first_valid - 1 >= e_lo) cont_prev = static_cast<int>((g32[first_valid - 1] >> 16) - c0) == hc;
@@ -433,13 +441,26 @@ __device__ void seg_round(const uint32_t* __restrict__ g32, int64_t round_start,
         ss.warp_f[warp] = f;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        T excl = ss.carry;  // chain value entering warp 0 (open run of the previous round)
-        for (int w = 0; w < kFastThreads / 32; w++) {
-            ss.warp_excl[w] = excl;
-            excl = ss.warp_f[w] ? ss.warp_v[w] : excl + ss.warp_v[w];
+    if (warp == 0) {
+        // same scan over the warp aggregates, seeded with the round's carry
+        constexpr int kWarps = kFastThreads / 32;
+        T wv = lane < kWarps ? ss.warp_v[lane] : T(0);
+        bool wf = lane < kWarps ? ss.warp_f[lane] != 0 : true;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const T vu = __shfl_up_sync(0xffffffffu, wv, d);
+            const bool fu = __shfl_up_sync(0xffffffffu, wf, d);
+            if (lane >= d) {
+                if (!wf) wv += vu;
+                wf = wf || fu;
+            }
         }
-        ss.carry = excl;  // open chain leaving the round (used only if the run continues)
+        const T carry = ss.carry;
+        const T incl = wf ? wv : wv + carry;  // chain value at the end of warp `lane`
+        T excl = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) excl = carry;
+        if (lane < kWarps) ss.warp_excl[lane] = excl;
+        if (lane == kWarps - 1) ss.carry = incl;  // open chain leaving the round
     }
     __syncthreads();
     const T excl_w = ss.warp_excl[warp];
@@ -463,7 +484,8 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
                                                                        const uint32_t* __restrict__ chunk_start,
                                                                        const T* __restrict__ y,
                                                                        T* __restrict__ partial,
-                                                                       const int* __restrict__ done)
+                                                                       const int* __restrict__ done, int item_base,
+                                                                       int64_t y_block0)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ SegSmem<T> ss;
@@ -471,7 +493,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
     const int width_max = kChunkCols * tv.per_sc;
     T* acc = reinterpret_cast<T*>(smem_raw);
     T* ytile = acc + width_max;
-    const int item = blockIdx.x;
+    const int item = blockIdx.x + item_base;
     const int sc = tv.item_sc[item];
     int p = 0;
     while (p + 1 < g.npat && tv.sc_base[p + 1] <= sc) p++;
@@ -485,7 +507,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
     for (int64_t blk = tv.item_b0[item]; blk < tv.item_b1[item]; blk++) {
         const int nb = static_cast<int>(g.block_rows(blk));
         __syncthreads();
-        const T* yb = y + blk * kBlockRows;
+        const T* yb = y + (blk - y_block0) * kBlockRows;
         for (int i = threadIdx.x; i < nb; i += kFastThreads) ytile[i] = yb[i];
         if (threadIdx.x == 0) ss.carry = 0;
         __syncthreads();
@@ -496,8 +518,38 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
             seg_round<T>(g32, rs, e_lo, e_hi, c0, ytile, acc, ss);
     }
     __syncthreads();
-    T* out = partial + tv.item_part[item];
+    T* out = partial + (tv.item_part[item] - tv.item_part[item_base]);
     for (int i = threadIdx.x; i < width; i += kFastThreads) out[i] = acc[i];
+}
+
+// Evaluator forward on a row range: score[r - row0] = sum_j w[col_rj], one
+// thread per row, 16-byte index loads, gathers of w through L1/L2 (the range
+// is a minibatch, too short to amortise staging w in shared memory).
+__global__ void __launch_bounds__(256) fast_rows_forward_kernel(FastGeometry g, const uint16_t* __restrict__ a16,
+                                                                const float* __restrict__ w, int64_t row0,
+                                                                int64_t row1, float* __restrict__ out)
+{
+    for (int64_t r = row0 + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < row1;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = r / kBlockRows, rb = r - b * kBlockRows;
+        float acc = 0;
+        for (int p = 0; p < g.npat; p++)
+            gather_row<float>(a16 + g.seg(b, p) + rb * g.slots[p], g.slots[p], w + g.off[p], w + g.off[p], 0, false,
+                              acc);
+        out[r - row0] = acc;
+    }
+}
+
+// Dense column sums of per-block partials laid out [block][cols].
+__global__ void block_partial_sum_kernel(const float* __restrict__ partial, int nb, int64_t cols,
+                                         float* __restrict__ out)
+{
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cols;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        float acc = 0;
+        for (int j = 0; j < nb; j++) acc += partial[static_cast<int64_t>(j) * cols + c];
+        out[c] = acc;
+    }
 }
 
 template <typename T>
@@ -571,6 +623,40 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
     CAS_CUDA(cudaMemcpy(t.item_b1, item_b1.data(), sizeof(int) * t.nitems, cudaMemcpyHostToDevice));
     CAS_CUDA(cudaMemcpy(t.item_part, item_part.data(), sizeof(int64_t) * t.nitems, cudaMemcpyHostToDevice));
     CAS_CUDA(cudaMemcpy(t.sc_item0, sc_item0.data(), sizeof(int) * (nsc + 1), cudaMemcpyHostToDevice));
+    return CAS_OK;
+}
+
+// Work list of one item per (block, chunk), block-major, for adjoints over a
+// block range (minibatches): item b * nchunks + ch; partial offsets give the
+// layout [block][global column] relative to the first item of the range.
+cas_status build_block_items(const FastGeometry& g, FastTranspose& t)
+{
+    t.per_sc = 1;
+    for (int p = 0; p < g.npat; p++) t.sc_base[p] = g.chunk0[p];
+    t.sc_base[g.npat] = g.nchunks;
+    t.nsc = g.nchunks;
+    const int64_t n = g.nblocks * g.nchunks;
+    t.nitems = static_cast<int>(n);
+    std::vector<int> isc(n), ib0(n), ib1(n);
+    std::vector<int64_t> ipart(n);
+    for (int64_t b = 0; b < g.nblocks; b++)
+        for (int ch = 0; ch < g.nchunks; ch++) {
+            int p = 0;
+            while (p + 1 < g.npat && g.chunk0[p + 1] <= ch) p++;
+            const int64_t i = b * g.nchunks + ch;
+            isc[i] = ch;
+            ib0[i] = static_cast<int>(b);
+            ib1[i] = static_cast<int>(b + 1);
+            ipart[i] = b * g.cols + g.off[p] + static_cast<int64_t>(ch - g.chunk0[p]) * kChunkCols;
+        }
+    CAS_CUDA(cudaMalloc(&t.item_sc, sizeof(int) * n));
+    CAS_CUDA(cudaMalloc(&t.item_b0, sizeof(int) * n));
+    CAS_CUDA(cudaMalloc(&t.item_b1, sizeof(int) * n));
+    CAS_CUDA(cudaMalloc(&t.item_part, sizeof(int64_t) * n));
+    CAS_CUDA(cudaMemcpy(t.item_sc, isc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CAS_CUDA(cudaMemcpy(t.item_b0, ib0.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CAS_CUDA(cudaMemcpy(t.item_b1, ib1.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CAS_CUDA(cudaMemcpy(t.item_part, ipart.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
     return CAS_OK;
 }
 
@@ -650,6 +736,8 @@ void fast_free(FastLayout& f)
     cudaFree(f.chunk_start);
     free_transpose(f.t32);
     free_transpose(f.t64);
+    free_transpose(f.tb);
+    cudaFree(f.eval_partial);
     f = FastLayout{};
 }
 
@@ -720,6 +808,7 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
     if (g.nblocks > 0) {
         CAS_TRY(build_items(g, entries, 4, sizeof(float), f.t32));
         CAS_TRY(build_items(g, entries, 1, sizeof(double), f.t64));
+        CAS_TRY(build_block_items(g, f.tb));
     }
     return fast_set_attributes();
 }
@@ -758,7 +847,7 @@ cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag,
     if (t.nitems == 0) return CAS_OK;
     const size_t smem = spmv_t_smem<T>(t);
     { fast_spmv_t_kernel<T><<<t.nitems, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.chunk_start, y,
-                                                                static_cast<T*>(t.partial), done_flag); cas::count_launch(); }
+                                                                static_cast<T*>(t.partial), done_flag, 0, 0); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     return CAS_OK;
 }
@@ -787,6 +876,44 @@ cas_status fast_spmv_t(const FastLayout& f, const T* y, T* x, cudaStream_t s)
         return CAS_OK;
     }
     { fast_col_sum_kernel<T><<<fgrid(f.g.cols, 256), 256, 0, s>>>(fast_cols<T>(f), static_cast<const T*>(t.partial), x); cas::count_launch(); }
+    CAS_CHECK_LAUNCH();
+    return CAS_OK;
+}
+
+cas_status fast_eval_forward(const FastLayout& f, int64_t row0, int64_t row1, const float* w, float* score,
+                             cudaStream_t s)
+{
+    if (row1 <= row0) return CAS_OK;
+    { fast_rows_forward_kernel<<<fgrid(row1 - row0, 256) * 4, 256, 0, s>>>(f.g, f.a16, w, row0, row1, score); cas::count_launch(); }
+    CAS_CHECK_LAUNCH();
+    return CAS_OK;
+}
+
+cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float* g, float* grad, cudaStream_t s)
+{
+    const int64_t nb = b1 - b0;
+    if (f.g.cols == 0) return CAS_OK;
+    if (nb <= 0) {
+        CAS_CUDA(cudaMemsetAsync(grad, 0, sizeof(float) * f.g.cols, s));
+        return CAS_OK;
+    }
+    if (nb > f.eval_blocks) {
+        if (f.eval_partial) {
+            CAS_CUDA(cudaStreamSynchronize(s));
+            cudaFree(f.eval_partial);
+            f.eval_partial = nullptr;
+        }
+        CAS_CUDA(cudaMalloc(&f.eval_partial, sizeof(float) * nb * f.g.cols));
+        f.eval_blocks = nb;
+    }
+    const size_t smem = sizeof(float) * (static_cast<size_t>(kChunkCols) + kBlockRows);
+    const int items = static_cast<int>(nb * f.g.nchunks);
+    { fast_spmv_t_kernel<float><<<items, kFastThreads, smem, s>>>(f.g, tview(f.tb), f.g32, f.chunk_start, g,
+                                                                 f.eval_partial, nullptr,
+                                                                 static_cast<int>(b0 * f.g.nchunks), b0); cas::count_launch(); }
+    CAS_CHECK_LAUNCH();
+    { block_partial_sum_kernel<<<fgrid(f.g.cols, 256), 256, 0, s>>>(f.eval_partial, static_cast<int>(nb), f.g.cols,
+                                                                  grad); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     return CAS_OK;
 }

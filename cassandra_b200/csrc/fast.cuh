@@ -82,7 +82,10 @@ struct FastLayout {
     uint16_t* a16 = nullptr;
     uint32_t* g32 = nullptr;
     uint32_t* chunk_start = nullptr;   // [nblocks][nchunks] absolute index in G32
-    FastTranspose t32, t64;
+    FastTranspose t32, t64;            // A'y work lists of the solvers (FP32, FP64)
+    FastTranspose tb;                  // one item per (block, chunk): adjoints over block ranges
+    float* eval_partial = nullptr;     // [blocks][cols] partials of the last adjoint
+    int64_t eval_blocks = 0;
 };
 
 // Device view used by the column reductions of the solver.
@@ -134,6 +137,13 @@ __device__ __forceinline__ double fast_col_sum(const FastCols& fc, const T* part
 
 // Jacobi diagonal from G32 (integer, deterministic).
 cas_status fast_diag(const FastLayout& f, uint64_t* diag, cudaStream_t s);
+
+// Evaluator forward over rows [row0, row1) (FP32 scores) and its adjoint
+// grad = A' g over the rows of blocks [b0, b1) (deterministic; grad has cols
+// entries and is overwritten).
+cas_status fast_eval_forward(const FastLayout& f, int64_t row0, int64_t row1, const float* w, float* score,
+                             cudaStream_t s);
+cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float* g, float* grad, cudaStream_t s);
 
 // Full A'y into a dense vector (standalone product).
 template <typename T>

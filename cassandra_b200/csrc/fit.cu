@@ -34,18 +34,17 @@ __global__ void true_weights_kernel(uint64_t seed, int64_t cols, double sigma, d
     }
 }
 
-// b_r = clamp(2 rint((A w*)_r + e_r) / 2), -64, 64), e_r ~ N(0, noise^2).
-__global__ void targets_kernel(const uint32_t* __restrict__ idx, int64_t rows, int k, const double* __restrict__ w,
-                               uint64_t seed, double noise, double* __restrict__ b)
+// b_r = clamp(2 rint(((A w*)_r + e_r) / 2), -64, 64), e_r ~ N(0, noise^2);
+// aw holds (A w*)_r, computed on whichever layout the CSR has.
+__global__ void targets_kernel(const double* __restrict__ aw, int64_t rows, uint64_t seed, double noise,
+                               double* __restrict__ b)
 {
     for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < rows;
          r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        double acc = 0;
-        for (int j = 0; j < k; j++) acc += w[idx[r * k + j]];
         Stream rng(seed ^ 0xB0A5EDD15EA5EULL, static_cast<uint64_t>(r));
         const double u1 = rng.unit(), u2 = rng.unit();
         const double e = noise * sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
-        b[r] = fmin(64.0, fmax(-64.0, 2.0 * rint((acc + e) * 0.5)));
+        b[r] = fmin(64.0, fmax(-64.0, 2.0 * rint((aw[r] + e) * 0.5)));
     }
 }
 
@@ -129,7 +128,9 @@ CAS_API cas_status cas_generate_targets(const cas_csr* a, uint64_t seed, double 
     { true_weights_kernel<<<grid(a->cols), 256, 0, s>>>(seed, a->cols, w_sigma, w); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     if (a->rows) {
-        { targets_kernel<<<grid(a->rows), 256, 0, s>>>(a->idx, a->rows, a->k, w, seed, noise_sigma, d_b); cas::count_launch(); }
+        // A w* into d_b first (FP64 product on the CSR's layout), then noise and rounding in place
+        CAS_TRY(cas_spmv(a, CAS_F64, w, d_b, stream));
+        { targets_kernel<<<grid(a->rows), 256, 0, s>>>(d_b, a->rows, seed, noise_sigma, d_b); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
     }
     if (!d_w_true) cudaFreeAsync(w, s);

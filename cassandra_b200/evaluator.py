@@ -1,0 +1,136 @@
+"""Differentiable pattern evaluator: score = A w with a hand-written adjoint.
+
+The reference scores a position as the sum of its pattern weights
+(ScoreEstimator::Eval, Pattern/Evaluator.cpp:48-54), which over a batch of
+positions is the sparse product A w of the fitting path.  ``EvaluatorFunction``
+wraps the device kernels as a ``torch.autograd.Function``:
+
+* forward  ``cas_eval_forward``: score = A w over a row range (FP32);
+* backward ``cas_eval_backward``: dL/dw = A' dL/dscore on the per-block
+  column-sorted copy of A (deterministic, no atomics).
+
+Minibatches are whole 16384-row blocks (``cas_block_rows``): batch membership
+is fixed and the batch order is shuffled per epoch, so every batch's
+transposed copy exists before training starts.  This is the Python side where
+the reference's NeuralNetwork/ code trains value models.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import torch
+
+from . import _lib as L
+from .api import GroupIndexer, MatrixCSR, _ptr, _stream
+
+
+def block_rows() -> int:
+    return int(L.load().cas_block_rows())
+
+
+class EvaluatorFunction(torch.autograd.Function):
+    """score = A[row0:row1] w  (A implicit 0/1, FP32)."""
+
+    @staticmethod
+    def forward(ctx, w: torch.Tensor, csr: MatrixCSR, row0: int, row1: int) -> torch.Tensor:
+        if w.dtype != torch.float32 or not w.is_cuda or not w.is_contiguous():
+            raise TypeError("weights must be a contiguous CUDA float32 tensor")
+        if w.numel() != csr.cols():
+            raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+        score = torch.empty(row1 - row0, dtype=torch.float32, device=w.device)
+        L.check(L.load().cas_eval_forward(csr.handle, row0, row1, _ptr(w), _ptr(score), _stream()))
+        ctx.csr, ctx.row0, ctx.row1 = csr, row0, row1
+        return score
+
+    @staticmethod
+    def backward(ctx, g: torch.Tensor):
+        g = g.contiguous().to(torch.float32)
+        grad = torch.empty(ctx.csr.cols(), dtype=torch.float32, device=g.device)
+        L.check(L.load().cas_eval_backward(ctx.csr.handle, ctx.row0, ctx.row1, _ptr(g), _ptr(grad), _stream()))
+        return grad, None, None, None
+
+
+class PatternEvaluator(torch.nn.Module):
+    """Pattern weights over a fixed set of positions (the training set)."""
+
+    def __init__(self, masks, positions: torch.Tensor, mode: str = "expanded", weights: torch.Tensor | None = None):
+        super().__init__()
+        self.indexer = GroupIndexer(masks, mode)
+        self.csr = MatrixCSR.from_positions(self.indexer, positions, "blocked")
+        cols = self.indexer.index_space_size
+        w = torch.zeros(cols, dtype=torch.float32, device=positions.device) if weights is None else weights
+        self.weight = torch.nn.Parameter(w.to(torch.float32).contiguous())
+
+    @property
+    def rows(self) -> int:
+        return self.csr.rows()
+
+    def forward(self, row0: int = 0, row1: int | None = None) -> torch.Tensor:
+        return EvaluatorFunction.apply(self.weight, self.csr, row0, self.rows if row1 is None else row1)
+
+    def batches(self, batch: int) -> list[tuple[int, int]]:
+        """Fixed block-aligned minibatches of about `batch` rows."""
+        br = block_rows()
+        per = max(1, batch // br) * br
+        return [(r, min(r + per, self.rows)) for r in range(0, self.rows, per)]
+
+
+def objective(score: torch.Tensor, target: torch.Tensor, w: torch.Tensor, delta: float, l2: float) -> torch.Tensor:
+    """Mean Huber loss (delta) plus l2 * ||w||^2."""
+    return torch.nn.functional.huber_loss(score, target, delta=delta) + l2 * torch.dot(w, w)
+
+
+def train(model: PatternEvaluator, target: torch.Tensor, epochs: int = 5, batch: int = 65536, lr: float = 1e-2,
+          l2: float = 1e-4, delta: float = 4.0, seed: int = 0) -> list[float]:
+    """Adam on the Huber + L2 objective over fixed minibatches whose order is
+    shuffled every epoch.  Returns the mean batch loss of every epoch."""
+    target = target.to(torch.float32)
+    opt = torch.optim.Adam(model.parameters(), lr=lr)
+    gen = torch.Generator().manual_seed(seed)
+    batches = model.batches(batch)
+    history = []
+    for _ in range(epochs):
+        order = torch.randperm(len(batches), generator=gen).tolist()
+        total = 0.0
+        for i in order:
+            r0, r1 = batches[i]
+            opt.zero_grad(set_to_none=True)
+            loss = objective(model(r0, r1), target[r0:r1], model.weight, delta, l2)
+            loss.backward()
+            opt.step()
+            total += float(loss.detach())
+        history.append(total / len(batches))
+    return history
+
+
+def full_objective(model: PatternEvaluator, target: torch.Tensor, w: torch.Tensor | None = None,
+                   delta: float = 4.0, l2: float = 1e-4) -> float:
+    """The objective over all rows for weights w (default: the model's)."""
+    w = model.weight.detach() if w is None else w.to(torch.float32).contiguous()
+    with torch.no_grad():
+        s = EvaluatorFunction.apply(w, model.csr, 0, model.rows)
+        return float(objective(s, target.to(torch.float32), w, delta, l2))
+
+
+def central_difference(model: PatternEvaluator, target: torch.Tensor, coords: torch.Tensor, row0: int, row1: int,
+                       h: float = 0.25) -> torch.Tensor:
+    """Central finite differences of L(w) = 0.5 ||A w - t||^2 over [row0, row1)
+    (evaluated in FP64 from the FP32 scores) at the given coordinates."""
+    w = model.weight.detach().clone()
+    t = target[row0:row1].to(torch.float64)
+    out = torch.empty(len(coords), dtype=torch.float64)
+    for j, c in enumerate(coords.tolist()):
+        vals = []
+        for sgn in (1.0, -1.0):
+            wp = w.clone()
+            wp[c] += sgn * h
+            s = EvaluatorFunction.apply(wp, model.csr, row0, row1).to(torch.float64)
+            vals.append(0.5 * float(torch.sum((s - t) ** 2)))
+        out[j] = (vals[0] - vals[1]) / (2 * h)
+    return out
+
+
+__all__ = ["EvaluatorFunction", "PatternEvaluator", "train", "objective", "full_objective", "central_difference",
+           "block_rows"]
+_ = math

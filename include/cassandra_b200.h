@@ -156,6 +156,25 @@ CAS_API cas_status cas_spmv_t(const cas_csr* a, cas_dtype dtype, const void* d_y
 CAS_API cas_status cas_jacobi(const cas_csr* a, cas_dtype dtype, void* d_out, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Differentiable evaluator: score = A w and its adjoint                     */
+/* ------------------------------------------------------------------------ */
+
+/* Rows per block of the BLOCKED layout (16384); minibatches of the evaluator
+ * are whole blocks. */
+CAS_API int64_t cas_block_rows(void);
+/* Forward of the pattern evaluator on rows [row0, row1): score[i] = sum of
+ * w over the row's columns, FP32 (ScoreEstimator::Eval of every position,
+ * Pattern/Evaluator.cpp:48-54, for the CSR's index mode).  Needs BLOCKED. */
+CAS_API cas_status cas_eval_forward(const cas_csr* a, int64_t row0, int64_t row1, const float* d_w, float* d_score,
+                                    void* stream);
+/* Adjoint: grad = A_rows' g for the rows [row0, row1) (block boundaries; row1
+ * may be the last row); g has row1 - row0 entries, grad cols entries
+ * (overwritten).  Computed on the per-block column-sorted copy:
+ * deterministic, no atomics.  Needs BLOCKED. */
+CAS_API cas_status cas_eval_backward(const cas_csr* a, int64_t row0, int64_t row1, const float* d_g, float* d_grad,
+                                     void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Solvers: PCG, LSQR, CG (Math/Solver.h)                                    */
 /* ------------------------------------------------------------------------ */
 

@@ -90,6 +90,96 @@ inline Vector to_host_f32(const DeviceBuffer<double>& b, size_t n)
 }
 }  // namespace detail
 
+// Vector algebra of Math/Vector.h:7-31 on host vectors (the solvers keep
+// their own vectors on the device; these serve callers' host-side code).
+namespace vector_ops {
+inline void same_size(const Vector& a, const Vector& b)
+{
+    if (a.size() != b.size()) throw std::runtime_error("Size mismatch");
+}
+}  // namespace vector_ops
+inline void operator+=(Vector& l, const Vector& o)
+{
+    vector_ops::same_size(l, o);
+    for (size_t i = 0; i < l.size(); i++) l[i] += o[i];
+}
+inline void operator-=(Vector& l, const Vector& o)
+{
+    vector_ops::same_size(l, o);
+    for (size_t i = 0; i < l.size(); i++) l[i] -= o[i];
+}
+inline void operator*=(Vector& l, float f)
+{
+    for (float& v : l) v *= f;
+}
+inline void operator/=(Vector& l, float f)
+{
+    for (float& v : l) v /= f;
+}
+inline Vector operator+(Vector l, const Vector& r)
+{
+    l += r;
+    return l;
+}
+inline Vector operator-(Vector l, const Vector& r)
+{
+    l -= r;
+    return l;
+}
+inline Vector operator*(Vector v, float f)
+{
+    v *= f;
+    return v;
+}
+inline Vector operator*(float f, Vector v)
+{
+    v *= f;
+    return v;
+}
+inline Vector operator/(Vector v, float f)
+{
+    v /= f;
+    return v;
+}
+inline Vector elementwise_multiplication(Vector l, const Vector& o)
+{
+    vector_ops::same_size(l, o);
+    for (size_t i = 0; i < l.size(); i++) l[i] *= o[i];
+    return l;
+}
+inline Vector elementwise_division(Vector l, const Vector& o)
+{
+    vector_ops::same_size(l, o);
+    for (size_t i = 0; i < l.size(); i++) l[i] /= o[i];
+    return l;
+}
+inline Vector inv(Vector v)
+{
+    for (float& x : v) x = 1.0f / x;
+    return v;
+}
+inline float dot(const Vector& l, const Vector& r)
+{
+    vector_ops::same_size(l, r);
+    double s = 0;
+    for (size_t i = 0; i < l.size(); i++) s += double(l[i]) * r[i];
+    return static_cast<float>(s);
+}
+inline float norm(const Vector& x) { return std::sqrt(dot(x, x)); }
+inline float L2_norm(const Vector& x) { return norm(x); }
+inline float L1_norm(const Vector& x)
+{
+    double s = 0;
+    for (float v : x) s += std::fabs(v);
+    return static_cast<float>(s);
+}
+inline float sum(const Vector& x)
+{
+    double s = 0;
+    for (float v : x) s += v;
+    return static_cast<float>(s);
+}
+
 // Compressed sparse row matrix with a fixed number of entries per row and
 // implicit 1.0 values; duplicate column indices in a row add up.
 class MatrixCSR {

@@ -1,0 +1,108 @@
+"""The differentiable evaluator: forward A w and the hand-written adjoint
+A' g behind torch.autograd.Function, against the oracle, the compiled
+reference's x * A, central finite differences, and a short training run."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import cassandra_b200 as cb
+from cassandra_b200 import evaluator as ev
+from tests.golden.make_golden import SET8
+
+pytestmark = pytest.mark.gpu
+
+BR = 16384
+
+
+@pytest.fixture(scope="module")
+def setup(orc):
+    rows = 3 * BR + 1234  # three full blocks and a partial one
+    pos = cb.generate_positions(44, rows, 10, 50)
+    model = ev.PatternEvaluator(SET8, pos, "expanded")
+    idx = orc.group_index(SET8, 1, pos.cpu().numpy().view(np.uint64))
+    rng = np.random.default_rng(44)
+    w = rng.normal(0, 0.5, model.weight.numel()).astype(np.float32)
+    with torch.no_grad():
+        model.weight.copy_(torch.from_numpy(w))
+    target = torch.from_numpy(np.clip(2 * np.rint(orc.spmv(idx, len(w), w.astype(np.float64)) / 2), -64, 64)
+                              .astype(np.float32)).cuda()
+    return model, idx, w, target
+
+
+def test_block_rows():
+    assert ev.block_rows() == BR
+
+
+@pytest.mark.parametrize("r0,r1", [(0, BR), (BR, 3 * BR), (3 * BR, 3 * BR + 1234), (0, 3 * BR + 1234), (5, 77)])
+def test_forward_matches_oracle(cuda, orc, setup, r0, r1):
+    model, idx, w, _ = setup
+    got = model(r0, r1).detach().cpu().numpy().astype(np.float64)
+    want = orc.spmv(idx[r0:r1], len(w), w.astype(np.float64))
+    assert np.abs(got - want).max() <= 64 * 2 ** -23 * max(1.0, np.abs(want).max())
+
+
+@pytest.mark.parametrize("r0,r1", [(0, BR), (BR, 3 * BR), (3 * BR, 3 * BR + 1234), (0, 3 * BR + 1234)])
+def test_adjoint_matches_oracle_and_reference(cuda, orc, setup, r0, r1):
+    model, idx, w, _ = setup
+    g = torch.randn(r1 - r0, dtype=torch.float32, device="cuda")
+    s = model(r0, r1)
+    (grad,) = torch.autograd.grad(s, model.weight, g)
+    gh = g.cpu().numpy()
+    want = orc.spmv_t(idx[r0:r1], len(w), gh.astype(np.float64))
+    scale = np.abs(want).max()
+    np.testing.assert_allclose(grad.cpu().numpy(), want, rtol=0, atol=1e-5 * scale)
+    import oracle
+
+    if oracle.ref_available():
+        sub = np.ascontiguousarray(idx[r0:r1])
+        ref = np.empty(len(w), np.float32)
+        oracle.ref_lib().ref_spmv_t(sub.shape[1], sub.shape[0], len(w), sub.ctypes.data_as(C.c_void_p),
+                                    gh.ctypes.data_as(C.c_void_p), ref.ctypes.data_as(C.c_void_p))
+        np.testing.assert_allclose(grad.cpu().numpy(), ref, rtol=0, atol=2e-5 * scale)
+    # deterministic: the same bits twice
+    (grad2,) = torch.autograd.grad(model(r0, r1), model.weight, g)
+    assert grad.cpu().numpy().tobytes() == grad2.cpu().numpy().tobytes()
+
+
+def test_adjoint_rejects_unaligned_ranges(cuda, setup):
+    model, _, _, _ = setup
+    s = model(5, BR)
+    with pytest.raises(cb.CasError):
+        s.sum().backward()
+
+
+def test_gradient_matches_central_differences(cuda, setup):
+    model, idx, w, target = setup
+    r0, r1 = BR, 2 * BR
+    s = model(r0, r1)
+    loss = 0.5 * torch.sum((s.double() - target[r0:r1].double()) ** 2)
+    (grad,) = torch.autograd.grad(loss, model.weight)
+    rng = np.random.default_rng(1)
+    hit = np.unique(idx[r0:r1])
+    coords = np.concatenate([rng.choice(hit, 900, replace=False),
+                             rng.choice(np.setdiff1d(np.arange(len(w)), hit), 100, replace=False)])
+    fd = ev.central_difference(model, target, torch.from_numpy(coords), r0, r1).numpy()
+    got = grad.detach().cpu().numpy()[coords].astype(np.float64)
+    np.testing.assert_allclose(got, fd, rtol=1e-3, atol=1e-2)
+
+
+def test_training_reduces_loss_towards_least_squares(cuda, orc, setup):
+    rows = 6 * BR
+    pos = cb.generate_positions(45, rows, 10, 50)
+    model = ev.PatternEvaluator(SET8, pos, "expanded")
+    g = cb.GroupIndexer(SET8, "expanded")
+    a = cb.MatrixCSR.from_positions(g, pos, "rows")
+    b = cb.generate_targets(a, 45)
+    target = b.float()
+    before = ev.full_objective(model, target)
+    hist = ev.train(model, target, epochs=5, batch=2 * BR, lr=1e-2, l2=1e-4, delta=4.0, seed=0)
+    after = ev.full_objective(model, target)
+    assert hist[-1] < hist[0] and after < before
+    s = cb.PCG(a, b, tol=1e-8)
+    assert s.run()["converged"]
+    ls_obj = ev.full_objective(model, target, s.x().float())
+    # Adam on Huber+L2 for 5 epochs lands in the same range as the
+    # least-squares optimum evaluated on the same objective
+    assert after <= 3.0 * ls_obj + 1.0, (after, ls_obj)
