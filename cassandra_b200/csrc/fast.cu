@@ -271,13 +271,102 @@ __device__ __forceinline__ void gather_row(const uint16_t* __restrict__ src, int
     }
 }
 
-template <typename T, typename Y, int MODE>
-__global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_kernel(FastGeometry g, const uint16_t* __restrict__ a16,
-                                                                     const T* __restrict__ x, Y* __restrict__ y,
-                                                                     const double* __restrict__ b,
-                                                                     const double* __restrict__ coef,
-                                                                     double* __restrict__ part,
-                                                                     const int* __restrict__ done)
+// One index word (two 16-bit columns) of a row gathered into acc.
+template <typename T, bool ALL_IN>
+__device__ __forceinline__ void gather_word(uint32_t wd, const T* __restrict__ table, const T* __restrict__ xg,
+                                            int cap, typename AccOf<T>::type& acc)
+{
+    using Acc = typename AccOf<T>::type;
+    const int c0 = static_cast<int>(wd & 0xFFFFu), c1 = static_cast<int>(wd >> 16);
+    acc += static_cast<Acc>(ALL_IN || c0 < cap ? table[c0] : __ldg(xg + c0));
+    acc += static_cast<Acc>(ALL_IN || c1 < cap ? table[c1] : __ldg(xg + c1));
+}
+
+// Scalar stores of one 16-byte vector (the destination need not be aligned).
+__device__ __forceinline__ void store_vec(float* d, uint4 u)
+{
+    d[0] = __uint_as_float(u.x);
+    d[1] = __uint_as_float(u.y);
+    d[2] = __uint_as_float(u.z);
+    d[3] = __uint_as_float(u.w);
+}
+__device__ __forceinline__ void store_vec(double* d, uint4 u)
+{
+    d[0] = __hiloint2double(static_cast<int>(u.y), static_cast<int>(u.x));
+    d[1] = __hiloint2double(static_cast<int>(u.w), static_cast<int>(u.z));
+}
+
+// Copies a pattern's slice of x (cap entries) into shared memory with
+// 16-byte loads, several in flight per thread.
+template <typename T>
+__device__ __forceinline__ void load_table(T* __restrict__ table, const T* __restrict__ xg, int cap)
+{
+    constexpr int kPer = 16 / sizeof(T);
+    const int mis = static_cast<int>((reinterpret_cast<uintptr_t>(xg) & 15) / sizeof(T));
+    const int head = min(cap, mis ? kPer - mis : 0);
+    if (static_cast<int>(threadIdx.x) < head) table[threadIdx.x] = xg[threadIdx.x];
+    const int nvec = (cap - head) / kPer;
+    const uint4* src = reinterpret_cast<const uint4*>(xg + head);
+    T* dst = table + head;
+    for (int v0 = threadIdx.x; v0 < nvec; v0 += 4 * blockDim.x) {
+        uint4 u[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int v = v0 + k * blockDim.x;
+            if (v < nvec) u[k] = __ldg(src + v);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int v = v0 + k * blockDim.x;
+            if (v < nvec) store_vec(dst + v * kPer, u[k]);
+        }
+    }
+    const int done = head + nvec * kPer;
+    for (int i = done + threadIdx.x; i < cap; i += blockDim.x) table[i] = xg[i];
+}
+
+// Rows of one 8-slot pattern segment (the expanded layout): each thread owns
+// kAxRows rows (stride kAxThreads); the 16-byte index word of row j+kAxAhead
+// is loaded while row j is gathered, so kAxAhead loads per thread stay in
+// flight.
+template <typename T, bool ALL_IN>
+__device__ __forceinline__ void gather_segment8(const uint16_t* __restrict__ base, int nb,
+                                                const T* __restrict__ table, const T* __restrict__ xg, int cap,
+                                                typename AccOf<T>::type (&acc)[kAxRows])
+{
+    uint4 w[kAxAhead];
+#pragma unroll
+    for (int j = 0; j < kAxAhead; j++) {
+        const int r = threadIdx.x + j * kAxThreads;
+        w[j] = r < nb ? *reinterpret_cast<const uint4*>(base + static_cast<int64_t>(r) * 8) : make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int j = 0; j < kAxRows; j++) {
+        const uint4 cur = w[j % kAxAhead];
+        if (j + kAxAhead < kAxRows) {
+            const int rn = threadIdx.x + (j + kAxAhead) * kAxThreads;
+            w[j % kAxAhead] = rn < nb ? *reinterpret_cast<const uint4*>(base + static_cast<int64_t>(rn) * 8)
+                                      : make_uint4(0, 0, 0, 0);
+        }
+        const int r = threadIdx.x + j * kAxThreads;
+        if (r < nb) {
+            gather_word<T, ALL_IN>(cur.x, table, xg, cap, acc[j]);
+            gather_word<T, ALL_IN>(cur.y, table, xg, cap, acc[j]);
+            gather_word<T, ALL_IN>(cur.z, table, xg, cap, acc[j]);
+            gather_word<T, ALL_IN>(cur.w, table, xg, cap, acc[j]);
+        }
+    }
+}
+
+// ALL8: every pattern has 8 slots (the expanded layout), so only the
+// pipelined 8-slot path is compiled in.
+template <typename T, typename Y, int MODE, bool ALL8>
+__global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g, const uint16_t* __restrict__ a16,
+                                                                   const T* __restrict__ x, Y* __restrict__ y,
+                                                                   const double* __restrict__ b,
+                                                                   const double* __restrict__ coef,
+                                                                   double* __restrict__ part,
+                                                                   const int* __restrict__ done)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* table = reinterpret_cast<T*>(smem_raw);
@@ -289,27 +378,34 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_kernel(FastGeometry
     Comp mine;
     for (int64_t blk = blockIdx.x; blk < g.nblocks; blk += gridDim.x) {
         const int nb = static_cast<int>(g.block_rows(blk));
-        Acc acc[kRowsPerThread];
+        Acc acc[kAxRows];
 #pragma unroll
-        for (int j = 0; j < kRowsPerThread; j++) acc[j] = 0;
+        for (int j = 0; j < kAxRows; j++) acc[j] = 0;
         for (int p = 0; p < g.npat; p++) {
             const int cap = min(g.space[p], kCap);
             const T* xg = x + g.off[p];
             __syncthreads();
-            for (int i = threadIdx.x; i < cap; i += kFastThreads) table[i] = xg[i];
+            load_table<T>(table, xg, cap);
             __syncthreads();
-            const int ns = g.slots[p];
             const uint16_t* base = a16 + g.seg(blk, p);
             const bool all_in = g.space[p] <= kCap;
+            const int ns = g.slots[p];
+            if (ALL8 || ns == 8) {
+                if (all_in)
+                    gather_segment8<T, true>(base, nb, table, xg, cap, acc);
+                else
+                    gather_segment8<T, false>(base, nb, table, xg, cap, acc);
+            } else if (!ALL8) {
 #pragma unroll
-            for (int j = 0; j < kRowsPerThread; j++) {
-                const int r = threadIdx.x + j * kFastThreads;
-                if (r < nb) gather_row<T>(base + static_cast<int64_t>(r) * ns, ns, table, xg, cap, all_in, acc[j]);
+                for (int j = 0; j < kAxRows; j++) {
+                    const int r = threadIdx.x + j * kAxThreads;
+                    if (r < nb) gather_row<T>(base + static_cast<int64_t>(r) * ns, ns, table, xg, cap, all_in, acc[j]);
+                }
             }
         }
 #pragma unroll
-        for (int j = 0; j < kRowsPerThread; j++) {
-            const int r = threadIdx.x + j * kFastThreads;
+        for (int j = 0; j < kAxRows; j++) {
+            const int r = threadIdx.x + j * kAxThreads;
             if (r < nb) {
                 const int64_t row = blk * kBlockRows + r;
                 double v = static_cast<double>(acc[j]);
@@ -322,7 +418,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_kernel(FastGeometry
         }
     }
     if (part) {
-        const Comp r = block_sum_comp<kFastThreads>(mine, red);
+        const Comp r = block_sum_comp<kAxThreads>(mine, red);
         if (threadIdx.x == 0) {
             part[2 * blockIdx.x] = r.s;
             part[2 * blockIdx.x + 1] = r.c;
@@ -364,64 +460,78 @@ struct SegSmem {
 // round_start is a multiple of 4 entries, so every thread reads its
 // entries with 16-byte loads.
 template <typename T>
-__device__ void seg_round(const uint32_t* __restrict__ g32, int64_t round_start, int64_t e_lo, int64_t e_hi,
+__device__ __forceinline__ void run_step(uint32_t e, uint32_t c0, const T* __restrict__ ytile, T* __restrict__ acc,
+                                         int& hc, int& tc, T& hs, T& sum, bool& single, bool& any)
+{
+    const int col = static_cast<int>((e >> 16) - c0);
+    const T v = ytile[e & 0xFFFFu];
+    if (!any) {
+        any = true;
+        hc = tc = col;
+        sum = v;
+    } else if (col == tc) {
+        sum += v;
+    } else {
+        if (single) {
+            hs = sum;  // the head run closes inside this thread
+            single = false;
+        } else {
+            acc[tc] += sum;  // interior run: only this thread touches tc
+        }
+        tc = col;
+        sum = v;
+    }
+}
+
+template <typename T>
+__device__ void seg_round(const uint32_t* __restrict__ g32, uint32_t round_start, uint32_t e_lo, uint32_t e_hi,
                           uint32_t c0, const T* __restrict__ ytile, T* __restrict__ acc, SegSmem<T>& ss)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t e_first = round_start + static_cast<int64_t>(threadIdx.x) * kItemsPerThread;
+    const uint32_t e_first = round_start + threadIdx.x * kItemsPerThread;
     int hc = -1, tc = -1;
     T hs = 0, sum = 0;
     bool single = true, any = false;
+    const bool full = e_first >= e_lo && e_first + kItemsPerThread <= e_hi;
+    uint32_t first_ent = 0, last_ent = 0;
+    if (full) {
+        // every entry valid: 16-byte loads, no per-entry checks
 #pragma unroll
-    for (int half = 0; half < kItemsPerThread / 8; half++) {
-        const int64_t e8 = e_first + half * 8;
-        uint32_t ent[8];
-        if (e8 + 8 <= e_hi && e8 >= e_lo) {
-            const uint4 u0 = *reinterpret_cast<const uint4*>(g32 + e8);
-            const uint4 u1 = *reinterpret_cast<const uint4*>(g32 + e8 + 4);
-            ent[0] = u0.x, ent[1] = u0.y, ent[2] = u0.z, ent[3] = u0.w;
-            ent[4] = u1.x, ent[5] = u1.y, ent[6] = u1.z, ent[7] = u1.w;
-        } else {
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const int64_t e = e8 + i;
-                ent[i] = (e >= e_lo && e < e_hi) ? g32[e] : 0xFFFFFFFFu;
-            }
+        for (int q = 0; q < kItemsPerThread / 4; q++) {
+            const uint4 u = *reinterpret_cast<const uint4*>(g32 + e_first + 4 * q);
+            if (q == 0) first_ent = u.x;
+            if (q == kItemsPerThread / 4 - 1) last_ent = u.w;
+            run_step<T>(u.x, c0, ytile, acc, hc, tc, hs, sum, single, any);
+            run_step<T>(u.y, c0, ytile, acc, hc, tc, hs, sum, single, any);
+            run_step<T>(u.z, c0, ytile, acc, hc, tc, hs, sum, single, any);
+            run_step<T>(u.w, c0, ytile, acc, hc, tc, hs, sum, single, any);
         }
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int64_t e = e8 + i;
-            if (e < e_lo || e >= e_hi) continue;
-            const int col = static_cast<int>((ent[i] >> 16) - c0);
-            const T v = ytile[ent[i] & 0xFFFFu];
-            if (!any) {
-                any = true;
-                hc = tc = col;
-                sum = v;
-            } else if (col == tc) {
-                sum += v;
-            } else {
-                if (single) {
-                    hs = sum;  // the head run closes inside this thread
-                    single = false;
-                } else {
-                    acc[tc] += sum;  // interior run: only this thread touches tc
-                }
-                tc = col;
-                sum = v;
-            }
-        }
+    } else if (e_first + kItemsPerThread > e_lo && e_first < e_hi) {
+        const uint32_t lo = max(e_first, e_lo), hi = min(e_first + kItemsPerThread, e_hi);
+        first_ent = g32[lo];
+        last_ent = g32[hi - 1];
+        for (uint32_t e = lo; e < hi; e++) run_step<T>(g32[e], c0, ytile, acc, hc, tc, hs, sum, single, any);
     }
     const T ts = sum;
     if (single) hs = sum;
-    // neighbours: does my head continue the previous entry's run, does my
-    // tail continue into the next entry?
-    const int64_t first_valid = e_first < e_lo ? e_lo : e_first;
-    const int64_t last_valid = min(e_first + kItemsPerThread - 1, e_hi - 1);
+    // neighbours: the previous thread's last entry and the next thread's
+    // first entry, by shuffle inside the warp, from memory at warp edges
+    const uint32_t first_valid = max(e_first, e_lo);
+    const uint32_t last_valid = min(e_first + kItemsPerThread, e_hi) - 1;
+    const uint32_t prev_ent_sh = __shfl_up_sync(0xffffffffu, last_ent, 1);
+    const uint32_t next_ent_sh = __shfl_down_sync(0xffffffffu, first_ent, 1);
+    const bool prev_any = __shfl_up_sync(0xffffffffu, any, 1);
+    const bool next_any = __shfl_down_sync(0xffffffffu, any, 1);
     bool cont_prev = false, cont_next = false;
     if (any) {
-        if (first_valid - 1 >= e_lo) cont_prev = static_cast<int>((g32[first_valid - 1] >> 16) - c0) == hc;
-        if (last_valid + 1 < e_hi) cont_next = static_cast<int>((g32[last_valid + 1] >> 16) - c0) == tc;
+        if (first_valid > e_lo) {
+            const uint32_t pe = (lane > 0 && prev_any) ? prev_ent_sh : g32[first_valid - 1];
+            cont_prev = static_cast<int>((pe >> 16) - c0) == hc;
+        }
+        if (last_valid + 1 < e_hi) {
+            const uint32_t ne = (lane < 31 && next_any) ? next_ent_sh : g32[last_valid + 1];
+            cont_next = static_cast<int>((ne >> 16) - c0) == tc;
+        }
     }
     // segmented inclusive scan of tail partials over threads: a thread joins
     // the previous chain when its whole range is one run that continues it.
@@ -511,10 +621,11 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
         for (int i = threadIdx.x; i < nb; i += kFastThreads) ytile[i] = yb[i];
         if (threadIdx.x == 0) ss.carry = 0;
         __syncthreads();
-        const int64_t e_lo = chunk_start[blk * g.nchunks + ch0];
-        const int64_t e_hi = ch1_local < pat_chunks ? static_cast<int64_t>(chunk_start[blk * g.nchunks + g.chunk0[p] + ch1_local])
-                                                    : g.seg(blk, p) + g.seg_len(blk, p);
-        for (int64_t rs = e_lo & ~int64_t(3); rs < e_hi; rs += int64_t(kFastThreads) * kItemsPerThread)
+        const uint32_t e_lo = chunk_start[blk * g.nchunks + ch0];
+        const uint32_t e_hi = ch1_local < pat_chunks
+                                  ? chunk_start[blk * g.nchunks + g.chunk0[p] + ch1_local]
+                                  : static_cast<uint32_t>(g.seg(blk, p) + g.seg_len(blk, p));
+        for (uint32_t rs = e_lo & ~3u; rs < e_hi; rs += kFastThreads * kItemsPerThread)
             seg_round<T>(g32, rs, e_lo, e_hi, c0, ytile, acc, ss);
     }
     __syncthreads();
@@ -703,15 +814,24 @@ cas_status fast_set_attributes()
     const int t32 = static_cast<int>(sizeof(float) * (static_cast<size_t>(kChunkCols) * 4 + kBlockRows));
     const int t64 = static_cast<int>(sizeof(double) * (static_cast<size_t>(kChunkCols) * 1 + kBlockRows));
     const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 0>, attr, s32));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 1>, attr, s32));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 2>, attr, s32));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, double, 0>, attr, s64));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, double, 1>, attr, s64));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, double, 2>, attr, s64));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 0>, attr, s64));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 1>, attr, s64));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 2>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 0, true>, attr, s32));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 0, false>, attr, s32));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 1, true>, attr, s32));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 1, false>, attr, s32));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 2, true>, attr, s32));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 2, false>, attr, s32));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, double, 0, true>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, double, 0, false>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, double, 1, true>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, double, 1, false>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, double, 2, true>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, double, 2, false>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 0, true>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 0, false>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 1, true>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 1, false>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 2, true>, attr, s64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 2, false>, attr, s64));
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<float>, attr, t32));
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<double>, attr, t64));
     return CAS_OK;
@@ -831,13 +951,20 @@ cas_status fast_spmv(const FastLayout& f, const T* x, Y* y, const double* b, con
     if (f.g.nblocks == 0) return CAS_OK;
     const size_t smem = sizeof(T) * (sizeof(T) == 4 ? kTable32 : kTable64);
     auto launch = [&](auto kern) -> cas_status {
-        { kern<<<grid, kFastThreads, smem, s>>>(f.g, f.a16, x, y, b, coef, part, done_flag); cas::count_launch(); }
+        { kern<<<grid, kAxThreads, smem, s>>>(f.g, f.a16, x, y, b, coef, part, done_flag); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     };
-    if (mode == 0) return launch(fast_spmv_kernel<T, Y, 0>);
-    if (mode == 1) return launch(fast_spmv_kernel<T, Y, 1>);
-    return launch(fast_spmv_kernel<T, Y, 2>);
+    bool all8 = true;
+    for (int p = 0; p < f.g.npat; p++) all8 = all8 && f.g.slots[p] == 8;
+    if (all8) {
+        if (mode == 0) return launch(fast_spmv_kernel<T, Y, 0, true>);
+        if (mode == 1) return launch(fast_spmv_kernel<T, Y, 1, true>);
+        return launch(fast_spmv_kernel<T, Y, 2, true>);
+    }
+    if (mode == 0) return launch(fast_spmv_kernel<T, Y, 0, false>);
+    if (mode == 1) return launch(fast_spmv_kernel<T, Y, 1, false>);
+    return launch(fast_spmv_kernel<T, Y, 2, false>);
 }
 
 template <typename T>

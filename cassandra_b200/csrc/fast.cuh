@@ -21,8 +21,10 @@
 namespace cas {
 
 constexpr int kBlockRows = 16384;        // rows per block (and per A'y tile)
-constexpr int kFastThreads = 1024;       // threads of the product kernels
-constexpr int kRowsPerThread = kBlockRows / kFastThreads;
+constexpr int kFastThreads = 1024;       // threads of the A'y kernel
+constexpr int kAxThreads = 1024;         // threads of the A x kernel
+constexpr int kAxRows = kBlockRows / kAxThreads;  // rows per thread in A x
+constexpr int kAxAhead = 3;              // index loads in flight per thread in A x
 constexpr int kChunkCols = 8192;         // column chunk of the A'y accumulators
 constexpr int kMaxFastPatterns = 32;
 constexpr int kTable32 = 57344;          // x entries staged per pattern, FP32

@@ -49,7 +49,9 @@ enum Slot {
     kTrue = 16,    // ||A'(b - A x)||^2 of the last true-residual evaluation
     kSlots = 17
 };
-enum Flag { kDone = 0, kStatus = 1, kIter = 2, kRefine = 3, kFlags = 4 };
+// kPending: LSQR met its tolerance in the last step; the step's x/w update
+// still has to run, so kDone is raised by the next step's first kernel.
+enum Flag { kDone = 0, kStatus = 1, kIter = 2, kRefine = 3, kPending = 4, kFlags = 5 };
 
 struct Dev {
     double* scal;
@@ -386,7 +388,7 @@ __global__ void __launch_bounds__(kVecThreads) lsqr_v_kernel(ColSum cs,
                                                              Dev dv, int init)
 {
     __shared__ double smem[64];
-    if (!init && finished(dv.flags)) return;
+    if (init != 1 && finished(dv.flags)) return;
     const double inv_beta = dv.scal[kInvBeta];
     const double beta = dv.scal[kLBeta];
     const double inv_alpha_prev = dv.scal[kLAlpha] != 0 ? 1.0 / dv.scal[kLAlpha] : 0.0;
@@ -408,13 +410,14 @@ __global__ void __launch_bounds__(kRedThreads) lsqr_beta_kernel(const double* __
                                                                 int init)
 {
     __shared__ double smem[64];
-    if (!init && finished(dv.flags)) return;
+    if (init != 1 && finished(dv.flags)) return;
     const double s = reduce_partials<COMP>(part, n, smem);
     if (threadIdx.x == 0) {
         const double beta = sqrt(s);
         dv.scal[kLBeta] = beta;
         dv.scal[kInvBeta] = beta > 0 ? 1.0 / beta : 0.0;
         if (init) dv.scal[kPhiBar] = beta;  // phi_bar = beta (Math/Solver.h:149)
+        if (init == 2) dv.flags[kRefine] += 1;  // restart from the true residual
     }
 }
 
@@ -424,7 +427,7 @@ __global__ void __launch_bounds__(kRedThreads) lsqr_alpha_kernel(const double* _
                                                                  int init)
 {
     __shared__ double smem[64];
-    if (!init && finished(dv.flags)) return;
+    if (init != 1 && finished(dv.flags)) return;
     const double s = reduce_partials<COMP>(part, n, smem);
     if (threadIdx.x == 0) {
         const double alpha = sqrt(s);
@@ -459,7 +462,7 @@ __global__ void __launch_bounds__(kRedThreads) lsqr_alpha_kernel(const double* _
         const double bn2 = dv.scal[kBn2];
         const double res = bn2 > 0 ? arn / sqrt(bn2) : arn;
         dv.scal[kRes] = res;
-        if (dv.scal[kTol] > 0 && res <= dv.scal[kTol]) dv.flags[kDone] = 1;
+        if (dv.scal[kTol] > 0 && res <= dv.scal[kTol]) dv.flags[kPending] = 1;
     }
 }
 
@@ -469,7 +472,7 @@ __global__ void __launch_bounds__(kVecThreads) lsqr_xw_kernel(int64_t n, double*
                                                               double* __restrict__ w, const double* __restrict__ v,
                                                               T* __restrict__ vg, Dev dv, int init)
 {
-    if (!init && finished(dv.flags)) return;
+    if (init != 1 && finished(dv.flags)) return;
     const double inv_alpha = dv.scal[kLAlpha] != 0 ? 1.0 / dv.scal[kLAlpha] : 0.0;
     const double phi_rho = dv.scal[kPhiRho], theta_rho = dv.scal[kThetaRho];
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
@@ -486,9 +489,15 @@ __global__ void __launch_bounds__(kVecThreads) lsqr_xw_kernel(int64_t n, double*
 }
 
 // coefficient of the u recursion: alpha / beta_prev (u_hat holds beta_prev u).
+// First kernel of an LSQR step: a tolerance met by the previous step stops
+// the solver here, after that step's x/w update has run.
 __global__ void lsqr_coef_kernel(Dev dv, int slot)
 {
     if (finished(dv.flags)) return;
+    if (dv.flags[kPending]) {
+        dv.flags[kDone] = 1;
+        return;
+    }
     dv.scal[slot] = dv.scal[kLAlpha] * dv.scal[kInvBeta];
 }
 
@@ -672,12 +681,40 @@ struct SolverImpl {
         return CAS_OK;
     }
 
+    // LSQR (re)start from the current x (Math/Solver.h:139-151 with b - A x
+    // for b): beta u = b - A x ; alpha v = A'u ; w = v ; phi_bar = beta ;
+    // rho_bar = alpha.  mode 1 = setup, 2 = restart inside a graph chunk
+    // (the mixed solver's refinement: the true residual replaces b).
+    cas_status issue_lsqr_start(int mode)
+    {
+        const Dev D = dv();
+        const bool gate = mode == 2;
+        if (mixed) {
+            CAS_TRY((product<true, double, float>(x, static_cast<float*>(q), 2, b, 0, gate)));
+            { lsqr_beta_kernel<true><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, mode); cas::count_launch(); }
+            CAS_TRY(product_t<float>(static_cast<const float*>(q), gate));
+            { lsqr_v_kernel<true, float><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<float>(), v, part_a, D, mode); cas::count_launch(); }
+            { lsqr_alpha_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
+            { lsqr_xw_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, pg32, D, mode); cas::count_launch(); }
+        } else {
+            CAS_TRY((product<false, double, double>(x, static_cast<double*>(q), 2, b, 0, gate)));
+            { lsqr_beta_kernel<false><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, mode); cas::count_launch(); }
+            CAS_TRY(product_t<double>(static_cast<const double*>(q), gate));
+            { lsqr_v_kernel<false, double><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), v, part_a, D, mode); cas::count_launch(); }
+            { lsqr_alpha_kernel<false><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
+            { lsqr_xw_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, p, D, mode); cas::count_launch(); }
+        }
+        CAS_CHECK_LAUNCH();
+        return CAS_OK;
+    }
+
     cas_status issue_iteration(int global_index)
     {
         const bool lsqr = o.method == CAS_LSQR;
         if (lsqr) {
             if (mixed) CAS_TRY((issue_lsqr_iteration<true, float>()));
             else CAS_TRY((issue_lsqr_iteration<false, double>()));
+            if (mixed && o.refine_every > 0 && (global_index + 1) % o.refine_every == 0) CAS_TRY(issue_lsqr_start(2));
             return CAS_OK;
         }
         if (mixed) CAS_TRY((issue_pcg_iteration<true, float>()));
@@ -690,7 +727,7 @@ struct SolverImpl {
     // CUDA graph when the chunk shape allows.
     cas_status issue_chunk(int first, int n)
     {
-        const int period = (mixed && o.method != CAS_LSQR && o.refine_every > 0) ? o.refine_every : 1;
+        const int period = (mixed && o.refine_every > 0) ? o.refine_every : 1;
         const int phase = first % period;
         if (n > 1) {
             if (!graph || graph_len != n || graph_phase != phase) {
@@ -803,23 +840,7 @@ struct SolverImpl {
         CAS_CHECK_LAUNCH();
 
         if (o.method == CAS_LSQR) {
-            // beta u = b - A x0 ; alpha v = A'u ; w = v ; phi_bar = beta ; rho_bar = alpha
-            if (mixed) {
-                CAS_TRY((product<true, double, float>(x, static_cast<float*>(q), 2, b, 0, false)));
-                { lsqr_beta_kernel<true><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, 1); cas::count_launch(); }
-                CAS_TRY(product_t<float>(static_cast<const float*>(q), false));
-                { lsqr_v_kernel<true, float><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<float>(), v, part_a, D, 1); cas::count_launch(); }
-                { lsqr_alpha_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 1); cas::count_launch(); }
-                { lsqr_xw_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, pg32, D, 1); cas::count_launch(); }
-            } else {
-                CAS_TRY((product<false, double, double>(x, static_cast<double*>(q), 2, b, 0, false)));
-                { lsqr_beta_kernel<false><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, 1); cas::count_launch(); }
-                CAS_TRY(product_t<double>(static_cast<const double*>(q), false));
-                { lsqr_v_kernel<false, double><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), v, part_a, D, 1); cas::count_launch(); }
-                { lsqr_alpha_kernel<false><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 1); cas::count_launch(); }
-                { lsqr_xw_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, p, D, 1); cas::count_launch(); }
-            }
-            CAS_CHECK_LAUNCH();
+            CAS_TRY(issue_lsqr_start(1));
         } else {
             if (mixed) CAS_TRY(issue_pcg_refine<true>(true, true));
             else CAS_TRY(issue_pcg_refine<false>(true, true));
@@ -1006,22 +1027,38 @@ CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
             st = static_cast<cas_status>(m.host_flags[kStatus]);
             break;
         }
-        if (m.host_flags[kDone]) {
+        const bool done = m.host_flags[kDone] || m.host_flags[kPending];
+        if (m.o.method == CAS_LSQR && m.o.tol > 0 && !done && it > 0) {
+            // LSQR's recursive residual estimates lose their meaning once the
+            // bidiagonalisation loses orthogonality, and iterating past
+            // convergence can diverge (the reference's LSQR has no stopping
+            // test), so its stopping test is the true FP64 residual, checked
+            // at every chunk boundary.
+            CAS_TRY(m.true_residual(&rel));
+            if (rel <= m.o.tol) break;
+        }
+        if (done) {
             // verify with the true FP64 residual
             CAS_TRY(m.true_residual(&rel));
-            if (m.o.tol <= 0 || rel <= m.o.tol || it >= m.o.max_iterations || extra_checks > 20) break;
+            if (m.o.tol <= 0 || rel <= m.o.tol || it >= m.o.max_iterations) break;
+            if (extra_checks > 20) {
+                st = CAS_ERR_NOT_CONVERGED;
+                break;
+            }
             // recursive residual drifted: replace it and continue
             extra_checks++;
-            int zero = 0;
+            static const int zero = 0;
             CAS_CUDA(cudaMemcpyAsync(m.flags + kDone, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
+            CAS_CUDA(cudaMemcpyAsync(m.flags + kPending, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
             if (m.o.method == CAS_LSQR) {
                 // LSQR has no residual to replace: tighten the recursive target
                 double t = m.host_scal[kTol] * 0.5;
                 CAS_CUDA(cudaMemcpyAsync(m.scal + kTol, &t, sizeof t, cudaMemcpyHostToDevice, m.s));
             } else if (m.mixed) {
-                CAS_TRY(m.issue_pcg_refine<true>(false, true));
+                // the converged step skipped p = z + beta p: restart p = z
+                CAS_TRY(m.issue_pcg_refine<true>(true, true));
             } else {
-                CAS_TRY(m.issue_pcg_refine<false>(false, true));
+                CAS_TRY(m.issue_pcg_refine<false>(true, true));
             }
             continue;
         }
