@@ -279,6 +279,29 @@ CAS_API cas_status cas_generate_positions_host(uint64_t seed, int64_t first, int
 CAS_API cas_status cas_generate_targets(const cas_csr* a, uint64_t seed, double w_sigma, double noise_sigma,
                                         double* d_b, double* d_w_true, void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Allocation-free product                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* No counterpart in the reference.  y = A x and *d_norm2 = ||y||^2, in FP64,
+ * over caller-owned row-major indices (rows * nnz_per_row uint32 column
+ * indices, each < cols) — the product and the norm the PCG step needs —
+ * without allocating any device memory.  For callers that cannot let the
+ * library allocate: device memory owned by another allocator or held to a
+ * fixed budget, or a code path where cudaMalloc/cudaFree may not run because
+ * they synchronise the device.  The per-CTA
+ * partial sums live in a fixed 128 KB device array inside the library
+ * (resident on every GPU that loads it until exit), which caps rows at
+ * cas_spmv_norm_noalloc_max_rows() = 16,777,216; larger inputs are rejected
+ * with CAS_ERR_INVALID_ARGUMENT.  The first call on a device looks up that
+ * array's device address (no allocation); make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  The result does not depend on the GPU model
+ * (fixed 2048 rows per CTA). */
+CAS_API int64_t cas_spmv_norm_noalloc_max_rows(void);
+CAS_API cas_status cas_spmv_norm_noalloc(const uint32_t* d_indices, int nnz_per_row, int64_t rows, int64_t cols,
+                                         const double* d_x, double* d_y, double* d_norm2, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
