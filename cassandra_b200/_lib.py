@@ -64,6 +64,20 @@ class SolveReport(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class Schedule(C.Structure):
+    _fields_ = [
+        ("chunks_per_item", C.c_int),
+        ("ring", C.c_int),
+        ("items_per_sm", C.c_int),
+        ("pack", C.c_int),
+        ("persistent", C.c_int),
+        ("ms", C.c_float),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class CasError(RuntimeError):
     """A cas_status other than CAS_OK, with the library's message."""
 
@@ -129,6 +143,7 @@ SIGNATURES: dict[str, tuple] = {
     "cas_generate_positions": (C.c_int, [_U64, _I64, C.c_int, C.c_int, _VP, _VP]),
     "cas_generate_positions_host": (C.c_int, [_U64, _I64, _I64, C.c_int, C.c_int, _VP]),
     "cas_generate_targets": (C.c_int, [_VP, _U64, C.c_double, C.c_double, _VP, _VP, _VP]),
+    "cas_csr_schedules": (C.c_int, [_VP, _VP, C.c_int, _VP]),
     "cas_spmv_norm_noalloc_max_rows": (_I64, []),
     "cas_spmv_norm_noalloc": (C.c_int, [_VP, C.c_int, _I64, _I64, _VP, _VP, _VP, _VP]),
 }

@@ -116,6 +116,16 @@ class MatrixCSR:
                                                       _stream(), C.byref(h)))
         return cls(h, keep=indexer)
 
+    def schedules(self) -> dict:
+        """A'y schedules timed by the build-time autotuner on this matrix and
+        the one in use (blocked layout only)."""
+        out = (L.Schedule * 16)()
+        cur = L.Schedule()
+        n = self._lib.cas_csr_schedules(self.handle, out, 16, C.byref(cur))
+        if n < 0:
+            return {}
+        return {"in_use": cur.as_dict(), "timed": [out[i].as_dict() for i in range(n)]}
+
     def layouts(self) -> set[str]:
         m = int(self._lib.cas_csr_layouts(self._h))
         return {n for n, bit in (("rows", L.CAS_LAYOUT_ROWS), ("blocked", L.CAS_LAYOUT_BLOCKED)) if m & bit}

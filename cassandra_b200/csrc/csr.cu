@@ -577,6 +577,30 @@ CAS_API int cas_csr_layouts(const cas_csr* a) { return a ? a->layouts : 0; }
 
 CAS_API int64_t cas_block_rows(void) { return kBlockRows; }
 
+CAS_API int cas_csr_schedules(const cas_csr* a, cas_schedule* out, int max, cas_schedule* in_use)
+{
+    if (!a || !a->fast) return -1;
+    const FastLayout& f = *a->fast;
+    if (in_use) {
+        in_use->chunks_per_item = f.t32.per_sc;
+        in_use->ring = f.t32.ring ? 1 : 0;
+        in_use->items_per_sm = f.t32.items_per_sm;
+        in_use->pack = f.t32.pack ? 1 : 0;
+        in_use->persistent = f.t32.persistent ? 1 : 0;
+        in_use->ms = 0;
+        for (int i = 0; i < f.ntune; i++)
+            if (f.tune[i].per_sc == f.t32.per_sc && f.tune[i].ring == in_use->ring &&
+                f.tune[i].items_per_sm == f.t32.items_per_sm && f.tune[i].pack == in_use->pack &&
+                f.tune[i].persistent == in_use->persistent)
+                in_use->ms = f.tune[i].ms;
+    }
+    int n = 0;
+    for (int i = 0; i < f.ntune && out && n < max; i++, n++)
+        out[n] = cas_schedule{f.tune[i].per_sc, f.tune[i].ring, f.tune[i].items_per_sm, f.tune[i].pack,
+                              f.tune[i].persistent, f.tune[i].ms};
+    return n;
+}
+
 CAS_API cas_status cas_eval_forward(const cas_csr* a, int64_t row0, int64_t row1, const float* d_w, float* d_score,
                                     void* stream)
 {

@@ -15,6 +15,11 @@
 //       of the chunk.  Items write partial column sums that the caller adds
 //       in a fixed order: no atomics anywhere, bitwise reproducible.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -27,7 +32,16 @@ namespace {
 
 constexpr int kSortThreads = 1024;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kItemsPerThread = 16;  // A'y entries per thread and round (a multiple of 8)
+constexpr int kItemsPerThread = 8;  // A'y entries per lane and round (a multiple of 4)
+constexpr int kRingStages = 3;      // A'y FP32 ring schedules: rounds in the per-lane cp.async ring
+
+// A'y streams its entries either one round ahead in registers or, for FP32
+// schedules with narrow accumulators, through a per-lane ring of cp.async
+// copies in shared memory (kRingStages rounds in flight).  The build-time
+// autotuner picks the schedule (accumulator width, streaming, items per SM).
+constexpr size_t kRingBytes = sizeof(uint32_t) * kFastThreads * kRingStages * kItemsPerThread;
+constexpr int kMaxScRing = 2;  // widest FP32 accumulator (chunks) that leaves room for the ring
+constexpr int kMaxScRegs = 4;
 
 unsigned fgrid(int64_t work, int per)
 {
@@ -430,35 +444,46 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
 // A'y on the blocked layout.
 // ---------------------------------------------------------------------------
 struct TView {
-    int per_sc;
     const int* item_sc;
     const int* item_b0;
     const int* item_b1;
     const int64_t* item_part;
-    int sc_base[kMaxFastPatterns + 1];
+    const int* sc_piece0;
+    const int* sc_width;
+    const int* piece_pat;
+    const int* piece_ch0;
+    const int* piece_ch1;
+    const int* piece_acc;
+    int per_sc;
+    int nitems;
 };
 
+// Column-sorted entries are reduced warp by warp.  The (block, chunk range)
+// entry list is cut into 32 nearly equal pieces, one per warp, so warps
+// stream their entries without block barriers whatever the run lengths
+// (one column can hold thousands of a block's entries).  Inside a warp each
+// lane owns kItemsPerThread consecutive entries per round; runs of equal
+// columns are summed and added to acc[col] exactly once, in an order fixed by
+// the data, so the result is bitwise reproducible:
+//   1. each lane sums its runs; runs wholly inside the lane are added to acc
+//      directly (no other lane or warp touches that column);
+//   2. the partial runs at lane boundaries are combined by a segmented scan
+//      over the warp's lanes (shuffles); the run still open at the end of
+//      the previous round enters as `carry`;
+//   3. the lane where a boundary run ends adds the combined sum, except for
+//      the warp's first and last run, which may continue in the neighbouring
+//      warps: their sums go to the warp's record;
+//   4. after the block, warp 0 combines the 32 records with the same
+//      segmented scan (one lane per warp) and adds them.
+
+// Sums of a warp's first and last run (columns relative to c0).
 template <typename T>
-struct SegSmem {
-    T warp_v[32];
-    int warp_f[32];
-    T warp_excl[32];
-    T carry;
+struct WarpRec {
+    T fs, ls;          // first-run sum, last-run sum (ls unused when fc == lc)
+    int fc, lc;        // first and last column of the warp's range
+    int valid, cp, cn; // range non-empty; first run continues the previous warp; last run continues in the next
 };
 
-// Segmented reduction of one round of column-sorted entries into acc.
-// Each thread owns kItemsPerThread consecutive entries of [e_lo, e_hi); runs
-// of equal columns are summed and added to acc[col] exactly once, in an
-// order fixed by the data, so the result is bitwise reproducible:
-//   1. each thread sums its runs; runs wholly inside the thread are added to
-//      acc directly (no other thread touches that column in this tile);
-//   2. the partial runs at thread boundaries are combined by a segmented
-//      scan: shuffles inside each warp, then warp 0 scans the 32 warp
-//      aggregates; the chain entering the round (an open run of the previous
-//      round) is ss.carry;
-//   3. the thread where a boundary run ends adds the combined sum.
-// round_start is a multiple of 4 entries, so every thread reads its
-// entries with 16-byte loads.
 template <typename T>
 __device__ __forceinline__ void run_step(uint32_t e, uint32_t c0, const T* __restrict__ ytile, T* __restrict__ acc,
                                          int& hc, int& tc, T& hs, T& sum, bool& single, bool& any)
@@ -473,70 +498,26 @@ __device__ __forceinline__ void run_step(uint32_t e, uint32_t c0, const T* __res
         sum += v;
     } else {
         if (single) {
-            hs = sum;  // the head run closes inside this thread
+            hs = sum;  // the head run closes inside this lane
             single = false;
         } else {
-            acc[tc] += sum;  // interior run: only this thread touches tc
+            acc[tc] += sum;  // interior run: only this lane touches tc
         }
         tc = col;
         sum = v;
     }
 }
 
-template <typename T>
-__device__ void seg_round(const uint32_t* __restrict__ g32, uint32_t round_start, uint32_t e_lo, uint32_t e_hi,
-                          uint32_t c0, const T* __restrict__ ytile, T* __restrict__ acc, SegSmem<T>& ss)
+// Segmented inclusive scan over the 32 lanes of (any, single, cont_prev,
+// tail sum) and the resulting adds of head and tail runs; `sink` receives
+// every closed boundary run.  Lanes without entries pass the chain through.
+template <typename T, typename Sink>
+__device__ __forceinline__ T lane_chain(bool any, bool single, bool cont_prev, bool cont_next, int hc, int tc, T hs,
+                                        T ts, T carry, Sink&& sink)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t e_first = round_start + threadIdx.x * kItemsPerThread;
-    int hc = -1, tc = -1;
-    T hs = 0, sum = 0;
-    bool single = true, any = false;
-    const bool full = e_first >= e_lo && e_first + kItemsPerThread <= e_hi;
-    uint32_t first_ent = 0, last_ent = 0;
-    if (full) {
-        // every entry valid: 16-byte loads, no per-entry checks
-#pragma unroll
-        for (int q = 0; q < kItemsPerThread / 4; q++) {
-            const uint4 u = *reinterpret_cast<const uint4*>(g32 + e_first + 4 * q);
-            if (q == 0) first_ent = u.x;
-            if (q == kItemsPerThread / 4 - 1) last_ent = u.w;
-            run_step<T>(u.x, c0, ytile, acc, hc, tc, hs, sum, single, any);
-            run_step<T>(u.y, c0, ytile, acc, hc, tc, hs, sum, single, any);
-            run_step<T>(u.z, c0, ytile, acc, hc, tc, hs, sum, single, any);
-            run_step<T>(u.w, c0, ytile, acc, hc, tc, hs, sum, single, any);
-        }
-    } else if (e_first + kItemsPerThread > e_lo && e_first < e_hi) {
-        const uint32_t lo = max(e_first, e_lo), hi = min(e_first + kItemsPerThread, e_hi);
-        first_ent = g32[lo];
-        last_ent = g32[hi - 1];
-        for (uint32_t e = lo; e < hi; e++) run_step<T>(g32[e], c0, ytile, acc, hc, tc, hs, sum, single, any);
-    }
-    const T ts = sum;
-    if (single) hs = sum;
-    // neighbours: the previous thread's last entry and the next thread's
-    // first entry, by shuffle inside the warp, from memory at warp edges
-    const uint32_t first_valid = max(e_first, e_lo);
-    const uint32_t last_valid = min(e_first + kItemsPerThread, e_hi) - 1;
-    const uint32_t prev_ent_sh = __shfl_up_sync(0xffffffffu, last_ent, 1);
-    const uint32_t next_ent_sh = __shfl_down_sync(0xffffffffu, first_ent, 1);
-    const bool prev_any = __shfl_up_sync(0xffffffffu, any, 1);
-    const bool next_any = __shfl_down_sync(0xffffffffu, any, 1);
-    bool cont_prev = false, cont_next = false;
-    if (any) {
-        if (first_valid > e_lo) {
-            const uint32_t pe = (lane > 0 && prev_any) ? prev_ent_sh : g32[first_valid - 1];
-            cont_prev = static_cast<int>((pe >> 16) - c0) == hc;
-        }
-        if (last_valid + 1 < e_hi) {
-            const uint32_t ne = (lane < 31 && next_any) ? next_ent_sh : g32[last_valid + 1];
-            cont_next = static_cast<int>((ne >> 16) - c0) == tc;
-        }
-    }
-    // segmented inclusive scan of tail partials over threads: a thread joins
-    // the previous chain when its whole range is one run that continues it.
+    const int lane = threadIdx.x & 31;
     T v = any ? ts : T(0);
-    bool f = !(any && single && cont_prev);
+    bool f = any && !(single && cont_prev);
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         const T vu = __shfl_up_sync(0xffffffffu, v, d);
@@ -546,91 +527,345 @@ __device__ void seg_round(const uint32_t* __restrict__ g32, uint32_t round_start
             f = f || fu;
         }
     }
-    if (lane == 31) {
-        ss.warp_v[warp] = v;
-        ss.warp_f[warp] = f;
+    const T X = f ? v : v + carry;  // chain value ending at this lane
+    T Xprev = __shfl_up_sync(0xffffffffu, X, 1);
+    if (lane == 0) Xprev = carry;
+    if (any) {
+        if (single) {
+            if (!cont_next) sink(hc, X);
+        } else {
+            sink(hc, cont_prev ? Xprev + hs : hs);
+            if (!cont_next) sink(tc, ts);
+        }
+    }
+    return __shfl_sync(0xffffffffu, X, 31);  // open chain leaving the lanes
+}
+
+constexpr int kLaneVecs = kItemsPerThread / 4;  // 16-byte loads per lane and round
+
+// A lane's entries of a round are all inside the warp's range.
+__device__ __forceinline__ bool lane_full(uint32_t e_first, uint32_t w_lo, uint32_t w_hi)
+{
+    return e_first >= w_lo && e_first + kItemsPerThread <= w_hi;
+}
+
+// Streaming loads of a lane's entries (read once per product: evict first,
+// so that the y and x slices stay in L2).
+__device__ __forceinline__ void load_lane(const uint32_t* __restrict__ g32, uint32_t e_first, uint4 (&u)[kLaneVecs])
+{
+#pragma unroll
+    for (int q = 0; q < kLaneVecs; q++) u[q] = __ldcs(reinterpret_cast<const uint4*>(g32 + e_first) + q);
+}
+
+// 16-byte asynchronous global -> shared copy (L2 only) and its group
+// bookkeeping; wait_group waits for this thread's own copies only.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// One round of a warp over [w_lo, w_hi): lanes take kItemsPerThread entries
+// each from round_start (a multiple of 4).  A lane whose entries are all in
+// range gets them in `cur` (loaded one round ahead by the caller) and sums
+// its runs without branches; edge lanes load and walk their entries one by
+// one.
+template <typename T>
+__device__ __forceinline__ void warp_round(const uint32_t* __restrict__ g32, uint32_t round_start, uint32_t w_lo,
+                                           uint32_t w_hi, uint32_t c0, const T* __restrict__ ytile,
+                                           T* __restrict__ acc, T& carry, WarpRec<T>& rec,
+                                           const uint4 (&cur)[kLaneVecs], bool full)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t e_first = round_start + lane * kItemsPerThread;
+    int hc = -1, tc = -1;
+    T hs = 0, ts = 0;
+    bool single = true, any = false;
+    uint32_t first_ent = 0, last_ent = 0;
+    if (full) {
+        uint32_t e[kItemsPerThread];
+#pragma unroll
+        for (int q = 0; q < kLaneVecs; q++) {
+            e[4 * q] = cur[q].x;
+            e[4 * q + 1] = cur[q].y;
+            e[4 * q + 2] = cur[q].z;
+            e[4 * q + 3] = cur[q].w;
+        }
+        T yv[kItemsPerThread];
+#pragma unroll
+        for (int i = 0; i < kItemsPerThread; i++) yv[i] = ytile[e[i] & 0xFFFFu];
+        int kp = static_cast<int>((e[0] >> 16) - c0);
+        T sum = yv[0];
+        bool open = true;  // the lane's first run has not closed yet
+        hc = kp;
+#pragma unroll
+        for (int i = 1; i < kItemsPerThread; i++) {
+            const int k = static_cast<int>((e[i] >> 16) - c0);
+            const bool brk = k != kp;
+            hs = (brk && open) ? sum : hs;
+            if (brk && !open) acc[kp] += sum;  // interior run: only this lane touches kp
+            open = open && !brk;
+            sum = brk ? yv[i] : sum + yv[i];
+            kp = k;
+        }
+        tc = kp;
+        ts = sum;
+        single = open;
+        if (single) hs = sum;
+        any = true;
+        first_ent = e[0];
+        last_ent = e[kItemsPerThread - 1];
+    } else if (e_first + kItemsPerThread > w_lo && e_first < w_hi) {
+        const uint32_t lo = max(e_first, w_lo), hi = min(e_first + kItemsPerThread, w_hi);
+        first_ent = g32[lo];
+        last_ent = g32[hi - 1];
+        T sum = 0;
+        for (uint32_t e = lo; e < hi; e++) run_step<T>(g32[e], c0, ytile, acc, hc, tc, hs, sum, single, any);
+        ts = sum;
+        if (single) hs = sum;
+    }
+    // neighbours: the previous lane's last entry and the next lane's first
+    // entry by shuffle, from memory across the round's edges
+    const uint32_t first_valid = max(e_first, w_lo);
+    const uint32_t last_valid = min(e_first + kItemsPerThread, w_hi) - 1;
+    const uint32_t prev_ent_sh = __shfl_up_sync(0xffffffffu, last_ent, 1);
+    const uint32_t next_ent_sh = __shfl_down_sync(0xffffffffu, first_ent, 1);
+    const unsigned any_mask = __ballot_sync(0xffffffffu, any);
+    const bool prev_any = lane > 0 && ((any_mask >> (lane - 1)) & 1u);
+    const bool next_any = lane < 31 && ((any_mask >> (lane + 1)) & 1u);
+    bool cont_prev = false, cont_next = false;
+    if (any) {
+        if (first_valid > w_lo) {
+            const uint32_t pe = prev_any ? prev_ent_sh : g32[first_valid - 1];
+            cont_prev = static_cast<int>((pe >> 16) - c0) == hc;
+        }
+        if (last_valid + 1 < w_hi) {
+            const uint32_t ne = next_any ? next_ent_sh : g32[last_valid + 1];
+            cont_next = static_cast<int>((ne >> 16) - c0) == tc;
+        }
+    }
+    const int fc = rec.fc, lc = rec.lc;
+    auto sink = [&](int col, T val) {
+        if (col == fc)
+            rec.fs = val;
+        else if (col == lc)
+            rec.ls = val;
+        else
+            acc[col] += val;
+    };
+    if (__ballot_sync(0xffffffffu, any && single && cont_prev) == 0) {
+        // no lane is one run continued from its left: every chain is at
+        // most two lanes long, one shuffle combines them
+        T prev_ts = __shfl_up_sync(0xffffffffu, ts, 1);
+        if (lane == 0) prev_ts = carry;
+        if (any) {
+            if (single) {
+                if (!cont_next) sink(hc, ts);
+            } else {
+                sink(hc, cont_prev ? prev_ts + hs : hs);
+                if (!cont_next) sink(tc, ts);
+            }
+        }
+        carry = __shfl_sync(0xffffffffu, ts, 31);
+    } else {
+        carry = lane_chain<T>(any, single, cont_prev, cont_next, hc, tc, hs, ts, carry, sink);
+    }
+}
+
+// The warp-range reduction of one block's entries [e_lo, e_hi) into acc.
+// Ends with a block barrier; the next block may restage ytile after it.
+template <typename T, bool RING>
+__device__ __forceinline__ void reduce_block_entries(const uint32_t* __restrict__ g32, uint32_t e_lo, uint32_t e_hi,
+                                                     uint32_t c0, const T* __restrict__ ytile, T* __restrict__ acc,
+                                                     WarpRec<T>* recs, uint32_t* __restrict__ ring)
+{
+    constexpr int kWarps = kFastThreads / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t n = e_hi - e_lo;
+    auto cut = [&](int w) -> uint32_t {
+        if (w == 0) return e_lo;
+        if (w == kWarps) return e_hi;
+        return max(e_lo, (e_lo + static_cast<uint32_t>(n * w / kWarps)) & ~3u);
+    };
+    const uint32_t w_lo = cut(warp), w_hi = cut(warp + 1);
+    WarpRec<T>& rec = recs[warp];
+    if (lane == 0) {
+        rec.valid = w_lo < w_hi;
+        rec.fs = rec.ls = T(0);
+        rec.fc = rec.lc = -1;
+        rec.cp = rec.cn = 0;
+        if (w_lo < w_hi) {
+            const uint32_t ef = g32[w_lo], el = g32[w_hi - 1];
+            rec.fc = static_cast<int>((ef >> 16) - c0);
+            rec.lc = static_cast<int>((el >> 16) - c0);
+            rec.cp = w_lo > e_lo && (g32[w_lo - 1] >> 16) == (ef >> 16);
+            rec.cn = w_hi < e_hi && (g32[w_hi] >> 16) == (el >> 16);
+        }
+    }
+    __syncwarp();
+    T carry = 0;
+    if constexpr (RING) {
+        // round r of this lane lands in ring slot r % kRingStages; the copies
+        // of rounds r+1 .. r+kRingStages-1 are in flight while r is reduced
+        uint32_t* mine = ring + (static_cast<size_t>(warp) * kRingStages * 32 + lane) * kItemsPerThread;
+        const uint32_t rs0 = w_lo & ~3u;
+        const uint32_t round_len = 32 * kItemsPerThread;
+        const uint32_t nrounds = w_hi > rs0 ? (w_hi - rs0 + round_len - 1) / round_len : 0;
+        auto issue = [&](uint32_t r) {
+            const uint32_t ef = rs0 + r * round_len + lane * kItemsPerThread;
+            if (r < nrounds && lane_full(ef, w_lo, w_hi)) {
+                uint32_t* d = mine + (r % kRingStages) * 32 * kItemsPerThread;
+#pragma unroll
+                for (int q = 0; q < kLaneVecs; q++) cp_async16(d + 4 * q, g32 + ef + 4 * q);
+            }
+            cp_async_commit();
+        };
+#pragma unroll
+        for (int j = 0; j < kRingStages - 1; j++) issue(j);
+        for (uint32_t r = 0; r < nrounds; r++) {
+            issue(r + kRingStages - 1);
+            cp_async_wait<kRingStages - 1>();
+            const uint32_t rs = rs0 + r * round_len;
+            const bool full = lane_full(rs + lane * kItemsPerThread, w_lo, w_hi);
+            uint4 cur[kLaneVecs];
+            if (full) {
+                const uint4* src = reinterpret_cast<const uint4*>(mine + (r % kRingStages) * 32 * kItemsPerThread);
+#pragma unroll
+                for (int q = 0; q < kLaneVecs; q++) cur[q] = src[q];
+            }
+            warp_round<T>(g32, rs, w_lo, w_hi, c0, ytile, acc, carry, rec, cur, full);
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        if (warp == 0) {
+            const WarpRec<T> r = recs[lane];
+            const bool single = r.fc == r.lc;
+            lane_chain<T>(r.valid != 0, single, r.cp != 0, r.cn != 0, r.fc, r.lc, r.fs, single ? r.fs : r.ls, T(0),
+                          [&](int col, T val) { acc[col] += val; });
+        }
+        return;
+    }
+    uint32_t rs = w_lo & ~3u;
+    uint4 cur[kLaneVecs], nxt[kLaneVecs];
+    bool cur_full = rs < w_hi && lane_full(rs + lane * kItemsPerThread, w_lo, w_hi);
+    if (cur_full) load_lane(g32, rs + lane * kItemsPerThread, cur);
+    for (; rs < w_hi; rs += 32 * kItemsPerThread) {
+        // the next round's entries are loaded while this round is reduced
+        const uint32_t rn = rs + 32 * kItemsPerThread;
+        const bool nxt_full = rn < w_hi && lane_full(rn + lane * kItemsPerThread, w_lo, w_hi);
+        if (nxt_full) load_lane(g32, rn + lane * kItemsPerThread, nxt);
+        warp_round<T>(g32, rs, w_lo, w_hi, c0, ytile, acc, carry, rec, cur, cur_full);
+#pragma unroll
+        for (int q = 0; q < kLaneVecs; q++) cur[q] = nxt[q];
+        cur_full = nxt_full;
     }
     __syncthreads();
     if (warp == 0) {
-        // same scan over the warp aggregates, seeded with the round's carry
-        constexpr int kWarps = kFastThreads / 32;
-        T wv = lane < kWarps ? ss.warp_v[lane] : T(0);
-        bool wf = lane < kWarps ? ss.warp_f[lane] != 0 : true;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const T vu = __shfl_up_sync(0xffffffffu, wv, d);
-            const bool fu = __shfl_up_sync(0xffffffffu, wf, d);
-            if (lane >= d) {
-                if (!wf) wv += vu;
-                wf = wf || fu;
-            }
-        }
-        const T carry = ss.carry;
-        const T incl = wf ? wv : wv + carry;  // chain value at the end of warp `lane`
-        T excl = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) excl = carry;
-        if (lane < kWarps) ss.warp_excl[lane] = excl;
-        if (lane == kWarps - 1) ss.carry = incl;  // open chain leaving the round
+        const WarpRec<T> r = recs[lane];
+        const bool single = r.fc == r.lc;
+        lane_chain<T>(r.valid != 0, single, r.cp != 0, r.cn != 0, r.fc, r.lc, r.fs, single ? r.fs : r.ls, T(0),
+                      [&](int col, T val) { acc[col] += val; });
     }
-    __syncthreads();
-    const T excl_w = ss.warp_excl[warp];
-    const T X = f ? v : v + excl_w;  // chain value ending at this thread
-    T Xprev = __shfl_up_sync(0xffffffffu, X, 1);
-    if (lane == 0) Xprev = excl_w;
-    if (any) {
-        if (single) {
-            if (!cont_next) acc[hc] += X;
-        } else {
-            acc[hc] += cont_prev ? Xprev + hs : hs;
-            if (!cont_next) acc[tc] += ts;
-        }
-    }
-    __syncthreads();
 }
 
-template <typename T>
+// One work item: the partial column sums of super-chunk item_sc[item] over
+// the blocks [item_b0, item_b1), written to partial + item_part[item] -
+// item_part[item_base].
+template <typename T, bool RING>
+__device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv, const uint32_t* __restrict__ g32,
+                                         const uint32_t* __restrict__ chunk_start, const T* __restrict__ y,
+                                         T* __restrict__ partial, int item, int item_base, int64_t y_block0,
+                                         T* __restrict__ acc, T* __restrict__ ytile, uint32_t* __restrict__ ring,
+                                         WarpRec<T> (*recs)[kFastThreads / 32])
+{
+    const int sc = tv.item_sc[item];
+    const int pc0 = tv.sc_piece0[sc], pc1 = tv.sc_piece0[sc + 1];
+    const int width = tv.sc_width[sc];
+    for (int i = threadIdx.x; i < width; i += kFastThreads) acc[i] = 0;
+    int flip = 0;
+    for (int64_t blk = tv.item_b0[item]; blk < tv.item_b1[item]; blk++) {
+        const int nb = static_cast<int>(g.block_rows(blk));
+        __syncthreads();
+        const T* yb = y + (blk - y_block0) * kBlockRows;
+        if ((reinterpret_cast<uintptr_t>(yb) & 15) == 0) {
+            constexpr int kPer = 16 / sizeof(T);
+            const int nvec = nb / kPer;
+            for (int i = threadIdx.x; i < nvec; i += kFastThreads)
+                reinterpret_cast<uint4*>(ytile)[i] = __ldg(reinterpret_cast<const uint4*>(yb) + i);
+            for (int i = nvec * kPer + threadIdx.x; i < nb; i += kFastThreads) ytile[i] = yb[i];
+        } else {
+            for (int i = threadIdx.x; i < nb; i += kFastThreads) ytile[i] = yb[i];
+        }
+        __syncthreads();
+        for (int pc = pc0; pc < pc1; pc++) {
+            const int p = tv.piece_pat[pc];
+            const int ch0 = tv.piece_ch0[pc], ch1 = tv.piece_ch1[pc];
+            const int pat_end = p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks;
+            const uint32_t e_lo = chunk_start[blk * g.nchunks + ch0];
+            const uint32_t e_hi = ch1 < pat_end ? chunk_start[blk * g.nchunks + ch1]
+                                                : static_cast<uint32_t>(g.seg(blk, p) + g.seg_len(blk, p));
+            const uint32_t c0 = static_cast<uint32_t>(ch0 - g.chunk0[p]) * kChunkCols;
+            reduce_block_entries<T, RING>(g32, e_lo, e_hi, c0, ytile, acc + tv.piece_acc[pc], recs[flip], ring);
+            flip ^= 1;
+        }
+    }
+    __syncthreads();
+    T* out = partial + (tv.item_part[item] - tv.item_part[item_base]);
+    for (int i = threadIdx.x; i < width; i += kFastThreads) out[i] = acc[i];
+}
+
+// A'y over a work list.  With ctr (persistent schedule: one CTA per SM) the
+// CTAs take items in order from the counter ctr[0] until the list is done,
+// so no SM idles while items of uneven duration remain; which CTA runs an
+// item does not change its output, so results stay bitwise reproducible.
+// The last CTA to finish resets the counters for the next launch (launches
+// on one work list must therefore be stream-ordered).  Without ctr, CTA i
+// runs item item_base + i.
+template <typename T, bool RING>
 __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeometry g, TView tv,
                                                                        const uint32_t* __restrict__ g32,
                                                                        const uint32_t* __restrict__ chunk_start,
                                                                        const T* __restrict__ y,
                                                                        T* __restrict__ partial,
                                                                        const int* __restrict__ done, int item_base,
-                                                                       int64_t y_block0)
+                                                                       int64_t y_block0, int* __restrict__ ctr)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ SegSmem<T> ss;
+    // two record sets, alternating per piece: warp 0 may still combine one
+    // piece's records while the other warps start on the next piece
+    __shared__ WarpRec<T> recs[2][kFastThreads / 32];
+    __shared__ int s_item;
     if (done && *(volatile const int*)done) return;
-    const int width_max = kChunkCols * tv.per_sc;
     T* acc = reinterpret_cast<T*>(smem_raw);
-    T* ytile = acc + width_max;
-    const int item = blockIdx.x + item_base;
-    const int sc = tv.item_sc[item];
-    int p = 0;
-    while (p + 1 < g.npat && tv.sc_base[p + 1] <= sc) p++;
-    const int pat_chunks = (p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks) - g.chunk0[p];
-    const int ch0_local = (sc - tv.sc_base[p]) * tv.per_sc;
-    const int ch1_local = min(ch0_local + tv.per_sc, pat_chunks);
-    const int ch0 = g.chunk0[p] + ch0_local;
-    const uint32_t c0 = static_cast<uint32_t>(ch0_local) * kChunkCols;
-    const int width = min(g.space[p], ch1_local * kChunkCols) - static_cast<int>(c0);
-    for (int i = threadIdx.x; i < width; i += kFastThreads) acc[i] = 0;
-    for (int64_t blk = tv.item_b0[item]; blk < tv.item_b1[item]; blk++) {
-        const int nb = static_cast<int>(g.block_rows(blk));
-        __syncthreads();
-        const T* yb = y + (blk - y_block0) * kBlockRows;
-        for (int i = threadIdx.x; i < nb; i += kFastThreads) ytile[i] = yb[i];
-        if (threadIdx.x == 0) ss.carry = 0;
-        __syncthreads();
-        const uint32_t e_lo = chunk_start[blk * g.nchunks + ch0];
-        const uint32_t e_hi = ch1_local < pat_chunks
-                                  ? chunk_start[blk * g.nchunks + g.chunk0[p] + ch1_local]
-                                  : static_cast<uint32_t>(g.seg(blk, p) + g.seg_len(blk, p));
-        for (uint32_t rs = e_lo & ~3u; rs < e_hi; rs += kFastThreads * kItemsPerThread)
-            seg_round<T>(g32, rs, e_lo, e_hi, c0, ytile, acc, ss);
+    T* ytile = acc + kChunkCols * tv.per_sc;
+    uint32_t* ring = reinterpret_cast<uint32_t*>(ytile + kBlockRows);  // RING schedules only
+    if (!ctr) {
+        aty_item<T, RING>(g, tv, g32, chunk_start, y, partial, blockIdx.x + item_base, item_base, y_block0, acc, ytile,
+                          ring, recs);
+        return;
     }
-    __syncthreads();
-    T* out = partial + (tv.item_part[item] - tv.item_part[item_base]);
-    for (int i = threadIdx.x; i < width; i += kFastThreads) out[i] = acc[i];
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(ctr, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= tv.nitems) break;
+        aty_item<T, RING>(g, tv, g32, chunk_start, y, partial, item, 0, 0, acc, ytile, ring, recs);
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(ctr + 1, 1) == static_cast<int>(gridDim.x) - 1) {
+            ctr[0] = 0;
+            ctr[1] = 0;
+            __threadfence();
+        }
+    }
 }
 
 // Evaluator forward on a row range: score[r - row0] = sum_j w[col_rj], one
@@ -671,46 +906,115 @@ __global__ void fast_col_sum_kernel(FastCols fc, const T* __restrict__ partial, 
         x[c] = static_cast<T>(fast_col_sum<T>(fc, partial, c));
 }
 
+// Device copy of a host int vector (at least one element allocated).
+template <typename V>
+cas_status upload(const std::vector<V>& h, V** d)
+{
+    CAS_CUDA(cudaMalloc(d, sizeof(V) * std::max<size_t>(h.size(), 1)));
+    if (!h.empty()) CAS_CUDA(cudaMemcpy(*d, h.data(), sizeof(V) * h.size(), cudaMemcpyHostToDevice));
+    return CAS_OK;
+}
+
+// Columns of a global chunk (the last chunk of a pattern may be partial).
+int chunk_width(const FastGeometry& g, int ch)
+{
+    int p = 0;
+    while (p + 1 < g.npat && g.chunk0[p + 1] <= ch) p++;
+    return std::min(kChunkCols, g.space[p] - (ch - g.chunk0[p]) * kChunkCols);
+}
+
+int pattern_of_chunk(const FastGeometry& g, int ch)
+{
+    int p = 0;
+    while (p + 1 < g.npat && g.chunk0[p + 1] <= ch) p++;
+    return p;
+}
+
+// Super-chunk pieces, host side.
+struct Pieces {
+    std::vector<int> sc_piece0, sc_width, pat, ch0, ch1, acc, chunk_sc, chunk_acc;
+};
+
+// Packs the chunks, in pattern order, into accumulators of cap columns: a
+// chunk joins the current super-chunk while it fits, and consecutive chunks
+// of one pattern in one super-chunk form one piece.
+Pieces pack_chunks(const FastGeometry& g, int cap, bool across_patterns)
+{
+    Pieces pc;
+    pc.chunk_sc.resize(g.nchunks);
+    pc.chunk_acc.resize(g.nchunks);
+    int w = 0;
+    for (int ch = 0; ch < g.nchunks; ch++) {
+        const int p = pattern_of_chunk(g, ch);
+        const int cw = chunk_width(g, ch);
+        const bool new_pattern = !pc.pat.empty() && pc.pat.back() != p;
+        if (pc.sc_piece0.empty() || w + cw > cap || (new_pattern && !across_patterns)) {
+            if (!pc.sc_piece0.empty()) pc.sc_width.push_back(w);
+            pc.sc_piece0.push_back(static_cast<int>(pc.pat.size()));
+            w = 0;
+        }
+        const bool extend = !pc.pat.empty() && pc.sc_piece0.back() < static_cast<int>(pc.pat.size()) &&
+                            pc.pat.back() == p && pc.ch1.back() == ch;
+        if (extend) {
+            pc.ch1.back() = ch + 1;
+        } else {
+            pc.pat.push_back(p);
+            pc.ch0.push_back(ch);
+            pc.ch1.push_back(ch + 1);
+            pc.acc.push_back(w);
+        }
+        pc.chunk_sc[ch] = static_cast<int>(pc.sc_piece0.size()) - 1;
+        pc.chunk_acc[ch] = w;
+        w += cw;
+    }
+    if (!pc.sc_piece0.empty()) pc.sc_width.push_back(w);
+    pc.sc_piece0.push_back(static_cast<int>(pc.pat.size()));
+    return pc;
+}
+
+cas_status upload_pieces(const Pieces& pc, FastTranspose& t)
+{
+    t.nsc = static_cast<int>(pc.sc_width.size());
+    t.npieces = static_cast<int>(pc.pat.size());
+    CAS_TRY(upload(pc.sc_piece0, &t.sc_piece0));
+    CAS_TRY(upload(pc.sc_width, &t.sc_width));
+    CAS_TRY(upload(pc.pat, &t.piece_pat));
+    CAS_TRY(upload(pc.ch0, &t.piece_ch0));
+    CAS_TRY(upload(pc.ch1, &t.piece_ch1));
+    CAS_TRY(upload(pc.acc, &t.piece_acc));
+    CAS_TRY(upload(pc.chunk_sc, &t.chunk_sc));
+    CAS_TRY(upload(pc.chunk_acc, &t.chunk_acc));
+    return CAS_OK;
+}
+
 // Builds the work list of one A'y variant from the entry counts per (block,
-// chunk): super-chunks of per_sc chunks, each split into block ranges so that
-// items carry about equal numbers of entries.
-cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entries_bc, int per_sc, size_t elem,
-                       FastTranspose& t)
+// chunk): super-chunks of at most per_sc chunks of columns, each split into
+// block ranges so that items carry about equal numbers of entries.
+cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entries_bc, int per_sc, int items_per_sm,
+                       bool ring, bool pack, bool persistent, size_t elem, FastTranspose& t)
 {
     t.per_sc = per_sc;
-    std::vector<int> sc_pat;
-    int nsc = 0;
-    for (int p = 0; p < g.npat; p++) {
-        t.sc_base[p] = nsc;
-        const int pch = (p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks) - g.chunk0[p];
-        const int n = (pch + per_sc - 1) / per_sc;
-        for (int i = 0; i < n; i++) sc_pat.push_back(p);
-        nsc += n;
-    }
-    t.sc_base[g.npat] = nsc;
-    t.nsc = nsc;
-    // entries per super-chunk
+    t.ring = ring;
+    t.items_per_sm = items_per_sm;
+    t.pack = pack;
+    t.persistent = persistent;
+    const Pieces pc = pack_chunks(g, per_sc * kChunkCols, pack);
+    CAS_TRY(upload_pieces(pc, t));
+    const int nsc = t.nsc;
     std::vector<int64_t> sc_entries(nsc, 0);
     int64_t total = 0;
     for (int64_t b = 0; b < g.nblocks; b++)
         for (int ch = 0; ch < g.nchunks; ch++) {
-            int p = 0;
-            while (p + 1 < g.npat && g.chunk0[p + 1] <= ch) p++;
-            const int sc = t.sc_base[p] + (ch - g.chunk0[p]) / per_sc;
-            sc_entries[sc] += entries_bc[b * g.nchunks + ch];
+            sc_entries[pc.chunk_sc[ch]] += entries_bc[b * g.nchunks + ch];
             total += entries_bc[b * g.nchunks + ch];
         }
-    const int64_t target_items = static_cast<int64_t>(sm_count()) * 2;
+    const int64_t target_items = static_cast<int64_t>(sm_count()) * items_per_sm;
     const double per_item = std::max<double>(1.0, static_cast<double>(total) / target_items);
     std::vector<int> item_sc, item_b0, item_b1, sc_item0;
     std::vector<int64_t> item_part;
     int64_t part_elems = 0;
     for (int sc = 0; sc < nsc; sc++) {
         sc_item0.push_back(static_cast<int>(item_sc.size()));
-        const int p = sc_pat[sc];
-        const int pch = (p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks) - g.chunk0[p];
-        const int c0l = (sc - t.sc_base[p]) * per_sc;
-        const int width = std::min<int>(g.space[p], std::min(c0l + per_sc, pch) * kChunkCols) - c0l * kChunkCols;
         int64_t n = static_cast<int64_t>(std::llround(sc_entries[sc] / per_item));
         n = std::max<int64_t>(1, std::min<int64_t>(n, g.nblocks));
         for (int64_t i = 0; i < n; i++) {
@@ -718,56 +1022,59 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
             item_b0.push_back(static_cast<int>(g.nblocks * i / n));
             item_b1.push_back(static_cast<int>(g.nblocks * (i + 1) / n));
             item_part.push_back(part_elems);
-            part_elems += width;
+            part_elems += pc.sc_width[sc];
         }
     }
     sc_item0.push_back(static_cast<int>(item_sc.size()));
     t.nitems = static_cast<int>(item_sc.size());
-    CAS_CUDA(cudaMalloc(&t.item_sc, sizeof(int) * t.nitems));
-    CAS_CUDA(cudaMalloc(&t.item_b0, sizeof(int) * t.nitems));
-    CAS_CUDA(cudaMalloc(&t.item_b1, sizeof(int) * t.nitems));
-    CAS_CUDA(cudaMalloc(&t.item_part, sizeof(int64_t) * t.nitems));
-    CAS_CUDA(cudaMalloc(&t.sc_item0, sizeof(int) * (nsc + 1)));
+    CAS_TRY(upload(item_sc, &t.item_sc));
+    CAS_TRY(upload(item_b0, &t.item_b0));
+    CAS_TRY(upload(item_b1, &t.item_b1));
+    CAS_TRY(upload(item_part, &t.item_part));
+    CAS_TRY(upload(sc_item0, &t.sc_item0));
     CAS_CUDA(cudaMalloc(&t.partial, elem * std::max<int64_t>(part_elems, 1)));
-    CAS_CUDA(cudaMemcpy(t.item_sc, item_sc.data(), sizeof(int) * t.nitems, cudaMemcpyHostToDevice));
-    CAS_CUDA(cudaMemcpy(t.item_b0, item_b0.data(), sizeof(int) * t.nitems, cudaMemcpyHostToDevice));
-    CAS_CUDA(cudaMemcpy(t.item_b1, item_b1.data(), sizeof(int) * t.nitems, cudaMemcpyHostToDevice));
-    CAS_CUDA(cudaMemcpy(t.item_part, item_part.data(), sizeof(int64_t) * t.nitems, cudaMemcpyHostToDevice));
-    CAS_CUDA(cudaMemcpy(t.sc_item0, sc_item0.data(), sizeof(int) * (nsc + 1), cudaMemcpyHostToDevice));
+    CAS_CUDA(cudaMalloc(&t.ctr, sizeof(int) * 2));
+    CAS_CUDA(cudaMemset(t.ctr, 0, sizeof(int) * 2));
     return CAS_OK;
 }
 
 // Work list of one item per (block, chunk), block-major, for adjoints over a
-// block range (minibatches): item b * nchunks + ch; partial offsets give the
-// layout [block][global column] relative to the first item of the range.
+// block range (minibatches): item b * nchunks + ch, one piece per chunk;
+// partial offsets give the layout [block][global column] relative to the
+// first item of the range.
 cas_status build_block_items(const FastGeometry& g, FastTranspose& t)
 {
     t.per_sc = 1;
-    for (int p = 0; p < g.npat; p++) t.sc_base[p] = g.chunk0[p];
-    t.sc_base[g.npat] = g.nchunks;
-    t.nsc = g.nchunks;
+    Pieces pc;
+    for (int ch = 0; ch < g.nchunks; ch++) {
+        pc.sc_piece0.push_back(ch);
+        pc.sc_width.push_back(chunk_width(g, ch));
+        pc.pat.push_back(pattern_of_chunk(g, ch));
+        pc.ch0.push_back(ch);
+        pc.ch1.push_back(ch + 1);
+        pc.acc.push_back(0);
+        pc.chunk_sc.push_back(ch);
+        pc.chunk_acc.push_back(0);
+    }
+    pc.sc_piece0.push_back(g.nchunks);
+    CAS_TRY(upload_pieces(pc, t));
     const int64_t n = g.nblocks * g.nchunks;
     t.nitems = static_cast<int>(n);
     std::vector<int> isc(n), ib0(n), ib1(n);
     std::vector<int64_t> ipart(n);
     for (int64_t b = 0; b < g.nblocks; b++)
         for (int ch = 0; ch < g.nchunks; ch++) {
-            int p = 0;
-            while (p + 1 < g.npat && g.chunk0[p + 1] <= ch) p++;
+            const int p = pattern_of_chunk(g, ch);
             const int64_t i = b * g.nchunks + ch;
             isc[i] = ch;
             ib0[i] = static_cast<int>(b);
             ib1[i] = static_cast<int>(b + 1);
             ipart[i] = b * g.cols + g.off[p] + static_cast<int64_t>(ch - g.chunk0[p]) * kChunkCols;
         }
-    CAS_CUDA(cudaMalloc(&t.item_sc, sizeof(int) * n));
-    CAS_CUDA(cudaMalloc(&t.item_b0, sizeof(int) * n));
-    CAS_CUDA(cudaMalloc(&t.item_b1, sizeof(int) * n));
-    CAS_CUDA(cudaMalloc(&t.item_part, sizeof(int64_t) * n));
-    CAS_CUDA(cudaMemcpy(t.item_sc, isc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CAS_CUDA(cudaMemcpy(t.item_b0, ib0.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CAS_CUDA(cudaMemcpy(t.item_b1, ib1.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CAS_CUDA(cudaMemcpy(t.item_part, ipart.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
+    CAS_TRY(upload(isc, &t.item_sc));
+    CAS_TRY(upload(ib0, &t.item_b0));
+    CAS_TRY(upload(ib1, &t.item_b1));
+    CAS_TRY(upload(ipart, &t.item_part));
     return CAS_OK;
 }
 
@@ -779,7 +1086,13 @@ TView tview(const FastTranspose& t)
     v.item_b0 = t.item_b0;
     v.item_b1 = t.item_b1;
     v.item_part = t.item_part;
-    for (int i = 0; i <= kMaxFastPatterns; i++) v.sc_base[i] = t.sc_base[i];
+    v.sc_piece0 = t.sc_piece0;
+    v.sc_width = t.sc_width;
+    v.piece_pat = t.piece_pat;
+    v.piece_ch0 = t.piece_ch0;
+    v.piece_ch1 = t.piece_ch1;
+    v.piece_acc = t.piece_acc;
+    v.nitems = t.nitems;
     return v;
 }
 
@@ -790,19 +1103,18 @@ const FastTranspose& transpose_of(const FastLayout& f)
 }
 
 template <typename T>
-size_t spmv_t_smem(const FastTranspose& t)
+size_t spmv_t_smem(int per_sc, bool ring)
 {
-    return sizeof(T) * (static_cast<size_t>(kChunkCols) * t.per_sc + kBlockRows);
+    return sizeof(T) * (static_cast<size_t>(kChunkCols) * per_sc + kBlockRows) + (ring ? kRingBytes : 0);
 }
 
 void free_transpose(FastTranspose& t)
 {
-    cudaFree(t.item_sc);
-    cudaFree(t.item_b0);
-    cudaFree(t.item_b1);
-    cudaFree(t.item_part);
-    cudaFree(t.sc_item0);
-    cudaFree(t.partial);
+    for (void* ptr : {(void*)t.sc_piece0, (void*)t.sc_width, (void*)t.piece_pat, (void*)t.piece_ch0,
+                      (void*)t.piece_ch1, (void*)t.piece_acc, (void*)t.chunk_sc, (void*)t.chunk_acc,
+                      (void*)t.item_sc, (void*)t.item_b0, (void*)t.item_b1, (void*)t.item_part, (void*)t.sc_item0,
+                      t.partial, (void*)t.ctr})
+        cudaFree(ptr);
     t = FastTranspose{};
 }
 
@@ -811,8 +1123,9 @@ void free_transpose(FastTranspose& t)
 cas_status fast_set_attributes()
 {
     const int s32 = static_cast<int>(sizeof(float) * kTable32), s64 = static_cast<int>(sizeof(double) * kTable64);
-    const int t32 = static_cast<int>(sizeof(float) * (static_cast<size_t>(kChunkCols) * 4 + kBlockRows));
-    const int t64 = static_cast<int>(sizeof(double) * (static_cast<size_t>(kChunkCols) * 1 + kBlockRows));
+    const int t32 = static_cast<int>(spmv_t_smem<float>(kMaxScRegs, false));
+    const int t32r = static_cast<int>(spmv_t_smem<float>(kMaxScRing, true));
+    const int t64 = static_cast<int>(spmv_t_smem<double>(1, false));
     const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 0, true>, attr, s32));
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 0, false>, attr, s32));
@@ -832,9 +1145,123 @@ cas_status fast_set_attributes()
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 1, false>, attr, s64));
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 2, true>, attr, s64));
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 2, false>, attr, s64));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<float>, attr, t32));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<double>, attr, t64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<float, false>, attr, t32));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<float, true>, attr, t32r));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<double, false>, attr, t64));
     return CAS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Build-time autotuner of the FP32 A'y schedule.  Every candidate work list
+// is built and timed (partials + column sums, CUDA events, one warm-up
+// launch) on this layout; the fastest is kept and remembered per geometry
+// for the rest of the process, so later builds of the same shape skip the
+// timing.  CAS_ATY_SCHEDULE="chunks,ring,items_per_sm,pack,persistent"
+// forces a schedule.
+// ---------------------------------------------------------------------------
+struct Sched {
+    int per_sc;
+    bool ring;
+    int ips;
+    bool pack;
+    bool persistent;
+};
+constexpr Sched kSchedDefault = {4, false, 2, false, false};
+constexpr Sched kSchedCandidates[] = {
+    {4, false, 2, false, false}, {4, false, 3, false, false}, {3, false, 2, false, false},
+    {4, false, 2, true, false},  {4, false, 2, true, true},   {4, false, 4, true, true},
+    {4, false, 4, false, true},  {2, false, 2, true, false},  {2, true, 3, true, false},
+    {2, true, 4, true, true},    {2, true, 2, false, false},  {4, false, 6, false, true}};
+static_assert(sizeof(kSchedCandidates) / sizeof(Sched) <= kMaxTune, "tune table");
+constexpr int64_t kTuneMinBlocks = 64;  // smaller layouts take the default schedule
+
+std::mutex g_tune_mu;
+std::map<std::string, Sched> g_tune_cache;
+
+std::string tune_key(const FastGeometry& g)
+{
+    std::string k = std::to_string(g.k) + "/" + std::to_string(g.nblocks) + "/" + std::to_string(g.rows);
+    for (int p = 0; p < g.npat; p++) k += "/" + std::to_string(g.space[p]) + "x" + std::to_string(g.slots[p]);
+    return k;
+}
+
+bool valid_sched(const Sched& c)
+{
+    return c.per_sc >= 1 && c.per_sc <= (c.ring ? kMaxScRing : kMaxScRegs) && c.ips >= 1 && c.ips <= 16;
+}
+
+cas_status tune_transpose(FastLayout& f, const std::vector<int64_t>& entries, cudaStream_t s)
+{
+    const FastGeometry& g = f.g;
+    f.ntune = 0;
+    f.tune_cached = 0;
+    auto build = [&](const Sched& c) {
+        return build_items(g, entries, c.per_sc, c.ips, c.ring, c.pack, c.persistent, sizeof(float), f.t32);
+    };
+    if (const char* env = std::getenv("CAS_ATY_SCHEDULE")) {
+        int a = 0, b = 0, c = 0, d = 0, e = 0;
+        const int n = std::sscanf(env, "%d,%d,%d,%d,%d", &a, &b, &c, &d, &e);
+        const Sched forced{a, b != 0, c, d != 0, e != 0};
+        CAS_REQUIRE(n == 5 && valid_sched(forced), CAS_ERR_INVALID_ARGUMENT,
+                    "CAS_ATY_SCHEDULE must be \"chunks,ring,items_per_sm,pack,persistent\" within limits");
+        return build(forced);
+    }
+    if (g.nblocks < kTuneMinBlocks) return build(kSchedDefault);
+    const std::string key = tune_key(g);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            f.tune_cached = 1;
+            return build(it->second);
+        }
+    }
+    float* y = nullptr;
+    float* x = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cas_status st = CAS_OK;
+    auto fail = [&](cudaError_t e) {
+        if (e != cudaSuccess && st == CAS_OK) {
+            set_error(std::string("autotuner: ") + cudaGetErrorString(e));
+            st = CAS_ERR_CUDA;
+        }
+    };
+    fail(cudaMalloc(&y, sizeof(float) * g.rows));
+    fail(cudaMalloc(&x, sizeof(float) * std::max<int64_t>(g.cols, 1)));
+    fail(cudaEventCreate(&e0));
+    fail(cudaEventCreate(&e1));
+    if (st == CAS_OK) fail(cudaMemsetAsync(y, 0, sizeof(float) * g.rows, s));
+    Sched best = kSchedDefault;
+    float best_ms = 1e30f;
+    for (const Sched& c : kSchedCandidates) {
+        if (st != CAS_OK) break;
+        st = build(c);
+        if (st == CAS_OK) st = fast_spmv_t<float>(f, y, x, s);  // warm-up
+        if (st == CAS_OK) fail(cudaEventRecord(e0, s));
+        for (int r = 0; r < 2 && st == CAS_OK; r++) st = fast_spmv_t<float>(f, y, x, s);
+        if (st == CAS_OK) fail(cudaEventRecord(e1, s));
+        if (st == CAS_OK) fail(cudaEventSynchronize(e1));
+        float ms = 0;
+        if (st == CAS_OK) fail(cudaEventElapsedTime(&ms, e0, e1));
+        free_transpose(f.t32);
+        if (st != CAS_OK) break;
+        ms *= 0.5f;
+        f.tune[f.ntune++] = FastTuneEntry{c.per_sc, c.ring ? 1 : 0, c.ips, c.pack ? 1 : 0, c.persistent ? 1 : 0, ms};
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    cudaFree(y);
+    cudaFree(x);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st != CAS_OK) return st;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = best;
+    }
+    return build(best);
 }
 
 }  // namespace
@@ -865,6 +1292,7 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
                       uint64_t* diag_int, FastLayout& f, cudaStream_t s)
 {
     CAS_REQUIRE(fast_supported(ps), CAS_ERR_INVALID_ARGUMENT, "pattern set does not fit the blocked layout");
+    CAS_TRY(fast_set_attributes());
     FastGeometry& g = f.g;
     g = FastGeometry{};
     g.npat = static_cast<int>(ps.indexers.size());
@@ -883,6 +1311,8 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
         chunk += (g.space[p] + kChunkCols - 1) / kChunkCols;
     }
     g.nchunks = chunk;
+    CAS_REQUIRE(g.total_elems() < 0xFFFFFFFFLL, CAS_ERR_INVALID_ARGUMENT,
+                "blocked layout: 2^32 or more entries (with block padding) are not supported");
     const int64_t elems = std::max<int64_t>(g.total_elems(), 8);
     CAS_CUDA(cudaMalloc(&f.a16, sizeof(uint16_t) * elems));
     CAS_CUDA(cudaMalloc(&f.g32, sizeof(uint32_t) * elems));
@@ -926,11 +1356,11 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
             }
         }
     if (g.nblocks > 0) {
-        CAS_TRY(build_items(g, entries, 4, sizeof(float), f.t32));
-        CAS_TRY(build_items(g, entries, 1, sizeof(double), f.t64));
+        CAS_TRY(tune_transpose(f, entries, s));
+        CAS_TRY(build_items(g, entries, 1, 2, false, true, false, sizeof(double), f.t64));
         CAS_TRY(build_block_items(g, f.tb));
     }
-    return fast_set_attributes();
+    return CAS_OK;
 }
 
 cas_status fast_diag(const FastLayout& f, uint64_t* diag, cudaStream_t s)
@@ -972,9 +1402,21 @@ cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag,
 {
     const FastTranspose& t = transpose_of<T>(f);
     if (t.nitems == 0) return CAS_OK;
-    const size_t smem = spmv_t_smem<T>(t);
-    { fast_spmv_t_kernel<T><<<t.nitems, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.chunk_start, y,
-                                                                static_cast<T*>(t.partial), done_flag, 0, 0); cas::count_launch(); }
+    const size_t smem = spmv_t_smem<T>(t.per_sc, t.ring);
+    const unsigned grid = static_cast<unsigned>(t.persistent ? std::min(t.nitems, sm_count()) : t.nitems);
+    int* ctr = t.persistent ? t.ctr : nullptr;
+    if constexpr (sizeof(T) == 4) {
+        if (t.ring) {
+            { fast_spmv_t_kernel<T, true><<<grid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.chunk_start, y,
+                                                                        static_cast<T*>(t.partial), done_flag, 0, 0,
+                                                                        ctr); cas::count_launch(); }
+            CAS_CHECK_LAUNCH();
+            return CAS_OK;
+        }
+    }
+    { fast_spmv_t_kernel<T, false><<<grid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.chunk_start, y,
+                                                                 static_cast<T*>(t.partial), done_flag, 0, 0,
+                                                                 ctr); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     return CAS_OK;
 }
@@ -985,10 +1427,10 @@ FastCols fast_cols(const FastLayout& f)
     const FastTranspose& t = transpose_of<T>(f);
     FastCols c;
     c.g = f.g;
-    c.per_sc = t.per_sc;
+    c.chunk_sc = t.chunk_sc;
+    c.chunk_acc = t.chunk_acc;
     c.sc_item0 = t.sc_item0;
     c.item_part = t.item_part;
-    for (int i = 0; i <= kMaxFastPatterns; i++) c.sc_base[i] = t.sc_base[i];
     return c;
 }
 
@@ -1033,11 +1475,11 @@ cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float
         CAS_CUDA(cudaMalloc(&f.eval_partial, sizeof(float) * nb * f.g.cols));
         f.eval_blocks = nb;
     }
-    const size_t smem = sizeof(float) * (static_cast<size_t>(kChunkCols) + kBlockRows);
+    const size_t smem = spmv_t_smem<float>(1, false);
     const int items = static_cast<int>(nb * f.g.nchunks);
-    { fast_spmv_t_kernel<float><<<items, kFastThreads, smem, s>>>(f.g, tview(f.tb), f.g32, f.chunk_start, g,
+    { fast_spmv_t_kernel<float, false><<<items, kFastThreads, smem, s>>>(f.g, tview(f.tb), f.g32, f.chunk_start, g,
                                                                  f.eval_partial, nullptr,
-                                                                 static_cast<int>(b0 * f.g.nchunks), b0); cas::count_launch(); }
+                                                                 static_cast<int>(b0 * f.g.nchunks), b0, nullptr); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     { block_partial_sum_kernel<<<fgrid(f.g.cols, 256), 256, 0, s>>>(f.eval_partial, static_cast<int>(nb), f.g.cols,
                                                                   grad); cas::count_launch(); }

@@ -62,25 +62,55 @@ struct FastGeometry {
     }
 };
 
-// Work list of one A'y variant: a "super-chunk" is up to `per_sc` consecutive
-// chunks of one pattern; an item is (super-chunk, block range).  Every item
-// writes the partial sums of its super-chunk's columns; a column's value is
-// the sum of its super-chunk's items in item order.
+// Work list of one A'y variant.  Columns are grouped into "super-chunks":
+// sets of column pieces (whole 8192-column chunks of one pattern, or a
+// pattern's last partial chunk) packed into one shared-memory accumulator of
+// per_sc chunks, so several narrow patterns share one pass over a block's y
+// slice.  An item is (super-chunk, block range); every item writes the
+// partial sums of its super-chunk's columns, and a column's value is the sum
+// of its super-chunk's items in item order.
 struct FastTranspose {
-    int per_sc = 1;        // chunks per super-chunk
+    int per_sc = 1;        // accumulator capacity in chunks
+    bool ring = false;     // FP32 only: entries streamed through a cp.async ring in shared memory
+    int items_per_sm = 2;  // work items per SM the entries are balanced over
+    bool pack = true;      // super-chunks may hold pieces of several patterns
+    bool persistent = false;  // one CTA per SM taking items from a counter (else one CTA per item)
     int nsc = 0;
+    int npieces = 0;
     int nitems = 0;
-    int sc_base[kMaxFastPatterns + 1];  // first super-chunk of each pattern
-    int* item_sc = nullptr;             // [nitems]
-    int* item_b0 = nullptr;             // [nitems]
-    int* item_b1 = nullptr;             // [nitems]
-    int64_t* item_part = nullptr;       // [nitems] offset of the item's partials
-    int* sc_item0 = nullptr;            // [nsc + 1] first item of each super-chunk
-    void* partial = nullptr;            // float or double partials
+    int* sc_piece0 = nullptr;  // [nsc + 1] first piece of each super-chunk
+    int* sc_width = nullptr;   // [nsc] accumulator columns in use
+    int* piece_pat = nullptr;  // [npieces] pattern of the piece
+    int* piece_ch0 = nullptr;  // [npieces] first global chunk
+    int* piece_ch1 = nullptr;  // [npieces] one past the last global chunk (same pattern)
+    int* piece_acc = nullptr;  // [npieces] accumulator offset of the piece's first column
+    int* chunk_sc = nullptr;   // [nchunks] super-chunk of every chunk
+    int* chunk_acc = nullptr;  // [nchunks] accumulator offset of the chunk's first column
+    int* item_sc = nullptr;    // [nitems]
+    int* item_b0 = nullptr;    // [nitems]
+    int* item_b1 = nullptr;    // [nitems]
+    int64_t* item_part = nullptr;  // [nitems] offset of the item's partials
+    int* sc_item0 = nullptr;       // [nsc + 1] first item of each super-chunk
+    void* partial = nullptr;       // float or double partials
+    int* ctr = nullptr;            // [2] work counter and finished CTAs of the persistent schedule (reset by the kernel)
 };
+
+// One measured A'y schedule of the build-time autotuner.
+struct FastTuneEntry {
+    int per_sc;
+    int ring;
+    int items_per_sm;
+    int pack;
+    int persistent;
+    float ms;  // mean time of one FP32 A'y (partials + column sums) on this layout
+};
+constexpr int kMaxTune = 12;
 
 struct FastLayout {
     FastGeometry g;
+    FastTuneEntry tune[kMaxTune];      // candidates timed at build (empty: default schedule)
+    int ntune = 0;
+    int tune_cached = 0;               // schedule taken from the per-process cache
     uint16_t* a16 = nullptr;
     uint32_t* g32 = nullptr;
     uint32_t* chunk_start = nullptr;   // [nblocks][nchunks] absolute index in G32
@@ -93,10 +123,10 @@ struct FastLayout {
 // Device view used by the column reductions of the solver.
 struct FastCols {
     FastGeometry g;
-    int per_sc;
+    const int* chunk_sc;
+    const int* chunk_acc;
     const int* sc_item0;
     const int64_t* item_part;
-    int sc_base[kMaxFastPatterns + 1];
 };
 
 // Builds the blocked layout from positions (indexes them itself).  Returns
@@ -129,11 +159,11 @@ __device__ __forceinline__ double fast_col_sum(const FastCols& fc, const T* part
     int p = 0;
     while (p + 1 < fc.g.npat && fc.g.off[p + 1] <= c) p++;
     const int local = static_cast<int>(c - fc.g.off[p]);
-    const int width = kChunkCols * fc.per_sc;
-    const int sc = fc.sc_base[p] + local / width;
-    const int lc = local - (local / width) * width;
+    const int ch = fc.g.chunk0[p] + local / kChunkCols;
+    const int sc = fc.chunk_sc[ch];
+    const int pos = fc.chunk_acc[ch] + local % kChunkCols;
     double acc = 0;
-    for (int it = fc.sc_item0[sc]; it < fc.sc_item0[sc + 1]; it++) acc += static_cast<double>(partial[fc.item_part[it] + lc]);
+    for (int it = fc.sc_item0[sc]; it < fc.sc_item0[sc + 1]; it++) acc += static_cast<double>(partial[fc.item_part[it] + pos]);
     return acc;
 }
 

@@ -68,7 +68,8 @@ def main(argv=None) -> int:
     bt = idx_aty + es * (R + cols)
     print(json.dumps({"rows": R, "cols": cols, "nnz": nnz, "layout": args.layout, "dtype": args.dtype,
                       "ax_s": t_ax, "ax_gbs": bx / t_ax / 1e9, "ax_bytes": bx,
-                      "aty_s": t_aty, "aty_gbs": bt / t_aty / 1e9, "aty_bytes": bt}))
+                      "aty_s": t_aty, "aty_gbs": bt / t_aty / 1e9, "aty_bytes": bt,
+                      "aty_schedules": a.schedules() if args.layout == "blocked" else None}))
     return 0
 
 

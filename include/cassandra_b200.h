@@ -145,6 +145,27 @@ CAS_API const uint32_t* cas_csr_indices(const cas_csr* a);
  * row index of every entry, sorted by (column, row). */
 CAS_API cas_status cas_csr_transposed(const cas_csr* a, const int64_t** d_col_ptr, const uint32_t** d_row_idx);
 
+/* No counterpart in the reference: the schedules of the FP32 transposed
+ * product on the BLOCKED layout that the build-time autotuner timed for this
+ * matrix (accumulator width in 8192-column chunks per work item, entries
+ * streamed through a shared-memory cp.async ring or in registers, work items
+ * per SM, accumulators shared by several patterns, persistent CTAs taking
+ * items from a counter; mean milliseconds per product), and the schedule in
+ * use.  Returns
+ * the number of timed schedules written (at most max): 0 when the schedule
+ * came from the per-process cache of an earlier build of the same shape, from
+ * the CAS_ATY_SCHEDULE environment variable, or is the default of layouts
+ * under 64 blocks; -1 without a blocked layout. */
+typedef struct cas_schedule {
+    int chunks_per_item;
+    int ring;
+    int items_per_sm;
+    int pack;
+    int persistent;
+    float ms;
+} cas_schedule;
+CAS_API int cas_csr_schedules(const cas_csr* a, cas_schedule* out, int max, cas_schedule* in_use);
+
 /* y = A x (operator*(const MatrixCSR&, const Vector&), Math/MatrixCSR.cpp:49-65).
  * x has cols entries, y rows entries, both of dtype. */
 CAS_API cas_status cas_spmv(const cas_csr* a, cas_dtype dtype, const void* d_x, void* d_y, void* stream);

@@ -49,6 +49,45 @@ def test_blocked_products_match_oracle(cuda, orc, rows, masks, mode):
         np.testing.assert_array_equal(cb.jacobi_preconditioner_of_ata(a).cpu().numpy(), orc.jacobi(idx, cols))
 
 
+SCHEDULES = ["4,0,2,0,0", "4,0,1,1,0", "3,0,2,1,1", "2,0,2,0,1", "2,1,2,1,0", "1,1,2,0,0", "2,1,3,1,1",
+             "1,0,5,1,1"]
+
+
+@pytest.mark.parametrize("sched", SCHEDULES)
+def test_aty_schedules_match_oracle(cuda, orc, monkeypatch, sched):
+    """Every A'y schedule the autotuner can pick (forced through
+    CAS_ATY_SCHEDULE): exact on integer-valued FP32 vectors, on a matrix with
+    a partial last block and heavy columns (narrow empty-count range)."""
+    monkeypatch.setenv("CAS_ATY_SCHEDULE", sched)
+    rows = 3 * 16384 + 1234
+    a, pos, g = _build(rows, SET8, "expanded", "blocked", seed=31)
+    want = tuple(int(v) for v in sched.split(","))
+    cur = a.schedules()["in_use"]
+    assert (cur["chunks_per_item"], cur["ring"], cur["items_per_sm"], cur["pack"], cur["persistent"]) == want
+    idx = orc.group_index(SET8, 1, pos.cpu().numpy().view(np.uint64))
+    yi = np.random.default_rng(5).integers(-50, 50, rows).astype(np.float32)
+    np.testing.assert_array_equal((torch.from_numpy(yi).cuda() @ a).cpu().numpy(),
+                                  orc.spmv_t(idx, g.index_space_size, yi.astype(np.float64)).astype(np.float32))
+    y = torch.randn(rows, dtype=torch.float32, device="cuda")
+    assert (y @ a).cpu().numpy().tobytes() == (y @ a).cpu().numpy().tobytes()  # persistent CTAs: same bits
+
+
+def test_autotuner_times_candidates_and_caches(cuda, monkeypatch):
+    monkeypatch.delenv("CAS_ATY_SCHEDULE", raising=False)
+    rows = 64 * 16384  # smallest layout that is tuned
+    a, pos, g = _build(rows, SET8, "expanded", "blocked", seed=32)
+    sch = a.schedules()
+    timed = sch["timed"]
+    assert len(timed) == 12 and all(t["ms"] > 0 for t in timed)
+    best = min(timed, key=lambda t: t["ms"])
+    cur = sch["in_use"]
+    keys = ("chunks_per_item", "ring", "items_per_sm", "pack", "persistent")
+    assert tuple(cur[k] for k in keys) == tuple(best[k] for k in keys)
+    b = cb.MatrixCSR.from_positions(g, pos, "blocked")  # same shape: cached, not re-timed
+    sb = b.schedules()
+    assert sb["timed"] == [] and sb["in_use"]["chunks_per_item"] == cur["chunks_per_item"]
+
+
 def test_blocked_and_rows_layouts_agree(cuda):
     both, pos, g = _build(40_000, SET8, "expanded", "rows+blocked")
     rows_only = cb.MatrixCSR.from_positions(g, pos, "rows")
