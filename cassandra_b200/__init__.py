@@ -17,6 +17,7 @@ from .api import (  # noqa: F401
     generate_positions_host,
     generate_targets,
     jacobi_preconditioner_of_ata,
+    solve_batched,
     solve_opts,
 )
 

@@ -116,6 +116,30 @@ class MatrixCSR:
                                                       _stream(), C.byref(h)))
         return cls(h, keep=indexer)
 
+    @classmethod
+    def from_positions_batched(cls, indexer: GroupIndexer, positions: torch.Tensor,
+                               problem_rows) -> "MatrixCSR":
+        """A batch of independent fits over the same patterns (one per
+        empty-count stage): problem q is the next problem_rows[q] positions
+        and owns columns [q * C, (q + 1) * C).  The result is the
+        block-diagonal matrix of the problems, in the blocked layout."""
+        _require_cuda(positions, "positions")
+        lib = L.load()
+        rows = np.ascontiguousarray(np.asarray(problem_rows, dtype=np.int64))
+        if int(rows.sum()) != positions.shape[0]:
+            raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+        h = C.c_void_p()
+        L.check(lib.cas_csr_from_positions_batched(indexer.handle, _ptr(positions), rows.ctypes.data_as(C.c_void_p),
+                                                   len(rows), _stream(), C.byref(h)))
+        return cls(h, keep=indexer)
+
+    def problems(self) -> np.ndarray:
+        """First row of every problem and the total (problems + 1 entries)."""
+        n = int(self._lib.cas_csr_problems(self._h, None))
+        out = np.zeros(n + 1, dtype=np.int64)
+        self._lib.cas_csr_problems(self._h, out.ctypes.data_as(C.c_void_p))
+        return out
+
     def schedules(self) -> dict:
         """A'y schedules timed by the build-time autotuner on this matrix and
         the one in use (blocked layout only)."""
@@ -324,6 +348,32 @@ class LSQR(_Solver):
     """LSQR(A, x0, b) (Math/Solver.h:128-182)."""
 
     method = "lsqr"
+
+
+def solve_batched(a: MatrixCSR, b: torch.Tensor, precision: str = "mixed", tol: float = 1e-8,
+                  max_iterations: int = 20000, refine_every: int = 50, check_every: int = 50, method: str = "pcg",
+                  jacobi: bool = True) -> tuple[torch.Tensor, list[dict], bool]:
+    """Every problem of a batched matrix solved by its own PCG (or CG) in one
+    run (cas_solve_batched).  Returns x as [problems, C], one report per
+    problem and whether all reached the tolerance."""
+    _require_cuda(b, "b")
+    b = b.double().contiguous()
+    if b.numel() != a.rows():
+        raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+    lib = L.load()
+    n = len(a.problems()) - 1
+    opts = solve_opts(method, precision, tol, max_iterations, refine_every, check_every, jacobi)
+    x = torch.empty(a.cols(), dtype=torch.float64, device="cuda")
+    reps = (L.SolveReport * n)()
+    st = lib.cas_solve_batched(a.handle, C.byref(opts), _ptr(b), _ptr(x), reps, _stream())
+    if st not in (L.CAS_OK, L.CAS_ERR_NOT_CONVERGED):
+        L.check(st)
+    out = []
+    for r in reps:
+        d = r.as_dict()
+        d["converged"] = bool(tol <= 0 or d["rel_residual"] <= tol)
+        out.append(d)
+    return x.view(n, -1), out, st == L.CAS_OK
 
 
 def fit_weights(masks, positions: np.ndarray, scores: np.ndarray, mode: str = "reference", method: str = "pcg",

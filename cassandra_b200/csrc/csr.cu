@@ -534,8 +534,8 @@ CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const ui
     if (layouts & CAS_LAYOUT_BLOCKED) {
         a->fast = new FastLayout;
         // diag(A'A) comes from the blocked copy unless the row layout builds it
-        st = fast_build(*dp, pattern_set(p), d_positions, rows, (layouts & CAS_LAYOUT_ROWS) ? nullptr : a->diag_int,
-                        *a->fast, s);
+        st = fast_build(*dp, pattern_set(p), d_positions, rows, nullptr, 1,
+                        (layouts & CAS_LAYOUT_ROWS) ? nullptr : a->diag_int, *a->fast, s);
         if (st != CAS_OK) {
             free_csr(a);
             return st;
@@ -563,6 +563,74 @@ CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const ui
     }
     *out = a;
     return CAS_OK;
+}
+
+CAS_API cas_status cas_csr_from_positions_batched(const cas_patterns* p, const uint64_t* d_positions,
+                                                  const int64_t* h_problem_rows, int problems, void* stream,
+                                                  cas_csr** out)
+{
+    CAS_REQUIRE(p && out && h_problem_rows && problems >= 1 && problems <= kMaxProblems, CAS_ERR_INVALID_ARGUMENT,
+                "cas_csr_from_positions_batched: bad argument (1 to 64 problems)");
+    CAS_REQUIRE(fast_supported(pattern_set(p)), CAS_ERR_INVALID_ARGUMENT,
+                "cas_csr_from_positions_batched: the blocked layout needs index spaces <= 65536 per pattern");
+    int64_t rows = 0;
+    for (int q = 0; q < problems; q++) {
+        CAS_REQUIRE(h_problem_rows[q] >= 0, CAS_ERR_INVALID_ARGUMENT,
+                    "cas_csr_from_positions_batched: negative problem size");
+        rows += h_problem_rows[q];
+    }
+    CAS_REQUIRE(rows == 0 || d_positions, CAS_ERR_INVALID_ARGUMENT, "cas_csr_from_positions_batched: null positions");
+    CAS_REQUIRE((reinterpret_cast<uintptr_t>(d_positions) & 15) == 0, CAS_ERR_INVALID_ARGUMENT,
+                "cas_csr_from_positions_batched: position records must be 16-byte aligned");
+    *out = nullptr;
+    const DevicePatterns* dp = nullptr;
+    CAS_TRY(patterns_on_device(p, &dp));
+    auto s = static_cast<cudaStream_t>(stream);
+    auto* a = new cas_csr;
+    CAS_CUDA(cudaGetDevice(&a->device));
+    a->rows = rows;
+    a->cols = dp->cols * problems;
+    a->k = dp->k;
+    a->layouts = CAS_LAYOUT_BLOCKED;
+    cudaError_t e = cudaMalloc(&a->diag_int, sizeof(uint64_t) * std::max<int64_t>(a->cols, 1));
+    if (e == cudaSuccess) e = cudaMemsetAsync(a->diag_int, 0, sizeof(uint64_t) * std::max<int64_t>(a->cols, 1), s);
+    if (e != cudaSuccess) {
+        free_csr(a);
+        set_error("cas_csr_from_positions_batched: cannot allocate the column statistics");
+        return CAS_ERR_OUT_OF_MEMORY;
+    }
+    a->fast = new FastLayout;
+    cas_status st = fast_build(*dp, pattern_set(p), d_positions, rows, h_problem_rows, problems, a->diag_int,
+                               *a->fast, s);
+    if (st == CAS_OK) {
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            set_error(std::string("batched CSR build: ") + cudaGetErrorString(e));
+            st = CAS_ERR_CUDA;
+        }
+    }
+    if (st != CAS_OK) {
+        free_csr(a);
+        return st;
+    }
+    *out = a;
+    return CAS_OK;
+}
+
+CAS_API int cas_csr_problems(const cas_csr* a, int64_t* h_row0)
+{
+    if (!a) return -1;
+    if (!a->fast) {
+        if (h_row0) {
+            h_row0[0] = 0;
+            h_row0[1] = a->rows;
+        }
+        return 1;
+    }
+    const FastGeometry& g = a->fast->g;
+    if (h_row0)
+        for (int q = 0; q <= g.nprob; q++) h_row0[q] = g.prow0[q];
+    return g.nprob;
 }
 
 CAS_API cas_status cas_csr_from_positions(const cas_patterns* p, const uint64_t* d_positions, int64_t rows,
@@ -615,6 +683,8 @@ CAS_API cas_status cas_eval_backward(const cas_csr* a, int64_t row0, int64_t row
                                      void* stream)
 {
     CAS_REQUIRE(a && a->fast, CAS_ERR_INVALID_ARGUMENT, "cas_eval_backward: the CSR needs the blocked layout");
+    CAS_REQUIRE(a->fast->g.nprob == 1, CAS_ERR_INVALID_ARGUMENT,
+                "cas_eval_backward: needs the layout of a single fit, not a batch");
     CAS_REQUIRE(0 <= row0 && row0 <= row1 && row1 <= a->rows, CAS_ERR_SIZE_MISMATCH,
                 "cas_eval_backward: row range outside the matrix");
     CAS_REQUIRE(row0 % kBlockRows == 0 && (row1 % kBlockRows == 0 || row1 == a->rows), CAS_ERR_INVALID_ARGUMENT,

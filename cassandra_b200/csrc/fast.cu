@@ -65,7 +65,8 @@ __global__ void __launch_bounds__(256) fast_index_kernel(const Instance* __restr
         const ulonglong2 ps = pos[r];
         const uint32_t plo = static_cast<uint32_t>(ps.x), phi = static_cast<uint32_t>(ps.x >> 32);
         const uint32_t olo = static_cast<uint32_t>(ps.y), ohi = static_cast<uint32_t>(ps.y >> 32);
-        const int64_t b = r / kBlockRows, rb = r - b * kBlockRows;
+        int64_t b, rb;
+        g.locate_row(r, b, rb);
         for (int p = 0; p < g.npat; p++) {
             const int s0 = g.slot0[p], ns = g.slots[p];
             const uint32_t off = static_cast<uint32_t>(g.off[p]);
@@ -241,7 +242,7 @@ __global__ void fast_diag_kernel(FastGeometry g, const uint32_t* __restrict__ g3
             const unsigned peers = __match_any_sync(0xffffffffu, col);
             const uint32_t sum = __reduce_add_sync(peers, contrib);
             if (e < n && lane == __ffs(peers) - 1)
-                atomicAdd(reinterpret_cast<unsigned long long*>(diag + g.off[p] + col), sum);
+                atomicAdd(reinterpret_cast<unsigned long long*>(diag + g.col_base(b) + g.off[p] + col), sum);
         }
     }
 }
@@ -374,13 +375,17 @@ __device__ __forceinline__ void gather_segment8(const uint16_t* __restrict__ bas
 
 // ALL8: every pattern has 8 slots (the expanded layout), so only the
 // pipelined 8-slot path is compiled in.
+// part (optional) receives one compensated partial of ||y||^2 per block, so
+// that the norms of the problems of a batched layout can be summed apart.
+// Blocks of problems whose pdone flag is set are skipped (partial 0).
 template <typename T, typename Y, int MODE, bool ALL8>
 __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g, const uint16_t* __restrict__ a16,
                                                                    const T* __restrict__ x, Y* __restrict__ y,
                                                                    const double* __restrict__ b,
                                                                    const double* __restrict__ coef,
                                                                    double* __restrict__ part,
-                                                                   const int* __restrict__ done)
+                                                                   const int* __restrict__ done,
+                                                                   const int* __restrict__ pdone)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* table = reinterpret_cast<T*>(smem_raw);
@@ -389,15 +394,25 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
     constexpr int kCap = sizeof(T) == 4 ? kTable32 : kTable64;
     using Acc = typename AccOf<T>::type;
     const double c = MODE == 1 ? *coef : 0.0;
-    Comp mine;
     for (int64_t blk = blockIdx.x; blk < g.nblocks; blk += gridDim.x) {
+        const int q = g.prob_of_block(blk);
+        if (pdone && pdone[q]) {
+            if (part && threadIdx.x == 0) {
+                part[2 * blk] = 0;
+                part[2 * blk + 1] = 0;
+            }
+            continue;
+        }
         const int nb = static_cast<int>(g.block_rows(blk));
+        const int64_t row0 = g.block_row0(blk);
+        const T* xq = x + q * g.pcols;
+        Comp mine;
         Acc acc[kAxRows];
 #pragma unroll
         for (int j = 0; j < kAxRows; j++) acc[j] = 0;
         for (int p = 0; p < g.npat; p++) {
             const int cap = min(g.space[p], kCap);
-            const T* xg = x + g.off[p];
+            const T* xg = xq + g.off[p];
             __syncthreads();
             load_table<T>(table, xg, cap);
             __syncthreads();
@@ -421,7 +436,7 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
         for (int j = 0; j < kAxRows; j++) {
             const int r = threadIdx.x + j * kAxThreads;
             if (r < nb) {
-                const int64_t row = blk * kBlockRows + r;
+                const int64_t row = row0 + r;
                 double v = static_cast<double>(acc[j]);
                 if (MODE == 1) v = static_cast<double>(y[row]) * -c + v;
                 if (MODE == 2) v = (b ? b[row] : 0.0) - v;
@@ -430,12 +445,12 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
                 mine.add(static_cast<double>(yv) * static_cast<double>(yv));
             }
         }
-    }
-    if (part) {
-        const Comp r = block_sum_comp<kAxThreads>(mine, red);
-        if (threadIdx.x == 0) {
-            part[2 * blockIdx.x] = r.s;
-            part[2 * blockIdx.x + 1] = r.c;
+        if (part) {
+            const Comp r = block_sum_comp<kAxThreads>(mine, red);
+            if (threadIdx.x == 0) {
+                part[2 * blk] = r.s;
+                part[2 * blk + 1] = r.c;
+            }
         }
     }
 }
@@ -782,8 +797,9 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
                                          const uint32_t* __restrict__ chunk_start, const T* __restrict__ y,
                                          T* __restrict__ partial, int item, int item_base, int64_t y_block0,
                                          T* __restrict__ acc, T* __restrict__ ytile, uint32_t* __restrict__ ring,
-                                         WarpRec<T> (*recs)[kFastThreads / 32])
+                                         WarpRec<T> (*recs)[kFastThreads / 32], const int* __restrict__ pdone)
 {
+    if (pdone && pdone[g.prob_of_block(tv.item_b0[item])]) return;  // retired problem: partials unused
     const int sc = tv.item_sc[item];
     const int pc0 = tv.sc_piece0[sc], pc1 = tv.sc_piece0[sc + 1];
     const int width = tv.sc_width[sc];
@@ -792,7 +808,7 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
     for (int64_t blk = tv.item_b0[item]; blk < tv.item_b1[item]; blk++) {
         const int nb = static_cast<int>(g.block_rows(blk));
         __syncthreads();
-        const T* yb = y + (blk - y_block0) * kBlockRows;
+        const T* yb = y + (g.block_row0(blk) - g.block_row0(y_block0));
         if ((reinterpret_cast<uintptr_t>(yb) & 15) == 0) {
             constexpr int kPer = 16 / sizeof(T);
             const int nvec = nb / kPer;
@@ -834,7 +850,8 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
                                                                        const T* __restrict__ y,
                                                                        T* __restrict__ partial,
                                                                        const int* __restrict__ done, int item_base,
-                                                                       int64_t y_block0, int* __restrict__ ctr)
+                                                                       int64_t y_block0, int* __restrict__ ctr,
+                                                                       const int* __restrict__ pdone)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // two record sets, alternating per piece: warp 0 may still combine one
@@ -847,7 +864,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
     uint32_t* ring = reinterpret_cast<uint32_t*>(ytile + kBlockRows);  // RING schedules only
     if (!ctr) {
         aty_item<T, RING>(g, tv, g32, chunk_start, y, partial, blockIdx.x + item_base, item_base, y_block0, acc, ytile,
-                          ring, recs);
+                          ring, recs, pdone);
         return;
     }
     while (true) {
@@ -856,7 +873,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
         __syncthreads();
         const int item = s_item;
         if (item >= tv.nitems) break;
-        aty_item<T, RING>(g, tv, g32, chunk_start, y, partial, item, 0, 0, acc, ytile, ring, recs);
+        aty_item<T, RING>(g, tv, g32, chunk_start, y, partial, item, 0, 0, acc, ytile, ring, recs, pdone);
     }
     if (threadIdx.x == 0) {
         __threadfence();
@@ -877,10 +894,12 @@ __global__ void __launch_bounds__(256) fast_rows_forward_kernel(FastGeometry g, 
 {
     for (int64_t r = row0 + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < row1;
          r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t b = r / kBlockRows, rb = r - b * kBlockRows;
+        int64_t b, rb;
+        g.locate_row(r, b, rb);
+        const float* wq = w + g.col_base(b);
         float acc = 0;
         for (int p = 0; p < g.npat; p++)
-            gather_row<float>(a16 + g.seg(b, p) + rb * g.slots[p], g.slots[p], w + g.off[p], w + g.off[p], 0, false,
+            gather_row<float>(a16 + g.seg(b, p) + rb * g.slots[p], g.slots[p], wq + g.off[p], wq + g.off[p], 0, false,
                               acc);
         out[r - row0] = acc;
     }
@@ -1001,28 +1020,34 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
     const Pieces pc = pack_chunks(g, per_sc * kChunkCols, pack);
     CAS_TRY(upload_pieces(pc, t));
     const int nsc = t.nsc;
-    std::vector<int64_t> sc_entries(nsc, 0);
+    // entries per (problem, super-chunk); items never span problems
+    std::vector<int64_t> sc_entries(static_cast<size_t>(g.nprob) * nsc, 0);
     int64_t total = 0;
-    for (int64_t b = 0; b < g.nblocks; b++)
-        for (int ch = 0; ch < g.nchunks; ch++) {
-            sc_entries[pc.chunk_sc[ch]] += entries_bc[b * g.nchunks + ch];
-            total += entries_bc[b * g.nchunks + ch];
-        }
+    for (int q = 0; q < g.nprob; q++)
+        for (int64_t b = g.pblk0[q]; b < g.pblk0[q + 1]; b++)
+            for (int ch = 0; ch < g.nchunks; ch++) {
+                sc_entries[static_cast<size_t>(q) * nsc + pc.chunk_sc[ch]] += entries_bc[b * g.nchunks + ch];
+                total += entries_bc[b * g.nchunks + ch];
+            }
     const int64_t target_items = static_cast<int64_t>(sm_count()) * items_per_sm;
     const double per_item = std::max<double>(1.0, static_cast<double>(total) / target_items);
     std::vector<int> item_sc, item_b0, item_b1, sc_item0;
     std::vector<int64_t> item_part;
     int64_t part_elems = 0;
-    for (int sc = 0; sc < nsc; sc++) {
-        sc_item0.push_back(static_cast<int>(item_sc.size()));
-        int64_t n = static_cast<int64_t>(std::llround(sc_entries[sc] / per_item));
-        n = std::max<int64_t>(1, std::min<int64_t>(n, g.nblocks));
-        for (int64_t i = 0; i < n; i++) {
-            item_sc.push_back(sc);
-            item_b0.push_back(static_cast<int>(g.nblocks * i / n));
-            item_b1.push_back(static_cast<int>(g.nblocks * (i + 1) / n));
-            item_part.push_back(part_elems);
-            part_elems += pc.sc_width[sc];
+    for (int q = 0; q < g.nprob; q++) {
+        const int64_t qb0 = g.pblk0[q], qnb = g.pblk0[q + 1] - g.pblk0[q];
+        for (int sc = 0; sc < nsc; sc++) {
+            sc_item0.push_back(static_cast<int>(item_sc.size()));
+            if (qnb == 0) continue;
+            int64_t n = static_cast<int64_t>(std::llround(sc_entries[static_cast<size_t>(q) * nsc + sc] / per_item));
+            n = std::max<int64_t>(1, std::min<int64_t>(n, qnb));
+            for (int64_t i = 0; i < n; i++) {
+                item_sc.push_back(sc);
+                item_b0.push_back(static_cast<int>(qb0 + qnb * i / n));
+                item_b1.push_back(static_cast<int>(qb0 + qnb * (i + 1) / n));
+                item_part.push_back(part_elems);
+                part_elems += pc.sc_width[sc];
+            }
         }
     }
     sc_item0.push_back(static_cast<int>(item_sc.size()));
@@ -1182,6 +1207,7 @@ std::string tune_key(const FastGeometry& g)
 {
     std::string k = std::to_string(g.k) + "/" + std::to_string(g.nblocks) + "/" + std::to_string(g.rows);
     for (int p = 0; p < g.npat; p++) k += "/" + std::to_string(g.space[p]) + "x" + std::to_string(g.slots[p]);
+    for (int q = 0; q <= g.nprob; q++) k += ":" + std::to_string(g.pblk0[q]);
     return k;
 }
 
@@ -1289,17 +1315,34 @@ void fast_free(FastLayout& f)
 }
 
 cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint64_t* d_pos, int64_t rows,
-                      uint64_t* diag_int, FastLayout& f, cudaStream_t s)
+                      const int64_t* prob_rows, int nprob, uint64_t* diag_int, FastLayout& f, cudaStream_t s)
 {
     CAS_REQUIRE(fast_supported(ps), CAS_ERR_INVALID_ARGUMENT, "pattern set does not fit the blocked layout");
+    CAS_REQUIRE(nprob >= 1 && nprob <= kMaxProblems, CAS_ERR_INVALID_ARGUMENT,
+                "blocked layout: 1 to 64 problems per batch");
     CAS_TRY(fast_set_attributes());
     FastGeometry& g = f.g;
     g = FastGeometry{};
     g.npat = static_cast<int>(ps.indexers.size());
     g.k = dp.k;
     g.rows = rows;
-    g.cols = ps.cols;
-    g.nblocks = (rows + kBlockRows - 1) / kBlockRows;
+    g.nprob = nprob;
+    g.pcols = ps.cols;
+    g.cols = ps.cols * nprob;
+    // problem table: rows and whole blocks of each problem
+    int64_t r0 = 0, b0 = 0;
+    for (int q = 0; q < nprob; q++) {
+        const int64_t rq = prob_rows ? prob_rows[q] : rows;
+        CAS_REQUIRE(rq >= 0, CAS_ERR_INVALID_ARGUMENT, "blocked layout: negative problem size");
+        g.prow0[q] = r0;
+        g.pblk0[q] = static_cast<int>(b0);
+        r0 += rq;
+        b0 += (rq + kBlockRows - 1) / kBlockRows;
+    }
+    g.prow0[nprob] = r0;
+    g.pblk0[nprob] = static_cast<int>(b0);
+    CAS_REQUIRE(r0 == rows, CAS_ERR_SIZE_MISMATCH, "blocked layout: problem sizes do not add up to the rows");
+    g.nblocks = b0;
     int slot = 0, chunk = 0;
     for (int p = 0; p < g.npat; p++) {
         g.slot0[p] = slot;
@@ -1358,7 +1401,7 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
     if (g.nblocks > 0) {
         CAS_TRY(tune_transpose(f, entries, s));
         CAS_TRY(build_items(g, entries, 1, 2, false, true, false, sizeof(double), f.t64));
-        CAS_TRY(build_block_items(g, f.tb));
+        if (g.nprob == 1) CAS_TRY(build_block_items(g, f.tb));  // evaluator minibatches: single fits only
     }
     return CAS_OK;
 }
@@ -1374,14 +1417,14 @@ cas_status fast_diag(const FastLayout& f, uint64_t* diag, cudaStream_t s)
 
 template <typename T, typename Y>
 cas_status fast_spmv(const FastLayout& f, const T* x, Y* y, const double* b, const double* coef, double* part,
-                     int* done_flag, int mode, cudaStream_t s, int* n_parts)
+                     int* done_flag, int mode, cudaStream_t s, int* n_parts, const int* pdone)
 {
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(f.g.nblocks, sm_count())));
-    if (n_parts) *n_parts = static_cast<int>(grid);
+    if (n_parts) *n_parts = static_cast<int>(f.g.nblocks);  // one norm partial per block
     if (f.g.nblocks == 0) return CAS_OK;
     const size_t smem = sizeof(T) * (sizeof(T) == 4 ? kTable32 : kTable64);
     auto launch = [&](auto kern) -> cas_status {
-        { kern<<<grid, kAxThreads, smem, s>>>(f.g, f.a16, x, y, b, coef, part, done_flag); cas::count_launch(); }
+        { kern<<<grid, kAxThreads, smem, s>>>(f.g, f.a16, x, y, b, coef, part, done_flag, pdone); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     };
@@ -1398,7 +1441,7 @@ cas_status fast_spmv(const FastLayout& f, const T* x, Y* y, const double* b, con
 }
 
 template <typename T>
-cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag, cudaStream_t s)
+cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag, cudaStream_t s, const int* pdone)
 {
     const FastTranspose& t = transpose_of<T>(f);
     if (t.nitems == 0) return CAS_OK;
@@ -1409,14 +1452,14 @@ cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag,
         if (t.ring) {
             { fast_spmv_t_kernel<T, true><<<grid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.chunk_start, y,
                                                                         static_cast<T*>(t.partial), done_flag, 0, 0,
-                                                                        ctr); cas::count_launch(); }
+                                                                        ctr, pdone); cas::count_launch(); }
             CAS_CHECK_LAUNCH();
             return CAS_OK;
         }
     }
     { fast_spmv_t_kernel<T, false><<<grid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.chunk_start, y,
                                                                  static_cast<T*>(t.partial), done_flag, 0, 0,
-                                                                 ctr); cas::count_launch(); }
+                                                                 ctr, pdone); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     return CAS_OK;
 }
@@ -1427,6 +1470,7 @@ FastCols fast_cols(const FastLayout& f)
     const FastTranspose& t = transpose_of<T>(f);
     FastCols c;
     c.g = f.g;
+    c.nsc = t.nsc;
     c.chunk_sc = t.chunk_sc;
     c.chunk_acc = t.chunk_acc;
     c.sc_item0 = t.sc_item0;
@@ -1479,7 +1523,8 @@ cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float
     const int items = static_cast<int>(nb * f.g.nchunks);
     { fast_spmv_t_kernel<float, false><<<items, kFastThreads, smem, s>>>(f.g, tview(f.tb), f.g32, f.chunk_start, g,
                                                                  f.eval_partial, nullptr,
-                                                                 static_cast<int>(b0 * f.g.nchunks), b0, nullptr); cas::count_launch(); }
+                                                                 static_cast<int>(b0 * f.g.nchunks), b0, nullptr,
+                                                                 nullptr); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     { block_partial_sum_kernel<<<fgrid(f.g.cols, 256), 256, 0, s>>>(f.eval_partial, static_cast<int>(nb), f.g.cols,
                                                                   grad); cas::count_launch(); }
@@ -1488,13 +1533,13 @@ cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float
 }
 
 template cas_status fast_spmv<float, float>(const FastLayout&, const float*, float*, const double*, const double*,
-                                            double*, int*, int, cudaStream_t, int*);
+                                            double*, int*, int, cudaStream_t, int*, const int*);
 template cas_status fast_spmv<double, double>(const FastLayout&, const double*, double*, const double*,
-                                              const double*, double*, int*, int, cudaStream_t, int*);
+                                              const double*, double*, int*, int, cudaStream_t, int*, const int*);
 template cas_status fast_spmv<double, float>(const FastLayout&, const double*, float*, const double*, const double*,
-                                             double*, int*, int, cudaStream_t, int*);
-template cas_status fast_spmv_t_partials<float>(const FastLayout&, const float*, int*, cudaStream_t);
-template cas_status fast_spmv_t_partials<double>(const FastLayout&, const double*, int*, cudaStream_t);
+                                             double*, int*, int, cudaStream_t, int*, const int*);
+template cas_status fast_spmv_t_partials<float>(const FastLayout&, const float*, int*, cudaStream_t, const int*);
+template cas_status fast_spmv_t_partials<double>(const FastLayout&, const double*, int*, cudaStream_t, const int*);
 template FastCols fast_cols<float>(const FastLayout&);
 template FastCols fast_cols<double>(const FastLayout&);
 template cas_status fast_spmv_t<float>(const FastLayout&, const float*, float*, cudaStream_t);

@@ -30,23 +30,75 @@ constexpr int kMaxFastPatterns = 32;
 constexpr int kTable32 = 57344;          // x entries staged per pattern, FP32
 constexpr int kTable64 = 28672;          // x entries staged per pattern, FP64
 
+constexpr int kMaxProblems = 64;         // independent fits in one batched layout
+
 // Per-pattern geometry, passed to kernels by value.
+//
+// A layout may hold several independent problems (a batch of fits over the
+// same patterns): problem q owns rows [prow0[q], prow0[q+1]) and blocks
+// [pblk0[q], pblk0[q+1]) -- blocks never straddle problems, so a problem's
+// last block may be partial -- and columns [q * pcols, (q + 1) * pcols).
+// The matrix is block diagonal.  A single fit is the case nprob == 1.
 struct FastGeometry {
     int npat = 0;
     int k = 0;                           // entries per row (sum of slots)
-    int64_t rows = 0, cols = 0;
+    int64_t rows = 0, cols = 0;          // cols = nprob * pcols
     int64_t nblocks = 0;
     int slot0[kMaxFastPatterns];
     int slots[kMaxFastPatterns];
-    int64_t off[kMaxFastPatterns];       // global column offset
+    int64_t off[kMaxFastPatterns];       // column offset of the pattern inside a problem
     int space[kMaxFastPatterns];         // columns of the pattern
     int chunk0[kMaxFastPatterns];        // first global chunk of the pattern
     int nchunks = 0;
+    int nprob = 1;
+    int64_t pcols = 0;                   // columns per problem
+    int64_t prow0[kMaxProblems + 1];     // first row of each problem
+    int pblk0[kMaxProblems + 1];         // first block of each problem
 
+    __host__ __device__ int prob_of_block(int64_t b) const
+    {
+        int lo = 0, hi = nprob - 1;  // largest q with pblk0[q] <= b
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pblk0[mid] <= b)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        return lo;
+    }
+    __host__ __device__ int prob_of_row(int64_t r) const
+    {
+        int lo = 0, hi = nprob - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prow0[mid] <= r)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        return lo;
+    }
+    __host__ __device__ int64_t block_row0(int64_t b) const
+    {
+        const int q = prob_of_block(b);
+        return prow0[q] + (b - pblk0[q]) * kBlockRows;
+    }
     __host__ __device__ int64_t block_rows(int64_t b) const
     {
-        const int64_t r = rows - b * kBlockRows;
+        const int q = prob_of_block(b);
+        const int64_t r = prow0[q + 1] - (prow0[q] + (b - pblk0[q]) * kBlockRows);
         return r < kBlockRows ? r : kBlockRows;
+    }
+    // First column of the problem that owns block b.
+    __host__ __device__ int64_t col_base(int64_t b) const { return prob_of_block(b) * pcols; }
+    // Block and row inside the block of row r.
+    __host__ __device__ void locate_row(int64_t r, int64_t& b, int64_t& rb) const
+    {
+        const int q = prob_of_row(r);
+        const int64_t local = r - prow0[q];
+        b = pblk0[q] + local / kBlockRows;
+        rb = local - (local / kBlockRows) * kBlockRows;
     }
     // Rows of a block rounded up to 8 so that every segment is 16-byte aligned.
     __host__ __device__ int64_t padded_rows(int64_t b) const { return (block_rows(b) + 7) & ~int64_t(7); }
@@ -123,6 +175,7 @@ struct FastLayout {
 // Device view used by the column reductions of the solver.
 struct FastCols {
     FastGeometry g;
+    int nsc;                 // super-chunks per problem
     const int* chunk_sc;
     const int* chunk_acc;
     const int* sc_item0;
@@ -133,22 +186,28 @@ struct FastCols {
 // CAS_ERR_INVALID_ARGUMENT without touching `out` if the pattern set does
 // not fit the layout (a pattern wider than 16-bit columns, too many patterns
 // or a slot count other than 1, 2, 4, 8).
+// prob_rows (host, nprob entries) splits the rows into independent problems
+// (a batch of fits, in row order); null with nprob == 1 is a single fit.
 cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint64_t* d_pos, int64_t rows,
-                      uint64_t* diag_int, FastLayout& out, cudaStream_t s);
+                      const int64_t* prob_rows, int nprob, uint64_t* diag_int, FastLayout& out, cudaStream_t s);
 bool fast_supported(const PatternSet& ps);
 void fast_free(FastLayout& f);
 
-// y = A x on the blocked layout; also writes per-CTA partials of ||y||^2
-// (part may be null).  mode 0: y = A x; 1: y = A x - coef * y (coef read
-// from *coef); 2: y = b - A x (b may be null: y = -A x).
+// y = A x on the blocked layout; also writes per-block partials of ||y||^2
+// (part may be null; *n_parts = blocks).  mode 0: y = A x; 1: y = A x -
+// coef * y (coef read from *coef); 2: y = b - A x (b may be null: y = -A x).
+// done_flag set: nothing runs; pdone[q] set: the rows of problem q are
+// skipped (their partials are 0).
 template <typename T, typename Y>
 cas_status fast_spmv(const FastLayout& f, const T* x, Y* y, const double* b, const double* coef, double* part,
-                     int* done_flag, int mode, cudaStream_t s, int* n_parts);
+                     int* done_flag, int mode, cudaStream_t s, int* n_parts, const int* pdone = nullptr);
 
 // Partials of A' y on the blocked layout (FP32: float partials, FP64:
-// double partials); columns are summed by fast_col_sum().
+// double partials); columns are summed by fast_col_sum().  Items of
+// problems whose pdone flag is set are skipped.
 template <typename T>
-cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag, cudaStream_t s);
+cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag, cudaStream_t s,
+                                const int* pdone = nullptr);
 
 template <typename T>
 FastCols fast_cols(const FastLayout& f);
@@ -156,11 +215,16 @@ FastCols fast_cols(const FastLayout& f);
 template <typename T>
 __device__ __forceinline__ double fast_col_sum(const FastCols& fc, const T* partial, int64_t c)
 {
+    int64_t q = 0;
+    if (fc.g.nprob > 1) {
+        q = c / fc.g.pcols;
+        c -= q * fc.g.pcols;
+    }
     int p = 0;
     while (p + 1 < fc.g.npat && fc.g.off[p + 1] <= c) p++;
     const int local = static_cast<int>(c - fc.g.off[p]);
     const int ch = fc.g.chunk0[p] + local / kChunkCols;
-    const int sc = fc.chunk_sc[ch];
+    const int sc = static_cast<int>(q) * fc.nsc + fc.chunk_sc[ch];
     const int pos = fc.chunk_acc[ch] + local % kChunkCols;
     double acc = 0;
     for (int it = fc.sc_item0[sc]; it < fc.sc_item0[sc + 1]; it++) acc += static_cast<double>(partial[fc.item_part[it] + pos]);

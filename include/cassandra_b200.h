@@ -263,6 +263,35 @@ CAS_API cas_status cas_solver_rel_residual(cas_solver* s, double* h_out);
 CAS_API cas_status cas_solver_run(cas_solver* s, cas_solve_report* rep);
 CAS_API int cas_solver_iterations(const cas_solver* s);
 
+/* ------------------------------------------------------------------------ */
+/* Batched fits: one problem per empty-count stage                           */
+/* ------------------------------------------------------------------------ */
+
+/* The independent per-stage fits of the training loop
+ * (PatternFit/PatternFit.cpp:53-84 builds and fits one estimator per
+ * empty-count stage, one after another; Pattern/Evaluator.cpp:77-88 keeps one
+ * per stage) as one block-diagonal matrix in the BLOCKED layout: problem q is
+ * rows [sum of h_problem_rows[0..q)) ...) of d_positions and owns columns
+ * [q * C, (q + 1) * C), C = cas_patterns_cols(p).  1 to 64 problems; any
+ * problem may be empty.  cas_spmv / cas_spmv_t / cas_jacobi work on it as on
+ * any CSR (the products of the block-diagonal matrix). */
+CAS_API cas_status cas_csr_from_positions_batched(const cas_patterns* p, const uint64_t* d_positions,
+                                                  const int64_t* h_problem_rows, int problems, void* stream,
+                                                  cas_csr** out);
+/* Number of problems of a CSR (1 for a single fit); h_row0 (problems + 1
+ * entries, may be null) receives each problem's first row and the total. */
+CAS_API int cas_csr_problems(const cas_csr* a, int64_t* h_row0);
+/* Solves every problem of a batched CSR with its own Jacobi-PCG (or CG)
+ * (Math/Solver.h:78-117 per problem: own alpha, beta, residual and stopping
+ * test) in one run: the products of an iteration cover all problems in one
+ * launch each, problems that reach opts.tol are retired and skipped, and
+ * iterations are replayed as CUDA graph chunks of opts.check_every.  d_b has
+ * the rows of all problems, d_x receives problems * C weights; reports (may
+ * be null) receives one report per problem (FP64 true relative residual).
+ * Returns CAS_ERR_NOT_CONVERGED if any problem missed the tolerance. */
+CAS_API cas_status cas_solve_batched(const cas_csr* a, const cas_solve_opts* o, const double* d_b, double* d_x,
+                                     cas_solve_report* reports, void* stream);
+
 /* One-shot solve: create, run, copy x, destroy. */
 CAS_API cas_status cas_solve(const cas_csr* a, const cas_solve_opts* o, const double* d_b, double* d_x,
                              cas_solve_report* rep, void* stream);

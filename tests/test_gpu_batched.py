@@ -1,0 +1,128 @@
+"""Batched per-stage fits (one problem per empty count, as the reference's
+training loop fits them one after another, PatternFit/PatternFit.cpp:53-84):
+the block-diagonal batch layout and the batched PCG, checked per problem
+against the oracle and against single fits."""
+import numpy as np
+import pytest
+import torch
+
+import cassandra_b200 as cb
+from tests.golden.make_golden import SET8
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch(sizes, seed=40, empties=None):
+    parts = []
+    for q, n in enumerate(sizes):
+        e = empties[q] if empties else 12 + (7 * q) % 40
+        if n:
+            parts.append(cb.generate_positions(seed + q, n, e, e))
+    pos = torch.cat(parts) if parts else torch.empty((0, 2), dtype=torch.int64, device="cuda")
+    g = cb.GroupIndexer(SET8, "expanded")
+    a = cb.MatrixCSR.from_positions_batched(g, pos, sizes)
+    return a, pos, g
+
+
+def _oracle_problems(orc, a, pos):
+    row0 = a.problems()
+    ph = pos.cpu().numpy().view(np.uint64)
+    return row0, [orc.group_index(SET8, 1, ph[row0[q]:row0[q + 1]]) for q in range(len(row0) - 1)]
+
+
+def test_batched_layout_geometry(cuda):
+    sizes = [16385, 1, 0, 7000, 16384]
+    a, pos, g = _batch(sizes)
+    C = g.index_space_size
+    assert a.layouts() == {"blocked"}
+    assert a.rows() == sum(sizes) and a.cols() == len(sizes) * C
+    np.testing.assert_array_equal(a.problems(), np.concatenate([[0], np.cumsum(sizes)]))
+
+
+def test_batched_products_match_oracle_per_problem(cuda, orc):
+    sizes = [16385, 1, 0, 7000, 16384]
+    a, pos, g = _batch(sizes)
+    C = g.index_space_size
+    row0, idx = _oracle_problems(orc, a, pos)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(a.cols())
+    y = rng.standard_normal(a.rows())
+    ax = (a @ torch.from_numpy(x).cuda()).cpu().numpy()
+    aty = (torch.from_numpy(y).cuda() @ a).cpu().numpy()
+    with np.errstate(divide="ignore"):
+        jac = cb.jacobi_preconditioner_of_ata(a).cpu().numpy()
+    xi = rng.integers(-50, 50, a.cols()).astype(np.float32)
+    yi = rng.integers(-50, 50, a.rows()).astype(np.float32)
+    axi = (a @ torch.from_numpy(xi).cuda()).cpu().numpy()
+    atyi = (torch.from_numpy(yi).cuda() @ a).cpu().numpy()
+    for q in range(len(sizes)):
+        rs, cs = slice(row0[q], row0[q + 1]), slice(q * C, (q + 1) * C)
+        if sizes[q] == 0:
+            assert not np.any(aty[cs]) and not np.any(atyi[cs])
+            continue
+        np.testing.assert_allclose(ax[rs], orc.spmv(idx[q], C, x[cs]), rtol=1e-12, atol=1e-11)
+        np.testing.assert_allclose(aty[cs], orc.spmv_t(idx[q], C, y[rs]), rtol=1e-11, atol=1e-10)
+        np.testing.assert_array_equal(axi[rs], orc.spmv(idx[q], C, xi[cs].astype(np.float64)).astype(np.float32))
+        np.testing.assert_array_equal(atyi[cs], orc.spmv_t(idx[q], C, yi[rs].astype(np.float64)).astype(np.float32))
+        with np.errstate(divide="ignore"):
+            np.testing.assert_array_equal(jac[cs], orc.jacobi(idx[q], C))
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batched_pcg_reaches_tolerance_per_problem(cuda, orc, precision):
+    sizes = [30000, 5000, 12000, 0]
+    a, pos, g = _batch(sizes, seed=50, empties=[15, 45, 30, 20])
+    C = g.index_space_size
+    b = cb.generate_targets(a, 50)
+    x, reps, ok = cb.solve_batched(a, b, precision=precision, tol=1e-8, max_iterations=5000)
+    assert ok, reps
+    row0, idx = _oracle_problems(orc, a, pos)
+    bh, xh = b.cpu().numpy(), x.cpu().numpy()
+    iters = []
+    for q in range(len(sizes)):
+        rs = slice(row0[q], row0[q + 1])
+        assert reps[q]["converged"] and reps[q]["rel_residual"] <= 1e-8
+        if sizes[q] == 0:
+            assert reps[q]["iterations"] == 0 and not np.any(xh[q])
+            continue
+        iters.append(reps[q]["iterations"])
+        assert orc.normal_residual(idx[q], C, bh[rs], xh[q]) <= 1.5e-8
+        want, _, _ = orc.pcg(idx[q], C, bh[rs], 5000, tol=1e-8, check_every=10)
+        pred, pw = orc.spmv(idx[q], C, xh[q]), orc.spmv(idx[q], C, want)
+        np.testing.assert_allclose(pred, pw, rtol=0, atol=1e-5 * np.abs(pw).max())
+    assert len(set(iters)) > 1  # problems converge (and retire) at different iterations
+
+
+def test_batched_matches_single_fits(cuda):
+    """The batch gives each problem the fit a single solve of it gives."""
+    sizes = [20000, 9000]
+    a, pos, g = _batch(sizes, seed=60, empties=[22, 38])
+    b = cb.generate_targets(a, 60)
+    x, reps, ok = cb.solve_batched(a, b, precision="mixed", tol=1e-8)
+    assert ok
+    row0 = a.problems()
+    for q in range(len(sizes)):
+        rs = slice(int(row0[q]), int(row0[q + 1]))
+        single = cb.MatrixCSR.from_positions(g, pos[rs].contiguous(), "blocked")
+        s = cb.PCG(single, b[rs].contiguous(), precision="mixed", tol=1e-8)
+        assert s.run()["converged"]
+        pb = (single @ x[q].contiguous()).cpu().numpy()
+        ps = (single @ s.x()).cpu().numpy()
+        np.testing.assert_allclose(pb, ps, rtol=0, atol=1e-5 * np.abs(ps).max())
+
+
+def test_batched_zero_targets_retire_at_setup(cuda):
+    a, pos, g = _batch([3000, 4000], seed=70)
+    b = torch.zeros(a.rows(), dtype=torch.float64, device="cuda")
+    x, reps, ok = cb.solve_batched(a, b, tol=1e-8)
+    assert ok and all(r["iterations"] == 0 for r in reps)
+    assert torch.count_nonzero(x) == 0
+
+
+def test_batched_rejects_bad_sizes(cuda):
+    pos = cb.generate_positions(1, 100, 20, 20)
+    g = cb.GroupIndexer(SET8, "expanded")
+    with pytest.raises(cb.SizeMismatch):
+        cb.MatrixCSR.from_positions_batched(g, pos, [50, 49])
+    with pytest.raises(cb.CasError):
+        cb.MatrixCSR.from_positions_batched(g, pos, [1] * 65 + [35])

@@ -81,6 +81,14 @@ def test_invalid_arguments_are_reported():
     o = cb.solve_opts()
     o.method = 9
     assert lib.cas_solver_create(None, C.byref(o), None, None, None, C.byref(h)) == L.CAS_ERR_INVALID_ARGUMENT
+    # batches: 1 to 64 problems of non-negative size, checked before any device work
+    g = cb.GroupIndexer(SET8, "expanded")
+    for sizes in ([], [1] * 65, [3, -1]):
+        rows = np.asarray(sizes or [0], np.int64)
+        st = lib.cas_csr_from_positions_batched(g.handle, None, rows.ctypes.data_as(C.c_void_p), len(sizes), None,
+                                                C.byref(h))
+        assert st == L.CAS_ERR_INVALID_ARGUMENT, sizes
+    assert lib.cas_solve_batched(None, C.byref(cb.solve_opts()), None, None, None, None) == L.CAS_ERR_INVALID_ARGUMENT
 
 
 def test_no_cpu_fallback_without_a_device():
