@@ -56,7 +56,18 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--workload", choices=["single", "batched"], default="single",
+                    help="single: the 20M-row fit; batched: 60 per-empty-count fits in one batched solve")
+    ap.add_argument("--problems", type=int, default=60, help="batched: problems (empty counts 1..problems)")
     return ap.parse_args(argv)
+
+
+def batched_problems(seed: int, problems: int = 60, lo: int = 20_000, hi: int = 1_500_000):
+    """Row counts (log-uniform in [lo, hi], seeded) and empty counts 1..problems
+    of the batched workload; problem q's positions come from seed 1000 * seed + q."""
+    rng = np.random.default_rng(seed)
+    rows = np.exp(rng.uniform(np.log(lo), np.log(hi), problems)).astype(np.int64)
+    return rows, np.arange(1, problems + 1)
 
 
 def dist_env():
@@ -313,6 +324,193 @@ def run_ours(args) -> dict | None:
     return result if rank == 0 else None
 
 
+def run_ours_batched(args) -> dict | None:
+    """60 per-empty-count fits (empty counts 1..60, rows log-uniform in
+    [20k, 1.5M], seeded) as one step: batched layout build + one batched
+    mixed-precision PCG to 1e-8 for every problem.  The plain FP64 GPU path
+    fits the same problems one after another on the rows layout."""
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    import cassandra_b200 as cb
+    from cassandra_b200 import _lib as L
+
+    lib = cb.load()
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    seed = args.seed + 7919 * rank
+    rows, empties = batched_problems(seed, args.problems)
+    R = int(rows.sum())
+    pos = torch.cat([cb.generate_positions(1000 * seed + q, int(n), int(e), int(e))
+                     for q, (n, e) in enumerate(zip(rows, empties))])
+    g = cb.GroupIndexer(PATTERNS_8, "expanded")
+    cols, K = g.index_space_size, g.nnz_per_row
+    P = len(rows)
+    a0 = cb.MatrixCSR.from_positions_batched(g, pos, rows)
+    b = cb.generate_targets(a0, seed)
+    torch.cuda.synchronize()
+    nnz = R * K
+
+    # roofline of the FP32 products on the batched layout (all problems active)
+    def time_kernel(fn, n=10):
+        for _ in range(2):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / n * 1e-3
+
+    x32 = torch.randn(P * cols, dtype=torch.float32, device="cuda")
+    y32 = torch.randn(R, dtype=torch.float32, device="cuda")
+    yo = torch.empty(R, dtype=torch.float32, device="cuda")
+    xo = torch.empty(P * cols, dtype=torch.float32, device="cuda")
+    t_ax = time_kernel(lambda: L.check(lib.cas_spmv(a0.handle, L.CAS_F32, C.c_void_p(x32.data_ptr()),
+                                                    C.c_void_p(yo.data_ptr()), sp)))
+    t_aty = time_kernel(lambda: L.check(lib.cas_spmv_t(a0.handle, L.CAS_F32, C.c_void_p(y32.data_ptr()),
+                                                       C.c_void_p(xo.data_ptr()), sp)))
+    bx = 2 * nnz + 4 * R + 4 * P * cols
+    bt = 4 * nnz + 4 * R + 4 * P * cols
+    kernels = {"batched_ax_f32": {"seconds": t_ax, "bytes": bx, "gbs": bx / t_ax / 1e9},
+               "batched_aty_f32": {"seconds": t_aty, "bytes": bt, "gbs": bt / t_aty / 1e9}}
+    schedules = a0.schedules()
+    del x32, y32, yo, xo, a0
+    torch.cuda.synchronize()
+
+    opts_mixed = cb.solve_opts("pcg", "mixed", args.tol, 20000, 50, 50)
+    opts_plain = cb.solve_opts("pcg", "fp64", args.tol, 20000, 50, 50)
+    w = torch.empty(P * cols, dtype=torch.float64, device="cuda")
+    rows_c = np.ascontiguousarray(rows, dtype=np.int64)
+
+    def fit_batched():
+        reps = (L.SolveReport * P)()
+        st = lib.cas_fit_weights_batched_device(g.handle, C.c_void_p(pos.data_ptr()), C.c_void_p(b.data_ptr()),
+                                                rows_c.ctypes.data_as(C.c_void_p), P, C.byref(opts_mixed),
+                                                C.c_void_p(w.data_ptr()), reps, sp)
+        if st != L.CAS_OK:
+            L.check(st)
+        return reps
+
+    for _ in range(args.warmup):
+        fit_batched()
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.cas_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    reps = [fit_batched() for _ in range(args.steps)]
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    launches = lib.cas_kernel_launches() - launches0
+    clk = clocks.stop()
+    elapsed = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        dist.barrier()
+        t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    per_step = elapsed / args.steps
+    last = reps[-1]
+    its = [r.iterations for r in last]
+
+    # plain FP64 GPU path: the problems fitted one after another (rows layout)
+    plain = None
+    if not args.no_plain:
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        r0 = np.concatenate([[0], np.cumsum(rows)])
+        plain_its, plain_rel, plain_t = [], [], []
+        wq = torch.empty(cols, dtype=torch.float64, device="cuda")
+        for q in range(P):
+            rep = L.SolveReport()
+            st = lib.cas_fit_weights_device(g.handle, C.c_void_p(pos[r0[q]:r0[q + 1]].data_ptr()),
+                                            C.c_void_p(b[r0[q]:r0[q + 1]].data_ptr()), int(rows[q]),
+                                            C.byref(opts_plain), C.c_void_p(wq.data_ptr()), C.byref(rep), sp)
+            if st != L.CAS_OK:
+                L.check(st)
+            plain_its.append(rep.iterations)
+            plain_rel.append(rep.rel_residual)
+            plain_t.append(rep.setup_seconds + rep.seconds)
+        p1.record(stream)
+        p1.synchronize()
+        plain = {"step_s": p0.elapsed_time(p1) * 1e-3, "iterations_max": max(plain_its),
+                 "iterations_sum": int(sum(plain_its)), "rel_residual_max": max(plain_rel),
+                 "speedup_batched_mixed_vs_sequential_plain": p0.elapsed_time(p1) * 1e-3 / per_step,
+                 "per_problem": [[int(i), round(t, 5)] for i, t in zip(plain_its, plain_t)]}
+
+    # end to end through the public C ABI with host buffers
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
+    pos_h = torch.empty((R, 2), dtype=torch.int64, pin_memory=True)
+    pos_h.copy_(pos)
+    sc_h = torch.empty(R, dtype=torch.float32, pin_memory=True)
+    sc_h.copy_(b.float())
+    w_h = torch.empty(P * cols, dtype=torch.float32, pin_memory=True)
+    masks = np.asarray(PATTERNS_8, np.uint64)
+    e2e_times = []
+    for _ in range(e2e_steps):
+        hreps = (L.SolveReport * P)()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = lib.cas_fit_weights_batched(masks.ctypes.data_as(C.c_void_p), len(masks), L.CAS_INDEX_EXPANDED,
+                                         C.c_void_p(pos_h.data_ptr()), C.c_void_p(sc_h.data_ptr()),
+                                         rows_c.ctypes.data_as(C.c_void_p), P, C.byref(opts_mixed),
+                                         C.c_void_p(w_h.data_ptr()), hreps)
+        e2e_times.append(time.perf_counter() - t0)
+        L.check(st)
+    e2e_val = statistics.mean(e2e_times) if e2e_times else None
+
+    peak, peak_kind = measured_peaks()
+    dom = max(kernels, key=lambda k: kernels[k]["seconds"])
+    ach = kernels[dom]["gbs"]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_batched(args, seed, rows, empties)
+    result = {
+        "metric": METRIC, "value": per_step, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 products / f64 scalars",
+        "data": "synthetic (seeded random-play positions per empty count, seeded targets)",
+        "config": {
+            "workload": f"{P} per-empty-count 8-pattern expanded fits (empties 1..{P}, rows log-uniform in "
+                        f"[20k, 1.5M], {R} rows in total), one batched mixed Jacobi-PCG to rel. normal-eq. "
+                        f"residual {args.tol:g} per problem",
+            "problems": P, "rows": R, "cols_per_problem": cols, "nnz_per_row": K, "nnz": nnz,
+            "rows_min": int(rows.min()), "rows_max": int(rows.max()), "precision": "mixed", "tol": args.tol,
+            "l2": "inputs larger than L2", "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        },
+        "breakdown": {"build_s": last[0].setup_seconds, "solve_s": last[0].seconds,
+                      "iterations_max": max(its), "iterations_min": min(its),
+                      "rel_residual_max": max(r.rel_residual for r in last),
+                      "per_problem": [[int(n), int(e), int(r.iterations), int(r.refinements)]
+                                      for n, e, r in zip(rows, empties, last)]},
+        "plain_fp64": plain,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": ach / peak, "peak_kind": peak_kind, "traffic": None},
+        "kernels": kernels, "aty_schedules": schedules,
+        "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": int(pos_h.numel() * 8 + sc_h.numel() * 4),
+                "d2h_bytes_per_step": int(w_h.numel() * 4), "steps": e2e_steps},
+        "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": cpu,
+    }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result if rank == 0 else None
+
+
 # ---------------------------------------------------------------- CPU reference
 
 class ReferenceSample:
@@ -380,6 +578,32 @@ def cpu_baseline(args, seed: int, gpu_iterations: int | None = None) -> dict | N
                       f"OpenMP threads {os.environ.get('OMP_NUM_THREADS', os.cpu_count())}"}
 
 
+def cpu_baseline_batched(args, seed: int, rows, empties) -> dict | None:
+    """The reference fitting the batched workload's problems one after another
+    (its training loop's order), on a bounded sample: the first problems in
+    order until about cpu_sample_rows rows, time scaled by total rows."""
+    try:
+        import oracle
+
+        if not oracle.ref_available():
+            return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+                    "sample": "unavailable: oracle/_ref not built"}
+    except Exception as e:  # pragma: no cover
+        return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference", "sample": f"error {e}"}
+    total, done_rows, t, its = int(np.sum(rows)), 0, 0.0, []
+    for q, (n, e) in enumerate(zip(rows, empties)):
+        if done_rows >= args.cpu_sample_rows:
+            break
+        s = ReferenceSample(int(n), 1000 * seed + q, int(e), int(e)).run()
+        t += s["index_s"] + s["solve_s"]
+        its.append(s["iterations"])
+        done_rows += int(n)
+    return {"value": t * total / done_rows, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"first {len(its)} of {len(rows)} problems ({done_rows} of {total} rows), each: reference "
+                      f"indexing + FP64 PCG to 1e-8 ({min(its)}..{max(its)} iterations); time scaled by rows "
+                      f"x{total / done_rows:.3g}"}
+
+
 def run_reference(args) -> dict | None:
     world, rank, _ = dist_env()
     if rank != 0:
@@ -389,6 +613,25 @@ def run_reference(args) -> dict | None:
     if not oracle.ref_available():
         return {"impl": "reference", "metric": METRIC,
                 "unavailable": "oracle/_ref (reference sources compiled here) is missing"}
+    if args.workload == "batched":
+        rows, empties = batched_problems(args.seed, args.problems)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            cbl = cpu_baseline_batched(args, args.seed, rows, empties)
+            if i >= args.warmup:
+                vals.append(cbl["value"])
+        value = statistics.mean(vals)
+        cbl["value"] = value
+        return {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded random-play positions per empty count, seeded targets)",
+            "config": {"workload": f"{args.problems} per-empty-count 8-pattern expanded fits, fitted one after "
+                                   f"another with FP64 Jacobi-PCG to {args.tol:g}", "rows": int(rows.sum())},
+            "cpu_baseline": cbl,
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
     times, last = [], None
     n = min(args.cpu_sample_rows, args.rows)
     sample = ReferenceSample(n, args.seed, args.min_empties, args.max_empties)
@@ -415,7 +658,12 @@ def run_reference(args) -> dict | None:
 
 def main(argv=None) -> int:
     args = parse_args(argv)
-    res = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if args.impl == "reference":
+        res = run_reference(args)
+    elif args.workload == "batched":
+        res = run_ours_batched(args)
+    else:
+        res = run_ours(args)
     if res is not None:
         print(json.dumps(res), flush=True)
     return 0

@@ -147,6 +147,8 @@ SIGNATURES: dict[str, tuple] = {
     "cas_csr_from_positions_batched": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP]),
     "cas_csr_problems": (C.c_int, [_VP, _VP]),
     "cas_solve_batched": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
+    "cas_fit_weights_batched": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int, _VP, _VP, _VP]),
+    "cas_fit_weights_batched_device": (C.c_int, [_VP, _VP, _VP, _VP, C.c_int, _VP, _VP, _VP, _VP]),
     "cas_spmv_norm_noalloc_max_rows": (_I64, []),
     "cas_spmv_norm_noalloc": (C.c_int, [_VP, C.c_int, _I64, _I64, _VP, _VP, _VP, _VP]),
 }

@@ -34,8 +34,19 @@ constexpr int kBVecThreads = 256;
 constexpr int kBRedThreads = 512;
 
 // Per-problem scalar slots (stride kBSlots) and flags (stride kBFlags).
-enum BSlot { bRz = 0, bPap, bAlpha, bBeta, bRr, bBn2, bRes, bTol, bTrue, kBSlots };
-enum BFlag { bStatus = 0, bIter, bRefine, kBFlags };
+enum BSlot { bRz = 0, bPap, bAlpha, bBeta, bRr, bBn2, bRes, bTol, bTrue, bRrRef, kBSlots };
+enum BFlag { bStatus = 0, bIter, bRefine, bRestart, bIterRef, kBFlags };
+
+// A replacement that finds the recursive residual off by more than this
+// (relative) restarts the problem's search direction (as in the single
+// solver: the FP32 product errors have reached p).
+constexpr double kBRestartDeviation = 0.1;
+
+// Residual replacements of the mixed solver are scheduled per problem as in
+// the single solver: after a drop of kBReplaceDrop since the last one, after
+// refine_every iterations, or when the recursive residual meets the
+// tolerance (a problem retires on its true residual only).
+constexpr double kBReplaceDrop = 1e-4;
 
 struct BDev {
     double* scal;   // [nprob][kBSlots]
@@ -43,10 +54,20 @@ struct BDev {
     int* pdone;     // [nprob] retired problems
     int* ndone;     // number of retired problems
     int* alldone;   // 1 once every problem is retired (products return at entry)
+    int* pskip;     // [nprob] no residual replacement due (retired problems included)
+    int* nneed;     // problems with a replacement due this iteration
+    int* skipall;   // 1 while no problem has a replacement due
     int nprob;
 };
 
 __device__ __forceinline__ bool retired(const BDev& d, int q) { return *(volatile const int*)(d.pdone + q) != 0; }
+
+__device__ __forceinline__ void retire(const BDev& d, int q)
+{
+    d.pdone[q] = 1;
+    d.pskip[q] = 1;
+    if (atomicAdd(d.ndone, 1) + 1 == d.nprob) *d.alldone = 1;
+}
 
 template <bool COMP>
 __device__ __forceinline__ void bacc(Comp& c, double x)
@@ -57,14 +78,66 @@ __device__ __forceinline__ void bacc(Comp& c, double x)
         c.s += x;
 }
 
-// Partial (s, c) of one CTA into part[2 * (q * nbx + bx)].
+// The problems a vector step works on, in problem order: the CTAs of the
+// step's 1D grid are dealt round-robin over them (CTA i serves list slot
+// i % n as its (i / n)-th CTA), so a lone remaining problem gets the whole
+// grid and 60 problems about 10 CTAs each.  Partials live at
+// part[q][rank]; a reduction over problem q sums the ranks its slot had.
+struct ActiveList {
+    int n;
+    int list[kMaxProblems];
+    int pos[kMaxProblems];  // slot of each problem, -1 if absent
+};
+
+struct Slot {
+    int q, rank, ranks;  // problem, CTA rank within it, CTAs serving it
+};
+
+__device__ __forceinline__ bool cta_slot(const ActiveList* al, Slot& sl)
+{
+    const int n = al->n;
+    if (n == 0) return false;
+    const int a = static_cast<int>(blockIdx.x) % n;
+    sl.q = al->list[a];
+    sl.rank = static_cast<int>(blockIdx.x) / n;
+    sl.ranks = (static_cast<int>(gridDim.x) - a + n - 1) / n;
+    return true;
+}
+
+// CTAs that served problem q in a step over G CTAs (0 if q is not listed).
+__device__ __forceinline__ int ranks_of(const ActiveList* al, int q, int G)
+{
+    const int n = al->n, a = al->pos[q];
+    return (n == 0 || a < 0) ? 0 : (G - a + n - 1) / n;
+}
+
+// Rebuilds the list of problems not retired (one warp per 32 problems).
+__global__ void bcompact_kernel(const int* __restrict__ pdone, int nprob, ActiveList* al)
+{
+    __shared__ int base[3];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;  // 64 threads
+    const bool act = t < nprob && !*(volatile const int*)(pdone + t);
+    const unsigned m = __ballot_sync(0xffffffffu, act);
+    if (lane == 0) base[w + 1] = __popc(m);
+    if (t == 0) base[0] = 0;
+    __syncthreads();
+    const int before = (w == 0 ? 0 : base[1]) + __popc(m & ((1u << lane) - 1));
+    if (t < nprob) {
+        al->pos[t] = act ? before : -1;
+        if (act) al->list[before] = t;
+    }
+    if (t == 0) al->n = base[1] + base[2];
+}
+
+// Partial (s, c) of one CTA into part[2 * (q * G + rank)].
 template <bool COMP>
-__device__ void bwrite(double* part, int q, int nbx, Comp v, double* smem)
+__device__ void bwrite(double* part, const Slot& sl, Comp v, double* smem)
 {
     const Comp r = block_sum_comp<kBVecThreads>(v, smem);
     if (threadIdx.x == 0) {
-        part[2 * (q * nbx + blockIdx.x)] = r.s;
-        part[2 * (q * nbx + blockIdx.x) + 1] = COMP ? r.c : 0.0;
+        const int64_t i = static_cast<int64_t>(sl.q) * gridDim.x + sl.rank;
+        part[2 * i] = r.s;
+        part[2 * i + 1] = COMP ? r.c : 0.0;
     }
 }
 
@@ -85,54 +158,64 @@ __device__ double bsum(const double* part, int n, double* smem)
     return block_sum<kBRedThreads>(acc.s, smem);
 }
 
-// ||A'q||^2 per problem from the product partials (T = partial type).
+// ||A'q||^2 per listed problem from the product partials (T = partial type).
 template <typename T>
-__global__ void __launch_bounds__(kBVecThreads) bnorm_kernel(FastCols fc, const T* __restrict__ partial, int nbx,
-                                                             double* __restrict__ part, BDev d, int skip_retired)
+__global__ void __launch_bounds__(kBVecThreads) bnorm_kernel(FastCols fc, const T* __restrict__ partial,
+                                                             double* __restrict__ part, const ActiveList* al)
 {
     __shared__ double smem[64];
-    const int q = blockIdx.y;
-    if (skip_retired && retired(d, q)) return;
-    const int64_t P = fc.g.pcols, base = q * P;
+    Slot sl;
+    if (!cta_slot(al, sl)) return;
+    const int64_t P = fc.g.pcols, base = sl.q * P;
     Comp acc;
-    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < P;
-         c += static_cast<int64_t>(nbx) * blockDim.x) {
+    for (int64_t c = static_cast<int64_t>(sl.rank) * blockDim.x + threadIdx.x; c < P;
+         c += static_cast<int64_t>(sl.ranks) * blockDim.x) {
         const double v = fast_col_sum<T>(fc, partial, base + c);
         acc.add(v * v);
     }
-    bwrite<true>(part, q, nbx, acc, smem);
+    bwrite<true>(part, sl, acc, smem);
 }
 
-__global__ void __launch_bounds__(kBRedThreads) bstore_kernel(const double* __restrict__ part, int nbx, BDev d,
-                                                              int slot, int skip_retired)
+__global__ void __launch_bounds__(kBRedThreads) bstore_kernel(const double* __restrict__ part, int G,
+                                                              const ActiveList* al, BDev d, int slot)
 {
     __shared__ double smem[64];
     const int q = blockIdx.x;
-    if (skip_retired && retired(d, q)) return;
-    const double v = bsum<true>(part + 2 * q * nbx, nbx, smem);
+    const int k = ranks_of(al, q, G);
+    if (k == 0) return;
+    const double v = bsum<true>(part + 2 * static_cast<int64_t>(q) * G, k, smem);
     if (threadIdx.x == 0) d.scal[q * kBSlots + slot] = v;
 }
 
 // r = A'(b - A x) from the FP64 product, z = D r; p = z on (re)start.
-// Partials of r.z and r.r per (problem, CTA).
+// Partials of r.z and r.r per (problem, CTA), and (part_dev not null) of
+// ||r_rec - r||^2 against the recursive residual being replaced.
 template <bool COMP, typename G>
 __global__ void __launch_bounds__(kBVecThreads) bresidual_kernel(FastCols fc, const double* __restrict__ partial,
                                                                  double* __restrict__ r, double* __restrict__ z,
                                                                  double* __restrict__ p, G* __restrict__ pg,
-                                                                 const double* __restrict__ dinv, int nbx,
+                                                                 const double* __restrict__ dinv,
+                                                                 const ActiveList* al,
                                                                  double* __restrict__ part_rz,
-                                                                 double* __restrict__ part_rr, int restart, BDev d)
+                                                                 double* __restrict__ part_rr, int restart, BDev d,
+                                                                 double* __restrict__ part_dev,
+                                                                 const int* __restrict__ qgate)
 {
     __shared__ double smem[64];
-    const int q = blockIdx.y;
-    if (retired(d, q)) return;
+    Slot sl;
+    if (!cta_slot(al, sl) || *(volatile const int*)(qgate + sl.q)) return;
+    const int q = sl.q;
     const int64_t P = fc.g.pcols, base = q * P;
-    Comp rz, rr;
-    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < P;
-         c += static_cast<int64_t>(nbx) * blockDim.x) {
+    Comp rz, rr, dev;
+    for (int64_t c = static_cast<int64_t>(sl.rank) * blockDim.x + threadIdx.x; c < P;
+         c += static_cast<int64_t>(sl.ranks) * blockDim.x) {
         const int64_t i = base + c;
         const double rc = fast_col_sum<double>(fc, partial, i);
         const double zc = dinv[i] * rc;
+        if (part_dev) {
+            const double dd = r[i] - rc;
+            bacc<COMP>(dev, dd * dd);
+        }
         r[i] = rc;
         z[i] = zc;
         if (restart) {
@@ -142,12 +225,31 @@ __global__ void __launch_bounds__(kBVecThreads) bresidual_kernel(FastCols fc, co
         bacc<COMP>(rz, rc * zc);
         bacc<COMP>(rr, rc * rc);
     }
-    bwrite<COMP>(part_rz, q, nbx, rz, smem);
-    bwrite<COMP>(part_rr, q, nbx, rr, smem);
+    bwrite<COMP>(part_rz, sl, rz, smem);
+    bwrite<COMP>(part_rr, sl, rr, smem);
+    if (part_dev) bwrite<COMP>(part_dev, sl, dev, smem);
+}
+
+// p = z (and the gather copy) for the problems whose replacement set bRestart.
+template <typename G>
+__global__ void __launch_bounds__(kBVecThreads) brestart_kernel(int64_t P, const ActiveList* al,
+                                                                const double* __restrict__ z, double* __restrict__ p,
+                                                                G* __restrict__ pg, BDev d)
+{
+    Slot sl;
+    if (!cta_slot(al, sl)) return;
+    const int q = sl.q;
+    if (retired(d, q) || !*(volatile const int*)(d.flags + q * kBFlags + bRestart)) return;
+    const int64_t base = q * P;
+    for (int64_t c = static_cast<int64_t>(sl.rank) * blockDim.x + threadIdx.x; c < P;
+         c += static_cast<int64_t>(sl.ranks) * blockDim.x) {
+        p[base + c] = z[base + c];
+        if (pg) pg[base + c] = static_cast<G>(z[base + c]);
+    }
 }
 
 // alpha = rz / p'A'Ap per problem; p'A'Ap = sum of the A p norm partials of
-// the problem's blocks.  Breakdown when p'A'Ap <= 0 with rz > 0.
+// the problem's blocks.
 template <bool COMP>
 __global__ void __launch_bounds__(kBRedThreads) balpha_kernel(FastGeometry g, const double* __restrict__ part_q, BDev d)
 {
@@ -161,10 +263,13 @@ __global__ void __launch_bounds__(kBRedThreads) balpha_kernel(FastGeometry g, co
         sc[bPap] = pap;
         const double rz = sc[bRz];
         if (!(pap > 0) || !isfinite(pap)) {
+            // not finite: breakdown.  <= 0: p lies in the null space of A (a
+            // rank-deficient problem, or the residual at rounding level);
+            // the problem retires and the FP64 true residual decides
+            // between converged and a restart from it.
             sc[bAlpha] = 0;
-            if (rz > 0 || !isfinite(pap)) d.flags[q * kBFlags + bStatus] = CAS_ERR_BREAKDOWN;
-            d.pdone[q] = 1;
-            if (atomicAdd(d.ndone, 1) + 1 == d.nprob) *d.alldone = 1;
+            if (!isfinite(pap)) d.flags[q * kBFlags + bStatus] = CAS_ERR_BREAKDOWN;
+            retire(d, q);
         } else {
             sc[bAlpha] = rz / pap;
         }
@@ -176,18 +281,20 @@ template <bool COMP, typename T>
 __global__ void __launch_bounds__(kBVecThreads) bupdate_kernel(FastCols fc, const T* __restrict__ partial,
                                                                double* __restrict__ x, double* __restrict__ r,
                                                                double* __restrict__ z, const double* __restrict__ p,
-                                                               const double* __restrict__ dinv, int nbx,
+                                                               const double* __restrict__ dinv,
+                                                               const ActiveList* al,
                                                                double* __restrict__ part_rz,
                                                                double* __restrict__ part_rr, BDev d)
 {
     __shared__ double smem[64];
-    const int q = blockIdx.y;
-    if (retired(d, q)) return;
+    Slot sl;
+    if (!cta_slot(al, sl) || retired(d, sl.q)) return;
+    const int q = sl.q;
     const double alpha = d.scal[q * kBSlots + bAlpha];
     const int64_t P = fc.g.pcols, base = q * P;
     Comp rz, rr;
-    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < P;
-         c += static_cast<int64_t>(nbx) * blockDim.x) {
+    for (int64_t c = static_cast<int64_t>(sl.rank) * blockDim.x + threadIdx.x; c < P;
+         c += static_cast<int64_t>(sl.ranks) * blockDim.x) {
         const int64_t i = base + c;
         const double s = fast_col_sum<T>(fc, partial, i);
         x[i] += alpha * p[i];
@@ -198,25 +305,32 @@ __global__ void __launch_bounds__(kBVecThreads) bupdate_kernel(FastCols fc, cons
         bacc<COMP>(rz, rc * zc);
         bacc<COMP>(rr, rc * rc);
     }
-    bwrite<COMP>(part_rz, q, nbx, rz, smem);
-    bwrite<COMP>(part_rr, q, nbx, rr, smem);
+    bwrite<COMP>(part_rz, sl, rz, smem);
+    bwrite<COMP>(part_rr, sl, rr, smem);
 }
 
 // rz_new, rr -> beta, relative residual, retirement.  replace != 0: residual
 // replacement (r.z replaced, beta and the iteration count left alone).
 template <bool COMP>
 __global__ void __launch_bounds__(kBRedThreads) bbeta_kernel(const double* __restrict__ part_rz,
-                                                             const double* __restrict__ part_rr, int nbx, BDev d,
-                                                             int replace)
+                                                             const double* __restrict__ part_rr, int G,
+                                                             const ActiveList* al, BDev d, int replace,
+                                                             const double* __restrict__ part_dev,
+                                                             const int* __restrict__ qgate, int plan_refine)
 {
     __shared__ double smem[64];
     const int q = blockIdx.x;
-    if (retired(d, q)) return;
-    const double rz_new = bsum<COMP>(part_rz + 2 * q * nbx, nbx, smem);
-    const double rr = bsum<COMP>(part_rr + 2 * q * nbx, nbx, smem);
+    if (*(volatile const int*)(qgate + q)) return;
+    const int k = ranks_of(al, q, G);
+    if (k == 0) return;
+    const int64_t o = 2 * static_cast<int64_t>(q) * G;
+    const double rz_new = bsum<COMP>(part_rz + o, k, smem);
+    const double rr = bsum<COMP>(part_rr + o, k, smem);
+    const double dev2 = part_dev ? bsum<COMP>(part_dev + o, k, smem) : 0.0;
     if (threadIdx.x == 0) {
         double* sc = d.scal + q * kBSlots;
         int* fl = d.flags + q * kBFlags;
+        if (part_dev) fl[bRestart] = dev2 > kBRestartDeviation * kBRestartDeviation * rr ? 1 : 0;
         const double rz = sc[bRz];
         const double bn2 = sc[bBn2];
         const double res = bn2 > 0 ? sqrt(rr / bn2) : sqrt(rr);
@@ -229,31 +343,47 @@ __global__ void __launch_bounds__(kBRedThreads) bbeta_kernel(const double* __res
         sc[bRz] = rz_new;
         sc[bRr] = rr;
         sc[bRes] = res;
-        bool stop = false;
+        if (replace) {
+            sc[bRrRef] = rr;
+            fl[bIterRef] = fl[bIter];
+        }
+        const bool met = rr == 0 || (sc[bTol] > 0 && res <= sc[bTol]);
         if (!isfinite(rz_new) || !isfinite(rr)) {
             fl[bStatus] = CAS_ERR_BREAKDOWN;
-            stop = true;
-        } else if (rr == 0 || (sc[bTol] > 0 && res <= sc[bTol])) {
-            stop = true;
-        }
-        if (stop) {
-            d.pdone[q] = 1;
-            if (atomicAdd(d.ndone, 1) + 1 == d.nprob) *d.alldone = 1;
+            retire(d, q);
+        } else if (!replace && plan_refine > 0) {
+            fl[bRestart] = 0;
+            const bool due = met || rr <= kBReplaceDrop * kBReplaceDrop * sc[bRrRef] ||
+                             fl[bIter] - fl[bIterRef] >= plan_refine;
+            d.pskip[q] = due ? 0 : 1;
+            if (due) atomicAdd(d.nneed, 1);
+        } else if (met) {
+            retire(d, q);
         }
     }
 }
 
+// Whole-launch gate of this iteration's replacement step: set while no
+// problem has one due; resets the count for the next iteration.
+__global__ void bgate_kernel(BDev d)
+{
+    *d.skipall = (*d.alldone || *d.nneed == 0) ? 1 : 0;
+    *d.nneed = 0;
+}
+
 // p = z + beta p (and the gather copy).
 template <typename G>
-__global__ void __launch_bounds__(kBVecThreads) bdirection_kernel(int64_t P, int nbx, const double* __restrict__ z,
-                                                                  double* __restrict__ p, G* __restrict__ pg, BDev d)
+__global__ void __launch_bounds__(kBVecThreads) bdirection_kernel(int64_t P, const ActiveList* al,
+                                                                  const double* __restrict__ z, double* __restrict__ p,
+                                                                  G* __restrict__ pg, BDev d)
 {
-    const int q = blockIdx.y;
-    if (retired(d, q)) return;
+    Slot sl;
+    if (!cta_slot(al, sl) || retired(d, sl.q)) return;
+    const int q = sl.q;
     const double beta = d.scal[q * kBSlots + bBeta];
     const int64_t base = q * P;
-    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < P;
-         c += static_cast<int64_t>(nbx) * blockDim.x) {
+    for (int64_t c = static_cast<int64_t>(sl.rank) * blockDim.x + threadIdx.x; c < P;
+         c += static_cast<int64_t>(sl.ranks) * blockDim.x) {
         const int64_t i = base + c;
         const double v = z[i] + beta * p[i];
         p[i] = v;
@@ -282,16 +412,18 @@ struct BatchSolver {
     cudaStream_t s = nullptr;
     bool own_stream = false;
     bool mixed = false;
-    int B = 0, nbx = 1;
+    int B = 0, G = 1;  // problems; CTAs of a vector step
     int64_t P = 0, C = 0, R = 0;
     double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *dinv = nullptr;
     float* pg32 = nullptr;
     void* q = nullptr;
     double* q64 = nullptr;
     const double* b = nullptr;
-    double *part_q = nullptr, *part_a = nullptr, *part_b = nullptr;
+    double *part_q = nullptr, *part_a = nullptr, *part_b = nullptr, *part_c = nullptr;
     double* scal = nullptr;
-    int* flags = nullptr;  // [B][kBFlags] then pdone[B], ndone, alldone
+    int* flags = nullptr;  // [B][kBFlags] then pdone[B], ndone, alldone, pskip[B], nneed, skipall
+    ActiveList* act = nullptr;  // problems not retired (rebuilt every iteration)
+    ActiveList* all = nullptr;  // every problem
     std::vector<double> h_scal;
     std::vector<int> h_flags;
     cudaGraphExec_t graph = nullptr;
@@ -307,11 +439,14 @@ struct BatchSolver {
         d.pdone = flags + B * kBFlags;
         d.ndone = d.pdone + B;
         d.alldone = d.ndone + 1;
+        d.pskip = d.alldone + 1;
+        d.nneed = d.pskip + B;
+        d.skipall = d.nneed + 1;
         d.nprob = B;
         return d;
     }
-    int nflags() const { return B * kBFlags + B + 2; }
-    dim3 vgrid() const { return dim3(static_cast<unsigned>(nbx), static_cast<unsigned>(B)); }
+    int nflags() const { return B * kBFlags + B + 2 + B + 2; }
+    dim3 vgrid() const { return dim3(static_cast<unsigned>(G)); }
 
     ~BatchSolver()
     {
@@ -321,35 +456,60 @@ struct BatchSolver {
             cudaStreamDestroy(s);
         }
         for (void* ptr : {(void*)x, (void*)r, (void*)z, (void*)p, (void*)dinv, (void*)pg32, q, (void*)q64,
-                          (void*)part_q, (void*)part_a, (void*)part_b, (void*)scal, (void*)flags})
+                          (void*)part_q, (void*)part_a, (void*)part_b, (void*)part_c, (void*)scal,
+                          (void*)flags, (void*)act, (void*)all})
             cudaFree(ptr);
     }
 
-    // A'(b - A x) in FP64 into the t64 partials; retired problems skipped
-    // when `gate`.
-    cas_status residual_products(bool gate)
+    // How a residual replacement selects its problems.
+    enum class Sel { All, Active, Due };
+
+    // A'(b - A x) in FP64 into the t64 partials, for all problems, the
+    // active ones, or those with a replacement due.
+    cas_status residual_products(Sel sel)
     {
         const BDev d = dev();
-        CAS_TRY((fast_spmv<double, double>(*f, x, q64, b, nullptr, part_q, gate ? d.alldone : nullptr, 2, s, nullptr,
-                                           gate ? d.pdone : nullptr)));
-        return fast_spmv_t_partials<double>(*f, q64, gate ? d.alldone : nullptr, s, gate ? d.pdone : nullptr);
+        int* whole = sel == Sel::All ? nullptr : (sel == Sel::Active ? d.alldone : d.skipall);
+        const int* per = sel == Sel::All ? nullptr : (sel == Sel::Active ? d.pdone : d.pskip);
+        CAS_TRY((fast_spmv<double, double>(*f, x, q64, b, nullptr, part_q, whole, 2, s, nullptr, per)));
+        return fast_spmv_t_partials<double>(*f, q64, whole, s, per);
     }
 
     // Residual replacement (restart: p = z too) for the active problems.
+    // Residual replacement.  Sel::All / Sel::Active (set-up, resumption):
+    // r, z and p = z restart.  Sel::Due (the in-graph step of the mixed
+    // solver, every iteration, gated by the beta kernel's schedule): measures
+    // the recursive residual's drift and restarts the direction of the
+    // problems whose drift exceeds kBRestartDeviation; retires the problems
+    // whose true residual meets the tolerance.
     template <bool COMP>
-    cas_status refine(bool restart, bool gate)
+    cas_status refine(Sel sel)
     {
-        CAS_TRY(residual_products(gate));
+        CAS_TRY(residual_products(sel));
         const BDev d = dev();
         const FastCols fc = fast_cols<double>(*f);
         const double* t64 = static_cast<const double*>(f->t64.partial);
+        const bool restart = sel != Sel::Due;
+        double* pdev = restart ? nullptr : part_c;
+        const int* qgate = sel == Sel::Due ? d.pskip : d.pdone;
+        // Sel::All works on every problem; the others on the active list
+        // (rebuilt here after the host resumed problems)
+        if (sel == Sel::Active) { bcompact_kernel<<<1, 64, 0, s>>>(d.pdone, B, act); cas::count_launch(); }
+        const ActiveList* al = sel == Sel::All ? all : act;
         if (mixed)
-            { bresidual_kernel<COMP, float><<<vgrid(), kBVecThreads, 0, s>>>(fc, t64, r, z, p, pg32, dinv, nbx, part_a,
-                                                                        part_b, restart ? 1 : 0, d); cas::count_launch(); }
+            { bresidual_kernel<COMP, float><<<vgrid(), kBVecThreads, 0, s>>>(fc, t64, r, z, p, pg32, dinv, al, part_a,
+                                                                        part_b, restart ? 1 : 0, d, pdev, qgate); cas::count_launch(); }
         else
-            { bresidual_kernel<COMP, double><<<vgrid(), kBVecThreads, 0, s>>>(fc, t64, r, z, p, nullptr, dinv, nbx,
-                                                                         part_a, part_b, restart ? 1 : 0, d); cas::count_launch(); }
-        { bbeta_kernel<COMP><<<B, kBRedThreads, 0, s>>>(part_a, part_b, nbx, d, 1); cas::count_launch(); }
+            { bresidual_kernel<COMP, double><<<vgrid(), kBVecThreads, 0, s>>>(fc, t64, r, z, p, nullptr, dinv, al,
+                                                                         part_a, part_b, restart ? 1 : 0, d, pdev,
+                                                                         qgate); cas::count_launch(); }
+        { bbeta_kernel<COMP><<<B, kBRedThreads, 0, s>>>(part_a, part_b, G, al, d, 1, pdev, qgate, 0); cas::count_launch(); }
+        if (pdev) {
+            if (mixed)
+                { brestart_kernel<float><<<vgrid(), kBVecThreads, 0, s>>>(P, al, z, p, pg32, d); cas::count_launch(); }
+            else
+                { brestart_kernel<double><<<vgrid(), kBVecThreads, 0, s>>>(P, al, z, p, nullptr, d); cas::count_launch(); }
+        }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     }
@@ -359,6 +519,7 @@ struct BatchSolver {
     {
         const BDev d = dev();
         const T* pgather = std::is_same<T, float>::value ? reinterpret_cast<const T*>(pg32) : reinterpret_cast<const T*>(p);
+        { bcompact_kernel<<<1, 64, 0, s>>>(d.pdone, B, act); cas::count_launch(); }
         CAS_TRY((fast_spmv<T, T>(*f, pgather, static_cast<T*>(q), nullptr, nullptr, part_q, d.alldone, 0, s, nullptr,
                                  d.pdone)));
         CAS_TRY(fast_spmv_t_partials<T>(*f, static_cast<const T*>(q), d.alldone, s, d.pdone));
@@ -366,12 +527,14 @@ struct BatchSolver {
         const FastCols fc = fast_cols<T>(*f);
         { bupdate_kernel<COMP, T><<<vgrid(), kBVecThreads, 0, s>>>(fc, static_cast<const T*>(sizeof(T) == 4 ? f->t32.partial
                                                                                                         : f->t64.partial),
-                                                                  x, r, z, p, dinv, nbx, part_a, part_b, d); cas::count_launch(); }
-        { bbeta_kernel<COMP><<<B, kBRedThreads, 0, s>>>(part_a, part_b, nbx, d, 0); cas::count_launch(); }
+                                                                  x, r, z, p, dinv, act, part_a, part_b, d); cas::count_launch(); }
+        { bbeta_kernel<COMP><<<B, kBRedThreads, 0, s>>>(part_a, part_b, G, act, d, 0, nullptr, d.pdone,
+                                                       mixed ? std::max(o.refine_every, 1) : 0); cas::count_launch(); }
+        if (mixed) { bgate_kernel<<<1, 1, 0, s>>>(d); cas::count_launch(); }
         if (mixed)
-            { bdirection_kernel<float><<<vgrid(), kBVecThreads, 0, s>>>(P, nbx, z, p, pg32, d); cas::count_launch(); }
+            { bdirection_kernel<float><<<vgrid(), kBVecThreads, 0, s>>>(P, act, z, p, pg32, d); cas::count_launch(); }
         else
-            { bdirection_kernel<double><<<vgrid(), kBVecThreads, 0, s>>>(P, nbx, z, p, nullptr, d); cas::count_launch(); }
+            { bdirection_kernel<double><<<vgrid(), kBVecThreads, 0, s>>>(P, act, z, p, nullptr, d); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     }
@@ -380,7 +543,7 @@ struct BatchSolver {
     {
         if (mixed) {
             CAS_TRY((iteration<true, float>()));
-            if (o.refine_every > 0 && (global_index + 1) % o.refine_every == 0) CAS_TRY(refine<true>(false, true));
+            CAS_TRY(refine<true>(Sel::Due));  // runs only for problems the beta kernel scheduled
         } else {
             CAS_TRY((iteration<false, double>()));
         }
@@ -389,8 +552,7 @@ struct BatchSolver {
 
     cas_status issue_chunk(int first, int n)
     {
-        const int period = (mixed && o.refine_every > 0) ? o.refine_every : 1;
-        const int phase = first % period;
+        const int phase = 0;  // every iteration is the same graph segment
         if (n > 1) {
             if (!graph || graph_len != n || graph_phase != phase) {
                 if (graph) {
@@ -436,11 +598,11 @@ struct BatchSolver {
     // ||A'(b - A x)||^2 of every problem into slot bTrue (all problems).
     cas_status true_residuals()
     {
-        CAS_TRY(residual_products(false));
+        CAS_TRY(residual_products(Sel::All));
         const BDev d = dev();
         { bnorm_kernel<double><<<vgrid(), kBVecThreads, 0, s>>>(fast_cols<double>(*f), static_cast<const double*>(f->t64.partial),
-                                                                nbx, part_a, d, 0); cas::count_launch(); }
-        { bstore_kernel<<<B, kBRedThreads, 0, s>>>(part_a, nbx, d, bTrue, 0); cas::count_launch(); }
+                                                                part_a, all); cas::count_launch(); }
+        { bstore_kernel<<<B, kBRedThreads, 0, s>>>(part_a, G, all, d, bTrue); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         return read_state();
     }
@@ -460,8 +622,7 @@ struct BatchSolver {
         R = f->g.rows;
         b = d_b;
         mixed = o.precision == CAS_MIXED;
-        nbx = static_cast<int>(std::max<int64_t>(
-            1, std::min<int64_t>((P + kBVecThreads - 1) / kBVecThreads, (4LL * sm_count() + B - 1) / B)));
+        G = 4 * sm_count();
         if (stream) {
             s = static_cast<cudaStream_t>(stream);
         } else {
@@ -474,8 +635,21 @@ struct BatchSolver {
         CAS_CUDA(cudaMalloc(&q, mixed ? sizeof(float) * std::max<int64_t>(R, 1) : rb));
         CAS_CUDA(cudaMalloc(&q64, rb));
         CAS_CUDA(cudaMalloc(&part_q, sizeof(double) * 2 * std::max<int64_t>(f->g.nblocks, 1)));
-        CAS_CUDA(cudaMalloc(&part_a, sizeof(double) * 2 * B * nbx));
-        CAS_CUDA(cudaMalloc(&part_b, sizeof(double) * 2 * B * nbx));
+        CAS_CUDA(cudaMalloc(&part_a, sizeof(double) * 2 * B * G));
+        CAS_CUDA(cudaMalloc(&part_b, sizeof(double) * 2 * B * G));
+        CAS_CUDA(cudaMalloc(&part_c, sizeof(double) * 2 * B * G));
+        CAS_CUDA(cudaMalloc(&act, sizeof(ActiveList)));
+        CAS_CUDA(cudaMalloc(&all, sizeof(ActiveList)));
+        {
+            ActiveList h{};
+            h.n = B;
+            for (int qq = 0; qq < kMaxProblems; qq++) {
+                h.list[qq] = qq < B ? qq : 0;
+                h.pos[qq] = qq < B ? qq : -1;
+            }
+            CAS_CUDA(cudaMemcpy(all, &h, sizeof h, cudaMemcpyHostToDevice));
+            CAS_CUDA(cudaMemcpy(act, &h, sizeof h, cudaMemcpyHostToDevice));
+        }
         CAS_CUDA(cudaMalloc(&scal, sizeof(double) * B * kBSlots));
         h_scal.assign(static_cast<size_t>(B) * kBSlots, 0.0);
         CAS_CUDA(cudaMalloc(&flags, sizeof(int) * nflags()));
@@ -492,18 +666,21 @@ struct BatchSolver {
         // ||A'b||^2 per problem
         CAS_TRY(fast_spmv_t_partials<double>(*f, b, nullptr, s, nullptr));
         { bnorm_kernel<double><<<vgrid(), kBVecThreads, 0, s>>>(fast_cols<double>(*f), static_cast<const double*>(f->t64.partial),
-                                                                nbx, part_a, d, 0); cas::count_launch(); }
-        { bstore_kernel<<<B, kBRedThreads, 0, s>>>(part_a, nbx, d, bBn2, 0); cas::count_launch(); }
+                                                                part_a, all); cas::count_launch(); }
+        { bstore_kernel<<<B, kBRedThreads, 0, s>>>(part_a, G, all, d, bBn2); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
-        // r = A'b, z = D r, p = z (x = 0)
+        // r = A'b, z = D r, p = z (x = 0); no replacement due yet
         if (mixed)
-            CAS_TRY(refine<true>(true, false));
+            CAS_TRY(refine<true>(Sel::All));
         else
-            CAS_TRY(refine<false>(true, false));
+            CAS_TRY(refine<false>(Sel::All));
         CAS_TRY(read_state());
-        // the initial residual counted as a refinement: reset the counters
+        // the initial residual counted as a refinement: reset the counters;
+        // no replacement is due before the first iteration's schedule
         for (int qq = 0; qq < B; qq++) h_flags[qq * kBFlags + bRefine] = 0;
-        CAS_CUDA(cudaMemcpyAsync(flags, h_flags.data(), sizeof(int) * B * kBFlags, cudaMemcpyHostToDevice, s));
+        for (int qq = 0; qq < B; qq++) h_flags[B * kBFlags + B + 2 + qq] = 1;
+        h_flags[B * kBFlags + B + 2 + B + 1] = 1;
+        CAS_CUDA(cudaMemcpyAsync(flags, h_flags.data(), sizeof(int) * nflags(), cudaMemcpyHostToDevice, s));
         CAS_CUDA(cudaStreamSynchronize(s));
         return CAS_OK;
     }
@@ -548,12 +725,15 @@ struct BatchSolver {
                 std::vector<int> tail(pdh);
                 tail.push_back(nd);
                 tail.push_back(0);
-                CAS_CUDA(cudaMemcpyAsync(flags + B * kBFlags, tail.data(), sizeof(int) * (B + 2),
+                tail.insert(tail.end(), pdh.begin(), pdh.end());  // pskip: retired ones stay skipped
+                tail.push_back(0);
+                tail.push_back(1);
+                CAS_CUDA(cudaMemcpyAsync(flags + B * kBFlags, tail.data(), sizeof(int) * (2 * B + 4),
                                          cudaMemcpyHostToDevice, s));
                 if (mixed)
-                    CAS_TRY(refine<true>(true, true));
+                    CAS_TRY(refine<true>(Sel::Active));
                 else
-                    CAS_TRY(refine<false>(true, true));
+                    CAS_TRY(refine<false>(Sel::Active));
                 CAS_CUDA(cudaStreamSynchronize(s));  // the host vector above must outlive the copy
                 verified = false;
                 continue;

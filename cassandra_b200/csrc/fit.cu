@@ -222,4 +222,91 @@ CAS_API cas_status cas_fit_weights(const uint64_t* masks, int n_masks, cas_index
     return st;
 }
 
+CAS_API cas_status cas_fit_weights_batched_device(const cas_patterns* p, const uint64_t* d_positions,
+                                                  const double* d_scores, const int64_t* h_problem_rows,
+                                                  int problems, const cas_solve_opts* o, double* d_weights,
+                                                  cas_solve_report* reports, void* stream)
+{
+    CAS_REQUIRE(p && o && d_weights && h_problem_rows, CAS_ERR_INVALID_ARGUMENT,
+                "cas_fit_weights_batched_device: null argument");
+    auto s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0, e1;
+    CAS_CUDA(cudaEventCreate(&e0));
+    CAS_CUDA(cudaEventCreate(&e1));
+    CAS_CUDA(cudaEventRecord(e0, s));
+    cas_csr* a = nullptr;
+    cas_status st = cas_csr_from_positions_batched(p, d_positions, h_problem_rows, problems, stream, &a);
+    if (st != CAS_OK) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return st;
+    }
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float setup_ms = 0;
+    cudaEventElapsedTime(&setup_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st = cas_solve_batched(a, o, d_scores, d_weights, reports, stream);
+    if (reports)
+        for (int q = 0; q < problems; q++) reports[q].setup_seconds = setup_ms * 1e-3;
+    cas_csr_destroy(a);
+    return st;
+}
+
+CAS_API cas_status cas_fit_weights_batched(const uint64_t* masks, int n_masks, cas_index_mode mode,
+                                           const uint64_t* h_positions, const float* h_scores,
+                                           const int64_t* h_problem_rows, int problems, const cas_solve_opts* o,
+                                           float* h_weights, cas_solve_report* reports)
+{
+    CAS_REQUIRE(masks && o && h_weights && h_problem_rows && problems >= 1, CAS_ERR_INVALID_ARGUMENT,
+                "cas_fit_weights_batched: bad argument");
+    int64_t rows = 0;
+    for (int q = 0; q < problems; q++) rows += std::max<int64_t>(h_problem_rows[q], 0);
+    CAS_REQUIRE(rows == 0 || (h_positions && h_scores), CAS_ERR_INVALID_ARGUMENT,
+                "cas_fit_weights_batched: null input");
+    CAS_TRY(require_device());
+    cas_patterns* p = nullptr;
+    CAS_TRY(cas_patterns_create(masks, n_masks, mode, &p));
+    const int64_t cols = cas_patterns_cols(p) * problems;
+    cudaStream_t s = nullptr;
+    CAS_CUDA(cudaStreamCreate(&s));
+    uint64_t* d_pos = nullptr;
+    float* d_s32 = nullptr;
+    double *d_s = nullptr, *d_w = nullptr;
+    float* d_w32 = nullptr;
+    cas_status st = CAS_OK;
+    auto fail = [&](cudaError_t e) {
+        set_error(std::string("cas_fit_weights_batched: ") + cudaGetErrorString(e));
+        st = e == cudaErrorMemoryAllocation ? CAS_ERR_OUT_OF_MEMORY : CAS_ERR_CUDA;
+    };
+    cudaError_t e = cudaMalloc(&d_pos, 16 * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_s32, sizeof(float) * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_s, sizeof(double) * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_w, sizeof(double) * std::max<int64_t>(cols, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_w32, sizeof(float) * std::max<int64_t>(cols, 1));
+    if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_pos, h_positions, 16 * rows, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_s32, h_scores, sizeof(float) * rows, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) fail(e);
+    if (st == CAS_OK) {
+        { f32_to_f64_kernel<<<grid(rows), 256, 0, s>>>(d_s32, rows, d_s); cas::count_launch(); }
+        st = cas_fit_weights_batched_device(p, d_pos, d_s, h_problem_rows, problems, o, d_w, reports, s);
+    }
+    if (st == CAS_OK || st == CAS_ERR_NOT_CONVERGED) {
+        { f64_to_f32_kernel<<<grid(cols), 256, 0, s>>>(d_w, cols, d_w32); cas::count_launch(); }
+        e = cudaMemcpyAsync(h_weights, d_w32, sizeof(float) * cols, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) fail(e);
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(d_pos);
+    cudaFree(d_s32);
+    cudaFree(d_s);
+    cudaFree(d_w);
+    cudaFree(d_w32);
+    cudaStreamDestroy(s);
+    cas_patterns_destroy(p);
+    return st;
+}
+
 }  // extern "C"

@@ -47,11 +47,38 @@ enum Slot {
     kLAlpha = 8, kLBeta = 9, kPhiBar = 10, kRhoBar = 11, kPhiRho = 12, kThetaRho = 13, kInvBeta = 14,
     kArNorm = 15,  // |phi_bar * alpha * c| estimate of ||A'r||
     kTrue = 16,    // ||A'(b - A x)||^2 of the last true-residual evaluation
-    kSlots = 17
+    kRrRef = 17,   // r.r right after the last residual replacement (mixed PCG)
+    kSlots = 18
 };
 // kPending: LSQR met its tolerance in the last step; the step's x/w update
 // still has to run, so kDone is raised by the next step's first kernel.
-enum Flag { kDone = 0, kStatus = 1, kIter = 2, kRefine = 3, kPending = 4, kFlags = 5 };
+// kRestart: the last residual replacement found the recursive residual off
+// by more than kRestartDeviation (relative): the search direction restarts.
+// kSkip: no residual replacement is due this iteration (mixed PCG); the
+// replacement step of every iteration returns at entry while it is set.
+// kIterRef: iteration count at the last replacement.
+enum Flag {
+    kDone = 0, kStatus = 1, kIter = 2, kRefine = 3, kPending = 4, kRestart = 5, kSkip = 6, kIterRef = 7,
+    kFlags = 8
+};
+
+// Reliable updating of the mixed solver: when the recursive residual has
+// drifted this far from the FP64 true residual that replaces it, the FP32
+// product errors it carries (components outside the range of A'A) have
+// reached the search direction too; the direction restarts as p = z.
+// Below it, the replacement keeps the direction (a restart would discard
+// the Krylov space built so far).
+constexpr double kRestartDeviation = 0.1;
+
+// Reliable updating: the mixed PCG replaces its recursive residual by the
+// FP64 true residual as soon as the recursive one has dropped by this factor
+// since the last replacement (so it never reaches the noise floor of the
+// FP32 products, where CG would start fitting that noise), after
+// refine_every iterations at the latest, and whenever it meets the
+// tolerance (convergence is declared on the true residual only).
+constexpr double kReplaceDrop = 1e-4;
+
+__device__ __forceinline__ bool gated(const int* gate) { return gate && *(volatile const int*)gate != 0; }
 
 struct Dev {
     double* scal;
@@ -116,10 +143,10 @@ __global__ void __launch_bounds__(kVecThreads) spmv_norm_kernel(const uint32_t* 
                                                                  const T* __restrict__ p, Q* __restrict__ q,
                                                                  const double* __restrict__ b,
                                                                  double* __restrict__ part, Dev dv, int coef_slot,
-                                                                 int force)
+                                                                 const int* __restrict__ gate)
 {
     __shared__ double smem[64];
-    if (!force && finished(dv.flags)) return;
+    if (gated(gate)) return;
     const int lane = threadIdx.x & 31;
     const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
     const double coef = MODE == 1 ? dv.scal[coef_slot] : 0.0;
@@ -145,10 +172,10 @@ __global__ void __launch_bounds__(kVecThreads) spmv_norm_kernel(const uint32_t* 
 // Partial sums of A' q per work unit (deterministic, FP64 accumulation).
 template <typename Q>
 __global__ void __launch_bounds__(kVecThreads) spmv_t_units_flag_kernel(CsrView a, const Q* __restrict__ q,
-                                                                        double* __restrict__ partial, Dev dv,
-                                                                        int ignore_flag)
+                                                                        double* __restrict__ partial,
+                                                                        const int* __restrict__ gate)
 {
-    if (!ignore_flag && finished(dv.flags)) return;
+    if (gated(gate)) return;
     const int lane = threadIdx.x & 31;
     const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
     for (int64_t u = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); u < a.units;
@@ -194,7 +221,7 @@ struct ColSum {
 // PCG vector steps.
 // ---------------------------------------------------------------------------
 
-// alpha = rz / pAp (single block).  Breakdown when pAp <= 0 with rz > 0.
+// alpha = rz / pAp (single block).  Breakdown when pAp is not finite.
 template <bool COMP>
 __global__ void __launch_bounds__(kRedThreads) pcg_alpha_kernel(const double* __restrict__ part, int n, Dev dv)
 {
@@ -204,10 +231,20 @@ __global__ void __launch_bounds__(kRedThreads) pcg_alpha_kernel(const double* __
     if (threadIdx.x == 0) {
         const double rz = dv.scal[kRz];
         dv.scal[kPap] = pap;
-        if (!(pap > 0) || !isfinite(pap)) {
+        if (!isfinite(pap)) {
             dv.scal[kAlpha] = 0;
-            if (rz != 0) dv.flags[kStatus] = CAS_ERR_BREAKDOWN;
+            dv.flags[kStatus] = CAS_ERR_BREAKDOWN;
             dv.flags[kDone] = 1;
+            dv.flags[kSkip] = 1;
+        } else if (!(pap > 0)) {
+            // p has no component outside the null space of A: the normal
+            // equations are solved as far as the products resolve them (a
+            // rank-deficient A, or the residual at rounding level).  Stop;
+            // the FP64 true residual decides between converged and a
+            // restart from it.
+            dv.scal[kAlpha] = 0;
+            dv.flags[kDone] = 1;
+            dv.flags[kSkip] = 1;
         } else {
             dv.scal[kAlpha] = rz / pap;
         }
@@ -246,16 +283,24 @@ __global__ void __launch_bounds__(kVecThreads) pcg_update_kernel(ColSum cs,
 // rz_new, rr -> beta, residual, convergence (single block).
 // replace != 0: residual-replacement step; r.z is replaced but beta and the
 // iteration count are left alone.
+// part_dev (replacement only, may be null): partials of ||r_rec - r_true||^2;
+// sets kRestart when the deviation exceeds kRestartDeviation.
+// plan_refine > 0 (mixed PCG, not a replacement): the tolerance test moves to
+// the replacement step, which this kernel schedules through kSkip (drop by
+// kReplaceDrop, plan_refine iterations, or tolerance met).
 template <bool COMP>
 __global__ void __launch_bounds__(kRedThreads) pcg_beta_kernel(const double* __restrict__ part_rz,
                                                                const double* __restrict__ part_rr, int n, Dev dv,
-                                                               int replace, int force)
+                                                               int replace, const int* __restrict__ gate,
+                                                               const double* __restrict__ part_dev, int plan_refine)
 {
     __shared__ double smem[64];
-    if (!force && finished(dv.flags)) return;
+    if (gated(gate)) return;
     const double rz_new = reduce_partials<COMP>(part_rz, n, smem);
     const double rr = reduce_partials<COMP>(part_rr, n, smem);
+    const double dev2 = part_dev ? reduce_partials<COMP>(part_dev, n, smem) : 0.0;
     if (threadIdx.x == 0) {
+        if (part_dev) dv.flags[kRestart] = dev2 > kRestartDeviation * kRestartDeviation * rr ? 1 : 0;
         const double rz = dv.scal[kRz];
         const double bn2 = dv.scal[kBn2];
         const double res = bn2 > 0 ? sqrt(rr / bn2) : sqrt(rr);
@@ -268,11 +313,23 @@ __global__ void __launch_bounds__(kRedThreads) pcg_beta_kernel(const double* __r
         dv.scal[kRz] = rz_new;
         dv.scal[kRr] = rr;
         dv.scal[kRes] = res;
+        const bool met = dv.scal[kTol] > 0 && res <= dv.scal[kTol];
+        if (replace) {
+            dv.scal[kRrRef] = rr;
+            dv.flags[kIterRef] = dv.flags[kIter];
+        }
         if (!isfinite(rz_new) || !isfinite(rr)) {
             dv.flags[kStatus] = CAS_ERR_BREAKDOWN;
             dv.flags[kDone] = 1;
-        } else if (dv.scal[kTol] > 0 && res <= dv.scal[kTol]) {
+            dv.flags[kSkip] = 1;
+        } else if (!replace && plan_refine > 0) {
+            dv.flags[kRestart] = 0;
+            const bool due = met || rr <= kReplaceDrop * kReplaceDrop * dv.scal[kRrRef] ||
+                             dv.flags[kIter] - dv.flags[kIterRef] >= plan_refine;
+            dv.flags[kSkip] = due ? 0 : 1;
+        } else if (met) {
             dv.flags[kDone] = 1;
+            dv.flags[kSkip] = 1;
         }
     }
 }
@@ -293,8 +350,23 @@ __global__ void __launch_bounds__(kVecThreads) pcg_direction_kernel(int64_t n, c
     }
 }
 
-// r = A'(b - A x) from unit partials; z = d r; partials of r.z and r.r.
-// Also initialises p = z (init != 0) and ||A'b||^2 (bn != 0, x = 0).
+// p = z (and the gather copy) when the last replacement set kRestart.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) pcg_restart_kernel(int64_t n, const double* __restrict__ z,
+                                                                  double* __restrict__ p, T* __restrict__ pg, Dev dv)
+{
+    if (finished(dv.flags) || !*(volatile const int*)(dv.flags + kRestart)) return;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        p[c] = z[c];
+        if (pg) pg[c] = static_cast<T>(z[c]);
+    }
+}
+
+// r = A'(b - A x) from unit partials; z = d r; partials of r.z and r.r, and
+// (part_dev not null) of ||r_old - r||^2 against the recursive residual it
+// replaces.  Also initialises p = z (init != 0) and ||A'b||^2 (bn != 0,
+// x = 0).
 template <bool COMP, typename T>
 __global__ void __launch_bounds__(kVecThreads) pcg_residual_kernel(ColSum cs,
                                                                    double* __restrict__ r, double* __restrict__ z,
@@ -302,15 +374,21 @@ __global__ void __launch_bounds__(kVecThreads) pcg_residual_kernel(ColSum cs,
                                                                    const double* __restrict__ d,
                                                                    double* __restrict__ part_rz,
                                                                    double* __restrict__ part_rr, int init, Dev dv,
-                                                                   int force, const double* __restrict__ bn)
+                                                                   const int* __restrict__ gate,
+                                                                   const double* __restrict__ bn,
+                                                                   double* __restrict__ part_dev)
 {
     __shared__ double smem[64];
-    if (!force && finished(dv.flags)) return;
-    Comp rz, rr;
+    if (gated(gate)) return;
+    Comp rz, rr, dev;
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cs.a.cols;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const double rc = (bn ? bn[c] : 0.0) + cs(c);
         const double zc = d[c] * rc;
+        if (part_dev) {
+            const double dd = r[c] - rc;
+            acc_add<COMP>(dev, dd * dd);
+        }
         r[c] = rc;
         z[c] = zc;
         if (init) {
@@ -322,6 +400,7 @@ __global__ void __launch_bounds__(kVecThreads) pcg_residual_kernel(ColSum cs,
     }
     write_partial<COMP>(part_rz, rz, smem);
     write_partial<COMP>(part_rr, rr, smem);
+    if (part_dev) write_partial<COMP>(part_dev, dev, smem);
 }
 
 // DiagonalPreconditioner (Math/Solver.h:25-38): d = 1/diag(A'A), entries that
@@ -538,7 +617,7 @@ struct SolverImpl {
     const double* bn = nullptr;  // cols-length normal-equation RHS A'b (PCG/CG only)
     double* b_own = nullptr;
     double* partial = nullptr;  // unit partials of the rows layout
-    double *part_q = nullptr, *part_a = nullptr, *part_b = nullptr;
+    double *part_q = nullptr, *part_a = nullptr, *part_b = nullptr, *part_c = nullptr;
     int n_row_blocks = 0, n_vec_blocks = 0, n_q_parts = 0;
     double* scal = nullptr;
     int* flags = nullptr;
@@ -560,7 +639,7 @@ struct SolverImpl {
             cudaStreamDestroy(s);
         }
         for (void* ptr : {(void*)x, (void*)r, (void*)z, (void*)p, (void*)d, (void*)w, (void*)v, (void*)pg32, q,
-                          (void*)q64, (void*)b_own, (void*)partial, (void*)part_q, (void*)part_a, (void*)part_b,
+                          (void*)q64, (void*)b_own, (void*)partial, (void*)part_q, (void*)part_a, (void*)part_b, (void*)part_c,
                           (void*)scal, (void*)flags})
             cudaFree(ptr);
         cudaFreeHost(host_scal);
@@ -586,40 +665,45 @@ struct SolverImpl {
         return cs;
     }
 
+    // Device flag words that let graph-captured kernels return at entry:
+    // done() once the solver has converged, skip() while no residual
+    // replacement is due.
+    const int* done() const { return flags + kDone; }
+    const int* skip() const { return flags + kSkip; }
+
     // q = A g (mode 0), A g - scal[coef_slot] q (1), rhs - A g (2), with
-    // partials of ||q||^2 in part_q (count in n_q_parts).  `gate` lets the
-    // kernels return at entry once the solver has converged.
+    // partials of ||q||^2 in part_q (count in n_q_parts).  The kernels
+    // return at entry while *gate != 0 (gate may be null).
     template <bool COMP, typename G, typename Q>
-    cas_status product(const G* g, Q* qq, int mode, const double* rhs, int coef_slot, bool gate)
+    cas_status product(const G* g, Q* qq, int mode, const double* rhs, int coef_slot, const int* gate)
     {
         const bool use_fast = sizeof(G) == 4 ? fast32 : fast64;
         if (use_fast) {
-            return fast_spmv<G, Q>(*fast, g, qq, rhs, scal + coef_slot, part_q, gate ? flags : nullptr, mode, s,
+            return fast_spmv<G, Q>(*fast, g, qq, rhs, scal + coef_slot, part_q, const_cast<int*>(gate), mode, s,
                                    &n_q_parts);
         }
         n_q_parts = n_row_blocks;
         const Dev D = dv();
-        const int force = gate ? 0 : 1;
         if (mode == 0)
             { spmv_norm_kernel<G, Q, COMP, 0><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, g, qq, rhs, part_q, D,
-                                                                               coef_slot, force); cas::count_launch(); }
+                                                                               coef_slot, gate); cas::count_launch(); }
         else if (mode == 1)
             { spmv_norm_kernel<G, Q, COMP, 1><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, g, qq, rhs, part_q, D,
-                                                                               coef_slot, force); cas::count_launch(); }
+                                                                               coef_slot, gate); cas::count_launch(); }
         else
             { spmv_norm_kernel<G, Q, COMP, 2><<<n_row_blocks, kVecThreads, 0, s>>>(a.idx, R, a.k, g, qq, rhs, part_q, D,
-                                                                               coef_slot, force); cas::count_launch(); }
+                                                                               coef_slot, gate); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     }
 
     // Partials of A' q (summed later through colsum<Q>()).
     template <typename Q>
-    cas_status product_t(const Q* qq, bool gate)
+    cas_status product_t(const Q* qq, const int* gate)
     {
         const bool use_fast = sizeof(Q) == 4 ? fast32 : fast64;
-        if (use_fast) return fast_spmv_t_partials<Q>(*fast, qq, gate ? flags : nullptr, s);
-        { spmv_t_units_flag_kernel<Q><<<row_grid(a.units), kVecThreads, 0, s>>>(a, qq, partial, dv(), gate ? 0 : 1); cas::count_launch(); }
+        if (use_fast) return fast_spmv_t_partials<Q>(*fast, qq, const_cast<int*>(gate), s);
+        { spmv_t_units_flag_kernel<Q><<<row_grid(a.units), kVecThreads, 0, s>>>(a, qq, partial, gate); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     }
@@ -629,11 +713,12 @@ struct SolverImpl {
     {
         const Dev D = dv();
         const T* pgather = std::is_same<T, float>::value ? reinterpret_cast<const T*>(pg32) : reinterpret_cast<const T*>(p);
-        CAS_TRY((product<COMP, T, T>(pgather, static_cast<T*>(q), 0, nullptr, 0, true)));
-        CAS_TRY(product_t<T>(static_cast<const T*>(q), true));
+        CAS_TRY((product<COMP, T, T>(pgather, static_cast<T*>(q), 0, nullptr, 0, done())));
+        CAS_TRY(product_t<T>(static_cast<const T*>(q), done()));
         { pcg_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D); cas::count_launch(); }
         { pcg_update_kernel<COMP><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<T>(), x, r, z, p, d, part_a, part_b, D); cas::count_launch(); }
-        { pcg_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, part_b, n_vec_blocks, D, 0, 0); cas::count_launch(); }
+        { pcg_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, part_b, n_vec_blocks, D, 0, done(), nullptr,
+                                                          mixed ? std::max(o.refine_every, 1) : 0); cas::count_launch(); }
         { pcg_direction_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(
             C, z, p, std::is_same<T, float>::value ? reinterpret_cast<T*>(pg32) : nullptr, D); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
@@ -641,24 +726,34 @@ struct SolverImpl {
     }
 
     // Residual replacement: r = A'(b - A x) (or b' - A'A x) in FP64, z = d r,
-    // r.z, r.r.  Inside a graph chunk (force == false) it is skipped once
-    // converged.
+    // r.z, r.r.  restart: also p = z (set-up, resumption after a failed
+    // verification).  Otherwise this is the in-graph step of the mixed PCG:
+    // gated by kSkip, it measures the recursive residual's drift, restarts
+    // the direction when the drift exceeds kRestartDeviation and declares
+    // convergence on the true residual.
     template <bool COMP>
-    cas_status issue_pcg_refine(bool init, bool force)
+    cas_status issue_pcg_refine(bool restart)
     {
         const Dev D = dv();
-        const int f = force ? 1 : 0;
-        CAS_TRY((product<COMP, double, double>(x, q64, 2, b, 0, !force)));
-        CAS_TRY(product_t<double>(q64, !force));
+        const int* gate = restart ? nullptr : skip();
+        CAS_TRY((product<COMP, double, double>(x, q64, 2, b, 0, gate)));
+        CAS_TRY(product_t<double>(q64, gate));
+        double* pdev = restart ? nullptr : part_c;
         if (mixed)
             { pcg_residual_kernel<COMP, float><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), r, z, p, pg32, d,
-                                                                                part_a, part_b, init ? 1 : 0, D, f,
-                                                                                bn); cas::count_launch(); }
+                                                                                part_a, part_b, restart ? 1 : 0, D,
+                                                                                gate, bn, pdev); cas::count_launch(); }
         else
             { pcg_residual_kernel<COMP, double><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), r, z, p, nullptr, d,
-                                                                                 part_a, part_b, init ? 1 : 0, D, f,
-                                                                                 bn); cas::count_launch(); }
-        { pcg_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, part_b, n_vec_blocks, D, 1, f); cas::count_launch(); }
+                                                                                 part_a, part_b, restart ? 1 : 0, D,
+                                                                                 gate, bn, pdev); cas::count_launch(); }
+        { pcg_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, part_b, n_vec_blocks, D, 1, gate, pdev, 0); cas::count_launch(); }
+        if (!restart) {
+            if (mixed)
+                { pcg_restart_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, z, p, pg32, D); cas::count_launch(); }
+            else
+                { pcg_restart_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, z, p, nullptr, D); cas::count_launch(); }
+        }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     }
@@ -670,10 +765,10 @@ struct SolverImpl {
         T* vg = reinterpret_cast<T*>(std::is_same<T, float>::value ? (void*)pg32 : (void*)p);
         // u_hat = A v - (alpha / beta_prev) u_hat_prev
         { lsqr_coef_kernel<<<1, 1, 0, s>>>(D, kPap); cas::count_launch(); }
-        CAS_TRY((product<COMP, T, T>(vg, static_cast<T*>(q), 1, nullptr, kPap, true)));
+        CAS_TRY((product<COMP, T, T>(vg, static_cast<T*>(q), 1, nullptr, kPap, done())));
         { lsqr_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, 0); cas::count_launch(); }
         // v_hat = (1/beta) A' u_hat - beta v
-        CAS_TRY(product_t<T>(static_cast<const T*>(q), true));
+        CAS_TRY(product_t<T>(static_cast<const T*>(q), done()));
         { lsqr_v_kernel<COMP, T><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<T>(), v, part_a, D, 0); cas::count_launch(); }
         { lsqr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 0); cas::count_launch(); }
         { lsqr_xw_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, vg, D, 0); cas::count_launch(); }
@@ -690,16 +785,16 @@ struct SolverImpl {
         const Dev D = dv();
         const bool gate = mode == 2;
         if (mixed) {
-            CAS_TRY((product<true, double, float>(x, static_cast<float*>(q), 2, b, 0, gate)));
+            CAS_TRY((product<true, double, float>(x, static_cast<float*>(q), 2, b, 0, gate ? done() : nullptr)));
             { lsqr_beta_kernel<true><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, mode); cas::count_launch(); }
-            CAS_TRY(product_t<float>(static_cast<const float*>(q), gate));
+            CAS_TRY(product_t<float>(static_cast<const float*>(q), gate ? done() : nullptr));
             { lsqr_v_kernel<true, float><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<float>(), v, part_a, D, mode); cas::count_launch(); }
             { lsqr_alpha_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
             { lsqr_xw_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, pg32, D, mode); cas::count_launch(); }
         } else {
-            CAS_TRY((product<false, double, double>(x, static_cast<double*>(q), 2, b, 0, gate)));
+            CAS_TRY((product<false, double, double>(x, static_cast<double*>(q), 2, b, 0, gate ? done() : nullptr)));
             { lsqr_beta_kernel<false><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, mode); cas::count_launch(); }
-            CAS_TRY(product_t<double>(static_cast<const double*>(q), gate));
+            CAS_TRY(product_t<double>(static_cast<const double*>(q), gate ? done() : nullptr));
             { lsqr_v_kernel<false, double><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), v, part_a, D, mode); cas::count_launch(); }
             { lsqr_alpha_kernel<false><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
             { lsqr_xw_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, p, D, mode); cas::count_launch(); }
@@ -717,9 +812,12 @@ struct SolverImpl {
             if (mixed && o.refine_every > 0 && (global_index + 1) % o.refine_every == 0) CAS_TRY(issue_lsqr_start(2));
             return CAS_OK;
         }
-        if (mixed) CAS_TRY((issue_pcg_iteration<true, float>()));
-        else CAS_TRY((issue_pcg_iteration<false, double>()));
-        if (mixed && o.refine_every > 0 && (global_index + 1) % o.refine_every == 0) CAS_TRY(issue_pcg_refine<true>(false, false));
+        if (mixed) {
+            CAS_TRY((issue_pcg_iteration<true, float>()));
+            CAS_TRY(issue_pcg_refine<true>(false));  // runs only when the beta kernel scheduled it
+        } else {
+            CAS_TRY((issue_pcg_iteration<false, double>()));
+        }
         return CAS_OK;
     }
 
@@ -727,7 +825,8 @@ struct SolverImpl {
     // CUDA graph when the chunk shape allows.
     cas_status issue_chunk(int first, int n)
     {
-        const int period = (mixed && o.refine_every > 0) ? o.refine_every : 1;
+        // mixed LSQR restarts at fixed iterations: its graphs depend on the phase
+        const int period = (mixed && o.method == CAS_LSQR && o.refine_every > 0) ? o.refine_every : 1;
         const int phase = first % period;
         if (n > 1) {
             if (!graph || graph_len != n || graph_phase != phase) {
@@ -774,8 +873,8 @@ struct SolverImpl {
     // ||A'(b - A x)|| / ||A'b|| in FP64 (does not touch solver state).
     cas_status true_residual(double* out)
     {
-        CAS_TRY((product<true, double, double>(x, q64, 2, b, 0, false)));
-        CAS_TRY(product_t<double>(q64, false));
+        CAS_TRY((product<true, double, double>(x, q64, 2, b, 0, nullptr)));
+        CAS_TRY(product_t<double>(q64, nullptr));
         { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), nullptr, part_a, bn); cas::count_launch(); }
         { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kTrue); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
@@ -810,6 +909,7 @@ struct SolverImpl {
         CAS_CUDA(cudaMalloc(&part_q, sizeof(double) * 2 * q_parts));
         CAS_CUDA(cudaMalloc(&part_a, sizeof(double) * 2 * std::max(n_vec_blocks, q_parts)));
         CAS_CUDA(cudaMalloc(&part_b, sizeof(double) * 2 * n_vec_blocks));
+        CAS_CUDA(cudaMalloc(&part_c, sizeof(double) * 2 * n_vec_blocks));
         CAS_CUDA(cudaMalloc(&scal, sizeof(double) * kSlots));
         CAS_CUDA(cudaMalloc(&flags, sizeof(int) * kFlags));
         CAS_CUDA(cudaMallocHost(&host_scal, sizeof(double) * kSlots));
@@ -834,7 +934,7 @@ struct SolverImpl {
             none.a = a;
             { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(none, nullptr, part_a, bn); cas::count_launch(); }
         } else {
-            CAS_TRY(product_t<double>(b, false));
+            CAS_TRY(product_t<double>(b, nullptr));
             { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), nullptr, part_a, nullptr); cas::count_launch(); }
         }
         { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kBn2); cas::count_launch(); }
@@ -843,8 +943,8 @@ struct SolverImpl {
         if (o.method == CAS_LSQR) {
             CAS_TRY(issue_lsqr_start(1));
         } else {
-            if (mixed) CAS_TRY(issue_pcg_refine<true>(true, true));
-            else CAS_TRY(issue_pcg_refine<false>(true, true));
+            if (mixed) CAS_TRY(issue_pcg_refine<true>(true));
+            else CAS_TRY(issue_pcg_refine<false>(true));
         }
         CAS_TRY(read_state());
         // the initial residual replacement counted as a refinement; reset
@@ -1057,9 +1157,9 @@ CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
                 CAS_CUDA(cudaMemcpyAsync(m.scal + kTol, &t, sizeof t, cudaMemcpyHostToDevice, m.s));
             } else if (m.mixed) {
                 // the converged step skipped p = z + beta p: restart p = z
-                CAS_TRY(m.issue_pcg_refine<true>(true, true));
+                CAS_TRY(m.issue_pcg_refine<true>(true));
             } else {
-                CAS_TRY(m.issue_pcg_refine<false>(true, true));
+                CAS_TRY(m.issue_pcg_refine<false>(true));
             }
             continue;
         }

@@ -310,6 +310,21 @@ CAS_API cas_status cas_fit_weights_device(const cas_patterns* p, const uint64_t*
                                           int64_t rows, const cas_solve_opts* o, double* d_weights,
                                           cas_solve_report* rep, void* stream);
 
+/* The per-stage fits of the training loop (PatternFit/PatternFit.cpp:53-84:
+ * one FitWeights per empty-count stage, one after another) as one batched
+ * solve (cas_csr_from_positions_batched + cas_solve_batched): problem q is
+ * the next h_problem_rows[q] positions and scores; weights out are
+ * problems * cols floats (problem-major), reports one per problem. */
+CAS_API cas_status cas_fit_weights_batched(const uint64_t* masks, int n_masks, cas_index_mode mode,
+                                           const uint64_t* h_positions, const float* h_scores,
+                                           const int64_t* h_problem_rows, int problems, const cas_solve_opts* o,
+                                           float* h_weights, cas_solve_report* reports);
+/* Device-resident variant: scores and weights are FP64 device vectors. */
+CAS_API cas_status cas_fit_weights_batched_device(const cas_patterns* p, const uint64_t* d_positions,
+                                                  const double* d_scores, const int64_t* h_problem_rows,
+                                                  int problems, const cas_solve_opts* o, double* d_weights,
+                                                  cas_solve_report* reports, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Synthetic data (seeded, deterministic, identical on host and device)      */
 /* ------------------------------------------------------------------------ */

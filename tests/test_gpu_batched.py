@@ -126,3 +126,66 @@ def test_batched_rejects_bad_sizes(cuda):
         cb.MatrixCSR.from_positions_batched(g, pos, [50, 49])
     with pytest.raises(cb.CasError):
         cb.MatrixCSR.from_positions_batched(g, pos, [1] * 65 + [35])
+
+
+def test_fit_weights_batched_host_api(cuda):
+    """cas_fit_weights_batched (host buffers) gives the weights of the
+    device-resident batched solve."""
+    import ctypes as C
+
+    from cassandra_b200 import _lib as L
+
+    sizes = [6000, 2500]
+    a, pos, g = _batch(sizes, seed=80, empties=[25, 35])
+    b = cb.generate_targets(a, 80)
+    x, reps, ok = cb.solve_batched(a, b, precision="mixed", tol=1e-8)
+    assert ok
+    lib = L.load()
+    masks = np.asarray(SET8, np.uint64)
+    pos_h = np.ascontiguousarray(pos.cpu().numpy().view(np.uint64))
+    sc_h = np.ascontiguousarray(b.cpu().numpy().astype(np.float32))
+    rows = np.asarray(sizes, np.int64)
+    w = np.empty(a.cols(), np.float32)
+    hreps = (L.SolveReport * len(sizes))()
+    opts = cb.solve_opts("pcg", "mixed", 1e-8)
+    L.check(lib.cas_fit_weights_batched(masks.ctypes.data_as(C.c_void_p), len(masks), L.CAS_INDEX_EXPANDED,
+                                        pos_h.ctypes.data_as(C.c_void_p), sc_h.ctypes.data_as(C.c_void_p),
+                                        rows.ctypes.data_as(C.c_void_p), len(sizes), C.byref(opts),
+                                        w.ctypes.data_as(C.c_void_p), hreps))
+    assert all(r.rel_residual <= 1e-8 for r in hreps)
+    pw = (a @ torch.from_numpy(w.astype(np.float64)).cuda()).cpu().numpy()
+    px = (a @ x.reshape(-1)).cpu().numpy()
+    np.testing.assert_allclose(pw, px, rtol=0, atol=1e-4 * np.abs(px).max())
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batched_degenerate_problems(cuda, orc, precision):
+    """Rank-deficient problems of the per-stage loop: 60 empties is the start
+    position only (all rows equal), 59 and 58 have a handful of distinct rows;
+    small problems beside a regular one.  Each reaches the tolerance (or the
+    exact solution) and fits like the FP64 oracle."""
+    sizes = [20000, 3000, 2500, 1500]
+    a, pos, g = _batch(sizes, seed=90, empties=[30, 60, 59, 58])
+    C = g.index_space_size
+    b = cb.generate_targets(a, 90)
+    x, reps, ok = cb.solve_batched(a, b, precision=precision, tol=1e-8, max_iterations=5000)
+    assert ok, reps
+    row0, idx = _oracle_problems(orc, a, pos)
+    bh, xh = b.cpu().numpy(), x.cpu().numpy()
+    for q in range(len(sizes)):
+        rs = slice(row0[q], row0[q + 1])
+        assert orc.normal_residual(idx[q], C, bh[rs], xh[q]) <= 1.5e-8, (q, reps[q])
+
+
+def test_single_solver_on_identical_rows(cuda, orc):
+    """One fit whose rows are all the start position (rank 1)."""
+    pos = cb.generate_positions(5, 4000, 60, 60)
+    g = cb.GroupIndexer(SET8, "expanded")
+    for layout, precision in (("rows", "fp64"), ("blocked", "mixed")):
+        a = cb.MatrixCSR.from_positions(g, pos, layout)
+        b = cb.generate_targets(a, 5)
+        s = cb.PCG(a, b, precision=precision, tol=1e-8, max_iterations=2000)
+        rep = s.run()
+        assert rep["converged"], (layout, rep)
+        idx = orc.group_index(SET8, 1, pos.cpu().numpy().view(np.uint64))
+        assert orc.normal_residual(idx, g.index_space_size, b.cpu().numpy(), s.x().cpu().numpy()) <= 1.5e-8
