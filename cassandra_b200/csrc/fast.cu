@@ -92,8 +92,9 @@ __global__ void __launch_bounds__(256) fast_index_kernel(const Instance* __restr
 // ---------------------------------------------------------------------------
 // Per-(block, pattern) stable sort of entries by local column: two 8-bit LSD
 // passes inside one CTA, through a per-CTA scratch slice (L2 resident).
-// Items are (column << 16) | row-in-block; the input order is row-major
-// (row, slot), so equal columns keep ascending rows.
+// Items are (column << 16) | (row-in-block << 2) | end, end (bit 0) set on
+// the last entry of each column; the input order is row-major (row, slot),
+// so equal columns keep ascending rows.
 // ---------------------------------------------------------------------------
 struct SortSmem {
     uint32_t hist[256];
@@ -136,7 +137,7 @@ __device__ void sort_pass(const uint16_t* __restrict__ a16_in, const uint32_t* _
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const unsigned lt_mask = (1u << lane) - 1;
     auto item_at = [&](int e) -> uint32_t {
-        if (FROM_A16) return (static_cast<uint32_t>(a16_in[e]) << 16) | static_cast<uint32_t>(e / slots);
+        if (FROM_A16) return (static_cast<uint32_t>(a16_in[e]) << 16) | (static_cast<uint32_t>(e / slots) << 2);
         return in[e];
     };
     if (t < 256) sm.hist[t] = 0;
@@ -191,6 +192,17 @@ __global__ void __launch_bounds__(kSortThreads, 1) fast_sort_kernel(FastGeometry
         const int64_t seg = g.seg(b, p);
         sort_pass<true>(a16 + seg, nullptr, n, g.slots[p], 16, mine, sm);
         sort_pass<false>(nullptr, mine, n, g.slots[p], 24, g32 + seg, sm);
+        __syncthreads();
+        // run-end flags: bit 0 marks the last entry of each column (found
+        // first for all of a thread's entries, then set)
+        uint32_t* out = g32 + seg;
+        uint32_t ends[kBlockRows * 8 / kSortThreads / 32] = {};
+        for (int e = threadIdx.x, k = 0; e < n; e += kSortThreads, k++)
+            if (e + 1 == n || (out[e + 1] >> 16) != (out[e] >> 16)) ends[k >> 5] |= 1u << (k & 31);
+        __syncthreads();
+        for (int e = threadIdx.x, k = 0; e < n; e += kSortThreads, k++)
+            if ((ends[k >> 5] >> (k & 31)) & 1u) out[e] |= 1u;
+        __syncthreads();
     }
 }
 
@@ -235,7 +247,7 @@ __global__ void fast_diag_kernel(FastGeometry g, const uint32_t* __restrict__ g3
             if (e < n) {
                 const uint32_t v = g32[seg + e];
                 int64_t j = 0;
-                while (e - j - 1 >= 0 && g32[seg + e - j - 1] == v) j++;
+                while (e - j - 1 >= 0 && (g32[seg + e - j - 1] >> 2) == (v >> 2)) j++;  // same (column, row)
                 col = v >> 16;
                 contrib = static_cast<uint32_t>(2 * j + 1);
             }
@@ -477,16 +489,18 @@ struct TView {
 // entry list is cut into 32 nearly equal pieces, one per warp, so warps
 // stream their entries without block barriers whatever the run lengths
 // (one column can hold thousands of a block's entries).  Inside a warp each
-// lane owns kItemsPerThread consecutive entries per round; runs of equal
-// columns are summed and added to acc[col] exactly once, in an order fixed by
-// the data, so the result is bitwise reproducible:
-//   1. each lane sums its runs; runs wholly inside the lane are added to acc
-//      directly (no other lane or warp touches that column);
-//   2. the partial runs at lane boundaries are combined by a segmented scan
-//      over the warp's lanes (shuffles); the run still open at the end of
-//      the previous round enters as `carry`;
-//   3. the lane where a boundary run ends adds the combined sum, except for
-//      the warp's first and last run, which may continue in the neighbouring
+// lane owns kItemsPerThread consecutive entries per round.  An entry's bit 0
+// marks the last entry of its column, so a lane sums y over its entries and
+// closes a run at every flagged entry, with no column comparisons.  Every
+// run's sum is added to acc[col] exactly once, in an order fixed by the
+// data, so the result is bitwise reproducible:
+//   1. runs that start and end inside a lane are added to acc directly (no
+//      other lane or warp touches that column);
+//   2. runs cut by lane boundaries are combined by a segmented scan over the
+//      warp's lanes (shuffles); the run still open at the end of the
+//      previous round enters as `carry`;
+//   3. the lane where a cut run ends adds the combined sum, except for the
+//      warp's first and last run, which may continue in the neighbouring
 //      warps: their sums go to the warp's record;
 //   4. after the block, warp 0 combines the 32 records with the same
 //      segmented scan (one lane per warp) and adds them.
@@ -499,36 +513,24 @@ struct WarpRec {
     int valid, cp, cn; // range non-empty; first run continues the previous warp; last run continues in the next
 };
 
+// y of an entry: its row, already scaled by 4, sits in bits 2..15.
 template <typename T>
-__device__ __forceinline__ void run_step(uint32_t e, uint32_t c0, const T* __restrict__ ytile, T* __restrict__ acc,
-                                         int& hc, int& tc, T& hs, T& sum, bool& single, bool& any)
+__device__ __forceinline__ T y_of(const T* __restrict__ ytile, uint32_t e)
 {
-    const int col = static_cast<int>((e >> 16) - c0);
-    const T v = ytile[e & 0xFFFFu];
-    if (!any) {
-        any = true;
-        hc = tc = col;
-        sum = v;
-    } else if (col == tc) {
-        sum += v;
-    } else {
-        if (single) {
-            hs = sum;  // the head run closes inside this lane
-            single = false;
-        } else {
-            acc[tc] += sum;  // interior run: only this lane touches tc
-        }
-        tc = col;
-        sum = v;
-    }
+    if constexpr (sizeof(T) == 4)
+        return *reinterpret_cast<const T*>(reinterpret_cast<const char*>(ytile) + (e & 0xFFFCu));
+    else
+        return ytile[(e & 0xFFFCu) >> 2];
 }
 
 // Segmented inclusive scan over the 32 lanes of (any, single, cont_prev,
-// tail sum) and the resulting adds of head and tail runs; `sink` receives
-// every closed boundary run.  Lanes without entries pass the chain through.
+// tail sum) and the closing adds of the runs cut by lane boundaries; `sink`
+// receives every such run.  single: no run ends in the lane; tail_open: the
+// lane's last run continues past its last entry.  Lanes without entries pass
+// the chain through.
 template <typename T, typename Sink>
-__device__ __forceinline__ T lane_chain(bool any, bool single, bool cont_prev, bool cont_next, int hc, int tc, T hs,
-                                        T ts, T carry, Sink&& sink)
+__device__ __forceinline__ T lane_chain(bool any, bool single, bool cont_prev, bool cont_next, bool tail_open,
+                                        int hc, int tc, T hs, T ts, T carry, Sink&& sink)
 {
     const int lane = threadIdx.x & 31;
     T v = any ? ts : T(0);
@@ -547,10 +549,10 @@ __device__ __forceinline__ T lane_chain(bool any, bool single, bool cont_prev, b
     if (lane == 0) Xprev = carry;
     if (any) {
         if (single) {
-            if (!cont_next) sink(hc, X);
+            if (!cont_next) sink(tc, X);
         } else {
             sink(hc, cont_prev ? Xprev + hs : hs);
-            if (!cont_next) sink(tc, ts);
+            if (tail_open && !cont_next) sink(tc, ts);
         }
     }
     return __shfl_sync(0xffffffffu, X, 31);  // open chain leaving the lanes
@@ -588,83 +590,60 @@ __device__ __forceinline__ void cp_async_wait()
 
 // One round of a warp over [w_lo, w_hi): lanes take kItemsPerThread entries
 // each from round_start (a multiple of 4).  A lane whose entries are all in
-// range gets them in `cur` (loaded one round ahead by the caller) and sums
-// its runs without branches; edge lanes load and walk their entries one by
-// one.
+// range gets them in `cur` (loaded ahead by the caller); edge lanes load
+// theirs one by one.  prev_end: the last entry before this round ended its
+// run (updated for the next round).
 template <typename T>
 __device__ __forceinline__ void warp_round(const uint32_t* __restrict__ g32, uint32_t round_start, uint32_t w_lo,
                                            uint32_t w_hi, uint32_t c0, const T* __restrict__ ytile,
-                                           T* __restrict__ acc, T& carry, WarpRec<T>& rec,
+                                           T* __restrict__ acc, T& carry, bool& prev_end, WarpRec<T>& rec,
                                            const uint4 (&cur)[kLaneVecs], bool full)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t e_first = round_start + lane * kItemsPerThread;
-    int hc = -1, tc = -1;
-    T hs = 0, ts = 0;
-    bool single = true, any = false;
-    uint32_t first_ent = 0, last_ent = 0;
+    bool any = false, open = true;
+    T sum = 0, hs = 0;
+    int hc = 0;
+    uint32_t last_ent = 1u;  // an empty lane looks like a closed run
+    auto step = [&](uint32_t e) {
+        sum += y_of<T>(ytile, e);
+        const bool end = (e & 1u) != 0;
+        const int col = static_cast<int>((e >> 16) - c0);
+        const bool close_head = end && open;
+        hs = close_head ? sum : hs;
+        hc = close_head ? col : hc;
+        if (end && !open) acc[col] += sum;  // interior run: only this lane touches col
+        open = open && !end;
+        sum = end ? T(0) : sum;
+    };
     if (full) {
-        uint32_t e[kItemsPerThread];
 #pragma unroll
         for (int q = 0; q < kLaneVecs; q++) {
-            e[4 * q] = cur[q].x;
-            e[4 * q + 1] = cur[q].y;
-            e[4 * q + 2] = cur[q].z;
-            e[4 * q + 3] = cur[q].w;
+            step(cur[q].x);
+            step(cur[q].y);
+            step(cur[q].z);
+            step(cur[q].w);
         }
-        T yv[kItemsPerThread];
-#pragma unroll
-        for (int i = 0; i < kItemsPerThread; i++) yv[i] = ytile[e[i] & 0xFFFFu];
-        int kp = static_cast<int>((e[0] >> 16) - c0);
-        T sum = yv[0];
-        bool open = true;  // the lane's first run has not closed yet
-        hc = kp;
-#pragma unroll
-        for (int i = 1; i < kItemsPerThread; i++) {
-            const int k = static_cast<int>((e[i] >> 16) - c0);
-            const bool brk = k != kp;
-            hs = (brk && open) ? sum : hs;
-            if (brk && !open) acc[kp] += sum;  // interior run: only this lane touches kp
-            open = open && !brk;
-            sum = brk ? yv[i] : sum + yv[i];
-            kp = k;
-        }
-        tc = kp;
-        ts = sum;
-        single = open;
-        if (single) hs = sum;
         any = true;
-        first_ent = e[0];
-        last_ent = e[kItemsPerThread - 1];
-    } else if (e_first + kItemsPerThread > w_lo && e_first < w_hi) {
+        last_ent = cur[kLaneVecs - 1].w;
+    } else {
         const uint32_t lo = max(e_first, w_lo), hi = min(e_first + kItemsPerThread, w_hi);
-        first_ent = g32[lo];
-        last_ent = g32[hi - 1];
-        T sum = 0;
-        for (uint32_t e = lo; e < hi; e++) run_step<T>(g32[e], c0, ytile, acc, hc, tc, hs, sum, single, any);
-        ts = sum;
-        if (single) hs = sum;
+        if (lo < hi) {
+            for (uint32_t e = lo; e < hi; e++) step(g32[e]);
+            any = true;
+            last_ent = g32[hi - 1];
+        }
     }
-    // neighbours: the previous lane's last entry and the next lane's first
-    // entry by shuffle, from memory across the round's edges
+    const bool single = any && open;  // no run ends in this lane
+    const bool tail_open = any && !(last_ent & 1u);
+    const int tc = static_cast<int>((last_ent >> 16) - c0);
     const uint32_t first_valid = max(e_first, w_lo);
     const uint32_t last_valid = min(e_first + kItemsPerThread, w_hi) - 1;
-    const uint32_t prev_ent_sh = __shfl_up_sync(0xffffffffu, last_ent, 1);
-    const uint32_t next_ent_sh = __shfl_down_sync(0xffffffffu, first_ent, 1);
-    const unsigned any_mask = __ballot_sync(0xffffffffu, any);
-    const bool prev_any = lane > 0 && ((any_mask >> (lane - 1)) & 1u);
-    const bool next_any = lane < 31 && ((any_mask >> (lane + 1)) & 1u);
-    bool cont_prev = false, cont_next = false;
-    if (any) {
-        if (first_valid > w_lo) {
-            const uint32_t pe = prev_any ? prev_ent_sh : g32[first_valid - 1];
-            cont_prev = static_cast<int>((pe >> 16) - c0) == hc;
-        }
-        if (last_valid + 1 < w_hi) {
-            const uint32_t ne = next_any ? next_ent_sh : g32[last_valid + 1];
-            cont_next = static_cast<int>((ne >> 16) - c0) == tc;
-        }
-    }
+    // the lane continues the run of the entry before it unless that entry
+    // ended its run (previous lane's last entry; last round's at lane 0)
+    const uint32_t prev_last = __shfl_up_sync(0xffffffffu, last_ent, 1);
+    const bool cont_prev = any && first_valid > w_lo && (lane == 0 ? !prev_end : !(prev_last & 1u));
+    const bool cont_next = tail_open && last_valid + 1 < w_hi;
     const int fc = rec.fc, lc = rec.lc;
     auto sink = [&](int col, T val) {
         if (col == fc)
@@ -674,23 +653,24 @@ __device__ __forceinline__ void warp_round(const uint32_t* __restrict__ g32, uin
         else
             acc[col] += val;
     };
-    if (__ballot_sync(0xffffffffu, any && single && cont_prev) == 0) {
-        // no lane is one run continued from its left: every chain is at
-        // most two lanes long, one shuffle combines them
-        T prev_ts = __shfl_up_sync(0xffffffffu, ts, 1);
+    if (__ballot_sync(0xffffffffu, single && cont_prev) == 0) {
+        // no lane is one run continued from its left: every cut run spans at
+        // most two lanes, one shuffle combines them
+        T prev_ts = __shfl_up_sync(0xffffffffu, sum, 1);
         if (lane == 0) prev_ts = carry;
         if (any) {
             if (single) {
-                if (!cont_next) sink(hc, ts);
+                if (!cont_next) sink(tc, sum);
             } else {
                 sink(hc, cont_prev ? prev_ts + hs : hs);
-                if (!cont_next) sink(tc, ts);
+                if (tail_open && !cont_next) sink(tc, sum);
             }
         }
-        carry = __shfl_sync(0xffffffffu, ts, 31);
+        carry = __shfl_sync(0xffffffffu, sum, 31);
     } else {
-        carry = lane_chain<T>(any, single, cont_prev, cont_next, hc, tc, hs, ts, carry, sink);
+        carry = lane_chain<T>(any, single, cont_prev, cont_next, tail_open, hc, tc, hs, sum, carry, sink);
     }
+    prev_end = (__shfl_sync(0xffffffffu, last_ent, 31) & 1u) != 0;
 }
 
 // The warp-range reduction of one block's entries [e_lo, e_hi) into acc.
@@ -719,18 +699,21 @@ __device__ __forceinline__ void reduce_block_entries(const uint32_t* __restrict_
             const uint32_t ef = g32[w_lo], el = g32[w_hi - 1];
             rec.fc = static_cast<int>((ef >> 16) - c0);
             rec.lc = static_cast<int>((el >> 16) - c0);
-            rec.cp = w_lo > e_lo && (g32[w_lo - 1] >> 16) == (ef >> 16);
-            rec.cn = w_hi < e_hi && (g32[w_hi] >> 16) == (el >> 16);
+            rec.cp = w_lo > e_lo && !(g32[w_lo - 1] & 1u);
+            rec.cn = !(el & 1u);
         }
     }
     __syncwarp();
     T carry = 0;
-    if constexpr (RING) {
+    bool prev_end = true;
+    const uint32_t round_len = 32 * kItemsPerThread;
+    const uint32_t rs0 = w_lo & ~3u;
+    if (w_lo >= w_hi) {
+        // empty range (its start need not be 4-aligned): no rounds
+    } else if constexpr (RING) {
         // round r of this lane lands in ring slot r % kRingStages; the copies
         // of rounds r+1 .. r+kRingStages-1 are in flight while r is reduced
         uint32_t* mine = ring + (static_cast<size_t>(warp) * kRingStages * 32 + lane) * kItemsPerThread;
-        const uint32_t rs0 = w_lo & ~3u;
-        const uint32_t round_len = 32 * kItemsPerThread;
         const uint32_t nrounds = w_hi > rs0 ? (w_hi - rs0 + round_len - 1) / round_len : 0;
         auto issue = [&](uint32_t r) {
             const uint32_t ef = rs0 + r * round_len + lane * kItemsPerThread;
@@ -754,37 +737,35 @@ __device__ __forceinline__ void reduce_block_entries(const uint32_t* __restrict_
 #pragma unroll
                 for (int q = 0; q < kLaneVecs; q++) cur[q] = src[q];
             }
-            warp_round<T>(g32, rs, w_lo, w_hi, c0, ytile, acc, carry, rec, cur, full);
+            warp_round<T>(g32, rs, w_lo, w_hi, c0, ytile, acc, carry, prev_end, rec, cur, full);
         }
         cp_async_wait<0>();
-        __syncthreads();
-        if (warp == 0) {
-            const WarpRec<T> r = recs[lane];
-            const bool single = r.fc == r.lc;
-            lane_chain<T>(r.valid != 0, single, r.cp != 0, r.cn != 0, r.fc, r.lc, r.fs, single ? r.fs : r.ls, T(0),
-                          [&](int col, T val) { acc[col] += val; });
+    } else {
+        // two register buffers that swap roles every round: the next round's
+        // entries load while this round is reduced
+        uint4 ba[kLaneVecs], bb[kLaneVecs];
+        uint32_t rs = rs0;
+        bool fa = rs < w_hi && lane_full(rs + lane * kItemsPerThread, w_lo, w_hi);
+        if (fa) load_lane(g32, rs + lane * kItemsPerThread, ba);
+        while (rs < w_hi) {
+            uint32_t rn = rs + round_len;
+            const bool fb = rn < w_hi && lane_full(rn + lane * kItemsPerThread, w_lo, w_hi);
+            if (fb) load_lane(g32, rn + lane * kItemsPerThread, bb);
+            warp_round<T>(g32, rs, w_lo, w_hi, c0, ytile, acc, carry, prev_end, rec, ba, fa);
+            rs = rn;
+            if (rs >= w_hi) break;
+            rn = rs + round_len;
+            fa = rn < w_hi && lane_full(rn + lane * kItemsPerThread, w_lo, w_hi);
+            if (fa) load_lane(g32, rn + lane * kItemsPerThread, ba);
+            warp_round<T>(g32, rs, w_lo, w_hi, c0, ytile, acc, carry, prev_end, rec, bb, fb);
+            rs = rn;
         }
-        return;
-    }
-    uint32_t rs = w_lo & ~3u;
-    uint4 cur[kLaneVecs], nxt[kLaneVecs];
-    bool cur_full = rs < w_hi && lane_full(rs + lane * kItemsPerThread, w_lo, w_hi);
-    if (cur_full) load_lane(g32, rs + lane * kItemsPerThread, cur);
-    for (; rs < w_hi; rs += 32 * kItemsPerThread) {
-        // the next round's entries are loaded while this round is reduced
-        const uint32_t rn = rs + 32 * kItemsPerThread;
-        const bool nxt_full = rn < w_hi && lane_full(rn + lane * kItemsPerThread, w_lo, w_hi);
-        if (nxt_full) load_lane(g32, rn + lane * kItemsPerThread, nxt);
-        warp_round<T>(g32, rs, w_lo, w_hi, c0, ytile, acc, carry, rec, cur, cur_full);
-#pragma unroll
-        for (int q = 0; q < kLaneVecs; q++) cur[q] = nxt[q];
-        cur_full = nxt_full;
     }
     __syncthreads();
     if (warp == 0) {
         const WarpRec<T> r = recs[lane];
         const bool single = r.fc == r.lc;
-        lane_chain<T>(r.valid != 0, single, r.cp != 0, r.cn != 0, r.fc, r.lc, r.fs, single ? r.fs : r.ls, T(0),
+        lane_chain<T>(r.valid != 0, single, r.cp != 0, r.cn != 0, true, r.fc, r.lc, r.fs, single ? r.fs : r.ls, T(0),
                       [&](int col, T val) { acc[col] += val; });
     }
 }

@@ -4,9 +4,11 @@
 // pattern (indexer) are stored together:
 //
 //   A16  uint16  [block][pattern][row][slot]   local column of every entry
-//   G32  uint32  [block][pattern][entry]       (local column << 16) | row in
-//                                              block, sorted by column then
-//                                              row (the transposed copy)
+//   G32  uint32  [block][pattern][entry]       (local column << 16) |
+//                                              (row in block << 2) | end,
+//                                              sorted by column then row (the
+//                                              transposed copy); end marks the
+//                                              last entry of each column
 //
 // so that a CTA touches one pattern's columns at a time.  A x stages that
 // pattern's slice of x in shared memory and gathers from there; A'y stages
