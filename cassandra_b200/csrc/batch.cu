@@ -458,7 +458,7 @@ struct BatchSolver {
         for (void* ptr : {(void*)x, (void*)r, (void*)z, (void*)p, (void*)dinv, (void*)pg32, q, (void*)q64,
                           (void*)part_q, (void*)part_a, (void*)part_b, (void*)part_c, (void*)scal,
                           (void*)flags, (void*)act, (void*)all})
-            cudaFree(ptr);
+            dfree(ptr);
     }
 
     // How a residual replacement selects its problems.
@@ -630,16 +630,16 @@ struct BatchSolver {
             own_stream = true;
         }
         const size_t cb = sizeof(double) * std::max<int64_t>(C, 1), rb = sizeof(double) * std::max<int64_t>(R, 1);
-        for (double** ptr : {&x, &r, &z, &p, &dinv}) CAS_CUDA(cudaMalloc(ptr, cb));
-        if (mixed) CAS_CUDA(cudaMalloc(&pg32, sizeof(float) * std::max<int64_t>(C, 1)));
-        CAS_CUDA(cudaMalloc(&q, mixed ? sizeof(float) * std::max<int64_t>(R, 1) : rb));
-        CAS_CUDA(cudaMalloc(&q64, rb));
-        CAS_CUDA(cudaMalloc(&part_q, sizeof(double) * 2 * std::max<int64_t>(f->g.nblocks, 1)));
-        CAS_CUDA(cudaMalloc(&part_a, sizeof(double) * 2 * B * G));
-        CAS_CUDA(cudaMalloc(&part_b, sizeof(double) * 2 * B * G));
-        CAS_CUDA(cudaMalloc(&part_c, sizeof(double) * 2 * B * G));
-        CAS_CUDA(cudaMalloc(&act, sizeof(ActiveList)));
-        CAS_CUDA(cudaMalloc(&all, sizeof(ActiveList)));
+        for (double** ptr : {&x, &r, &z, &p, &dinv}) CAS_CUDA(dmalloc(ptr, cb));
+        if (mixed) CAS_CUDA(dmalloc(&pg32, sizeof(float) * std::max<int64_t>(C, 1)));
+        CAS_CUDA(dmalloc(&q, mixed ? sizeof(float) * std::max<int64_t>(R, 1) : rb));
+        CAS_CUDA(dmalloc(&q64, rb));
+        CAS_CUDA(dmalloc(&part_q, sizeof(double) * 2 * std::max<int64_t>(f->g.nblocks, 1)));
+        CAS_CUDA(dmalloc(&part_a, sizeof(double) * 2 * B * G));
+        CAS_CUDA(dmalloc(&part_b, sizeof(double) * 2 * B * G));
+        CAS_CUDA(dmalloc(&part_c, sizeof(double) * 2 * B * G));
+        CAS_CUDA(dmalloc(&act, sizeof(ActiveList)));
+        CAS_CUDA(dmalloc(&all, sizeof(ActiveList)));
         {
             ActiveList h{};
             h.n = B;
@@ -650,9 +650,9 @@ struct BatchSolver {
             CAS_CUDA(cudaMemcpy(all, &h, sizeof h, cudaMemcpyHostToDevice));
             CAS_CUDA(cudaMemcpy(act, &h, sizeof h, cudaMemcpyHostToDevice));
         }
-        CAS_CUDA(cudaMalloc(&scal, sizeof(double) * B * kBSlots));
+        CAS_CUDA(dmalloc(&scal, sizeof(double) * B * kBSlots));
         h_scal.assign(static_cast<size_t>(B) * kBSlots, 0.0);
-        CAS_CUDA(cudaMalloc(&flags, sizeof(int) * nflags()));
+        CAS_CUDA(dmalloc(&flags, sizeof(int) * nflags()));
         h_flags.assign(static_cast<size_t>(nflags()), 0);
         CAS_CUDA(cudaMemsetAsync(scal, 0, sizeof(double) * B * kBSlots, s));
         CAS_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * nflags(), s));

@@ -29,6 +29,24 @@ struct Error {
     std::string msg;
 };
 
+// Device and pinned-host memory of the library's objects, from a cache that
+// keeps freed blocks for reuse (memory.cu).  dfree/hfree keep cudaFree's
+// guarantee that work still using the block finishes before it is reused.
+cudaError_t dmalloc_bytes(void** p, size_t bytes);
+void dfree(const void* p);
+cudaError_t hmalloc_bytes(void** p, size_t bytes);
+void hfree(const void* p);
+template <typename T>
+cudaError_t dmalloc(T** p, size_t bytes)
+{
+    return dmalloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
+template <typename T>
+cudaError_t hmalloc(T** p, size_t bytes)
+{
+    return hmalloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
+
 }  // namespace cas
 
 // Returns from the enclosing cas_status function on a CUDA error.

@@ -125,17 +125,17 @@ cas_status patterns_on_device(const cas_patterns* cp, const DevicePatterns** out
         if (p->device >= 0) {
             int cur = dev;
             cudaSetDevice(p->device);
-            cudaFree(p->dev.instances);
-            cudaFree(p->dev.tables);
+            dfree(p->dev.instances);
+            dfree(p->dev.tables);
             cudaSetDevice(cur);
             p->dev = DevicePatterns{};
         }
         const PatternSet& s = p->set;
-        CAS_CUDA(cudaMalloc(&p->dev.instances, sizeof(Instance) * s.instances.size()));
+        CAS_CUDA(dmalloc(&p->dev.instances, sizeof(Instance) * s.instances.size()));
         CAS_CUDA(cudaMemcpy(p->dev.instances, s.instances.data(), sizeof(Instance) * s.instances.size(),
                             cudaMemcpyHostToDevice));
         const size_t tb = std::max<size_t>(1, s.tables.size());
-        CAS_CUDA(cudaMalloc(&p->dev.tables, sizeof(uint32_t) * tb));
+        CAS_CUDA(dmalloc(&p->dev.tables, sizeof(uint32_t) * tb));
         if (!s.tables.empty())
             CAS_CUDA(cudaMemcpy(p->dev.tables, s.tables.data(), sizeof(uint32_t) * s.tables.size(),
                                 cudaMemcpyHostToDevice));
@@ -209,8 +209,8 @@ CAS_API void cas_patterns_destroy(cas_patterns* p)
         int cur = 0;
         cudaGetDevice(&cur);
         cudaSetDevice(p->device);
-        cudaFree(p->dev.instances);
-        cudaFree(p->dev.tables);
+        dfree(p->dev.instances);
+        dfree(p->dev.tables);
         cudaSetDevice(cur);
     }
     delete p;

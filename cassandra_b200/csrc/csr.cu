@@ -391,9 +391,9 @@ cas_status build_structure(cas_csr* a, cudaStream_t s)
                 "CSR with 2^32 or more entries is not supported (uint32 entry offsets)");
     CAS_REQUIRE(a->rows < 0xFFFFFFFFLL, CAS_ERR_INVALID_ARGUMENT, "rows must fit uint32");
     const int64_t cols = a->cols;
-    CAS_CUDA(cudaMalloc(&a->col_ptr, sizeof(int64_t) * (cols + 1)));
+    CAS_CUDA(dmalloc(&a->col_ptr, sizeof(int64_t) * (cols + 1)));
     if (!a->diag_int) {
-        CAS_CUDA(cudaMalloc(&a->diag_int, sizeof(uint64_t) * std::max<int64_t>(cols, 1)));
+        CAS_CUDA(dmalloc(&a->diag_int, sizeof(uint64_t) * std::max<int64_t>(cols, 1)));
         CAS_CUDA(cudaMemsetAsync(a->diag_int, 0, sizeof(uint64_t) * std::max<int64_t>(cols, 1), s));
     }
 
@@ -414,10 +414,10 @@ cas_status build_structure(cas_csr* a, cudaStream_t s)
     while (bits < 32 && (1LL << bits) < cols) bits++;
     uint32_t *kA = nullptr, *vA = nullptr, *kB = nullptr, *vB = nullptr;
     const size_t bytes = sizeof(uint32_t) * std::max<int64_t>(nnz, 1);
-    CAS_CUDA(cudaMalloc(&kA, bytes));
-    CAS_CUDA(cudaMalloc(&vA, bytes));
-    CAS_CUDA(cudaMalloc(&kB, bytes));
-    CAS_CUDA(cudaMalloc(&vB, bytes));
+    CAS_CUDA(dmalloc(&kA, bytes));
+    CAS_CUDA(dmalloc(&vA, bytes));
+    CAS_CUDA(dmalloc(&kB, bytes));
+    CAS_CUDA(dmalloc(&vB, bytes));
     uint32_t *keys = kA, *vals = vA;
     cas_status st = CAS_OK;
     if (nnz > 0) st = radix_sort_pairs(a->idx, nullptr, a->k, nnz, bits, kA, vA, kB, vB, &keys, &vals, s);
@@ -429,11 +429,11 @@ cas_status build_structure(cas_csr* a, cudaStream_t s)
     // keep the sorted rows, release the rest
     a->row_idx = vals;
     for (uint32_t* p : {kA, vA, kB, vB})
-        if (p != vals) cudaFree(p);
+        if (p != vals) dfree(p);
     if (st != CAS_OK) return st;
 
     // A'y work units
-    CAS_CUDA(cudaMalloc(&a->unit_ptr, sizeof(uint32_t) * (cols + 1)));
+    CAS_CUDA(dmalloc(&a->unit_ptr, sizeof(uint32_t) * (cols + 1)));
     if (cols > 0) {
         { unit_count_kernel<<<grid_for(cols, 256), 256, 0, s>>>(a->col_ptr, cols, a->unit_ptr); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
@@ -444,8 +444,8 @@ cas_status build_structure(cas_csr* a, cudaStream_t s)
     CAS_CUDA(cudaMemcpyAsync(&units, a->unit_ptr + cols, sizeof units, cudaMemcpyDeviceToHost, s));
     CAS_CUDA(cudaStreamSynchronize(s));
     a->units = units;
-    CAS_CUDA(cudaMalloc(&a->unit_col, sizeof(int32_t) * std::max<int64_t>(units, 1)));
-    CAS_CUDA(cudaMalloc(&a->unit_partial, sizeof(double) * std::max<int64_t>(units, 1)));
+    CAS_CUDA(dmalloc(&a->unit_col, sizeof(int32_t) * std::max<int64_t>(units, 1)));
+    CAS_CUDA(dmalloc(&a->unit_partial, sizeof(double) * std::max<int64_t>(units, 1)));
     if (cols > 0) {
         { unit_fill_kernel<<<grid_for(cols, 256), 256, 0, s>>>(a->unit_ptr, cols, a->unit_col); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
@@ -464,13 +464,13 @@ void free_csr(cas_csr* a)
     int cur = 0;
     cudaGetDevice(&cur);
     if (a->device >= 0) cudaSetDevice(a->device);
-    cudaFree(a->idx);
-    cudaFree(a->col_ptr);
-    cudaFree(a->row_idx);
-    cudaFree(a->unit_col);
-    cudaFree(a->unit_ptr);
-    cudaFree(a->diag_int);
-    cudaFree(a->unit_partial);
+    dfree(a->idx);
+    dfree(a->col_ptr);
+    dfree(a->row_idx);
+    dfree(a->unit_col);
+    dfree(a->unit_ptr);
+    dfree(a->diag_int);
+    dfree(a->unit_partial);
     if (a->fast) {
         fast_free(*a->fast);
         delete a->fast;
@@ -523,7 +523,7 @@ CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const ui
     a->cols = dp->cols;
     a->k = dp->k;
     a->layouts = layouts;
-    cudaError_t e = cudaMalloc(&a->diag_int, sizeof(uint64_t) * std::max<int64_t>(a->cols, 1));
+    cudaError_t e = dmalloc(&a->diag_int, sizeof(uint64_t) * std::max<int64_t>(a->cols, 1));
     if (e == cudaSuccess) e = cudaMemsetAsync(a->diag_int, 0, sizeof(uint64_t) * std::max<int64_t>(a->cols, 1), s);
     if (e != cudaSuccess) {
         free_csr(a);
@@ -542,7 +542,7 @@ CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const ui
         }
     }
     if (layouts & CAS_LAYOUT_ROWS) {
-        e = cudaMalloc(&a->idx, sizeof(uint32_t) * std::max<int64_t>(rows * a->k, 1));
+        e = dmalloc(&a->idx, sizeof(uint32_t) * std::max<int64_t>(rows * a->k, 1));
         if (e != cudaSuccess) {
             free_csr(a);
             set_error("cas_csr_from_positions: cannot allocate the index array");
@@ -592,7 +592,7 @@ CAS_API cas_status cas_csr_from_positions_batched(const cas_patterns* p, const u
     a->cols = dp->cols * problems;
     a->k = dp->k;
     a->layouts = CAS_LAYOUT_BLOCKED;
-    cudaError_t e = cudaMalloc(&a->diag_int, sizeof(uint64_t) * std::max<int64_t>(a->cols, 1));
+    cudaError_t e = dmalloc(&a->diag_int, sizeof(uint64_t) * std::max<int64_t>(a->cols, 1));
     if (e == cudaSuccess) e = cudaMemsetAsync(a->diag_int, 0, sizeof(uint64_t) * std::max<int64_t>(a->cols, 1), s);
     if (e != cudaSuccess) {
         free_csr(a);
@@ -711,7 +711,7 @@ CAS_API cas_status cas_csr_from_indices(const uint32_t* d_indices, int nnz_per_r
     a->k = nnz_per_row;
     a->layouts = CAS_LAYOUT_ROWS;
     const size_t bytes = sizeof(uint32_t) * rows * nnz_per_row;
-    cudaError_t e = cudaMalloc(&a->idx, std::max<size_t>(bytes, 4));
+    cudaError_t e = dmalloc(&a->idx, std::max<size_t>(bytes, 4));
     if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(a->idx, d_indices, bytes, cudaMemcpyDefault, s);
     if (e != cudaSuccess) {
         free_csr(a);

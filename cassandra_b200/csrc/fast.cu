@@ -15,6 +15,7 @@
 //       of the chunk.  Items write partial column sums that the caller adds
 //       in a fixed order: no atomics anywhere, bitwise reproducible.
 #include <algorithm>
+#include <cstring>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -906,14 +907,30 @@ __global__ void fast_col_sum_kernel(FastCols fc, const T* __restrict__ partial, 
         x[c] = static_cast<T>(fast_col_sum<T>(fc, partial, c));
 }
 
-// Device copy of a host int vector (at least one element allocated).
-template <typename V>
-cas_status upload(const std::vector<V>& h, V** d)
-{
-    CAS_CUDA(cudaMalloc(d, sizeof(V) * std::max<size_t>(h.size(), 1)));
-    if (!h.empty()) CAS_CUDA(cudaMemcpy(*d, h.data(), sizeof(V) * h.size(), cudaMemcpyHostToDevice));
-    return CAS_OK;
-}
+// The small arrays of a work list, gathered on the host and sent to the
+// device as one block: one allocation and one copy instead of one each, so
+// that building a layout makes few driver calls.
+struct MetaPack {
+    std::vector<unsigned char> host;
+    std::vector<std::pair<size_t, void**>> fields;
+
+    template <typename V>
+    void add(const std::vector<V>& v, V** field)
+    {
+        const size_t off = (host.size() + 15) & ~size_t(15);
+        host.resize(off + sizeof(V) * std::max<size_t>(v.size(), 1), 0);
+        if (!v.empty()) std::memcpy(host.data() + off, v.data(), sizeof(V) * v.size());
+        fields.emplace_back(off, reinterpret_cast<void**>(field));
+    }
+    // Uploads the block into *base and points every field into it.
+    cas_status upload(void** base)
+    {
+        CAS_CUDA(dmalloc(base, std::max<size_t>(host.size(), 16)));
+        if (!host.empty()) CAS_CUDA(cudaMemcpy(*base, host.data(), host.size(), cudaMemcpyHostToDevice));
+        for (auto& f : fields) *f.second = static_cast<unsigned char*>(*base) + f.first;
+        return CAS_OK;
+    }
+};
 
 // Columns of a global chunk (the last chunk of a pattern may be partial).
 int chunk_width(const FastGeometry& g, int ch)
@@ -972,19 +989,18 @@ Pieces pack_chunks(const FastGeometry& g, int cap, bool across_patterns)
     return pc;
 }
 
-cas_status upload_pieces(const Pieces& pc, FastTranspose& t)
+void pack_pieces(const Pieces& pc, FastTranspose& t, MetaPack& mp)
 {
     t.nsc = static_cast<int>(pc.sc_width.size());
     t.npieces = static_cast<int>(pc.pat.size());
-    CAS_TRY(upload(pc.sc_piece0, &t.sc_piece0));
-    CAS_TRY(upload(pc.sc_width, &t.sc_width));
-    CAS_TRY(upload(pc.pat, &t.piece_pat));
-    CAS_TRY(upload(pc.ch0, &t.piece_ch0));
-    CAS_TRY(upload(pc.ch1, &t.piece_ch1));
-    CAS_TRY(upload(pc.acc, &t.piece_acc));
-    CAS_TRY(upload(pc.chunk_sc, &t.chunk_sc));
-    CAS_TRY(upload(pc.chunk_acc, &t.chunk_acc));
-    return CAS_OK;
+    mp.add(pc.sc_piece0, &t.sc_piece0);
+    mp.add(pc.sc_width, &t.sc_width);
+    mp.add(pc.pat, &t.piece_pat);
+    mp.add(pc.ch0, &t.piece_ch0);
+    mp.add(pc.ch1, &t.piece_ch1);
+    mp.add(pc.acc, &t.piece_acc);
+    mp.add(pc.chunk_sc, &t.chunk_sc);
+    mp.add(pc.chunk_acc, &t.chunk_acc);
 }
 
 // Builds the work list of one A'y variant from the entry counts per (block,
@@ -999,7 +1015,8 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
     t.pack = pack;
     t.persistent = persistent;
     const Pieces pc = pack_chunks(g, per_sc * kChunkCols, pack);
-    CAS_TRY(upload_pieces(pc, t));
+    MetaPack mp;
+    pack_pieces(pc, t, mp);
     const int nsc = t.nsc;
     // entries per (problem, super-chunk); items never span problems
     std::vector<int64_t> sc_entries(static_cast<size_t>(g.nprob) * nsc, 0);
@@ -1033,14 +1050,14 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
     }
     sc_item0.push_back(static_cast<int>(item_sc.size()));
     t.nitems = static_cast<int>(item_sc.size());
-    CAS_TRY(upload(item_sc, &t.item_sc));
-    CAS_TRY(upload(item_b0, &t.item_b0));
-    CAS_TRY(upload(item_b1, &t.item_b1));
-    CAS_TRY(upload(item_part, &t.item_part));
-    CAS_TRY(upload(sc_item0, &t.sc_item0));
-    CAS_CUDA(cudaMalloc(&t.partial, elem * std::max<int64_t>(part_elems, 1)));
-    CAS_CUDA(cudaMalloc(&t.ctr, sizeof(int) * 2));
-    CAS_CUDA(cudaMemset(t.ctr, 0, sizeof(int) * 2));
+    mp.add(item_sc, &t.item_sc);
+    mp.add(item_b0, &t.item_b0);
+    mp.add(item_b1, &t.item_b1);
+    mp.add(item_part, &t.item_part);
+    mp.add(sc_item0, &t.sc_item0);
+    mp.add(std::vector<int>{0, 0}, &t.ctr);
+    CAS_TRY(mp.upload(&t.meta));
+    CAS_CUDA(dmalloc(&t.partial, elem * std::max<int64_t>(part_elems, 1)));
     return CAS_OK;
 }
 
@@ -1063,7 +1080,8 @@ cas_status build_block_items(const FastGeometry& g, FastTranspose& t)
         pc.chunk_acc.push_back(0);
     }
     pc.sc_piece0.push_back(g.nchunks);
-    CAS_TRY(upload_pieces(pc, t));
+    MetaPack mp;
+    pack_pieces(pc, t, mp);
     const int64_t n = g.nblocks * g.nchunks;
     t.nitems = static_cast<int>(n);
     std::vector<int> isc(n), ib0(n), ib1(n);
@@ -1077,11 +1095,11 @@ cas_status build_block_items(const FastGeometry& g, FastTranspose& t)
             ib1[i] = static_cast<int>(b + 1);
             ipart[i] = b * g.cols + g.off[p] + static_cast<int64_t>(ch - g.chunk0[p]) * kChunkCols;
         }
-    CAS_TRY(upload(isc, &t.item_sc));
-    CAS_TRY(upload(ib0, &t.item_b0));
-    CAS_TRY(upload(ib1, &t.item_b1));
-    CAS_TRY(upload(ipart, &t.item_part));
-    return CAS_OK;
+    mp.add(isc, &t.item_sc);
+    mp.add(ib0, &t.item_b0);
+    mp.add(ib1, &t.item_b1);
+    mp.add(ipart, &t.item_part);
+    return mp.upload(&t.meta);
 }
 
 TView tview(const FastTranspose& t)
@@ -1116,17 +1134,28 @@ size_t spmv_t_smem(int per_sc, bool ring)
 
 void free_transpose(FastTranspose& t)
 {
-    for (void* ptr : {(void*)t.sc_piece0, (void*)t.sc_width, (void*)t.piece_pat, (void*)t.piece_ch0,
-                      (void*)t.piece_ch1, (void*)t.piece_acc, (void*)t.chunk_sc, (void*)t.chunk_acc,
-                      (void*)t.item_sc, (void*)t.item_b0, (void*)t.item_b1, (void*)t.item_part, (void*)t.sc_item0,
-                      t.partial, (void*)t.ctr})
-        cudaFree(ptr);
+    dfree(t.meta);
+    dfree(t.partial);
     t = FastTranspose{};
 }
 
 // Opt-in shared memory for every product kernel (set outside any stream
-// capture, at build time).
+// capture, at the first build on each device).
+cas_status fast_set_attributes_now();
 cas_status fast_set_attributes()
+{
+    static std::mutex mu;
+    static std::vector<char> done;
+    int dev = 0;
+    CAS_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if (static_cast<int>(done.size()) <= dev) done.resize(dev + 1, 0);
+    if (done[dev]) return CAS_OK;
+    CAS_TRY(fast_set_attributes_now());
+    done[dev] = 1;
+    return CAS_OK;
+}
+cas_status fast_set_attributes_now()
 {
     const int s32 = static_cast<int>(sizeof(float) * kTable32), s64 = static_cast<int>(sizeof(double) * kTable64);
     const int t32 = static_cast<int>(spmv_t_smem<float>(kMaxScRegs, false));
@@ -1233,8 +1262,8 @@ cas_status tune_transpose(FastLayout& f, const std::vector<int64_t>& entries, cu
             st = CAS_ERR_CUDA;
         }
     };
-    fail(cudaMalloc(&y, sizeof(float) * g.rows));
-    fail(cudaMalloc(&x, sizeof(float) * std::max<int64_t>(g.cols, 1)));
+    fail(dmalloc(&y, sizeof(float) * g.rows));
+    fail(dmalloc(&x, sizeof(float) * std::max<int64_t>(g.cols, 1)));
     fail(cudaEventCreate(&e0));
     fail(cudaEventCreate(&e1));
     if (st == CAS_OK) fail(cudaMemsetAsync(y, 0, sizeof(float) * g.rows, s));
@@ -1259,8 +1288,8 @@ cas_status tune_transpose(FastLayout& f, const std::vector<int64_t>& entries, cu
             best = c;
         }
     }
-    cudaFree(y);
-    cudaFree(x);
+    dfree(y);
+    dfree(x);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (st != CAS_OK) return st;
@@ -1285,13 +1314,13 @@ bool fast_supported(const PatternSet& ps)
 
 void fast_free(FastLayout& f)
 {
-    cudaFree(f.a16);
-    cudaFree(f.g32);
-    cudaFree(f.chunk_start);
+    dfree(f.a16);
+    dfree(f.g32);
+    dfree(f.chunk_start);
     free_transpose(f.t32);
     free_transpose(f.t64);
     free_transpose(f.tb);
-    cudaFree(f.eval_partial);
+    dfree(f.eval_partial);
     f = FastLayout{};
 }
 
@@ -1338,9 +1367,9 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
     CAS_REQUIRE(g.total_elems() < 0xFFFFFFFFLL, CAS_ERR_INVALID_ARGUMENT,
                 "blocked layout: 2^32 or more entries (with block padding) are not supported");
     const int64_t elems = std::max<int64_t>(g.total_elems(), 8);
-    CAS_CUDA(cudaMalloc(&f.a16, sizeof(uint16_t) * elems));
-    CAS_CUDA(cudaMalloc(&f.g32, sizeof(uint32_t) * elems));
-    CAS_CUDA(cudaMalloc(&f.chunk_start, sizeof(uint32_t) * std::max<int64_t>(g.nblocks * g.nchunks, 1)));
+    CAS_CUDA(dmalloc(&f.a16, sizeof(uint16_t) * elems));
+    CAS_CUDA(dmalloc(&f.g32, sizeof(uint32_t) * elems));
+    CAS_CUDA(dmalloc(&f.chunk_start, sizeof(uint32_t) * std::max<int64_t>(g.nblocks * g.nchunks, 1)));
     if (rows > 0) {
         const int threads = 256;
         const unsigned grid = fgrid(rows, threads);
@@ -1350,10 +1379,10 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
         const int64_t groups = g.nblocks * g.npat;
         const unsigned sgrid = static_cast<unsigned>(std::min<int64_t>(groups, static_cast<int64_t>(sm_count())));
         uint32_t* scratch = nullptr;
-        CAS_CUDA(cudaMallocAsync(&scratch, sizeof(uint32_t) * kBlockRows * 8 * sgrid, s));
+        CAS_CUDA(dmalloc(&scratch, sizeof(uint32_t) * kBlockRows * 8 * sgrid));
         { fast_sort_kernel<<<sgrid, kSortThreads, 0, s>>>(g, f.a16, f.g32, scratch); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
-        cudaFreeAsync(scratch, s);
+        dfree(scratch);
         { fast_chunk_kernel<<<fgrid(g.nblocks * g.nchunks, 256), 256, 0, s>>>(g, f.g32, f.chunk_start); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         if (diag_int) {
@@ -1494,10 +1523,10 @@ cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float
     if (nb > f.eval_blocks) {
         if (f.eval_partial) {
             CAS_CUDA(cudaStreamSynchronize(s));
-            cudaFree(f.eval_partial);
+            dfree(f.eval_partial);
             f.eval_partial = nullptr;
         }
-        CAS_CUDA(cudaMalloc(&f.eval_partial, sizeof(float) * nb * f.g.cols));
+        CAS_CUDA(dmalloc(&f.eval_partial, sizeof(float) * nb * f.g.cols));
         f.eval_blocks = nb;
     }
     const size_t smem = spmv_t_smem<float>(1, false);

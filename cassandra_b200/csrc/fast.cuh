@@ -147,6 +147,7 @@ struct FastTranspose {
     int* sc_item0 = nullptr;       // [nsc + 1] first item of each super-chunk
     void* partial = nullptr;       // float or double partials
     int* ctr = nullptr;            // [2] work counter and finished CTAs of the persistent schedule (reset by the kernel)
+    void* meta = nullptr;          // one device block holding every array above except partial
 };
 
 // One measured A'y schedule of the build-time autotuner.

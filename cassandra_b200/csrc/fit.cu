@@ -193,11 +193,11 @@ CAS_API cas_status cas_fit_weights(const uint64_t* masks, int n_masks, cas_index
         set_error(std::string("cas_fit_weights: ") + cudaGetErrorString(e));
         st = e == cudaErrorMemoryAllocation ? CAS_ERR_OUT_OF_MEMORY : CAS_ERR_CUDA;
     };
-    cudaError_t e = cudaMalloc(&d_pos, 16 * std::max<int64_t>(rows, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&d_s32, sizeof(float) * std::max<int64_t>(rows, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&d_s, sizeof(double) * std::max<int64_t>(rows, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&d_w, sizeof(double) * std::max<int64_t>(cols, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&d_w32, sizeof(float) * std::max<int64_t>(cols, 1));
+    cudaError_t e = dmalloc(&d_pos, 16 * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = dmalloc(&d_s32, sizeof(float) * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = dmalloc(&d_s, sizeof(double) * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = dmalloc(&d_w, sizeof(double) * std::max<int64_t>(cols, 1));
+    if (e == cudaSuccess) e = dmalloc(&d_w32, sizeof(float) * std::max<int64_t>(cols, 1));
     if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_pos, h_positions, 16 * rows, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_s32, h_scores, sizeof(float) * rows, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) fail(e);
@@ -212,11 +212,11 @@ CAS_API cas_status cas_fit_weights(const uint64_t* masks, int n_masks, cas_index
         if (e != cudaSuccess) fail(e);
     }
     cudaStreamSynchronize(s);
-    cudaFree(d_pos);
-    cudaFree(d_s32);
-    cudaFree(d_s);
-    cudaFree(d_w);
-    cudaFree(d_w32);
+    dfree(d_pos);
+    dfree(d_s32);
+    dfree(d_s);
+    dfree(d_w);
+    dfree(d_w32);
     cudaStreamDestroy(s);
     cas_patterns_destroy(p);
     return st;
@@ -280,11 +280,11 @@ CAS_API cas_status cas_fit_weights_batched(const uint64_t* masks, int n_masks, c
         set_error(std::string("cas_fit_weights_batched: ") + cudaGetErrorString(e));
         st = e == cudaErrorMemoryAllocation ? CAS_ERR_OUT_OF_MEMORY : CAS_ERR_CUDA;
     };
-    cudaError_t e = cudaMalloc(&d_pos, 16 * std::max<int64_t>(rows, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&d_s32, sizeof(float) * std::max<int64_t>(rows, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&d_s, sizeof(double) * std::max<int64_t>(rows, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&d_w, sizeof(double) * std::max<int64_t>(cols, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&d_w32, sizeof(float) * std::max<int64_t>(cols, 1));
+    cudaError_t e = dmalloc(&d_pos, 16 * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = dmalloc(&d_s32, sizeof(float) * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = dmalloc(&d_s, sizeof(double) * std::max<int64_t>(rows, 1));
+    if (e == cudaSuccess) e = dmalloc(&d_w, sizeof(double) * std::max<int64_t>(cols, 1));
+    if (e == cudaSuccess) e = dmalloc(&d_w32, sizeof(float) * std::max<int64_t>(cols, 1));
     if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_pos, h_positions, 16 * rows, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_s32, h_scores, sizeof(float) * rows, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) fail(e);
@@ -299,11 +299,11 @@ CAS_API cas_status cas_fit_weights_batched(const uint64_t* masks, int n_masks, c
         if (e != cudaSuccess) fail(e);
     }
     cudaStreamSynchronize(s);
-    cudaFree(d_pos);
-    cudaFree(d_s32);
-    cudaFree(d_s);
-    cudaFree(d_w);
-    cudaFree(d_w32);
+    dfree(d_pos);
+    dfree(d_s32);
+    dfree(d_s);
+    dfree(d_w);
+    dfree(d_w32);
     cudaStreamDestroy(s);
     cas_patterns_destroy(p);
     return st;

@@ -59,7 +59,8 @@ enum Slot {
 // kIterRef: iteration count at the last replacement.
 enum Flag {
     kDone = 0, kStatus = 1, kIter = 2, kRefine = 3, kPending = 4, kRestart = 5, kSkip = 6, kIterRef = 7,
-    kFlags = 8
+    kVerified = 8,  // the tolerance was met by a freshly computed FP64 true residual
+    kFlags = 9
 };
 
 // Reliable updating of the mixed solver: when the recursive residual has
@@ -330,6 +331,7 @@ __global__ void __launch_bounds__(kRedThreads) pcg_beta_kernel(const double* __r
         } else if (met) {
             dv.flags[kDone] = 1;
             dv.flags[kSkip] = 1;
+            if (replace) dv.flags[kVerified] = 1;
         }
     }
 }
@@ -641,9 +643,9 @@ struct SolverImpl {
         for (void* ptr : {(void*)x, (void*)r, (void*)z, (void*)p, (void*)d, (void*)w, (void*)v, (void*)pg32, q,
                           (void*)q64, (void*)b_own, (void*)partial, (void*)part_q, (void*)part_a, (void*)part_b, (void*)part_c,
                           (void*)scal, (void*)flags})
-            cudaFree(ptr);
-        cudaFreeHost(host_scal);
-        cudaFreeHost(host_flags);
+            dfree(ptr);
+        hfree(host_scal);
+        hfree(host_flags);
     }
 
     // Column sums of the last A'q of precision T.
@@ -901,19 +903,19 @@ struct SolverImpl {
         // norm partials: one per row CTA (rows layout) or per block (blocked)
         const int q_parts = std::max({n_row_blocks, sm_count(), fast ? static_cast<int>(fast->g.nblocks) : 0});
         const size_t cb = sizeof(double) * std::max<int64_t>(C, 1), rb8 = sizeof(double) * std::max<int64_t>(R, 1);
-        for (double** ptr : {&x, &r, &z, &p, &d, &w, &v}) CAS_CUDA(cudaMalloc(ptr, cb));
-        if (mixed) CAS_CUDA(cudaMalloc(&pg32, sizeof(float) * std::max<int64_t>(C, 1)));
-        CAS_CUDA(cudaMalloc(&q, mixed ? sizeof(float) * std::max<int64_t>(R, 1) : rb8));
-        CAS_CUDA(cudaMalloc(&q64, rb8));
-        if (rows_layout) CAS_CUDA(cudaMalloc(&partial, sizeof(double) * std::max<int64_t>(a.units, 1)));
-        CAS_CUDA(cudaMalloc(&part_q, sizeof(double) * 2 * q_parts));
-        CAS_CUDA(cudaMalloc(&part_a, sizeof(double) * 2 * std::max(n_vec_blocks, q_parts)));
-        CAS_CUDA(cudaMalloc(&part_b, sizeof(double) * 2 * n_vec_blocks));
-        CAS_CUDA(cudaMalloc(&part_c, sizeof(double) * 2 * n_vec_blocks));
-        CAS_CUDA(cudaMalloc(&scal, sizeof(double) * kSlots));
-        CAS_CUDA(cudaMalloc(&flags, sizeof(int) * kFlags));
-        CAS_CUDA(cudaMallocHost(&host_scal, sizeof(double) * kSlots));
-        CAS_CUDA(cudaMallocHost(&host_flags, sizeof(int) * kFlags));
+        for (double** ptr : {&x, &r, &z, &p, &d, &w, &v}) CAS_CUDA(dmalloc(ptr, cb));
+        if (mixed) CAS_CUDA(dmalloc(&pg32, sizeof(float) * std::max<int64_t>(C, 1)));
+        CAS_CUDA(dmalloc(&q, mixed ? sizeof(float) * std::max<int64_t>(R, 1) : rb8));
+        CAS_CUDA(dmalloc(&q64, rb8));
+        if (rows_layout) CAS_CUDA(dmalloc(&partial, sizeof(double) * std::max<int64_t>(a.units, 1)));
+        CAS_CUDA(dmalloc(&part_q, sizeof(double) * 2 * q_parts));
+        CAS_CUDA(dmalloc(&part_a, sizeof(double) * 2 * std::max(n_vec_blocks, q_parts)));
+        CAS_CUDA(dmalloc(&part_b, sizeof(double) * 2 * n_vec_blocks));
+        CAS_CUDA(dmalloc(&part_c, sizeof(double) * 2 * n_vec_blocks));
+        CAS_CUDA(dmalloc(&scal, sizeof(double) * kSlots));
+        CAS_CUDA(dmalloc(&flags, sizeof(int) * kFlags));
+        CAS_CUDA(hmalloc(&host_scal, sizeof(double) * kSlots));
+        CAS_CUDA(hmalloc(&host_flags, sizeof(int) * kFlags));
         CAS_CUDA(cudaMemsetAsync(scal, 0, sizeof(double) * kSlots, s));
         CAS_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * kFlags, s));
         const double tol = o.tol;
@@ -1022,7 +1024,7 @@ cas_status create_solver(const cas_csr* a, const cas_solve_opts* o, const double
     m.b = d_b;
     if (d_bn) {
         // the normal-equation right-hand side is copied (cols doubles)
-        if (cudaMalloc(&m.b_own, sizeof(double) * std::max<int64_t>(a->cols, 1)) != cudaSuccess ||
+        if (dmalloc(&m.b_own, sizeof(double) * std::max<int64_t>(a->cols, 1)) != cudaSuccess ||
             cudaMemcpyAsync(m.b_own, d_bn, sizeof(double) * a->cols, cudaMemcpyDeviceToDevice, m.s) != cudaSuccess) {
             delete sv;
             set_error("cas_solver_create_normal: cannot copy the right-hand side");
@@ -1139,6 +1141,11 @@ CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
             if (rel <= m.o.tol) break;
         }
         if (done) {
+            if (m.host_flags[kVerified] && m.o.method != CAS_LSQR) {
+                // a residual replacement met the tolerance on the FP64 true residual
+                rel = m.host_scal[kRes];
+                break;
+            }
             // verify with the true FP64 residual
             CAS_TRY(m.true_residual(&rel));
             if (m.o.tol <= 0 || rel <= m.o.tol || it >= m.o.max_iterations) break;

@@ -62,6 +62,17 @@ CAS_API int cas_version(void);
  * replayed CUDA graph count at every replay).  Used to report launches. */
 CAS_API long long cas_kernel_launches(void);
 
+/* No counterpart in the reference (memory of the library's own objects).
+ * Layouts, solvers and the one-shot fits take device and pinned host memory
+ * from a per-device cache that keeps freed blocks for the next object of a
+ * similar size (the training loop fits the same shapes repeatedly), up to a
+ * quarter of the device's memory.  A cached block is reused only after the
+ * work that used it has finished, as with cudaFree.
+ * cas_cached_memory: bytes held in the cache now (free, not in use).
+ * cas_release_cached_memory: returns every cached block to the driver. */
+CAS_API size_t cas_cached_memory(void);
+CAS_API void cas_release_cached_memory(void);
+
 /* ------------------------------------------------------------------------ */
 /* Pattern sets: GroupIndexer (Pattern/Indexer.h:29-40)                      */
 /* ------------------------------------------------------------------------ */

@@ -14,6 +14,7 @@ The shipped library never imports this package.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import subprocess
 from pathlib import Path
@@ -118,6 +119,20 @@ def ref_lib() -> C.CDLL:
             getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, _VP, _VP]
         _ref = lib
     return _ref
+
+
+@contextlib.contextmanager
+def single_thread():
+    """Runs the compiled reference on one OpenMP thread: its `x * A`
+    (Math/MatrixCSR.cpp:67-87) merges thread sums in arrival order, so only a
+    single thread gives a reproducible target."""
+    gomp = C.CDLL("libgomp.so.1")
+    before = gomp.omp_get_max_threads()
+    gomp.omp_set_num_threads(1)
+    try:
+        yield
+    finally:
+        gomp.omp_set_num_threads(before)
 
 
 def ref64_lib() -> C.CDLL:

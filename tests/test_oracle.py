@@ -147,17 +147,20 @@ def _ref64_pcg(ref, idx, cols, b, iters):
 
 
 def test_pcg_matches_reference_fp64(orc, ref):
-    """Same iterates as the reference's PCG retyped to FP64.  CG amplifies the
-    rounding of differently ordered sums (the reference reduces with OpenMP),
-    so iterates agree to ~1e-14 after 10 steps and, after 60, the residuals
-    and predictions agree to the stated looser bounds."""
+    """Same iterates as the reference's PCG retyped to FP64 (run on one
+    thread: with more, its sums merge in arrival order and the target moves
+    run to run).  CG amplifies the rounding of differently ordered sums, so
+    iterates agree to ~1e-14 after 10 steps and, after 60, the residuals and
+    predictions agree to the stated looser bounds."""
     idx, cols, b = _small_system(orc)
     x, res, it = orc.pcg(idx, cols, b, 10)
     assert it == 10
-    want, _ = _ref64_pcg(ref, idx, cols, b, 10)
+    with orc.single_thread():
+        want, _ = _ref64_pcg(ref, idx, cols, b, 10)
     np.testing.assert_allclose(x, want, rtol=0, atol=1e-11 * np.abs(want).max())
     x, res, it = orc.pcg(idx, cols, b, 60)
-    want, rel = _ref64_pcg(ref, idx, cols, b, 60)
+    with orc.single_thread():
+        want, rel = _ref64_pcg(ref, idx, cols, b, 60)
     assert abs(orc.normal_residual(idx, cols, b, x) - rel) <= 1e-2 * rel
     aw = orc.spmv(idx, cols, want)
     np.testing.assert_allclose(orc.spmv(idx, cols, x), aw, rtol=0, atol=1e-5 * np.abs(aw).max())
