@@ -78,16 +78,13 @@ __device__ __forceinline__ void bacc(Comp& c, double x)
         c.s += x;
 }
 
-// The problems a vector step works on, in problem order: the CTAs of the
-// step's 1D grid are dealt round-robin over them (CTA i serves list slot
-// i % n as its (i / n)-th CTA), so a lone remaining problem gets the whole
-// grid and 60 problems about 10 CTAs each.  Partials live at
+// The problems a vector step works on (FastActive), in problem order: the
+// CTAs of the step's 1D grid are dealt round-robin over them (CTA i serves
+// list slot i % n as its (i / n)-th CTA), so a lone remaining problem gets
+// the whole grid and 60 problems about 10 CTAs each.  Partials live at
 // part[q][rank]; a reduction over problem q sums the ranks its slot had.
-struct ActiveList {
-    int n;
-    int list[kMaxProblems];
-    int pos[kMaxProblems];  // slot of each problem, -1 if absent
-};
+// The same list tells the products which problems' blocks and items run.
+using ActiveList = FastActive;
 
 struct Slot {
     int q, rank, ranks;  // problem, CTA rank within it, CTAs serving it
@@ -256,8 +253,9 @@ __global__ void __launch_bounds__(kBRedThreads) balpha_kernel(FastGeometry g, co
     __shared__ double smem[64];
     const int q = blockIdx.x;
     if (retired(d, q)) return;
+    // the A p norm partials of the problem's blocks, kAxSplitMax per block
     const int b0 = g.pblk0[q], nb = g.pblk0[q + 1] - g.pblk0[q];
-    const double pap = bsum<COMP>(part_q + 2 * b0, nb, smem);
+    const double pap = bsum<COMP>(part_q + 2 * static_cast<int64_t>(b0) * kAxSplitMax, nb * kAxSplitMax, smem);
     if (threadIdx.x == 0) {
         double* sc = d.scal + q * kBSlots;
         sc[bPap] = pap;
@@ -466,13 +464,16 @@ struct BatchSolver {
 
     // A'(b - A x) in FP64 into the t64 partials, for all problems, the
     // active ones, or those with a replacement due.
+    // (Sel::Active rebuilds the active list first: the host resumed problems.)
     cas_status residual_products(Sel sel)
     {
         const BDev d = dev();
         int* whole = sel == Sel::All ? nullptr : (sel == Sel::Active ? d.alldone : d.skipall);
         const int* per = sel == Sel::All ? nullptr : (sel == Sel::Active ? d.pdone : d.pskip);
-        CAS_TRY((fast_spmv<double, double>(*f, x, q64, b, nullptr, part_q, whole, 2, s, nullptr, per)));
-        return fast_spmv_t_partials<double>(*f, q64, whole, s, per);
+        if (sel == Sel::Active) { bcompact_kernel<<<1, 64, 0, s>>>(d.pdone, B, act); cas::count_launch(); }
+        const ActiveList* al = sel == Sel::All ? all : act;
+        CAS_TRY((fast_spmv<double, double>(*f, x, q64, b, nullptr, part_q, whole, 2, s, nullptr, per, al)));
+        return fast_spmv_t_partials<double>(*f, q64, whole, s, per, al);
     }
 
     // Residual replacement (restart: p = z too) for the active problems.
@@ -493,8 +494,6 @@ struct BatchSolver {
         double* pdev = restart ? nullptr : part_c;
         const int* qgate = sel == Sel::Due ? d.pskip : d.pdone;
         // Sel::All works on every problem; the others on the active list
-        // (rebuilt here after the host resumed problems)
-        if (sel == Sel::Active) { bcompact_kernel<<<1, 64, 0, s>>>(d.pdone, B, act); cas::count_launch(); }
         const ActiveList* al = sel == Sel::All ? all : act;
         if (mixed)
             { bresidual_kernel<COMP, float><<<vgrid(), kBVecThreads, 0, s>>>(fc, t64, r, z, p, pg32, dinv, al, part_a,
@@ -521,8 +520,8 @@ struct BatchSolver {
         const T* pgather = std::is_same<T, float>::value ? reinterpret_cast<const T*>(pg32) : reinterpret_cast<const T*>(p);
         { bcompact_kernel<<<1, 64, 0, s>>>(d.pdone, B, act); cas::count_launch(); }
         CAS_TRY((fast_spmv<T, T>(*f, pgather, static_cast<T*>(q), nullptr, nullptr, part_q, d.alldone, 0, s, nullptr,
-                                 d.pdone)));
-        CAS_TRY(fast_spmv_t_partials<T>(*f, static_cast<const T*>(q), d.alldone, s, d.pdone));
+                                 d.pdone, act)));
+        CAS_TRY(fast_spmv_t_partials<T>(*f, static_cast<const T*>(q), d.alldone, s, d.pdone, act));
         { balpha_kernel<COMP><<<B, kBRedThreads, 0, s>>>(f->g, part_q, d); cas::count_launch(); }
         const FastCols fc = fast_cols<T>(*f);
         { bupdate_kernel<COMP, T><<<vgrid(), kBVecThreads, 0, s>>>(fc, static_cast<const T*>(sizeof(T) == 4 ? f->t32.partial
@@ -634,7 +633,7 @@ struct BatchSolver {
         if (mixed) CAS_CUDA(dmalloc(&pg32, sizeof(float) * std::max<int64_t>(C, 1)));
         CAS_CUDA(dmalloc(&q, mixed ? sizeof(float) * std::max<int64_t>(R, 1) : rb));
         CAS_CUDA(dmalloc(&q64, rb));
-        CAS_CUDA(dmalloc(&part_q, sizeof(double) * 2 * std::max<int64_t>(f->g.nblocks, 1)));
+        CAS_CUDA(dmalloc(&part_q, sizeof(double) * 2 * kAxSplitMax * std::max<int64_t>(f->g.nblocks, 1)));
         CAS_CUDA(dmalloc(&part_a, sizeof(double) * 2 * B * G));
         CAS_CUDA(dmalloc(&part_b, sizeof(double) * 2 * B * G));
         CAS_CUDA(dmalloc(&part_c, sizeof(double) * 2 * B * G));

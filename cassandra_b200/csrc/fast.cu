@@ -207,18 +207,21 @@ __global__ void __launch_bounds__(kSortThreads, 1) fast_sort_kernel(FastGeometry
     }
 }
 
-// First entry of every (block, chunk) in G32: lower bound of the chunk's
-// first column in the sorted group.
-__global__ void fast_chunk_kernel(FastGeometry g, const uint32_t* __restrict__ g32, uint32_t* __restrict__ chunk_start)
+// First entry of every (block, column sub-chunk) in G32: lower bound of the
+// sub-chunk's first column in the sorted group (sub-chunks past the end of
+// a pattern's columns get the group's end).
+__global__ void fast_sub_kernel(FastGeometry g, const uint32_t* __restrict__ g32, uint32_t* __restrict__ sub_start)
 {
-    const int64_t total = g.nblocks * g.nchunks;
+    const int nsub = g.nchunks * kSubPerChunk;
+    const int64_t total = g.nblocks * nsub;
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t b = i / g.nchunks;
-        const int ch = static_cast<int>(i - b * g.nchunks);
+        const int64_t b = i / nsub;
+        const int j = static_cast<int>(i - b * nsub);
+        const int ch = j / kSubPerChunk;
         int p = 0;
         while (p + 1 < g.npat && g.chunk0[p + 1] <= ch) p++;
-        const uint32_t c0 = static_cast<uint32_t>(ch - g.chunk0[p]) * kChunkCols;
+        const uint32_t c0 = static_cast<uint32_t>(j - g.chunk0[p] * kSubPerChunk) * kSubCols;
         const int64_t seg = g.seg(b, p);
         int64_t lo = 0, hi = g.seg_len(b, p);
         while (lo < hi) {
@@ -228,7 +231,7 @@ __global__ void fast_chunk_kernel(FastGeometry g, const uint32_t* __restrict__ g
             else
                 hi = mid;
         }
-        chunk_start[i] = static_cast<uint32_t>(seg + lo);
+        sub_start[i] = static_cast<uint32_t>(seg + lo);
     }
 }
 
@@ -386,11 +389,65 @@ __device__ __forceinline__ void gather_segment8(const uint16_t* __restrict__ bas
     }
 }
 
+// Prefix sums over an active list of a per-problem count (cnt(q)) into
+// pref[0..n] in shared memory, by warp 0; every thread returns the total.
+template <typename F>
+__device__ __forceinline__ int active_prefix(const FastActive* __restrict__ act, int* pref, F cnt)
+{
+    const int n = act->n;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int carry = 0;
+        for (int base = 0; base < n; base += 32) {
+            const int t = base + lane;
+            int v = t < n ? cnt(act->list[t]) : 0;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, v, d);
+                if (lane >= d) v += u;
+            }
+            if (t < n) pref[t + 1] = carry + v;
+            carry += __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (lane == 0) pref[0] = 0;
+    }
+    __syncthreads();
+    return pref[n];
+}
+
+// Slot k of the active list with pref[k] <= i < pref[k + 1] (0 <= i < pref[n]).
+__device__ __forceinline__ int active_slot(const int* pref, int n, int i)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pref[mid] <= i)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Splits of a work unit when `units` units of a product are to fill `ctas`
+// CTAs: about two units per CTA, at most cap.
+__host__ __device__ __forceinline__ int unit_splits(int64_t units, int64_t ctas, int cap)
+{
+    if (units <= 0) return 1;
+    const int64_t k = (2 * ctas + units - 1) / units;
+    return static_cast<int>(k < 1 ? 1 : (k > cap ? cap : k));
+}
+
 // ALL8: every pattern has 8 slots (the expanded layout), so only the
 // pipelined 8-slot path is compiled in.
-// part (optional) receives one compensated partial of ||y||^2 per block, so
-// that the norms of the problems of a batched layout can be summed apart.
-// Blocks of problems whose pdone flag is set are skipped (partial 0).
+// A work unit is one of a block's row splits (a CTA stages x's pattern
+// slices once per unit, so splits pay only when units are few).  part
+// (optional) receives one compensated partial of ||y||^2 per unit, so that
+// the norms of the problems of a batched layout can be summed apart.
+// Blocks of problems whose pdone flag is set are skipped (partials 0).
+// Without act: units (block, split) for every block, `split` splits each,
+// partials [block][split].  With act: the listed problems' blocks only,
+// partials [block][kAxSplitMax] (splits past the one in use written 0).
 template <typename T, typename Y, int MODE, bool ALL8>
 __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g, const uint16_t* __restrict__ a16,
                                                                    const T* __restrict__ x, Y* __restrict__ y,
@@ -398,26 +455,47 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
                                                                    const double* __restrict__ coef,
                                                                    double* __restrict__ part,
                                                                    const int* __restrict__ done,
-                                                                   const int* __restrict__ pdone)
+                                                                   const int* __restrict__ pdone,
+                                                                   const FastActive* __restrict__ act, int split)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* table = reinterpret_cast<T*>(smem_raw);
     __shared__ double red[64];
+    __shared__ int pref[kMaxProblems + 1];
     if (done && *(volatile const int*)done) return;
     constexpr int kCap = sizeof(T) == 4 ? kTable32 : kTable64;
     using Acc = typename AccOf<T>::type;
     const double c = MODE == 1 ? *coef : 0.0;
-    for (int64_t blk = blockIdx.x; blk < g.nblocks; blk += gridDim.x) {
+    int S = split, stride = split;
+    int64_t units = g.nblocks * split;
+    if (act) {
+        const int nblk = active_prefix(act, pref, [&](int q) { return g.pblk0[q + 1] - g.pblk0[q]; });
+        S = unit_splits(nblk, gridDim.x, kAxSplitMax);
+        stride = kAxSplitMax;
+        units = static_cast<int64_t>(nblk) * S;
+    }
+    for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+        const int sp = static_cast<int>(u % S);
+        int64_t blk = u / S;
+        if (act) {
+            const int i = static_cast<int>(blk);
+            const int slot = active_slot(pref, act->n, i);
+            blk = g.pblk0[act->list[slot]] + (i - pref[slot]);
+        }
         const int q = g.prob_of_block(blk);
+        double* pu = part ? part + 2 * (blk * stride + sp) : nullptr;
+        if (pu && sp == 0 && static_cast<int>(threadIdx.x) < 2 * (stride - S)) pu[2 * S + threadIdx.x] = 0;
         if (pdone && pdone[q]) {
-            if (part && threadIdx.x == 0) {
-                part[2 * blk] = 0;
-                part[2 * blk + 1] = 0;
+            if (pu && threadIdx.x == 0) {
+                pu[0] = 0;
+                pu[1] = 0;
             }
             continue;
         }
-        const int nb = static_cast<int>(g.block_rows(blk));
-        const int64_t row0 = g.block_row0(blk);
+        const int rows_b = static_cast<int>(g.block_rows(blk));
+        const int r0 = static_cast<int>(static_cast<int64_t>(rows_b) * sp / S);
+        const int nb = static_cast<int>(static_cast<int64_t>(rows_b) * (sp + 1) / S) - r0;
+        const int64_t row0 = g.block_row0(blk) + r0;
         const T* xq = x + q * g.pcols;
         Comp mine;
         Acc acc[kAxRows];
@@ -429,9 +507,9 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
             __syncthreads();
             load_table<T>(table, xg, cap);
             __syncthreads();
-            const uint16_t* base = a16 + g.seg(blk, p);
-            const bool all_in = g.space[p] <= kCap;
             const int ns = g.slots[p];
+            const uint16_t* base = a16 + g.seg(blk, p) + static_cast<int64_t>(r0) * ns;
+            const bool all_in = g.space[p] <= kCap;
             if (ALL8 || ns == 8) {
                 if (all_in)
                     gather_segment8<T, true>(base, nb, table, xg, cap, acc);
@@ -458,11 +536,11 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
                 mine.add(static_cast<double>(yv) * static_cast<double>(yv));
             }
         }
-        if (part) {
+        if (pu) {
             const Comp r = block_sum_comp<kAxThreads>(mine, red);
             if (threadIdx.x == 0) {
-                part[2 * blk] = r.s;
-                part[2 * blk + 1] = r.c;
+                pu[0] = r.s;
+                pu[1] = r.c;
             }
         }
     }
@@ -482,6 +560,8 @@ struct TView {
     const int* piece_ch0;
     const int* piece_ch1;
     const int* piece_acc;
+    const int* sc_item0;  // [nprob * nsc + 1] first item of each (problem, super-chunk)
+    int nsc;
     int per_sc;
     int nitems;
 };
@@ -771,21 +851,46 @@ __device__ __forceinline__ void reduce_block_entries(const uint32_t* __restrict_
     }
 }
 
-// One work item: the partial column sums of super-chunk item_sc[item] over
-// the blocks [item_b0, item_b1), written to partial + item_part[item] -
-// item_part[item_base].
+// Accumulator columns [a0, a1) of piece pc that split `split` of `nsplit`
+// covers: its share of the piece's column sub-chunks.
+__device__ __forceinline__ void piece_share(const FastGeometry& g, const TView& tv, int pc, int split, int nsplit,
+                                            int& a0, int& a1)
+{
+    const int p = tv.piece_pat[pc];
+    const int cl0 = (tv.piece_ch0[pc] - g.chunk0[p]) * kChunkCols;
+    const int w = min(g.space[p], (tv.piece_ch1[pc] - g.chunk0[p]) * kChunkCols) - cl0;
+    const int ns = (w + kSubCols - 1) / kSubCols;
+    a0 = min(w, ns * split / nsplit * kSubCols);
+    a1 = min(w, ns * (split + 1) / nsplit * kSubCols);
+}
+
+// One work unit: split `split` of `nsplit` of item `item`, i.e. the partial
+// column sums of its share of super-chunk item_sc[item]'s columns (a share
+// of every piece's column sub-chunks) over the blocks [item_b0, item_b1),
+// written to those columns of partial + item_part[item] -
+// item_part[item_base].  A column's entries of a block are one run of the
+// sorted group, so splitting at sub-chunk bounds splits no run.
 template <typename T, bool RING>
 __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv, const uint32_t* __restrict__ g32,
-                                         const uint32_t* __restrict__ chunk_start, const T* __restrict__ y,
+                                         const uint32_t* __restrict__ sub_start, const T* __restrict__ y,
                                          T* __restrict__ partial, int item, int item_base, int64_t y_block0,
-                                         T* __restrict__ acc, T* __restrict__ ytile, uint32_t* __restrict__ ring,
-                                         WarpRec<T> (*recs)[kFastThreads / 32], const int* __restrict__ pdone)
+                                         int split, int nsplit, T* __restrict__ acc, T* __restrict__ ytile,
+                                         uint32_t* __restrict__ ring, WarpRec<T> (*recs)[kFastThreads / 32],
+                                         const int* __restrict__ pdone)
 {
     if (pdone && pdone[g.prob_of_block(tv.item_b0[item])]) return;  // retired problem: partials unused
     const int sc = tv.item_sc[item];
     const int pc0 = tv.sc_piece0[sc], pc1 = tv.sc_piece0[sc + 1];
-    const int width = tv.sc_width[sc];
-    for (int i = threadIdx.x; i < width; i += kFastThreads) acc[i] = 0;
+    const int nsub = g.nchunks * kSubPerChunk;
+    bool any = false;
+    for (int pc = pc0; pc < pc1; pc++) {
+        int a0, a1;
+        piece_share(g, tv, pc, split, nsplit, a0, a1);
+        any = any || a0 < a1;
+        T* ap = acc + tv.piece_acc[pc];
+        for (int i = a0 + threadIdx.x; i < a1; i += kFastThreads) ap[i] = 0;
+    }
+    if (!any) return;  // more splits than sub-chunks: nothing here
     int flip = 0;
     for (int64_t blk = tv.item_b0[item]; blk < tv.item_b1[item]; blk++) {
         const int nb = static_cast<int>(g.block_rows(blk));
@@ -802,12 +907,17 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
         }
         __syncthreads();
         for (int pc = pc0; pc < pc1; pc++) {
+            int a0, a1;
+            piece_share(g, tv, pc, split, nsplit, a0, a1);
+            if (a0 >= a1) continue;
             const int p = tv.piece_pat[pc];
-            const int ch0 = tv.piece_ch0[pc], ch1 = tv.piece_ch1[pc];
-            const int pat_end = p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks;
-            const uint32_t e_lo = chunk_start[blk * g.nchunks + ch0];
-            const uint32_t e_hi = ch1 < pat_end ? chunk_start[blk * g.nchunks + ch1]
-                                                : static_cast<uint32_t>(g.seg(blk, p) + g.seg_len(blk, p));
+            const int ch0 = tv.piece_ch0[pc];
+            const int pat_sub_end = (p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks) * kSubPerChunk;
+            const int j0 = ch0 * kSubPerChunk + a0 / kSubCols;
+            const int j1 = ch0 * kSubPerChunk + (a1 + kSubCols - 1) / kSubCols;
+            const uint32_t e_lo = sub_start[blk * nsub + j0];
+            const uint32_t e_hi = j1 < pat_sub_end ? sub_start[blk * nsub + j1]
+                                                   : static_cast<uint32_t>(g.seg(blk, p) + g.seg_len(blk, p));
             const uint32_t c0 = static_cast<uint32_t>(ch0 - g.chunk0[p]) * kChunkCols;
             reduce_block_entries<T, RING>(g32, e_lo, e_hi, c0, ytile, acc + tv.piece_acc[pc], recs[flip], ring);
             flip ^= 1;
@@ -815,47 +925,70 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
     }
     __syncthreads();
     T* out = partial + (tv.item_part[item] - tv.item_part[item_base]);
-    for (int i = threadIdx.x; i < width; i += kFastThreads) out[i] = acc[i];
+    for (int pc = pc0; pc < pc1; pc++) {
+        int a0, a1;
+        piece_share(g, tv, pc, split, nsplit, a0, a1);
+        const int o = tv.piece_acc[pc];
+        for (int i = a0 + threadIdx.x; i < a1; i += kFastThreads) out[o + i] = acc[o + i];
+    }
 }
 
-// A'y over a work list.  With ctr (persistent schedule: one CTA per SM) the
-// CTAs take items in order from the counter ctr[0] until the list is done,
-// so no SM idles while items of uneven duration remain; which CTA runs an
-// item does not change its output, so results stay bitwise reproducible.
-// The last CTA to finish resets the counters for the next launch (launches
-// on one work list must therefore be stream-ordered).  Without ctr, CTA i
-// runs item item_base + i.
+// A'y over a work list; a unit is one of the nsplit column splits of an
+// item.  With ctr (persistent schedule: one CTA per SM) the CTAs take units
+// in order from the counter ctr[0] until the list is done, so no SM idles
+// while units of uneven duration remain; which CTA runs a unit does not
+// change its output, so results stay bitwise reproducible.  The last CTA to
+// finish resets the counters for the next launch (launches on one work list
+// must therefore be stream-ordered).  Without ctr, CTA i runs unit i of the
+// items from item_base on.  With act (and ctr) the units are those of the
+// listed problems' items, split by a factor derived from their number.
 template <typename T, bool RING>
 __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeometry g, TView tv,
                                                                        const uint32_t* __restrict__ g32,
-                                                                       const uint32_t* __restrict__ chunk_start,
+                                                                       const uint32_t* __restrict__ sub_start,
                                                                        const T* __restrict__ y,
                                                                        T* __restrict__ partial,
                                                                        const int* __restrict__ done, int item_base,
                                                                        int64_t y_block0, int* __restrict__ ctr,
-                                                                       const int* __restrict__ pdone)
+                                                                       const int* __restrict__ pdone,
+                                                                       const FastActive* __restrict__ act, int nsplit)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // two record sets, alternating per piece: warp 0 may still combine one
     // piece's records while the other warps start on the next piece
     __shared__ WarpRec<T> recs[2][kFastThreads / 32];
     __shared__ int s_item;
+    __shared__ int pref[kMaxProblems + 1];
     if (done && *(volatile const int*)done) return;
     T* acc = reinterpret_cast<T*>(smem_raw);
     T* ytile = acc + kChunkCols * tv.per_sc;
     uint32_t* ring = reinterpret_cast<uint32_t*>(ytile + kBlockRows);  // RING schedules only
     if (!ctr) {
-        aty_item<T, RING>(g, tv, g32, chunk_start, y, partial, blockIdx.x + item_base, item_base, y_block0, acc, ytile,
-                          ring, recs, pdone);
+        const int u = static_cast<int>(blockIdx.x);
+        aty_item<T, RING>(g, tv, g32, sub_start, y, partial, u / nsplit + item_base, item_base, y_block0,
+                          u % nsplit, nsplit, acc, ytile, ring, recs, pdone);
         return;
+    }
+    int K = nsplit, units = tv.nitems * nsplit;
+    if (act) {
+        const int nit = active_prefix(act, pref, [&](int q) {
+            return tv.sc_item0[(q + 1) * tv.nsc] - tv.sc_item0[q * tv.nsc];
+        });
+        K = unit_splits(nit, gridDim.x, kAtySplitMax);
+        units = nit * K;
     }
     while (true) {
         __syncthreads();
         if (threadIdx.x == 0) s_item = atomicAdd(ctr, 1);
         __syncthreads();
-        const int item = s_item;
-        if (item >= tv.nitems) break;
-        aty_item<T, RING>(g, tv, g32, chunk_start, y, partial, item, 0, 0, acc, ytile, ring, recs, pdone);
+        const int u = s_item;
+        if (u >= units) break;
+        int item = u / K;
+        if (act) {
+            const int slot = active_slot(pref, act->n, item);
+            item = tv.sc_item0[act->list[slot] * tv.nsc] + (item - pref[slot]);
+        }
+        aty_item<T, RING>(g, tv, g32, sub_start, y, partial, item, 0, 0, u % K, K, acc, ytile, ring, recs, pdone);
     }
     if (threadIdx.x == 0) {
         __threadfence();
@@ -1116,6 +1249,8 @@ TView tview(const FastTranspose& t)
     v.piece_ch0 = t.piece_ch0;
     v.piece_ch1 = t.piece_ch1;
     v.piece_acc = t.piece_acc;
+    v.sc_item0 = t.sc_item0;
+    v.nsc = t.nsc;
     v.nitems = t.nitems;
     return v;
 }
@@ -1316,7 +1451,7 @@ void fast_free(FastLayout& f)
 {
     dfree(f.a16);
     dfree(f.g32);
-    dfree(f.chunk_start);
+    dfree(f.sub_start);
     free_transpose(f.t32);
     free_transpose(f.t64);
     free_transpose(f.tb);
@@ -1369,7 +1504,8 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
     const int64_t elems = std::max<int64_t>(g.total_elems(), 8);
     CAS_CUDA(dmalloc(&f.a16, sizeof(uint16_t) * elems));
     CAS_CUDA(dmalloc(&f.g32, sizeof(uint32_t) * elems));
-    CAS_CUDA(dmalloc(&f.chunk_start, sizeof(uint32_t) * std::max<int64_t>(g.nblocks * g.nchunks, 1)));
+    const int64_t nsub = g.nblocks * g.nchunks * kSubPerChunk;
+    CAS_CUDA(dmalloc(&f.sub_start, sizeof(uint32_t) * std::max<int64_t>(nsub, 1)));
     if (rows > 0) {
         const int threads = 256;
         const unsigned grid = fgrid(rows, threads);
@@ -1383,7 +1519,7 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
         { fast_sort_kernel<<<sgrid, kSortThreads, 0, s>>>(g, f.a16, f.g32, scratch); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         dfree(scratch);
-        { fast_chunk_kernel<<<fgrid(g.nblocks * g.nchunks, 256), 256, 0, s>>>(g, f.g32, f.chunk_start); cas::count_launch(); }
+        { fast_sub_kernel<<<fgrid(nsub, 256), 256, 0, s>>>(g, f.g32, f.sub_start); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         if (diag_int) {
             { fast_diag_kernel<<<std::min<unsigned>(static_cast<unsigned>(groups), sm_count() * 8), 256, 0, s>>>(
@@ -1392,18 +1528,19 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
         }
     }
     // entries per (block, chunk) -> work items
-    std::vector<uint32_t> cs(static_cast<size_t>(g.nblocks * g.nchunks));
-    if (!cs.empty()) {
-        CAS_CUDA(cudaMemcpyAsync(cs.data(), f.chunk_start, sizeof(uint32_t) * cs.size(), cudaMemcpyDeviceToHost, s));
+    std::vector<uint32_t> ss(static_cast<size_t>(nsub));
+    if (!ss.empty()) {
+        CAS_CUDA(cudaMemcpyAsync(ss.data(), f.sub_start, sizeof(uint32_t) * ss.size(), cudaMemcpyDeviceToHost, s));
         CAS_CUDA(cudaStreamSynchronize(s));
     }
-    std::vector<int64_t> entries(cs.size(), 0);
+    auto cs = [&](int64_t i) { return ss[static_cast<size_t>(i) * kSubPerChunk]; };  // first entry of (block, chunk) i
+    std::vector<int64_t> entries(static_cast<size_t>(g.nblocks * g.nchunks), 0);
     for (int64_t b = 0; b < g.nblocks; b++)
         for (int p = 0; p < g.npat; p++) {
             const int c_end = p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks;
             for (int ch = g.chunk0[p]; ch < c_end; ch++) {
-                const int64_t lo = cs[b * g.nchunks + ch];
-                const int64_t hi = ch + 1 < c_end ? static_cast<int64_t>(cs[b * g.nchunks + ch + 1])
+                const int64_t lo = cs(b * g.nchunks + ch);
+                const int64_t hi = ch + 1 < c_end ? static_cast<int64_t>(cs(b * g.nchunks + ch + 1))
                                                   : g.seg(b, p) + g.seg_len(b, p);
                 entries[b * g.nchunks + ch] = hi - lo;
             }
@@ -1425,16 +1562,20 @@ cas_status fast_diag(const FastLayout& f, uint64_t* diag, cudaStream_t s)
     return CAS_OK;
 }
 
+int fast_ax_splits(int64_t nblocks) { return unit_splits(nblocks, sm_count(), kAxSplitMax); }
+
 template <typename T, typename Y>
 cas_status fast_spmv(const FastLayout& f, const T* x, Y* y, const double* b, const double* coef, double* part,
-                     int* done_flag, int mode, cudaStream_t s, int* n_parts, const int* pdone)
+                     int* done_flag, int mode, cudaStream_t s, int* n_parts, const int* pdone, const FastActive* act)
 {
-    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(f.g.nblocks, sm_count())));
-    if (n_parts) *n_parts = static_cast<int>(f.g.nblocks);  // one norm partial per block
+    const int split = act ? 1 : fast_ax_splits(f.g.nblocks);
+    const int64_t units = f.g.nblocks * (act ? kAxSplitMax : split);
+    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(units, sm_count())));
+    if (n_parts) *n_parts = static_cast<int>(units);  // one norm partial per (block, split)
     if (f.g.nblocks == 0) return CAS_OK;
     const size_t smem = sizeof(T) * (sizeof(T) == 4 ? kTable32 : kTable64);
     auto launch = [&](auto kern) -> cas_status {
-        { kern<<<grid, kAxThreads, smem, s>>>(f.g, f.a16, x, y, b, coef, part, done_flag, pdone); cas::count_launch(); }
+        { kern<<<grid, kAxThreads, smem, s>>>(f.g, f.a16, x, y, b, coef, part, done_flag, pdone, act, split); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     };
@@ -1451,25 +1592,32 @@ cas_status fast_spmv(const FastLayout& f, const T* x, Y* y, const double* b, con
 }
 
 template <typename T>
-cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag, cudaStream_t s, const int* pdone)
+cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag, cudaStream_t s, const int* pdone,
+                                const FastActive* act)
 {
     const FastTranspose& t = transpose_of<T>(f);
     if (t.nitems == 0) return CAS_OK;
     const size_t smem = spmv_t_smem<T>(t.per_sc, t.ring);
-    const unsigned grid = static_cast<unsigned>(t.persistent ? std::min(t.nitems, sm_count()) : t.nitems);
-    int* ctr = t.persistent ? t.ctr : nullptr;
+    // with an active list the kernel splits the units itself (persistent);
+    // else the items are split so that a short list still fills the GPU
+    const int nsplit = act ? 1 : unit_splits(t.nitems, sm_count(), kAtySplitMax);
+    const int units = t.nitems * nsplit;
+    const bool persistent = t.persistent || act;
+    const unsigned grid = static_cast<unsigned>(persistent ? std::min(units, sm_count()) : units);
+    const unsigned pgrid = act ? static_cast<unsigned>(sm_count()) : grid;
+    int* ctr = persistent ? t.ctr : nullptr;
     if constexpr (sizeof(T) == 4) {
         if (t.ring) {
-            { fast_spmv_t_kernel<T, true><<<grid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.chunk_start, y,
-                                                                        static_cast<T*>(t.partial), done_flag, 0, 0,
-                                                                        ctr, pdone); cas::count_launch(); }
+            { fast_spmv_t_kernel<T, true><<<pgrid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.sub_start, y,
+                                                                         static_cast<T*>(t.partial), done_flag, 0, 0,
+                                                                         ctr, pdone, act, nsplit); cas::count_launch(); }
             CAS_CHECK_LAUNCH();
             return CAS_OK;
         }
     }
-    { fast_spmv_t_kernel<T, false><<<grid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.chunk_start, y,
-                                                                 static_cast<T*>(t.partial), done_flag, 0, 0,
-                                                                 ctr, pdone); cas::count_launch(); }
+    { fast_spmv_t_kernel<T, false><<<pgrid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.sub_start, y,
+                                                                  static_cast<T*>(t.partial), done_flag, 0, 0,
+                                                                  ctr, pdone, act, nsplit); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     return CAS_OK;
 }
@@ -1531,10 +1679,10 @@ cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float
     }
     const size_t smem = spmv_t_smem<float>(1, false);
     const int items = static_cast<int>(nb * f.g.nchunks);
-    { fast_spmv_t_kernel<float, false><<<items, kFastThreads, smem, s>>>(f.g, tview(f.tb), f.g32, f.chunk_start, g,
+    { fast_spmv_t_kernel<float, false><<<items, kFastThreads, smem, s>>>(f.g, tview(f.tb), f.g32, f.sub_start, g,
                                                                  f.eval_partial, nullptr,
                                                                  static_cast<int>(b0 * f.g.nchunks), b0, nullptr,
-                                                                 nullptr); cas::count_launch(); }
+                                                                 nullptr, nullptr, 1); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     { block_partial_sum_kernel<<<fgrid(f.g.cols, 256), 256, 0, s>>>(f.eval_partial, static_cast<int>(nb), f.g.cols,
                                                                   grad); cas::count_launch(); }
@@ -1543,13 +1691,16 @@ cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float
 }
 
 template cas_status fast_spmv<float, float>(const FastLayout&, const float*, float*, const double*, const double*,
-                                            double*, int*, int, cudaStream_t, int*, const int*);
+                                            double*, int*, int, cudaStream_t, int*, const int*, const FastActive*);
 template cas_status fast_spmv<double, double>(const FastLayout&, const double*, double*, const double*,
-                                              const double*, double*, int*, int, cudaStream_t, int*, const int*);
+                                              const double*, double*, int*, int, cudaStream_t, int*, const int*,
+                                              const FastActive*);
 template cas_status fast_spmv<double, float>(const FastLayout&, const double*, float*, const double*, const double*,
-                                             double*, int*, int, cudaStream_t, int*, const int*);
-template cas_status fast_spmv_t_partials<float>(const FastLayout&, const float*, int*, cudaStream_t, const int*);
-template cas_status fast_spmv_t_partials<double>(const FastLayout&, const double*, int*, cudaStream_t, const int*);
+                                             double*, int*, int, cudaStream_t, int*, const int*, const FastActive*);
+template cas_status fast_spmv_t_partials<float>(const FastLayout&, const float*, int*, cudaStream_t, const int*,
+                                                const FastActive*);
+template cas_status fast_spmv_t_partials<double>(const FastLayout&, const double*, int*, cudaStream_t, const int*,
+                                                 const FastActive*);
 template FastCols fast_cols<float>(const FastLayout&);
 template FastCols fast_cols<double>(const FastLayout&);
 template cas_status fast_spmv_t<float>(const FastLayout&, const float*, float*, cudaStream_t);

@@ -28,6 +28,10 @@ constexpr int kAxThreads = 1024;         // threads of the A x kernel
 constexpr int kAxRows = kBlockRows / kAxThreads;  // rows per thread in A x
 constexpr int kAxAhead = 3;              // index loads in flight per thread in A x
 constexpr int kChunkCols = 8192;         // column chunk of the A'y accumulators
+constexpr int kSubCols = 1024;           // column sub-chunk: the finest split of an A'y item
+constexpr int kSubPerChunk = kChunkCols / kSubCols;
+constexpr int kAxSplitMax = 32;          // most CTAs sharing one block's rows in A x
+constexpr int kAtySplitMax = 16;         // most CTAs sharing one A'y item's columns
 constexpr int kMaxFastPatterns = 32;
 constexpr int kTable32 = 57344;          // x entries staged per pattern, FP32
 constexpr int kTable64 = 28672;          // x entries staged per pattern, FP64
@@ -116,6 +120,17 @@ struct FastGeometry {
     }
 };
 
+// The problems a batched step works on (those not retired), in problem
+// order, rebuilt on the device before each iteration.  Given to the
+// products, it lets a few remaining small problems still fill the GPU: A x
+// and A'y split their work units (a block's rows, an item's columns) over
+// more CTAs the fewer units the listed problems have.
+struct FastActive {
+    int n;
+    int list[kMaxProblems];
+    int pos[kMaxProblems];  // slot of each problem in list, -1 if absent
+};
+
 // Work list of one A'y variant.  Columns are grouped into "super-chunks":
 // sets of column pieces (whole 8192-column chunks of one pattern, or a
 // pattern's last partial chunk) packed into one shared-memory accumulator of
@@ -168,7 +183,8 @@ struct FastLayout {
     int tune_cached = 0;               // schedule taken from the per-process cache
     uint16_t* a16 = nullptr;
     uint32_t* g32 = nullptr;
-    uint32_t* chunk_start = nullptr;   // [nblocks][nchunks] absolute index in G32
+    uint32_t* sub_start = nullptr;     // [nblocks][nchunks * kSubPerChunk] absolute index in G32 of the
+                                       // first entry of every column sub-chunk (a chunk starts at its first)
     FastTranspose t32, t64;            // A'y work lists of the solvers (FP32, FP64)
     FastTranspose tb;                  // one item per (block, chunk): adjoints over block ranges
     float* eval_partial = nullptr;     // [blocks][cols] partials of the last adjoint
@@ -196,21 +212,35 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
 bool fast_supported(const PatternSet& ps);
 void fast_free(FastLayout& f);
 
-// y = A x on the blocked layout; also writes per-block partials of ||y||^2
-// (part may be null; *n_parts = blocks).  mode 0: y = A x; 1: y = A x -
-// coef * y (coef read from *coef); 2: y = b - A x (b may be null: y = -A x).
-// done_flag set: nothing runs; pdone[q] set: the rows of problem q are
-// skipped (their partials are 0).
+// y = A x on the blocked layout; also writes partials of ||y||^2, one per
+// (block, row split) (part may be null; *n_parts = their number).  mode 0:
+// y = A x; 1: y = A x - coef * y (coef read from *coef); 2: y = b - A x (b
+// may be null: y = -A x).  done_flag set: nothing runs; pdone[q] set: the
+// rows of problem q are skipped (their partials are 0).
+//
+// Without act a block's rows are split over ax_splits(nblocks) CTAs and the
+// partials are laid out [block][split].  With act only the listed problems'
+// blocks run, split by a factor the kernel derives from the listed blocks,
+// and the partials are laid out [block][kAxSplitMax] (splits not used are 0):
+// problem q's partials are the 2 * kAxSplitMax * (pblk0[q+1] - pblk0[q])
+// doubles from part + 2 * kAxSplitMax * pblk0[q].
 template <typename T, typename Y>
 cas_status fast_spmv(const FastLayout& f, const T* x, Y* y, const double* b, const double* coef, double* part,
-                     int* done_flag, int mode, cudaStream_t s, int* n_parts, const int* pdone = nullptr);
+                     int* done_flag, int mode, cudaStream_t s, int* n_parts, const int* pdone = nullptr,
+                     const FastActive* act = nullptr);
+// Row splits per block of A x without an active list.
+int fast_ax_splits(int64_t nblocks);
 
 // Partials of A' y on the blocked layout (FP32: float partials, FP64:
 // double partials); columns are summed by fast_col_sum().  Items of
-// problems whose pdone flag is set are skipped.
+// problems whose pdone flag is set are skipped.  An item's columns may be
+// split over several CTAs (column sub-chunks), each writing its columns of
+// the item's partials, so the partial layout does not depend on the split.
+// With act only the listed problems' items run (one CTA per SM taking
+// units from the work counter).
 template <typename T>
 cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag, cudaStream_t s,
-                                const int* pdone = nullptr);
+                                const int* pdone = nullptr, const FastActive* act = nullptr);
 
 template <typename T>
 FastCols fast_cols(const FastLayout& f);

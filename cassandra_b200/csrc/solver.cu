@@ -900,8 +900,10 @@ struct SolverImpl {
         fast64 = fast && (mixed || !rows_layout);
         n_row_blocks = static_cast<int>(row_grid(R));
         n_vec_blocks = static_cast<int>(vec_grid(C));
-        // norm partials: one per row CTA (rows layout) or per block (blocked)
-        const int q_parts = std::max({n_row_blocks, sm_count(), fast ? static_cast<int>(fast->g.nblocks) : 0});
+        // norm partials: one per row CTA (rows layout) or per (block, row
+        // split) (blocked)
+        const int q_parts = std::max({n_row_blocks, sm_count(),
+                                      fast ? static_cast<int>(fast->g.nblocks * fast_ax_splits(fast->g.nblocks)) : 0});
         const size_t cb = sizeof(double) * std::max<int64_t>(C, 1), rb8 = sizeof(double) * std::max<int64_t>(R, 1);
         for (double** ptr : {&x, &r, &z, &p, &d, &w, &v}) CAS_CUDA(dmalloc(ptr, cb));
         if (mixed) CAS_CUDA(dmalloc(&pg32, sizeof(float) * std::max<int64_t>(C, 1)));
