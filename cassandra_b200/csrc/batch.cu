@@ -57,6 +57,8 @@ struct BDev {
     int* pskip;     // [nprob] no residual replacement due (retired problems included)
     int* nneed;     // problems with a replacement due this iteration
     int* skipall;   // 1 while no problem has a replacement due
+    int* fin;       // CTAs of the step's beta kernel that have finished (reset by the last)
+    int* nbody;     // graph replacement steps run (each due iteration adds one)
     int nprob;
 };
 
@@ -108,22 +110,29 @@ __device__ __forceinline__ int ranks_of(const ActiveList* al, int q, int G)
     return (n == 0 || a < 0) ? 0 : (G - a + n - 1) / n;
 }
 
-// Rebuilds the list of problems not retired (one warp per 32 problems).
-__global__ void bcompact_kernel(const int* __restrict__ pdone, int nprob, ActiveList* al)
+// Rebuilds the list of problems not retired (one warp per 32 problems:
+// threads 0..63 of the calling CTA; every thread of it must call).
+__device__ void compact_active(const int* __restrict__ pdone, int nprob, ActiveList* al, int* base)
 {
-    __shared__ int base[3];
-    const int t = threadIdx.x, lane = t & 31, w = t >> 5;  // 64 threads
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const bool act = t < nprob && !*(volatile const int*)(pdone + t);
-    const unsigned m = __ballot_sync(0xffffffffu, act);
-    if (lane == 0) base[w + 1] = __popc(m);
+    unsigned m = 0;
+    if (t < 64) m = __ballot_sync(0xffffffffu, act);
+    if (t < 64 && lane == 0) base[w + 1] = __popc(m);
     if (t == 0) base[0] = 0;
     __syncthreads();
-    const int before = (w == 0 ? 0 : base[1]) + __popc(m & ((1u << lane) - 1));
     if (t < nprob) {
+        const int before = (w == 0 ? 0 : base[1]) + __popc(m & ((1u << lane) - 1));
         al->pos[t] = act ? before : -1;
         if (act) al->list[before] = t;
     }
     if (t == 0) al->n = base[1] + base[2];
+}
+
+__global__ void bcompact_kernel(const int* __restrict__ pdone, int nprob, ActiveList* al)
+{
+    __shared__ int base[3];
+    compact_active(pdone, nprob, al, base);
 }
 
 // Partial (s, c) of one CTA into part[2 * (q * G + rank)].
@@ -138,8 +147,9 @@ __device__ void bwrite(double* part, const Slot& sl, Comp v, double* smem)
     }
 }
 
-// Sum of n partial pairs from part, by one block.
-template <bool COMP>
+// Sum of n partial pairs from part, by one block of THREADS threads (valid
+// in thread 0).
+template <bool COMP, int THREADS = kBRedThreads>
 __device__ double bsum(const double* part, int n, double* smem)
 {
     Comp acc;
@@ -151,8 +161,8 @@ __device__ double bsum(const double* part, int n, double* smem)
             acc.s += part[2 * i];
         }
     }
-    if (COMP) return block_sum_comp<kBRedThreads>(acc, smem).value();
-    return block_sum<kBRedThreads>(acc.s, smem);
+    if (COMP) return block_sum_comp<THREADS>(acc, smem).value();
+    return block_sum<THREADS>(acc.s, smem);
 }
 
 // ||A'q||^2 per listed problem from the product partials (T = partial type).
@@ -245,50 +255,47 @@ __global__ void __launch_bounds__(kBVecThreads) brestart_kernel(int64_t P, const
     }
 }
 
-// alpha = rz / p'A'Ap per problem; p'A'Ap = sum of the A p norm partials of
-// the problem's blocks.
-template <bool COMP>
-__global__ void __launch_bounds__(kBRedThreads) balpha_kernel(FastGeometry g, const double* __restrict__ part_q, BDev d)
-{
-    __shared__ double smem[64];
-    const int q = blockIdx.x;
-    if (retired(d, q)) return;
-    // the A p norm partials of the problem's blocks, kAxSplitMax per block
-    const int b0 = g.pblk0[q], nb = g.pblk0[q + 1] - g.pblk0[q];
-    const double pap = bsum<COMP>(part_q + 2 * static_cast<int64_t>(b0) * kAxSplitMax, nb * kAxSplitMax, smem);
-    if (threadIdx.x == 0) {
-        double* sc = d.scal + q * kBSlots;
-        sc[bPap] = pap;
-        const double rz = sc[bRz];
-        if (!(pap > 0) || !isfinite(pap)) {
-            // not finite: breakdown.  <= 0: p lies in the null space of A (a
-            // rank-deficient problem, or the residual at rounding level);
-            // the problem retires and the FP64 true residual decides
-            // between converged and a restart from it.
-            sc[bAlpha] = 0;
-            if (!isfinite(pap)) d.flags[q * kBFlags + bStatus] = CAS_ERR_BREAKDOWN;
-            retire(d, q);
-        } else {
-            sc[bAlpha] = rz / pap;
-        }
-    }
-}
-
-// x += alpha p; r -= alpha A'A p; z = D r; partials of r.z, r.r.
+// alpha = rz / p'A'Ap per problem, then x += alpha p; r -= alpha A'A p;
+// z = D r; partials of r.z, r.r.  p'A'Ap is the sum of the A p norm
+// partials of the problem's blocks (kAxSplitMax per block), summed by every
+// CTA of the problem in the same order, so all of them get the same alpha;
+// the problem's first CTA stores it.  p'A'Ap <= 0 means p lies in the null
+// space of A (a rank-deficient problem, or the residual at rounding level):
+// the problem retires and the FP64 true residual decides between converged
+// and a restart from it; a non-finite p'A'Ap is a breakdown.
 template <bool COMP, typename T>
 __global__ void __launch_bounds__(kBVecThreads) bupdate_kernel(FastCols fc, const T* __restrict__ partial,
                                                                double* __restrict__ x, double* __restrict__ r,
                                                                double* __restrict__ z, const double* __restrict__ p,
                                                                const double* __restrict__ dinv,
                                                                const ActiveList* al,
+                                                               const double* __restrict__ part_q,
                                                                double* __restrict__ part_rz,
                                                                double* __restrict__ part_rr, BDev d)
 {
     __shared__ double smem[64];
+    __shared__ double s_pap;
     Slot sl;
     if (!cta_slot(al, sl) || retired(d, sl.q)) return;
     const int q = sl.q;
-    const double alpha = d.scal[q * kBSlots + bAlpha];
+    const int b0 = fc.g.pblk0[q], nb = fc.g.pblk0[q + 1] - fc.g.pblk0[q];
+    const double pap_sum = bsum<COMP, kBVecThreads>(part_q + 2 * static_cast<int64_t>(b0) * kAxSplitMax,
+                                                    nb * kAxSplitMax, smem);
+    if (threadIdx.x == 0) s_pap = pap_sum;
+    __syncthreads();
+    const double pap = s_pap;
+    double* sc = d.scal + q * kBSlots;
+    const bool ok = pap > 0 && isfinite(pap);
+    if (sl.rank == 0 && threadIdx.x == 0) {
+        sc[bPap] = pap;
+        sc[bAlpha] = ok ? sc[bRz] / pap : 0.0;
+        if (!ok) {
+            if (!isfinite(pap)) d.flags[q * kBFlags + bStatus] = CAS_ERR_BREAKDOWN;
+            retire(d, q);
+        }
+    }
+    if (!ok) return;
+    const double alpha = sc[bRz] / pap;
     const int64_t P = fc.g.pcols, base = q * P;
     Comp rz, rr;
     for (int64_t c = static_cast<int64_t>(sl.rank) * blockDim.x + threadIdx.x; c < P;
@@ -309,64 +316,89 @@ __global__ void __launch_bounds__(kBVecThreads) bupdate_kernel(FastCols fc, cons
 
 // rz_new, rr -> beta, relative residual, retirement.  replace != 0: residual
 // replacement (r.z replaced, beta and the iteration count left alone).
+//
+// With next (the step's beta kernel), the last CTA to finish also prepares
+// the next steps: the whole-launch gate of this iteration's replacement
+// step (skipall, set while no problem has one due; the count of due
+// problems reset), with use_cond the condition of the replacement step's
+// graph node and the count of such steps run (nbody), and the list of
+// problems still active for the next iteration.
 template <bool COMP>
 __global__ void __launch_bounds__(kBRedThreads) bbeta_kernel(const double* __restrict__ part_rz,
                                                              const double* __restrict__ part_rr, int G,
                                                              const ActiveList* al, BDev d, int replace,
                                                              const double* __restrict__ part_dev,
-                                                             const int* __restrict__ qgate, int plan_refine)
+                                                             const int* __restrict__ qgate, int plan_refine,
+                                                             ActiveList* next, int use_cond,
+                                                             cudaGraphConditionalHandle cond)
 {
     __shared__ double smem[64];
+    __shared__ int s_last;
+    __shared__ int base[3];
     const int q = blockIdx.x;
-    if (*(volatile const int*)(qgate + q)) return;
     const int k = ranks_of(al, q, G);
-    if (k == 0) return;
-    const int64_t o = 2 * static_cast<int64_t>(q) * G;
-    const double rz_new = bsum<COMP>(part_rz + o, k, smem);
-    const double rr = bsum<COMP>(part_rr + o, k, smem);
-    const double dev2 = part_dev ? bsum<COMP>(part_dev + o, k, smem) : 0.0;
-    if (threadIdx.x == 0) {
-        double* sc = d.scal + q * kBSlots;
-        int* fl = d.flags + q * kBFlags;
-        if (part_dev) fl[bRestart] = dev2 > kBRestartDeviation * kBRestartDeviation * rr ? 1 : 0;
-        const double rz = sc[bRz];
-        const double bn2 = sc[bBn2];
-        const double res = bn2 > 0 ? sqrt(rr / bn2) : sqrt(rr);
-        if (!replace) {
-            sc[bBeta] = rz != 0 ? rz_new / rz : 0.0;
-            fl[bIter] += 1;
-        } else {
-            fl[bRefine] += 1;
-        }
-        sc[bRz] = rz_new;
-        sc[bRr] = rr;
-        sc[bRes] = res;
-        if (replace) {
-            sc[bRrRef] = rr;
-            fl[bIterRef] = fl[bIter];
-        }
-        const bool met = rr == 0 || (sc[bTol] > 0 && res <= sc[bTol]);
-        if (!isfinite(rz_new) || !isfinite(rr)) {
-            fl[bStatus] = CAS_ERR_BREAKDOWN;
-            retire(d, q);
-        } else if (!replace && plan_refine > 0) {
-            fl[bRestart] = 0;
-            const bool due = met || rr <= kBReplaceDrop * kBReplaceDrop * sc[bRrRef] ||
-                             fl[bIter] - fl[bIterRef] >= plan_refine;
-            d.pskip[q] = due ? 0 : 1;
-            if (due) atomicAdd(d.nneed, 1);
-        } else if (met) {
-            retire(d, q);
+    if (!*(volatile const int*)(qgate + q) && k != 0) {
+        const int64_t o = 2 * static_cast<int64_t>(q) * G;
+        const double rz_new = bsum<COMP>(part_rz + o, k, smem);
+        const double rr = bsum<COMP>(part_rr + o, k, smem);
+        const double dev2 = part_dev ? bsum<COMP>(part_dev + o, k, smem) : 0.0;
+        if (threadIdx.x == 0) {
+            double* sc = d.scal + q * kBSlots;
+            int* fl = d.flags + q * kBFlags;
+            if (part_dev) fl[bRestart] = dev2 > kBRestartDeviation * kBRestartDeviation * rr ? 1 : 0;
+            const double rz = sc[bRz];
+            const double bn2 = sc[bBn2];
+            const double res = bn2 > 0 ? sqrt(rr / bn2) : sqrt(rr);
+            if (!replace) {
+                sc[bBeta] = rz != 0 ? rz_new / rz : 0.0;
+                fl[bIter] += 1;
+            } else {
+                fl[bRefine] += 1;
+            }
+            sc[bRz] = rz_new;
+            sc[bRr] = rr;
+            sc[bRes] = res;
+            if (replace) {
+                sc[bRrRef] = rr;
+                fl[bIterRef] = fl[bIter];
+            }
+            const bool met = rr == 0 || (sc[bTol] > 0 && res <= sc[bTol]);
+            if (!isfinite(rz_new) || !isfinite(rr)) {
+                fl[bStatus] = CAS_ERR_BREAKDOWN;
+                retire(d, q);
+            } else if (!replace && plan_refine > 0) {
+                fl[bRestart] = 0;
+                const bool due = met || rr <= kBReplaceDrop * kBReplaceDrop * sc[bRrRef] ||
+                                 fl[bIter] - fl[bIterRef] >= plan_refine;
+                d.pskip[q] = due ? 0 : 1;
+                if (due) atomicAdd(d.nneed, 1);
+            } else if (met) {
+                retire(d, q);
+            }
         }
     }
-}
-
-// Whole-launch gate of this iteration's replacement step: set while no
-// problem has one due; resets the count for the next iteration.
-__global__ void bgate_kernel(BDev d)
-{
-    *d.skipall = (*d.alldone || *d.nneed == 0) ? 1 : 0;
-    *d.nneed = 0;
+    if (!next) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();  // this CTA's flags before its count
+        s_last = atomicAdd(d.fin, 1) == static_cast<int>(gridDim.x) - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        *d.fin = 0;
+        if (plan_refine > 0) {
+            const int skip = (*(volatile int*)d.alldone || atomicAdd(d.nneed, 0) == 0) ? 1 : 0;
+            *d.skipall = skip;
+            *d.nneed = 0;
+            if (use_cond) {
+                cudaGraphSetConditional(cond, skip ? 0u : 1u);
+                if (!skip) *d.nbody += 1;
+            }
+        }
+    }
+    compact_active(d.pdone, d.nprob, next, base);
 }
 
 // p = z + beta p (and the gather copy).
@@ -419,7 +451,7 @@ struct BatchSolver {
     const double* b = nullptr;
     double *part_q = nullptr, *part_a = nullptr, *part_b = nullptr, *part_c = nullptr;
     double* scal = nullptr;
-    int* flags = nullptr;  // [B][kBFlags] then pdone[B], ndone, alldone, pskip[B], nneed, skipall
+    int* flags = nullptr;  // [B][kBFlags] then pdone[B], ndone, alldone, pskip[B], nneed, skipall, fin, nbody
     ActiveList* act = nullptr;  // problems not retired (rebuilt every iteration)
     ActiveList* all = nullptr;  // every problem
     std::vector<double> h_scal;
@@ -427,6 +459,9 @@ struct BatchSolver {
     cudaGraphExec_t graph = nullptr;
     int graph_len = 0, graph_phase = -1;
     long long graph_kernels = 0;
+    cudaStream_t s2 = nullptr;     // captures the bodies of the replacement steps' graph nodes
+    long long body_kernels = 0;    // kernels of one replacement step
+    int nbody_seen = 0;            // replacement steps already counted
     int launched = 0;
 
     BDev dev() const
@@ -440,10 +475,13 @@ struct BatchSolver {
         d.pskip = d.alldone + 1;
         d.nneed = d.pskip + B;
         d.skipall = d.nneed + 1;
+        d.fin = d.skipall + 1;
+        d.nbody = d.fin + 1;
         d.nprob = B;
         return d;
     }
-    int nflags() const { return B * kBFlags + B + 2 + B + 2; }
+    int nflags() const { return B * kBFlags + B + 2 + B + 2 + 2; }
+    int nbody_index() const { return nflags() - 1; }
     dim3 vgrid() const { return dim3(static_cast<unsigned>(G)); }
 
     ~BatchSolver()
@@ -453,6 +491,7 @@ struct BatchSolver {
             cudaStreamSynchronize(s);
             cudaStreamDestroy(s);
         }
+        if (s2) cudaStreamDestroy(s2);
         for (void* ptr : {(void*)x, (void*)r, (void*)z, (void*)p, (void*)dinv, (void*)pg32, q, (void*)q64,
                           (void*)part_q, (void*)part_a, (void*)part_b, (void*)part_c, (void*)scal,
                           (void*)flags, (void*)act, (void*)all})
@@ -502,7 +541,7 @@ struct BatchSolver {
             { bresidual_kernel<COMP, double><<<vgrid(), kBVecThreads, 0, s>>>(fc, t64, r, z, p, nullptr, dinv, al,
                                                                          part_a, part_b, restart ? 1 : 0, d, pdev,
                                                                          qgate); cas::count_launch(); }
-        { bbeta_kernel<COMP><<<B, kBRedThreads, 0, s>>>(part_a, part_b, G, al, d, 1, pdev, qgate, 0); cas::count_launch(); }
+        { bbeta_kernel<COMP><<<B, kBRedThreads, 0, s>>>(part_a, part_b, G, al, d, 1, pdev, qgate, 0, nullptr, 0, 0); cas::count_launch(); }
         if (pdev) {
             if (mixed)
                 { brestart_kernel<float><<<vgrid(), kBVecThreads, 0, s>>>(P, al, z, p, pg32, d); cas::count_launch(); }
@@ -513,23 +552,26 @@ struct BatchSolver {
         return CAS_OK;
     }
 
+    // One iteration.  The active list was rebuilt by the previous
+    // iteration's beta kernel (or by the set-up / resumption); a problem
+    // retired since then is still listed and skipped by every kernel.  The
+    // beta kernel plans this iteration's replacement step and, with
+    // use_cond, sets the condition of its graph node.
     template <bool COMP, typename T>
-    cas_status iteration()
+    cas_status iteration(int use_cond, cudaGraphConditionalHandle cond)
     {
         const BDev d = dev();
         const T* pgather = std::is_same<T, float>::value ? reinterpret_cast<const T*>(pg32) : reinterpret_cast<const T*>(p);
-        { bcompact_kernel<<<1, 64, 0, s>>>(d.pdone, B, act); cas::count_launch(); }
         CAS_TRY((fast_spmv<T, T>(*f, pgather, static_cast<T*>(q), nullptr, nullptr, part_q, d.alldone, 0, s, nullptr,
                                  d.pdone, act)));
         CAS_TRY(fast_spmv_t_partials<T>(*f, static_cast<const T*>(q), d.alldone, s, d.pdone, act));
-        { balpha_kernel<COMP><<<B, kBRedThreads, 0, s>>>(f->g, part_q, d); cas::count_launch(); }
         const FastCols fc = fast_cols<T>(*f);
         { bupdate_kernel<COMP, T><<<vgrid(), kBVecThreads, 0, s>>>(fc, static_cast<const T*>(sizeof(T) == 4 ? f->t32.partial
                                                                                                         : f->t64.partial),
-                                                                  x, r, z, p, dinv, act, part_a, part_b, d); cas::count_launch(); }
+                                                                  x, r, z, p, dinv, act, part_q, part_a, part_b, d); cas::count_launch(); }
         { bbeta_kernel<COMP><<<B, kBRedThreads, 0, s>>>(part_a, part_b, G, act, d, 0, nullptr, d.pdone,
-                                                       mixed ? std::max(o.refine_every, 1) : 0); cas::count_launch(); }
-        if (mixed) { bgate_kernel<<<1, 1, 0, s>>>(d); cas::count_launch(); }
+                                                       mixed ? std::max(o.refine_every, 1) : 0, act, use_cond,
+                                                       cond); cas::count_launch(); }
         if (mixed)
             { bdirection_kernel<float><<<vgrid(), kBVecThreads, 0, s>>>(P, act, z, p, pg32, d); cas::count_launch(); }
         else
@@ -538,18 +580,62 @@ struct BatchSolver {
         return CAS_OK;
     }
 
-    cas_status issue_iteration(int global_index)
+    // The mixed solver's replacement step of an iteration being captured:
+    // a conditional graph node whose body (captured on s2) runs only when
+    // the beta kernel found a replacement due.  Kernels of the body are
+    // counted when they run (nbody).
+    cas_status capture_replacement(cudaGraphConditionalHandle h)
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        CAS_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeIf;
+        np.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        CAS_CUDA(cudaGraphAddNode(&node, cg, deps, nd, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        CAS_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+        CAS_CUDA(cudaStreamBeginCaptureToGraph(s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        std::swap(s, s2);
+        const long long before = launch_count();
+        const cas_status st = refine<true>(Sel::Due);
+        body_kernels = launch_count() - before;
+        count_launch(-body_kernels);  // counted when the body runs
+        std::swap(s, s2);
+        cudaGraph_t out = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s2, &out);
+        CAS_TRY(st);
+        CAS_CUDA(e);
+        return CAS_OK;
+    }
+
+    cas_status issue_iteration(bool capturing)
     {
         if (mixed) {
-            CAS_TRY((iteration<true, float>()));
-            CAS_TRY(refine<true>(Sel::Due));  // runs only for problems the beta kernel scheduled
+            if (capturing) {
+                cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+                cudaGraph_t cg = nullptr;
+                CAS_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, nullptr, nullptr));
+                cudaGraphConditionalHandle h = 0;
+                CAS_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
+                CAS_TRY((iteration<true, float>(1, h)));
+                CAS_TRY(capture_replacement(h));
+            } else {
+                CAS_TRY((iteration<true, float>(0, 0)));
+                CAS_TRY(refine<true>(Sel::Due));  // runs only for problems the beta kernel scheduled
+            }
         } else {
-            CAS_TRY((iteration<false, double>()));
+            CAS_TRY((iteration<false, double>(0, 0)));
         }
         return CAS_OK;
     }
 
-    cas_status issue_chunk(int first, int n)
+    cas_status issue_chunk(int n)
     {
         const int phase = 0;  // every iteration is the same graph segment
         if (n > 1) {
@@ -562,7 +648,7 @@ struct BatchSolver {
                 CAS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
                 cas_status st = CAS_OK;
                 const long long before = launch_count();
-                for (int i = 0; i < n && st == CAS_OK; i++) st = issue_iteration(first + i);
+                for (int i = 0; i < n && st == CAS_OK; i++) st = issue_iteration(true);
                 graph_kernels = launch_count() - before;
                 count_launch(-graph_kernels);  // captured, not launched
                 cudaError_t e = cudaStreamEndCapture(s, &g);
@@ -580,7 +666,7 @@ struct BatchSolver {
             CAS_CUDA(cudaGraphLaunch(graph, s));
             count_launch(graph_kernels);
         } else {
-            for (int i = 0; i < n; i++) CAS_TRY(issue_iteration(first + i));
+            for (int i = 0; i < n; i++) CAS_TRY(issue_iteration(false));
         }
         launched += n;
         return CAS_OK;
@@ -591,6 +677,9 @@ struct BatchSolver {
         CAS_CUDA(cudaMemcpyAsync(h_scal.data(), scal, sizeof(double) * h_scal.size(), cudaMemcpyDeviceToHost, s));
         CAS_CUDA(cudaMemcpyAsync(h_flags.data(), flags, sizeof(int) * h_flags.size(), cudaMemcpyDeviceToHost, s));
         CAS_CUDA(cudaStreamSynchronize(s));
+        const int nb = h_flags[nbody_index()];
+        if (nb > nbody_seen) count_launch(static_cast<long long>(nb - nbody_seen) * body_kernels);
+        nbody_seen = nb;
         return CAS_OK;
     }
 
@@ -628,6 +717,7 @@ struct BatchSolver {
             CAS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
             own_stream = true;
         }
+        if (mixed) CAS_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
         const size_t cb = sizeof(double) * std::max<int64_t>(C, 1), rb = sizeof(double) * std::max<int64_t>(R, 1);
         for (double** ptr : {&x, &r, &z, &p, &dinv}) CAS_CUDA(dmalloc(ptr, cb));
         if (mixed) CAS_CUDA(dmalloc(&pg32, sizeof(float) * std::max<int64_t>(C, 1)));
@@ -738,7 +828,7 @@ struct BatchSolver {
                 continue;
             }
             const int n = std::min(chunk, o.max_iterations - launched);
-            CAS_TRY(issue_chunk(launched, n));
+            CAS_TRY(issue_chunk(n));
         }
         if (!verified && st == CAS_OK) CAS_TRY(true_residuals());
         CAS_CUDA(cudaEventRecord(e1, s));

@@ -430,11 +430,13 @@ __device__ __forceinline__ int active_slot(const int* pref, int n, int i)
 }
 
 // Splits of a work unit when `units` units of a product are to fill `ctas`
-// CTAs: about two units per CTA, at most cap.
+// CTAs: as many as keep every split unit in one wave, at most cap.  A few
+// units' time is set by their chains of dependent loads, not by their
+// bytes, so one wave of larger units beats two of smaller ones.
 __host__ __device__ __forceinline__ int unit_splits(int64_t units, int64_t ctas, int cap)
 {
     if (units <= 0) return 1;
-    const int64_t k = (2 * ctas + units - 1) / units;
+    const int64_t k = ctas / units;
     return static_cast<int>(k < 1 ? 1 : (k > cap ? cap : k));
 }
 
@@ -447,7 +449,9 @@ __host__ __device__ __forceinline__ int unit_splits(int64_t units, int64_t ctas,
 // Blocks of problems whose pdone flag is set are skipped (partials 0).
 // Without act: units (block, split) for every block, `split` splits each,
 // partials [block][split].  With act: the listed problems' blocks only,
-// partials [block][kAxSplitMax] (splits past the one in use written 0).
+// split for `ctas` CTAs, partials [block][kAxSplitMax] (splits past the one
+// in use written 0); a split of kAxSplitMax is left to
+// fast_spmv_direct_kernel.
 template <typename T, typename Y, int MODE, bool ALL8>
 __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g, const uint16_t* __restrict__ a16,
                                                                    const T* __restrict__ x, Y* __restrict__ y,
@@ -456,7 +460,8 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
                                                                    double* __restrict__ part,
                                                                    const int* __restrict__ done,
                                                                    const int* __restrict__ pdone,
-                                                                   const FastActive* __restrict__ act, int split)
+                                                                   const FastActive* __restrict__ act, int split,
+                                                                   int ctas)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* table = reinterpret_cast<T*>(smem_raw);
@@ -470,10 +475,11 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
     int64_t units = g.nblocks * split;
     if (act) {
         const int nblk = active_prefix(act, pref, [&](int q) { return g.pblk0[q + 1] - g.pblk0[q]; });
-        S = unit_splits(nblk, gridDim.x, kAxSplitMax);
+        S = unit_splits(nblk, ctas, kAxSplitMax);
         stride = kAxSplitMax;
         units = static_cast<int64_t>(nblk) * S;
     }
+    if (act && S == kAxSplitMax) return;  // few rows per unit: fast_spmv_direct_kernel's launch
     for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
         const int sp = static_cast<int>(u % S);
         int64_t blk = u / S;
@@ -541,6 +547,107 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
             if (threadIdx.x == 0) {
                 pu[0] = r.s;
                 pu[1] = r.c;
+            }
+        }
+    }
+}
+
+constexpr int kDirectPatterns = 8;  // most 8-slot patterns of the direct A x's unrolled path
+
+// A x over units of at most kAxDirectRows rows (a block split kAxSplitMax
+// ways) without staging x: one thread per row gathers its entries through
+// L1/L2 in pattern and slot order, the order of the staged kernel, so both
+// give the same values.  Few remaining rows (the last small problems of a
+// batch, a small fit) are not worth staging every x slice per CTA.  Without
+// act it runs when the host chose kAxSplitMax splits; with act it decides on
+// the device, as the staged kernel (launched beside it) does with the same
+// `ctas`, and exactly one of the two does the work.  Partials as the staged
+// kernel's with stride kAxSplitMax.
+template <typename T, typename Y, int MODE, bool ALL8>
+__global__ void __launch_bounds__(kAxDirectRows) fast_spmv_direct_kernel(FastGeometry g,
+                                                                         const uint16_t* __restrict__ a16,
+                                                                         const T* __restrict__ x, Y* __restrict__ y,
+                                                                         const double* __restrict__ b,
+                                                                         const double* __restrict__ coef,
+                                                                         double* __restrict__ part,
+                                                                         const int* __restrict__ done,
+                                                                         const int* __restrict__ pdone,
+                                                                         const FastActive* __restrict__ act, int ctas)
+{
+    __shared__ double red[64];
+    __shared__ int pref[kMaxProblems + 1];
+    if (done && *(volatile const int*)done) return;
+    using Acc = typename AccOf<T>::type;
+    const double c = MODE == 1 ? *coef : 0.0;
+    int64_t nblk = g.nblocks;
+    if (act) {
+        nblk = active_prefix(act, pref, [&](int q) { return g.pblk0[q + 1] - g.pblk0[q]; });
+        if (unit_splits(nblk, ctas, kAxSplitMax) != kAxSplitMax) return;  // the staged kernel's work
+    }
+    const int64_t units = nblk * kAxSplitMax;
+    for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+        const int sp = static_cast<int>(u % kAxSplitMax);
+        int64_t blk = u / kAxSplitMax;
+        if (act) {
+            const int i = static_cast<int>(blk);
+            const int slot = active_slot(pref, act->n, i);
+            blk = g.pblk0[act->list[slot]] + (i - pref[slot]);
+        }
+        const int q = g.prob_of_block(blk);
+        double* pu = part ? part + 2 * (blk * kAxSplitMax + sp) : nullptr;
+        if (pdone && pdone[q]) {
+            if (pu && threadIdx.x == 0) {
+                pu[0] = 0;
+                pu[1] = 0;
+            }
+            continue;
+        }
+        const int rows_b = static_cast<int>(g.block_rows(blk));
+        const int r0 = static_cast<int>(static_cast<int64_t>(rows_b) * sp / kAxSplitMax);
+        const int nb = static_cast<int>(static_cast<int64_t>(rows_b) * (sp + 1) / kAxSplitMax) - r0;
+        const T* xq = x + q * g.pcols;
+        Comp mine;
+        const int r = threadIdx.x;
+        if (r < nb) {
+            Acc acc = 0;
+            if (ALL8) {
+                // up to kDirectPatterns patterns of 8 slots: every index word
+                // first, then all gathers, so that they are in flight together
+                uint4 w[kDirectPatterns];
+#pragma unroll
+                for (int p = 0; p < kDirectPatterns; p++)
+                    if (p < g.npat)
+                        w[p] = *reinterpret_cast<const uint4*>(a16 + g.seg(blk, p) + static_cast<int64_t>(r0 + r) * 8);
+#pragma unroll
+                for (int p = 0; p < kDirectPatterns; p++) {
+                    if (p < g.npat) {
+                        const T* xg = xq + g.off[p];
+                        gather_word<T, true>(w[p].x, xg, xg, 0, acc);
+                        gather_word<T, true>(w[p].y, xg, xg, 0, acc);
+                        gather_word<T, true>(w[p].z, xg, xg, 0, acc);
+                        gather_word<T, true>(w[p].w, xg, xg, 0, acc);
+                    }
+                }
+            } else {
+                for (int p = 0; p < g.npat; p++) {
+                    const int ns = g.slots[p];
+                    gather_row<T>(a16 + g.seg(blk, p) + static_cast<int64_t>(r0 + r) * ns, ns, xq, xq + g.off[p], 0,
+                                  false, acc);
+                }
+            }
+            const int64_t row = g.block_row0(blk) + r0 + r;
+            double v = static_cast<double>(acc);
+            if (MODE == 1) v = static_cast<double>(y[row]) * -c + v;
+            if (MODE == 2) v = (b ? b[row] : 0.0) - v;
+            const Y yv = static_cast<Y>(v);
+            y[row] = yv;
+            mine.add(static_cast<double>(yv) * static_cast<double>(yv));
+        }
+        if (pu) {
+            const Comp rs = block_sum_comp<kAxDirectRows>(mine, red);
+            if (threadIdx.x == 0) {
+                pu[0] = rs.s;
+                pu[1] = rs.c;
             }
         }
     }
@@ -897,10 +1004,22 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
         __syncthreads();
         const T* yb = y + (g.block_row0(blk) - g.block_row0(y_block0));
         if ((reinterpret_cast<uintptr_t>(yb) & 15) == 0) {
+            // 16-byte loads, kInFlight per thread issued before their stores
+            // (FP32: the whole tile in two rounds; FP64 keeps its registers)
             constexpr int kPer = 16 / sizeof(T);
+            constexpr int kInFlight = sizeof(T) == 4 ? 2 : 1;
             const int nvec = nb / kPer;
-            for (int i = threadIdx.x; i < nvec; i += kFastThreads)
-                reinterpret_cast<uint4*>(ytile)[i] = __ldg(reinterpret_cast<const uint4*>(yb) + i);
+            const uint4* src = reinterpret_cast<const uint4*>(yb);
+            uint4* dst = reinterpret_cast<uint4*>(ytile);
+            for (int i0 = threadIdx.x; i0 < nvec; i0 += kInFlight * kFastThreads) {
+                uint4 u[kInFlight];
+#pragma unroll
+                for (int k = 0; k < kInFlight; k++)
+                    if (i0 + k * kFastThreads < nvec) u[k] = __ldg(src + i0 + k * kFastThreads);
+#pragma unroll
+                for (int k = 0; k < kInFlight; k++)
+                    if (i0 + k * kFastThreads < nvec) dst[i0 + k * kFastThreads] = u[k];
+            }
             for (int i = nvec * kPer + threadIdx.x; i < nb; i += kFastThreads) ytile[i] = yb[i];
         } else {
             for (int i = threadIdx.x; i < nb; i += kFastThreads) ytile[i] = yb[i];
@@ -1570,17 +1689,33 @@ cas_status fast_spmv(const FastLayout& f, const T* x, Y* y, const double* b, con
 {
     const int split = act ? 1 : fast_ax_splits(f.g.nblocks);
     const int64_t units = f.g.nblocks * (act ? kAxSplitMax : split);
-    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(units, sm_count())));
+    const int ctas = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(units, sm_count())));
     if (n_parts) *n_parts = static_cast<int>(units);  // one norm partial per (block, split)
     if (f.g.nblocks == 0) return CAS_OK;
     const size_t smem = sizeof(T) * (sizeof(T) == 4 ? kTable32 : kTable64);
+    const bool direct = act || split == kAxSplitMax;
+    const bool staged = act || split != kAxSplitMax;
     auto launch = [&](auto kern) -> cas_status {
-        { kern<<<grid, kAxThreads, smem, s>>>(f.g, f.a16, x, y, b, coef, part, done_flag, pdone, act, split); cas::count_launch(); }
+        { kern<<<ctas, kAxThreads, smem, s>>>(f.g, f.a16, x, y, b, coef, part, done_flag, pdone, act, split, ctas); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     };
     bool all8 = true;
     for (int p = 0; p < f.g.npat; p++) all8 = all8 && f.g.slots[p] == 8;
+    if (direct) {
+        const unsigned dgrid = static_cast<unsigned>(
+            std::max<int64_t>(1, std::min<int64_t>(f.g.nblocks * kAxSplitMax, 4LL * sm_count())));
+        const bool d8 = all8 && f.g.npat <= kDirectPatterns;
+        auto kd = d8 ? (mode == 0 ? fast_spmv_direct_kernel<T, Y, 0, true>
+                                  : (mode == 1 ? fast_spmv_direct_kernel<T, Y, 1, true>
+                                               : fast_spmv_direct_kernel<T, Y, 2, true>))
+                     : (mode == 0 ? fast_spmv_direct_kernel<T, Y, 0, false>
+                                  : (mode == 1 ? fast_spmv_direct_kernel<T, Y, 1, false>
+                                               : fast_spmv_direct_kernel<T, Y, 2, false>));
+        { kd<<<dgrid, kAxDirectRows, 0, s>>>(f.g, f.a16, x, y, b, coef, part, done_flag, pdone, act, ctas); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+    }
+    if (!staged) return CAS_OK;
     if (all8) {
         if (mode == 0) return launch(fast_spmv_kernel<T, Y, 0, true>);
         if (mode == 1) return launch(fast_spmv_kernel<T, Y, 1, true>);

@@ -31,6 +31,8 @@ constexpr int kChunkCols = 8192;         // column chunk of the A'y accumulators
 constexpr int kSubCols = 1024;           // column sub-chunk: the finest split of an A'y item
 constexpr int kSubPerChunk = kChunkCols / kSubCols;
 constexpr int kAxSplitMax = 32;          // most CTAs sharing one block's rows in A x
+constexpr int kAxDirectRows = kAxThreads / 2;  // rows of a unit that gathers x without staging (one thread a row)
+static_assert(kBlockRows / kAxSplitMax <= kAxDirectRows, "a block split kAxSplitMax ways must fit the direct path");
 constexpr int kAtySplitMax = 16;         // most CTAs sharing one A'y item's columns
 constexpr int kMaxFastPatterns = 32;
 constexpr int kTable32 = 57344;          // x entries staged per pattern, FP32
