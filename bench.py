@@ -38,6 +38,18 @@ sys.path.insert(0, str(ROOT))
 METRIC = "time to rel. residual 1e-8: mixed/batched vs plain FP64 GPU; SpMV HBM GB/s"
 PATTERNS_8 = [0x42FF, 0x070707, 0x1F1F, 0x8040201008040201, 0xFF00, 0xFF0000, 0xFF000000, 0x0080402010080402]
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) per entry of the blocked FP32 products, measured
+# with ncu (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on a
+# 2M-row launch of the same kernels, 128M entries; traffic grows with the
+# entries, so a full launch's traffic is this times its entries.
+NCU_DRAM_BYTES_PER_ENTRY = {"aty_f32": (520.24e6 + 6.68e6) / 128e6, "ax_f32": (256.89e6 + 7.29e6) / 128e6}
+
+
+def ncu_traffic(kernel: str, entries: int):
+    for suffix, per in NCU_DRAM_BYTES_PER_ENTRY.items():
+        if kernel.endswith(suffix):
+            return per * entries
+    return None
 
 
 def parse_args(argv=None):
@@ -310,7 +322,8 @@ def run_ours(args) -> dict | None:
             "solve_speedup_mixed_vs_plain": plain.seconds / mixed.seconds if mixed.seconds else None,
         },
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
-                     "frac": ach / peak, "peak_kind": peak_kind, "traffic": None},
+                     "frac": ach / peak, "peak_kind": peak_kind, "traffic": ncu_traffic(dom, nnz),
+                     "traffic_unit": "bytes per launch, scaled from ncu at 2M rows"},
         "kernels": kernels,
         "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": int(pos_h.numel() * 8 + sc_h.numel() * 4),
                 "d2h_bytes_per_step": int(w_h.numel() * 4), "steps": e2e_steps},
@@ -499,7 +512,8 @@ def run_ours_batched(args) -> dict | None:
                                       for n, e, r in zip(rows, empties, last)]},
         "plain_fp64": plain,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
-                     "frac": ach / peak, "peak_kind": peak_kind, "traffic": None},
+                     "frac": ach / peak, "peak_kind": peak_kind, "traffic": ncu_traffic(dom, nnz),
+                     "traffic_unit": "bytes per launch, scaled from ncu at 2M rows"},
         "kernels": kernels, "aty_schedules": schedules,
         "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": int(pos_h.numel() * 8 + sc_h.numel() * 4),
                 "d2h_bytes_per_step": int(w_h.numel() * 4), "steps": e2e_steps},

@@ -235,6 +235,26 @@ __global__ void fast_sub_kernel(FastGeometry g, const uint32_t* __restrict__ g32
     }
 }
 
+// Entries of every (block, chunk): the distance between the chunk's first
+// sub-chunk start and the next chunk's (or the group's end).
+__global__ void fast_chunk_entries_kernel(FastGeometry g, const uint32_t* __restrict__ sub_start,
+                                          uint32_t* __restrict__ out)
+{
+    const int64_t total = g.nblocks * g.nchunks;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = i / g.nchunks;
+        const int ch = static_cast<int>(i - b * g.nchunks);
+        int p = 0;
+        while (p + 1 < g.npat && g.chunk0[p + 1] <= ch) p++;
+        const int c_end = p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks;
+        const int64_t lo = sub_start[i * kSubPerChunk];
+        const int64_t hi = ch + 1 < c_end ? static_cast<int64_t>(sub_start[(i + 1) * kSubPerChunk])
+                                          : g.seg(b, p) + g.seg_len(b, p);
+        out[i] = static_cast<uint32_t>(hi - lo);
+    }
+}
+
 // diag(A'A)_c = sum over rows of m^2: inside a sorted group equal
 // (column, row) pairs are adjacent, so the j-th copy contributes 2j+1.
 __global__ void fast_diag_kernel(FastGeometry g, const uint32_t* __restrict__ g32, uint64_t* __restrict__ diag)
@@ -1647,23 +1667,18 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
         }
     }
     // entries per (block, chunk) -> work items
-    std::vector<uint32_t> ss(static_cast<size_t>(nsub));
-    if (!ss.empty()) {
-        CAS_CUDA(cudaMemcpyAsync(ss.data(), f.sub_start, sizeof(uint32_t) * ss.size(), cudaMemcpyDeviceToHost, s));
-        CAS_CUDA(cudaStreamSynchronize(s));
-    }
-    auto cs = [&](int64_t i) { return ss[static_cast<size_t>(i) * kSubPerChunk]; };  // first entry of (block, chunk) i
     std::vector<int64_t> entries(static_cast<size_t>(g.nblocks * g.nchunks), 0);
-    for (int64_t b = 0; b < g.nblocks; b++)
-        for (int p = 0; p < g.npat; p++) {
-            const int c_end = p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks;
-            for (int ch = g.chunk0[p]; ch < c_end; ch++) {
-                const int64_t lo = cs(b * g.nchunks + ch);
-                const int64_t hi = ch + 1 < c_end ? static_cast<int64_t>(cs(b * g.nchunks + ch + 1))
-                                                  : g.seg(b, p) + g.seg_len(b, p);
-                entries[b * g.nchunks + ch] = hi - lo;
-            }
-        }
+    if (!entries.empty() && rows > 0) {
+        std::vector<uint32_t> ce(entries.size());
+        uint32_t* d_ce = nullptr;
+        CAS_CUDA(dmalloc(&d_ce, sizeof(uint32_t) * ce.size()));
+        { fast_chunk_entries_kernel<<<fgrid(static_cast<int64_t>(ce.size()), 256), 256, 0, s>>>(g, f.sub_start, d_ce); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+        CAS_CUDA(cudaMemcpyAsync(ce.data(), d_ce, sizeof(uint32_t) * ce.size(), cudaMemcpyDeviceToHost, s));
+        CAS_CUDA(cudaStreamSynchronize(s));
+        dfree(d_ce);
+        for (size_t i = 0; i < ce.size(); i++) entries[i] = ce[i];
+    }
     if (g.nblocks > 0) {
         CAS_TRY(tune_transpose(f, entries, s));
         CAS_TRY(build_items(g, entries, 1, 2, false, true, false, sizeof(double), f.t64));

@@ -161,7 +161,7 @@ struct FastTranspose {
     int* item_b0 = nullptr;    // [nitems]
     int* item_b1 = nullptr;    // [nitems]
     int64_t* item_part = nullptr;  // [nitems] offset of the item's partials
-    int* sc_item0 = nullptr;       // [nsc + 1] first item of each super-chunk
+    int* sc_item0 = nullptr;       // [nprob * nsc + 1] first item of each (problem, super-chunk)
     void* partial = nullptr;       // float or double partials
     int* ctr = nullptr;            // [2] work counter and finished CTAs of the persistent schedule (reset by the kernel)
     void* meta = nullptr;          // one device block holding every array above except partial
