@@ -8,15 +8,22 @@ behind the C ABI in include/cassandra_b200.h.
 from ._lib import CasError, SizeMismatch, load  # noqa: F401
 from .api import (  # noqa: F401
     CG,
+    DEFAULT_ACCURACY,
     LSQR,
     PCG,
     GroupIndexer,
     MatrixCSR,
+    MultiStageScoreEstimator,
+    estimator_stages,
     fit_weights,
     generate_positions,
     generate_positions_host,
     generate_targets,
     jacobi_preconditioner_of_ata,
+    load_estimator,
+    read_records,
+    read_scored_positions,
+    save_estimator,
     solve_batched,
     solve_opts,
 )

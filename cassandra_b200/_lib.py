@@ -151,6 +151,19 @@ SIGNATURES: dict[str, tuple] = {
     "cas_solve_batched": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "cas_fit_weights_batched": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int, _VP, _VP, _VP]),
     "cas_fit_weights_batched_device": (C.c_int, [_VP, _VP, _VP, _VP, C.c_int, _VP, _VP, _VP, _VP]),
+    "cas_estimator_stages": (C.c_int, [C.c_int]),
+    "cas_estimator_save": (C.c_int, [C.c_char_p, C.c_int, _VP, C.c_int, _VP, _VP, C.c_int]),
+    "cas_estimator_file_info": (C.c_int, [C.c_char_p, _VP, _VP, _VP, _VP, _VP]),
+    "cas_estimator_file_read": (C.c_int, [C.c_char_p, _VP, _VP, _VP]),
+    "cas_estimator_create": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP, _PP]),
+    "cas_estimator_destroy": (None, [_VP]),
+    "cas_estimator_info": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
+    "cas_estimator_patterns": (C.c_int, [_VP, _VP]),
+    "cas_estimator_tables": (C.c_int, [_VP, C.c_int, _VP, _VP]),
+    "cas_estimator_eval": (C.c_int, [_VP, _VP, _I64, _VP, _VP]),
+    "cas_estimator_weights": (C.c_int, [_VP, C.c_int, _VP, _VP]),
+    "cas_read_records": (C.c_int, [C.c_char_p, _VP, _VP, _I64, _VP]),
+    "cas_read_scored_positions": (C.c_int, [C.c_char_p, _VP, _VP, _I64, _VP]),
     "cas_spmv_norm_noalloc_max_rows": (_I64, []),
     "cas_spmv_norm_noalloc": (C.c_int, [_VP, C.c_int, _I64, _I64, _VP, _VP, _VP, _VP]),
 }

@@ -426,3 +426,142 @@ def generate_targets(a: MatrixCSR, seed: int, w_sigma: float = 0.5, noise_sigma:
     w = torch.empty(a.cols(), dtype=torch.float64, device="cuda") if return_true_weights else None
     L.check(L.load().cas_generate_targets(a.handle, seed, w_sigma, noise_sigma, _ptr(b), _ptr(w), _stream()))
     return (b, w) if return_true_weights else b
+
+
+# ---------------------------------------------------------------------------
+# Pattern-based score estimators (Pattern/Evaluator.h) and their files
+# (IO/Binary.cpp)
+# ---------------------------------------------------------------------------
+
+# The parameters of the reference's default AccuracyModel (Pattern/Evaluator.h),
+# written into estimator files saved without explicit ones.
+DEFAULT_ACCURACY = (-0.16594754, 0.95554334, 0.27973529, -0.01616647, 1.28078789)
+
+
+def estimator_stages(stage_size: int) -> int:
+    """Stages(stage_size) (Pattern/Evaluator.cpp:6-9): ceil(65 / stage_size)."""
+    return int(L.load().cas_estimator_stages(stage_size))
+
+
+def _reference_cols(masks) -> int:
+    return GroupIndexer(masks, "reference").index_space_size
+
+
+def save_estimator(path, masks, stage_size: int, weights, accuracy=DEFAULT_ACCURACY) -> None:
+    """Save(PatternBasedEstimator) (IO/Binary.cpp:46-63): weights is
+    [stages, C] (numpy or tensor, C = the reference-mode columns of masks);
+    the file is the reference's, byte for byte."""
+    w = weights.detach().cpu().numpy() if isinstance(weights, torch.Tensor) else np.asarray(weights)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    stages, cols = estimator_stages(stage_size), _reference_cols(masks)
+    if w.shape != (stages, cols):
+        raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+    m = np.asarray(masks, dtype=np.uint64)
+    a = np.ascontiguousarray(accuracy, dtype=np.float32)
+    L.check(L.load().cas_estimator_save(str(path).encode(), stage_size, m.ctypes.data_as(C.c_void_p), len(m),
+                                        w.ctypes.data_as(C.c_void_p), a.ctypes.data_as(C.c_void_p), len(a)))
+
+
+def load_estimator(path) -> dict:
+    """LoadPatternBasedEstimator (IO/Binary.cpp:65-68): stage size, the
+    stored patterns, the weights [stages, C] and the accuracy parameters."""
+    lib = L.load()
+    ss, nm, ns, na = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    wps = C.c_int64()
+    p = str(path).encode()
+    L.check(lib.cas_estimator_file_info(p, C.byref(ss), C.byref(nm), C.byref(ns), C.byref(wps), C.byref(na)))
+    masks = np.empty(nm.value, np.uint64)
+    w = np.empty((ns.value, wps.value), np.float32)
+    acc = np.empty(na.value, np.float32)
+    L.check(lib.cas_estimator_file_read(p, masks.ctypes.data_as(C.c_void_p), w.ctypes.data_as(C.c_void_p),
+                                        acc.ctypes.data_as(C.c_void_p)))
+    return {"stage_size": ss.value, "masks": [int(v) for v in masks], "weights": w, "accuracy": acc.tolist()}
+
+
+class MultiStageScoreEstimator:
+    """MultiStageScoreEstimator (Pattern/Evaluator.cpp:77-88) on the device:
+    every stage's dense weights expanded into per-variation tables
+    (ScoreEstimator, :11-29), batch evaluation bitwise equal to the
+    reference's Eval, and Weights() per stage."""
+
+    def __init__(self, masks, stage_size: int, weights):
+        self._lib = L.load()
+        self._h = C.c_void_p()
+        w = weights if isinstance(weights, torch.Tensor) else torch.from_numpy(np.asarray(weights, np.float32))
+        w = w.to(device="cuda", dtype=torch.float32).contiguous()
+        stages, cols = estimator_stages(stage_size), _reference_cols(masks)
+        if tuple(w.shape) != (stages, cols):
+            raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+        m = np.asarray(masks, dtype=np.uint64)
+        L.check(self._lib.cas_estimator_create(m.ctypes.data_as(C.c_void_p), len(m), stage_size, _ptr(w), _stream(),
+                                               C.byref(self._h)))
+        ss, st, nm = C.c_int(), C.c_int(), C.c_int()
+        wps, tps = C.c_int64(), C.c_int64()
+        L.check(self._lib.cas_estimator_info(self._h, C.byref(ss), C.byref(st), C.byref(nm), C.byref(wps),
+                                             C.byref(tps)))
+        self.stage_size, self.stages, self._n = ss.value, st.value, nm.value
+        self.weights_per_stage, self.table_floats = wps.value, tps.value
+
+    @classmethod
+    def load(cls, path) -> "MultiStageScoreEstimator":
+        f = load_estimator(path)
+        return cls(f["masks"], f["stage_size"], f["weights"])
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            torch.cuda.current_stream().synchronize()
+            self._lib.cas_estimator_destroy(h)
+            self._h = None
+
+    def pattern(self) -> list[int]:
+        out = np.empty(self._n, np.uint64)
+        L.check(self._lib.cas_estimator_patterns(self._h, out.ctypes.data_as(C.c_void_p)))
+        return [int(v) for v in out]
+
+    def eval(self, positions: torch.Tensor) -> torch.Tensor:
+        _require_cuda(positions, "positions")
+        out = torch.empty(positions.shape[0], dtype=torch.float32, device=positions.device)
+        L.check(self._lib.cas_estimator_eval(self._h, _ptr(positions), positions.shape[0], _ptr(out), _stream()))
+        return out
+
+    def tables(self, stage: int) -> torch.Tensor:
+        out = torch.empty(self.table_floats, dtype=torch.float32, device="cuda")
+        L.check(self._lib.cas_estimator_tables(self._h, stage, _ptr(out), _stream()))
+        return out
+
+    def weights(self, stage: int) -> torch.Tensor:
+        out = torch.empty(self.weights_per_stage, dtype=torch.float32, device="cuda")
+        L.check(self._lib.cas_estimator_weights(self._h, stage, _ptr(out), _stream()))
+        return out
+
+    def save(self, path, accuracy=DEFAULT_ACCURACY) -> None:
+        w = torch.stack([self.weights(s) for s in range(self.stages)])
+        save_estimator(path, self.pattern(), self.stage_size, w, accuracy)
+
+
+# ---------------------------------------------------------------------------
+# Training-data ingestion
+# ---------------------------------------------------------------------------
+
+def _read(fn, path) -> tuple[np.ndarray, np.ndarray]:
+    n = C.c_int64()
+    p = str(path).encode()
+    L.check(fn(p, None, None, 0, C.byref(n)))
+    pos = np.empty((n.value, 2), np.uint64)
+    sc = np.empty(n.value, np.int8)
+    got = C.c_int64()
+    L.check(fn(p, pos.ctypes.data_as(C.c_void_p), sc.ctypes.data_as(C.c_void_p), n.value, C.byref(got)))
+    return pos[:got.value], sc[:got.value]
+
+
+def read_records(path) -> tuple[np.ndarray, np.ndarray]:
+    """'<QQb' records (NeuralNetwork/NeuralNetwork.py:21-29): positions
+    [n, 2] uint64 ({P, O}) and int8 scores."""
+    return _read(L.load().cas_read_records, path)
+
+
+def read_scored_positions(path) -> tuple[np.ndarray, np.ndarray]:
+    """Text ScoredPosition lines (IO/File.cpp:16-24): positions [n, 2]
+    uint64 and int8 scores."""
+    return _read(L.load().cas_read_scored_positions, path)

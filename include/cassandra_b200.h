@@ -356,6 +356,77 @@ CAS_API cas_status cas_generate_targets(const cas_csr* a, uint64_t seed, double 
                                         double* d_b, double* d_w_true, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Pattern-based score estimators (Pattern/Evaluator.h, IO/Binary.cpp)       */
+/* ------------------------------------------------------------------------ */
+
+/* Stages(stage_size) (Pattern/Evaluator.cpp:6-9): ceil(65 / stage_size). */
+CAS_API int cas_estimator_stages(int stage_size);
+/* Save(PatternBasedEstimator) (IO/Binary.cpp:46-63) of the estimator whose
+ * stage s (s < cas_estimator_stages(stage_size)) holds the dense weights
+ * h_weights + s * C, C = the reference-mode column count of masks (the
+ * layout FitWeights fits, PatternFit/PatternFit.cpp:7-39), and whose
+ * accuracy model has the n_accuracy parameters (the reference's default
+ * model has 5, Pattern/Evaluator.h AccuracyModel).  The bytes are those the
+ * reference writes for ScoreEstimator(masks, weights) stages: the stored
+ * patterns of CreateIndexer and ScoreEstimator::Weights(), size_t counts,
+ * native byte order. */
+CAS_API cas_status cas_estimator_save(const char* path, int stage_size, const uint64_t* masks, int n_masks,
+                                      const float* h_weights, const float* accuracy, int n_accuracy);
+/* LoadPatternBasedEstimator (IO/Binary.cpp:65-68), in two calls: the sizes,
+ * then the stored patterns (n_masks), the weights of every stage (stages *
+ * weights_per_stage floats) and the accuracy parameters (any pointer may be
+ * NULL).  Files whose stages hold other patterns than the estimator are
+ * rejected. */
+CAS_API cas_status cas_estimator_file_info(const char* path, int* stage_size, int* n_masks, int* stages,
+                                           int64_t* weights_per_stage, int* n_accuracy);
+CAS_API cas_status cas_estimator_file_read(const char* path, uint64_t* h_masks, float* h_weights, float* h_accuracy);
+
+/* A MultiStageScoreEstimator on the device (Pattern/Evaluator.cpp:11-29,
+ * 77-83): d_weights holds cas_estimator_stages(stage_size) stages of dense
+ * weights (C floats each, as above); every stage is expanded into one table
+ * of 3^k floats per variation of every pattern, by a kernel. */
+typedef struct cas_estimator cas_estimator;
+CAS_API cas_status cas_estimator_create(const uint64_t* masks, int n_masks, int stage_size, const float* d_weights,
+                                        void* stream, cas_estimator** out);
+CAS_API void cas_estimator_destroy(cas_estimator* e);
+CAS_API cas_status cas_estimator_info(const cas_estimator* e, int* stage_size, int* stages, int* n_masks,
+                                      int64_t* weights_per_stage, int64_t* table_floats_per_stage);
+/* Pattern(): CreateIndexer's stored pattern of every mask. */
+CAS_API cas_status cas_estimator_patterns(const cas_estimator* e, uint64_t* h_out);
+/* The expanded tables of one stage (table_floats_per_stage floats, variation
+ * order). */
+CAS_API cas_status cas_estimator_tables(const cas_estimator* e, int stage, float* d_out, void* stream);
+/* MultiStageScoreEstimator::Eval (Pattern/Evaluator.cpp:48-54, 85-88) of n
+ * positions ({P, O} uint64 pairs, 16-byte aligned): the FP32 sum in the
+ * reference's order, bitwise its result.  A record with a square of both
+ * players (not a position) scores NaN. */
+CAS_API cas_status cas_estimator_eval(const cas_estimator* e, const uint64_t* d_positions, int64_t n, float* d_scores,
+                                      void* stream);
+/* ScoreEstimator::Weights() (Pattern/Evaluator.cpp:56-73) of one stage: C
+ * dense floats. */
+CAS_API cas_status cas_estimator_weights(const cas_estimator* e, int stage, float* d_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Training-data ingestion                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Binary '<QQb' records (NeuralNetwork/NeuralNetwork.py:21-29): 17 bytes
+ * each, P and O little-endian uint64 then an int8 score, no header.  Reads up
+ * to max_records into h_positions ({P, O} pairs) and h_scores; with both
+ * NULL only counts the whole records of the file.  A trailing partial record
+ * is not read (the reference's reader stops there). */
+CAS_API cas_status cas_read_records(const char* path, uint64_t* h_positions, int8_t* h_scores, int64_t max_records,
+                                    int64_t* n_records);
+/* Text lines of ScoredPosition (LoadScoredPositionFile, IO/File.cpp:16-24;
+ * ScoredPosition::FromString, Game/ScoredPosition.cpp:3-8): 64 board
+ * characters, the side to move in column 65, the score (sign, digits,
+ * halved, int8 as Score keeps it) from column 69.  Same calling convention
+ * as cas_read_records; a line that is not a scored position is an error
+ * naming the line. */
+CAS_API cas_status cas_read_scored_positions(const char* path, uint64_t* h_positions, int8_t* h_scores,
+                                             int64_t max_records, int64_t* n_records);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free product                                                   */
 /* ------------------------------------------------------------------------ */
 

@@ -117,6 +117,20 @@ def ref_lib() -> C.CDLL:
         for n in ("ref_pcg", "ref_lsqr"):
             getattr(lib, n).restype = None
             getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, _VP, _VP]
+        lib.ref_estimator_eval.restype = None
+        lib.ref_estimator_eval.argtypes = [_VP, C.c_int, _VP, _I64, _VP, _I64, _VP]
+        lib.ref_estimator_weights.restype = None
+        lib.ref_estimator_weights.argtypes = [_VP, C.c_int, _VP, _I64, _VP]
+        lib.ref_msse_eval.restype = None
+        lib.ref_msse_eval.argtypes = [C.c_int, _VP, C.c_int, _VP, _I64, _VP, _I64, _VP]
+        lib.ref_save_estimator.restype = None
+        lib.ref_save_estimator.argtypes = [C.c_char_p, C.c_int, _VP, C.c_int, _VP, _I64, _VP, C.c_int]
+        lib.ref_parse_scored_position.restype = C.c_int
+        lib.ref_parse_scored_position.argtypes = [C.c_char_p, _VP, _VP, _VP]
+        lib.ref_format_scored_position.restype = None
+        lib.ref_format_scored_position.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_char_p]
+        lib.ref_load_estimator.restype = C.c_int
+        lib.ref_load_estimator.argtypes = [C.c_char_p, _VP, _VP, _VP, C.c_int, _VP, _I64, _VP, _VP]
         _ref = lib
     return _ref
 

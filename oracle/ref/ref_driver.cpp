@@ -14,6 +14,9 @@
 #include "Math/MatrixCSR.h"
 #include "Math/MatrixProxy.h"
 #include "Math/Solver.h"
+#include "Pattern/Evaluator.h"
+#include "IO/Binary.h"
+#include "Game/ScoredPosition.h"
 #include <cstdint>
 #include <cstring>
 #include <span>
@@ -203,6 +206,94 @@ void ref_lsqr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const floa
     Vector x = solver.X();
     std::memcpy(x_out, x.data(), sizeof(float) * cols);
     *residuum = solver.Residuum();
+}
+
+// ScoreEstimator(pattern, weights) (Pattern/Evaluator.cpp:11-29) and its
+// Eval (:48-54) on every position.
+void ref_estimator_eval(const uint64_t* masks, int n, const float* weights, int64_t n_weights, const uint64_t* po,
+                        int64_t rows, float* out)
+{
+    ScoreEstimator se(std::vector<uint64_t>(masks, masks + n), std::span<const float>(weights, n_weights));
+    for (int64_t i = 0; i < rows; i++) out[i] = se.Eval(pos_at(po, i));
+}
+
+// ScoreEstimator::Weights() (Pattern/Evaluator.cpp:56-73) of the estimator
+// built from dense weights: writes n_weights floats.
+void ref_estimator_weights(const uint64_t* masks, int n, const float* weights, int64_t n_weights, float* out)
+{
+    ScoreEstimator se(std::vector<uint64_t>(masks, masks + n), std::span<const float>(weights, n_weights));
+    const std::vector<float> w = se.Weights();
+    std::memcpy(out, w.data(), sizeof(float) * std::min<size_t>(w.size(), static_cast<size_t>(n_weights)));
+}
+
+// MultiStageScoreEstimator (Pattern/Evaluator.cpp:77-88) whose stage s holds
+// ScoreEstimator(pattern, weights + s * n_weights); Eval of every position.
+void ref_msse_eval(int stage_size, const uint64_t* masks, int n, const float* weights, int64_t n_weights,
+                   const uint64_t* po, int64_t rows, float* out)
+{
+    std::vector<uint64_t> pattern(masks, masks + n);
+    MultiStageScoreEstimator msse(stage_size, pattern);
+    for (size_t s = 0; s < msse.estimators.size(); s++)
+        msse.estimators[s] = ScoreEstimator(pattern, std::span<const float>(weights + s * n_weights, n_weights));
+    for (int64_t i = 0; i < rows; i++) out[i] = msse.Eval(pos_at(po, i));
+}
+
+// Save(PatternBasedEstimator) (IO/Binary.cpp:46-63) of the estimator whose
+// stage s holds the dense weights weights + s * n_weights.
+void ref_save_estimator(const char* path, int stage_size, const uint64_t* masks, int n, const float* weights,
+                        int64_t n_weights, const float* accuracy, int n_accuracy)
+{
+    std::vector<uint64_t> pattern(masks, masks + n);
+    MultiStageScoreEstimator msse(stage_size, pattern);
+    for (size_t s = 0; s < msse.estimators.size(); s++)
+        msse.estimators[s] = ScoreEstimator(pattern, std::span<const float>(weights + s * n_weights, n_weights));
+    PatternBasedEstimator pbe(std::move(msse), AccuracyModel(std::vector<float>(accuracy, accuracy + n_accuracy)));
+    Save(pbe, std::filesystem::path(path));
+}
+
+// LoadPatternBasedEstimator (IO/Binary.cpp:65-68): stage size, stages,
+// masks (up to max_masks), each stage's Weights() (up to max_weights floats
+// per stage) and the accuracy parameters (up to 8).  Returns the number of
+// masks.
+int ref_load_estimator(const char* path, int* stage_size, int* stages, uint64_t* masks, int max_masks, float* weights,
+                       int64_t max_weights, float* accuracy, int* n_accuracy)
+{
+    const PatternBasedEstimator pbe = LoadPatternBasedEstimator(std::filesystem::path(path));
+    *stage_size = pbe.StageSize();
+    *stages = pbe.Stages();
+    const std::vector<uint64_t> pattern = pbe.Pattern();
+    for (size_t i = 0; i < pattern.size() && static_cast<int>(i) < max_masks; i++) masks[i] = pattern[i];
+    for (int s = 0; s < pbe.Stages(); s++) {
+        const std::vector<float> w = pbe.score.estimators[s].Weights();
+        std::memcpy(weights + s * max_weights, w.data(), sizeof(float) * std::min<size_t>(w.size(), max_weights));
+    }
+    const std::vector<float>& a = pbe.accuracy.ParameterValues();
+    *n_accuracy = static_cast<int>(a.size());
+    for (size_t i = 0; i < a.size() && i < 8; i++) accuracy[i] = a[i];
+    return static_cast<int>(pattern.size());
+}
+
+// ScoredPosition::FromString (Game/ScoredPosition.cpp:3-8) of one text line:
+// 0 on success, 1 if the reference throws.
+int ref_parse_scored_position(const char* line, uint64_t* p, uint64_t* o, int* score)
+{
+    try {
+        const ScoredPosition sp = ScoredPosition::FromString(std::string_view(line));
+        *p = sp.pos.Player();
+        *o = sp.pos.Opponent();
+        *score = static_cast<int>(sp.score);
+        return 0;
+    } catch (...) {
+        return 1;
+    }
+}
+
+// to_string(ScoredPosition) (Game/ScoredPosition.cpp:20-23) into out (at
+// least 80 bytes): the line the reference writes for a position and score.
+void ref_format_scored_position(uint64_t p, uint64_t o, int score, char* out)
+{
+    const std::string s = to_string(ScoredPosition{Position(p, o), Score(score)});
+    std::memcpy(out, s.c_str(), s.size() + 1);
 }
 
 }  // extern "C"

@@ -14,6 +14,12 @@ Outputs (all small, committed):
                    10 FP32 PCG / LSQR iterations on the 5-pattern system of
                    the fuzz positions with seeded targets.
   flips_ref.npz    the four flips of seeded random bitboards.
+  estimator_ref.npz  a PatternBasedEstimator file written by the reference's
+                   Save (IO/Binary.cpp:46-63) for ESTIMATOR_MASKS with seeded
+                   dense weights (stage size 33: 2 stages; 0xFF00 is stored flipped) and the default
+                   accuracy model, its file bytes, and the reference's
+                   MultiStageScoreEstimator::Eval and Weights() of it on the
+                   fuzz positions.
 """
 from __future__ import annotations
 
@@ -43,6 +49,11 @@ FIXTURES = {
     "vhdc": 0x8100000000000081,
 }
 SET5 = [0x42FF, 0x070707, 0x1F1F, 0x8040201008040201, 0xFF00]
+# Every indexer class of CreateIndexer, small enough for a committed file.
+ESTIMATOR_MASKS = [FIXTURES["a"], FIXTURES["v"], FIXTURES["vh"], FIXTURES["dc"], FIXTURES["vhdc"],
+                   FIXTURES["d"], 0x8040201008040201, 0xFF00]
+ESTIMATOR_STAGE_SIZE = 33
+DEFAULT_ACCURACY = [-0.16594754, 0.95554334, 0.27973529, -0.01616647, 1.28078789]
 SET8 = SET5 + [0xFF0000, 0xFF000000, 0x0080402010080402]
 
 
@@ -116,7 +127,40 @@ def main() -> None:
     boards = rng.integers(0, 2**63, size=64, dtype=np.uint64) * np.uint64(2) + rng.integers(0, 2, 64, dtype=np.uint64)
     flips = np.array([[lib.ref_flip(w, int(bb)) for w in range(4)] for bb in boards], dtype=np.uint64)
     np.savez_compressed(OUT / "flips_ref.npz", boards=boards, flips=flips)
+    estimator_fixture(lib, pos)
     print("wrote", *(p.name for p in OUT.glob("*.npz")))
+
+
+def estimator_fixture(lib, pos) -> None:
+    import os
+    import tempfile
+
+    m = np.asarray(ESTIMATOR_MASKS, np.uint64)
+    cols = np.zeros(1, np.int64)
+    lib.ref_group_info(_p(m), len(m), _p(cols), None)
+    c = int(cols[0])
+    stages = -(-65 // ESTIMATOR_STAGE_SIZE)
+    w = np.random.default_rng(20).normal(0, 2, (stages, c)).astype(np.float32)
+    acc = np.asarray(DEFAULT_ACCURACY, np.float32)
+    fd, path = tempfile.mkstemp(suffix=".bin")
+    os.close(fd)
+    try:
+        lib.ref_save_estimator(path.encode(), ESTIMATOR_STAGE_SIZE, _p(m), len(m), _p(w), c, _p(acc), len(acc))
+        blob = np.frombuffer(Path(path).read_bytes(), np.uint8).copy()
+    finally:
+        os.unlink(path)
+    scores = np.zeros(len(pos), np.float32)
+    lib.ref_msse_eval(ESTIMATOR_STAGE_SIZE, _p(m), len(m), _p(w), c, _p(pos), len(pos), _p(scores))
+    back = np.zeros_like(w)
+    for st in range(stages):
+        lib.ref_estimator_weights(_p(m), len(m), _p(w[st]), c, _p(back[st]))
+    stored = np.zeros(len(m), np.uint64)
+    for i, mk in enumerate(m):
+        sp, o, sz = np.zeros(1, np.uint64), np.zeros(1, np.int32), np.zeros(1, np.int32)
+        lib.ref_create_indexer(int(mk), _p(sp), _p(o), _p(sz))
+        stored[i] = sp[0]
+    np.savez_compressed(OUT / "estimator_ref.npz", masks=m, stored=stored, stage_size=np.int32(ESTIMATOR_STAGE_SIZE),
+                        weights=w, accuracy=acc, file_bytes=blob, positions=pos, scores=scores, weights_back=back)
 
 
 if __name__ == "__main__":
