@@ -9,6 +9,7 @@ from ._lib import CasError, SizeMismatch, load  # noqa: F401
 from .api import (  # noqa: F401
     CG,
     DEFAULT_ACCURACY,
+    LSMR,
     LSQR,
     PCG,
     GroupIndexer,

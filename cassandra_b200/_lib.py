@@ -31,6 +31,7 @@ CAS_F32 = 0
 CAS_F64 = 1
 CAS_PCG = 0
 CAS_LSQR = 1
+CAS_LSMR = 3
 CAS_CG = 2
 CAS_PLAIN_FP64 = 0
 CAS_MIXED = 1

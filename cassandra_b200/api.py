@@ -3,8 +3,8 @@
 Names follow the reference: ``GroupIndexer`` (Pattern/Indexer.h:29-40),
 ``MatrixCSR`` with ``A @ x`` / ``x @ A`` (Math/MatrixCSR.h:11-33),
 ``jacobi_preconditioner_of_ata`` (Math/MatrixCSR.h:30), the iterative solvers
-``PCG``, ``CG`` and ``LSQR`` with ``iterate`` / ``residuum`` / ``x`` / ``error``
-(Math/Solver.h:9-182), and ``fit_weights`` (PatternFit/PatternFit.cpp:7-39).
+``PCG``, ``CG``, ``LSQR`` and ``LSMR`` with ``iterate`` / ``residuum`` / ``x`` / ``error``
+(Math/Solver.h:9-287), and ``fit_weights`` (PatternFit/PatternFit.cpp:7-39).
 
 Device data is exchanged as CUDA torch tensors (PyTorch is used only for
 device memory and the current stream); host data as numpy arrays.  Size
@@ -259,7 +259,7 @@ def solve_opts(method: str = "pcg", precision: str = "fp64", tol: float = 1e-8, 
                refine_every: int = 50, check_every: int = 50, jacobi: bool = True) -> L.SolveOpts:
     o = L.SolveOpts()
     L.load().cas_solve_opts_default(C.byref(o))
-    o.method = {"pcg": L.CAS_PCG, "lsqr": L.CAS_LSQR, "cg": L.CAS_CG}[method]
+    o.method = {"pcg": L.CAS_PCG, "lsqr": L.CAS_LSQR, "cg": L.CAS_CG, "lsmr": L.CAS_LSMR}[method]
     o.precision = {"fp64": L.CAS_PLAIN_FP64, "mixed": L.CAS_MIXED}[precision]
     o.tol = tol
     o.max_iterations = max_iterations
@@ -348,6 +348,13 @@ class LSQR(_Solver):
     """LSQR(A, x0, b) (Math/Solver.h:128-182)."""
 
     method = "lsqr"
+
+
+class LSMR(_Solver):
+    """LSMR(A, x0, b) (Math/Solver.h:222-287).  residuum() is 0, as the
+    reference's Residuum(); rel_residual() is the FP64 true one."""
+
+    method = "lsmr"
 
 
 def solve_batched(a: MatrixCSR, b: torch.Tensor, precision: str = "mixed", tol: float = 1e-8,

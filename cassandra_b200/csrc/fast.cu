@@ -971,7 +971,8 @@ __device__ __forceinline__ void reduce_block_entries(const uint32_t* __restrict_
     }
     __syncthreads();
     if (warp == 0) {
-        const WarpRec<T> r = recs[lane];
+        WarpRec<T> r{};  // lanes past the CTA's warps carry no range
+        if (lane < kWarps) r = recs[lane];
         const bool single = r.fc == r.lc;
         lane_chain<T>(r.valid != 0, single, r.cp != 0, r.cn != 0, true, r.fc, r.lc, r.fs, single ? r.fs : r.ls, T(0),
                       [&](int col, T val) { acc[col] += val; });

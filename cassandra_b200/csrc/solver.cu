@@ -48,7 +48,10 @@ enum Slot {
     kArNorm = 15,  // |phi_bar * alpha * c| estimate of ||A'r||
     kTrue = 16,    // ||A'(b - A x)||^2 of the last true-residual evaluation
     kRrRef = 17,   // r.r right after the last residual replacement (mixed PCG)
-    kSlots = 18
+    // LSMR (shares kLAlpha, kLBeta, kInvBeta with LSQR)
+    kMAlphaBar = 18, kZetaBar = 19, kCBar = 20, kSBar = 21, kMRho = 22, kMRhoBar = 23,
+    kFHbar = 24, kFX = 25, kFH = 26,  // coefficients of the h_bar, x, h updates
+    kSlots = 27
 };
 // kPending: LSQR met its tolerance in the last step; the step's x/w update
 // still has to run, so kDone is raised by the next step's first kernel.
@@ -569,6 +572,128 @@ __global__ void __launch_bounds__(kVecThreads) lsqr_xw_kernel(int64_t n, double*
     }
 }
 
+// ---------------------------------------------------------------------------
+// LSMR steps (Math/Solver.h:222-287): the same bidiagonalisation as LSQR
+// (u_hat, v_hat with deferred normalisation), then three Givens rotations
+// on scalars and the h_bar, x, h updates.
+// ---------------------------------------------------------------------------
+
+// signum and GivensRotation (Math/Solver.h:184-220, the sym_ortho form of
+// scipy's lsqr.py): c, s, r with the signs of the reference.
+__device__ __forceinline__ double signum(double v) { return v < 0 ? -1.0 : (v > 0 ? 1.0 : 0.0); }
+__device__ __forceinline__ void givens(double a, double b, double& c, double& s, double& r)
+{
+    if (b == 0) {
+        c = signum(a);
+        s = 0;
+        r = fabs(a);
+    } else if (a == 0) {
+        c = 0;
+        s = signum(b);
+        r = fabs(b);
+    } else if (fabs(b) > fabs(a)) {
+        const double tau = a / b;
+        s = signum(b) / sqrt(1 + tau * tau);
+        c = s * tau;
+        r = b / s;
+    } else {
+        const double tau = b / a;
+        c = signum(a) / sqrt(1 + tau * tau);
+        s = c * tau;
+        r = a / c;
+    }
+}
+
+// alpha = ||v_hat||, then the rotations of one LSMR step and the update
+// coefficients; |zeta_bar| estimates ||A'r|| (the stopping test's
+// recursive residual).  init: the constructor's scalars (:236-251).  A
+// zero rho or rho_bar means the bidiagonalisation ended (the solution is
+// exact): the solver stops.  Single block.
+template <bool COMP>
+__global__ void __launch_bounds__(kRedThreads) lsmr_alpha_kernel(const double* __restrict__ part, int n, Dev dv,
+                                                                 int init)
+{
+    __shared__ double smem[64];
+    if (init != 1 && finished(dv.flags)) return;
+    const double sum = reduce_partials<COMP>(part, n, smem);
+    if (threadIdx.x != 0) return;
+    const double alpha = sqrt(sum);
+    double* sc = dv.scal;
+    const double beta = sc[kLBeta];
+    if (init) {
+        sc[kLAlpha] = alpha;
+        sc[kMAlphaBar] = alpha;
+        sc[kZetaBar] = alpha * beta;
+        sc[kMRho] = 1;
+        sc[kMRhoBar] = 1;
+        sc[kCBar] = 1;
+        sc[kSBar] = 0;
+        sc[kArNorm] = alpha * beta;
+        return;
+    }
+    const double rho_old = sc[kMRho], rho_bar_old = sc[kMRhoBar];
+    double c_hat, s_hat, alpha_hat;
+    givens(sc[kMAlphaBar], 0.0, c_hat, s_hat, alpha_hat);
+    double c, s, rho;
+    givens(alpha_hat, beta, c, s, rho);
+    const double theta_new = s * alpha;
+    const double theta_bar = sc[kSBar] * rho;
+    double c_bar, s_bar, rho_bar;
+    givens(sc[kCBar] * rho, theta_new, c_bar, s_bar, rho_bar);
+    const double zeta = c_bar * sc[kZetaBar];
+    const double zeta_bar = -s_bar * sc[kZetaBar];
+    if (!(rho != 0 && rho_bar != 0 && rho_old != 0 && rho_bar_old != 0) || !isfinite(rho) || !isfinite(rho_bar)) {
+        sc[kFHbar] = sc[kFX] = sc[kFH] = 0;
+        dv.flags[kDone] = 1;
+        if (!isfinite(rho) || !isfinite(rho_bar)) dv.flags[kStatus] = CAS_ERR_BREAKDOWN;
+        return;
+    }
+    sc[kMAlphaBar] = c * alpha;
+    sc[kMRho] = rho;
+    sc[kMRhoBar] = rho_bar;
+    sc[kCBar] = c_bar;
+    sc[kSBar] = s_bar;
+    sc[kZetaBar] = zeta_bar;
+    sc[kFHbar] = theta_bar * rho / rho_old / rho_bar_old;
+    sc[kFX] = zeta / rho / rho_bar;
+    sc[kFH] = theta_new / rho;
+    sc[kLAlpha] = alpha;
+    const double arn = fabs(zeta_bar);
+    sc[kArNorm] = arn;
+    dv.flags[kIter] += 1;
+    const double bn2 = sc[kBn2];
+    const double res = bn2 > 0 ? arn / sqrt(bn2) : arn;
+    sc[kRes] = res;
+    if (sc[kTol] > 0 && res <= sc[kTol]) dv.flags[kPending] = 1;
+}
+
+// h_bar = h - f_hbar h_bar; x += f_x h_bar; h = v - f_h h (v normalised);
+// gather copy vg = v.  init: h = v, h_bar = 0.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) lsmr_update_kernel(int64_t n, double* __restrict__ x,
+                                                                  double* __restrict__ h, double* __restrict__ hbar,
+                                                                  const double* __restrict__ v, T* __restrict__ vg,
+                                                                  Dev dv, int init)
+{
+    if (init != 1 && finished(dv.flags)) return;
+    const double inv_alpha = dv.scal[kLAlpha] != 0 ? 1.0 / dv.scal[kLAlpha] : 0.0;
+    const double f_hbar = dv.scal[kFHbar], f_x = dv.scal[kFX], f_h = dv.scal[kFH];
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double vn = v[c] * inv_alpha;
+        if (init) {
+            h[c] = vn;
+            hbar[c] = 0;
+        } else {
+            const double hb = h[c] - f_hbar * hbar[c];
+            hbar[c] = hb;
+            x[c] += f_x * hb;
+            h[c] = vn - f_h * h[c];
+        }
+        vg[c] = static_cast<T>(vn);
+    }
+}
+
 // coefficient of the u recursion: alpha / beta_prev (u_hat holds beta_prev u).
 // First kernel of an LSQR step: a tolerance met by the previous step stops
 // the solver here, after that step's x/w update has run.
@@ -603,6 +728,8 @@ struct SolverImpl {
     CsrView a;
     const FastLayout* fast = nullptr;
     cas_solve_opts o{};
+    // LSQR and LSMR: the bidiagonalisation methods on min ||Ax - b||
+    bool least_squares() const { return o.method == CAS_LSQR || o.method == CAS_LSMR; }
     cudaStream_t s = nullptr;
     int device = 0;
     bool mixed = false;
@@ -772,8 +899,14 @@ struct SolverImpl {
         // v_hat = (1/beta) A' u_hat - beta v
         CAS_TRY(product_t<T>(static_cast<const T*>(q), done()));
         { lsqr_v_kernel<COMP, T><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<T>(), v, part_a, D, 0); cas::count_launch(); }
-        { lsqr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 0); cas::count_launch(); }
-        { lsqr_xw_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, vg, D, 0); cas::count_launch(); }
+        if (o.method == CAS_LSMR) {
+            // LSMR: h in w, h_bar in z
+            { lsmr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 0); cas::count_launch(); }
+            { lsmr_update_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, z, v, vg, D, 0); cas::count_launch(); }
+        } else {
+            { lsqr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 0); cas::count_launch(); }
+            { lsqr_xw_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, vg, D, 0); cas::count_launch(); }
+        }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     }
@@ -791,15 +924,25 @@ struct SolverImpl {
             { lsqr_beta_kernel<true><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, mode); cas::count_launch(); }
             CAS_TRY(product_t<float>(static_cast<const float*>(q), gate ? done() : nullptr));
             { lsqr_v_kernel<true, float><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<float>(), v, part_a, D, mode); cas::count_launch(); }
-            { lsqr_alpha_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
-            { lsqr_xw_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, pg32, D, mode); cas::count_launch(); }
+            if (o.method == CAS_LSMR) {
+                { lsmr_alpha_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
+                { lsmr_update_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, z, v, pg32, D, mode); cas::count_launch(); }
+            } else {
+                { lsqr_alpha_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
+                { lsqr_xw_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, pg32, D, mode); cas::count_launch(); }
+            }
         } else {
             CAS_TRY((product<false, double, double>(x, static_cast<double*>(q), 2, b, 0, gate ? done() : nullptr)));
             { lsqr_beta_kernel<false><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, mode); cas::count_launch(); }
             CAS_TRY(product_t<double>(static_cast<const double*>(q), gate ? done() : nullptr));
             { lsqr_v_kernel<false, double><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), v, part_a, D, mode); cas::count_launch(); }
-            { lsqr_alpha_kernel<false><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
-            { lsqr_xw_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, p, D, mode); cas::count_launch(); }
+            if (o.method == CAS_LSMR) {
+                { lsmr_alpha_kernel<false><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
+                { lsmr_update_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, z, v, p, D, mode); cas::count_launch(); }
+            } else {
+                { lsqr_alpha_kernel<false><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
+                { lsqr_xw_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, p, D, mode); cas::count_launch(); }
+            }
         }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
@@ -807,7 +950,7 @@ struct SolverImpl {
 
     cas_status issue_iteration(int global_index)
     {
-        const bool lsqr = o.method == CAS_LSQR;
+        const bool lsqr = o.method == CAS_LSQR || o.method == CAS_LSMR;
         if (lsqr) {
             if (mixed) CAS_TRY((issue_lsqr_iteration<true, float>()));
             else CAS_TRY((issue_lsqr_iteration<false, double>()));
@@ -828,7 +971,7 @@ struct SolverImpl {
     cas_status issue_chunk(int first, int n)
     {
         // mixed LSQR restarts at fixed iterations: its graphs depend on the phase
-        const int period = (mixed && o.method == CAS_LSQR && o.refine_every > 0) ? o.refine_every : 1;
+        const int period = (mixed && least_squares() && o.refine_every > 0) ? o.refine_every : 1;
         const int phase = first % period;
         if (n > 1) {
             if (!graph || graph_len != n || graph_phase != phase) {
@@ -944,7 +1087,7 @@ struct SolverImpl {
         { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kBn2); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
 
-        if (o.method == CAS_LSQR) {
+        if (least_squares()) {
             CAS_TRY(issue_lsqr_start(1));
         } else {
             if (mixed) CAS_TRY(issue_pcg_refine<true>(true));
@@ -974,8 +1117,8 @@ namespace {
 cas_status validate_opts(const cas_solve_opts* o)
 {
     CAS_REQUIRE(o, CAS_ERR_INVALID_ARGUMENT, "null solver options");
-    CAS_REQUIRE(o->method == CAS_PCG || o->method == CAS_LSQR || o->method == CAS_CG, CAS_ERR_INVALID_ARGUMENT,
-                "unknown solver method");
+    CAS_REQUIRE(o->method == CAS_PCG || o->method == CAS_LSQR || o->method == CAS_CG || o->method == CAS_LSMR,
+                CAS_ERR_INVALID_ARGUMENT, "unknown solver method");
     CAS_REQUIRE(o->precision == CAS_PLAIN_FP64 || o->precision == CAS_MIXED, CAS_ERR_INVALID_ARGUMENT,
                 "unknown precision mode");
     CAS_REQUIRE(o->max_iterations >= 0 && o->check_every >= 0 && o->refine_every >= 0, CAS_ERR_INVALID_ARGUMENT,
@@ -1061,8 +1204,8 @@ CAS_API cas_status cas_solver_create_normal(const cas_csr* a, const cas_solve_op
     CAS_REQUIRE(a && out, CAS_ERR_INVALID_ARGUMENT, "cas_solver_create_normal: null argument");
     CAS_REQUIRE(d_normal_b || a->cols == 0, CAS_ERR_INVALID_ARGUMENT,
                 "cas_solver_create_normal: null right-hand side");
-    CAS_REQUIRE(o && o->method != CAS_LSQR, CAS_ERR_INVALID_ARGUMENT,
-                "cas_solver_create_normal: LSQR needs the rows-length right-hand side");
+    CAS_REQUIRE(o && o->method != CAS_LSQR && o->method != CAS_LSMR, CAS_ERR_INVALID_ARGUMENT,
+                "cas_solver_create_normal: LSQR and LSMR need the rows-length right-hand side");
     return create_solver(a, o, nullptr, d_normal_b, d_x0, stream, out);
 }
 
@@ -1087,7 +1230,8 @@ CAS_API cas_status cas_solver_residuum(cas_solver* sv, double* h_out)
 {
     CAS_REQUIRE(sv && h_out, CAS_ERR_INVALID_ARGUMENT, "cas_solver_residuum: null argument");
     CAS_TRY(sv->impl.read_state());
-    *h_out = sv->impl.o.method == CAS_LSQR ? sv->impl.host_scal[kPhiBar] : sv->impl.host_scal[kRr];
+    *h_out = sv->impl.o.method == CAS_LSQR ? sv->impl.host_scal[kPhiBar]
+                                           : (sv->impl.o.method == CAS_LSMR ? 0.0 : sv->impl.host_scal[kRr]);
     return CAS_OK;
 }
 
@@ -1133,7 +1277,7 @@ CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
             break;
         }
         const bool done = m.host_flags[kDone] || m.host_flags[kPending];
-        if (m.o.method == CAS_LSQR && m.o.tol > 0 && !done && it > 0) {
+        if (m.least_squares() && m.o.tol > 0 && !done && it > 0) {
             // LSQR's recursive residual estimates lose their meaning once the
             // bidiagonalisation loses orthogonality, and iterating past
             // convergence can diverge (the reference's LSQR has no stopping
@@ -1143,7 +1287,7 @@ CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
             if (rel <= m.o.tol) break;
         }
         if (done) {
-            if (m.host_flags[kVerified] && m.o.method != CAS_LSQR) {
+            if (m.host_flags[kVerified] && !m.least_squares()) {
                 // a residual replacement met the tolerance on the FP64 true residual
                 rel = m.host_scal[kRes];
                 break;
@@ -1160,8 +1304,8 @@ CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
             static const int zero = 0;
             CAS_CUDA(cudaMemcpyAsync(m.flags + kDone, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
             CAS_CUDA(cudaMemcpyAsync(m.flags + kPending, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
-            if (m.o.method == CAS_LSQR) {
-                // LSQR has no residual to replace: tighten the recursive target
+            if (m.least_squares()) {
+                // LSQR / LSMR have no residual to replace: tighten the recursive target
                 double t = m.host_scal[kTol] * 0.5;
                 CAS_CUDA(cudaMemcpyAsync(m.scal + kTol, &t, sizeof t, cudaMemcpyHostToDevice, m.s));
             } else if (m.mixed) {
@@ -1191,7 +1335,7 @@ CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
         rep->iterations = m.host_flags[kIter];
         rep->refinements = m.host_flags[kRefine];
         rep->rel_residual = rel;
-        rep->residuum = m.o.method == CAS_LSQR ? m.host_scal[kPhiBar] : m.host_scal[kRr];
+        rep->residuum = m.o.method == CAS_LSQR ? m.host_scal[kPhiBar] : (m.o.method == CAS_LSMR ? 0.0 : m.host_scal[kRr]);
         rep->seconds = ms * 1e-3;
         rep->setup_seconds = 0;
     }

@@ -213,7 +213,8 @@ CAS_API cas_status cas_eval_backward(const cas_csr* a, int64_t row0, int64_t row
 typedef enum cas_method {
     CAS_PCG = 0,  /* Jacobi-PCG on A'A x = A'b (Math/Solver.h:78-117 as FitWeights calls it) */
     CAS_LSQR = 1, /* LSQR on min ||Ax - b|| (Math/Solver.h:128-182) */
-    CAS_CG = 2    /* PCG with the identity preconditioner (Math/Solver.h:40-76) */
+    CAS_CG = 2,   /* PCG with the identity preconditioner (Math/Solver.h:40-76) */
+    CAS_LSMR = 3  /* LSMR on min ||Ax - b|| (Math/Solver.h:222-287); its Residuum() is 0, as there */
 } cas_method;
 
 typedef enum cas_precision {

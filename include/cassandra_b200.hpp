@@ -9,7 +9,7 @@
 //   JacobiPreconditionerOfATA     Math/MatrixCSR.h:30
 //   transposed(), A' * A proxy    Math/MatrixProxy.h:34-77
 //   DiagonalPreconditioner        Math/Solver.h:25-38
-//   PCG, CG, LSQR                 Math/Solver.h:40-182   Iterate/Residuum/Error/X
+//   PCG, CG, LSQR, LSMR           Math/Solver.h:40-287   Iterate/Residuum/Error/X
 //   GroupIndexer                  Pattern/Indexer.h:29-40
 //   FitWeights                    PatternFit/PatternFit.cpp:7-39
 //
@@ -496,6 +496,33 @@ public:
     }
 };
 
+// LSMR(A, x0, b) (Math/Solver.h:222-287) on the rows-length targets b.
+// Residuum() is 0, as the reference's (:284).
+template <typename M>
+class LSMR;
+
+template <>
+class LSMR<MatrixCSR> final : public detail::DeviceSolver {
+public:
+    LSMR(const MatrixCSR& a, Vector x0, Vector b) : DeviceSolver(a, b)
+    {
+        if (a.Cols() != x0.size()) throw std::runtime_error("Size mismatch.");
+        if (a.Rows() != b.size()) throw std::runtime_error("Size mismatch.");
+        cas_solve_opts o = opts(CAS_LSMR, 0);
+        auto dx0 = detail::to_device_f64(x0);
+        check(cas_solver_create(a.device(), &o, rhs.p, dx0.p, nullptr, &s));
+    }
+    // Error() = b - A x (Math/Solver.h:286).
+    Vector Error() const override
+    {
+        Vector r = a * X();
+        std::vector<double> hb(a.Rows());
+        rhs.download(hb.data(), hb.size());
+        for (size_t i = 0; i < r.size(); i++) r[i] = static_cast<float>(hb[i] - r[i]);
+        return r;
+    }
+};
+
 // Class template argument deduction as in the reference's
 // `PCG solver(transposed(A) * A, P, x0, b)`.
 PCG(const TwoMatrix<TransposedMatrix<MatrixCSR>, MatrixCSR>&, const Preconditioner&, Vector, Vector)
@@ -503,6 +530,7 @@ PCG(const TwoMatrix<TransposedMatrix<MatrixCSR>, MatrixCSR>&, const Precondition
 CG(const TwoMatrix<TransposedMatrix<MatrixCSR>, MatrixCSR>&, Vector, Vector)
     -> CG<TwoMatrix<TransposedMatrix<MatrixCSR>, MatrixCSR>>;
 LSQR(const MatrixCSR&, Vector, Vector) -> LSQR<MatrixCSR>;
+LSMR(const MatrixCSR&, Vector, Vector) -> LSMR<MatrixCSR>;
 
 // Pattern indexer (Pattern/Indexer.h:29-40).  Positions are {P, O} pairs.
 class GroupIndexer {

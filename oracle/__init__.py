@@ -72,9 +72,10 @@ def c_lib() -> C.CDLL:
         lib.or_pcg.restype = C.c_int
         lib.or_pcg.argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, C.c_int, C.c_double, C.c_int, _VP,
                                C.POINTER(C.c_double)]
-        lib.or_lsqr.restype = C.c_int
-        lib.or_lsqr.argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, C.c_double, C.c_int, _VP,
-                                C.POINTER(C.c_double)]
+        for n in ("or_lsqr", "or_lsmr"):
+            getattr(lib, n).restype = C.c_int
+            getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, C.c_double, C.c_int, _VP,
+                                        C.POINTER(C.c_double)]
         _c = lib
     return _c
 
@@ -114,7 +115,7 @@ def ref_lib() -> C.CDLL:
             getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, _VP]
         lib.ref_jacobi.restype = None
         lib.ref_jacobi.argtypes = [C.c_int, _I64, _I64, _VP, _VP]
-        for n in ("ref_pcg", "ref_lsqr"):
+        for n in ("ref_pcg", "ref_lsqr", "ref_lsmr"):
             getattr(lib, n).restype = None
             getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, _VP, _VP]
         lib.ref_estimator_eval.restype = None
@@ -160,7 +161,7 @@ def ref64_lib() -> C.CDLL:
             getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, _VP]
         lib.ref64_jacobi.restype = None
         lib.ref64_jacobi.argtypes = [C.c_int, _I64, _I64, _VP, _VP]
-        for n in ("ref64_pcg", "ref64_lsqr"):
+        for n in ("ref64_pcg", "ref64_lsqr", "ref64_lsmr"):
             getattr(lib, n).restype = C.c_int
             getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, C.c_double, C.c_int, _VP, _VP, _VP]
         lib.ref64_pcg_seconds_per_iteration.restype = C.c_double
@@ -236,5 +237,16 @@ def lsqr(idx, cols, b, iterations, tol=0.0, check_every=1):
     x = np.empty(cols, dtype=np.float64)
     res = C.c_double()
     it = c_lib().or_lsqr(idx.shape[1], idx.shape[0], cols, _p(idx), _p(b), iterations, tol, check_every, _p(x),
+                         C.byref(res))
+    return x, res.value, it
+
+
+def lsmr(idx, cols, b, iterations, tol=0.0, check_every=1):
+    """LSMR (Math/Solver.h:222-287) in FP64 from x0 = 0: x, |zeta_bar|, steps."""
+    idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.empty(cols, dtype=np.float64)
+    res = C.c_double()
+    it = c_lib().or_lsmr(idx.shape[1], idx.shape[0], cols, _p(idx), _p(b), iterations, tol, check_every, _p(x),
                          C.byref(res))
     return x, res.value, it

@@ -435,3 +435,74 @@ int or_lsqr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double
     free(u); free(tu); free(v); free(tv); free(w);
     return it;
 }
+
+/* signum and GivensRotation (Math/Solver.h:184-220: the scipy lsqr.py
+ * sym_ortho form): c, s, r with c*a + s*b = r, signs as there. */
+static double or_signum(double v) { return v < 0 ? -1.0 : (v > 0 ? 1.0 : 0.0); }
+static void or_givens(double a, double b, double* c, double* s, double* r)
+{
+    if (b == 0) { *c = or_signum(a); *s = 0; *r = fabs(a); return; }
+    if (a == 0) { *c = 0; *s = or_signum(b); *r = fabs(b); return; }
+    if (fabs(b) > fabs(a)) {
+        double tau = a / b;
+        *s = or_signum(b) / sqrt(1 + tau * tau);
+        *c = *s * tau;
+        *r = b / *s;
+    } else {
+        double tau = b / a;
+        *c = or_signum(a) / sqrt(1 + tau * tau);
+        *s = *c * tau;
+        *r = a / *c;
+    }
+}
+
+/* LSMR (Math/Solver.h:222-287) from x0 = 0, FP64.  Writes x and |zeta_bar|
+ * (the LSMR estimate of ||A'r||; the reference's Residuum() returns 0). */
+int or_lsmr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int iterations, double tol,
+            int check_every, double* x, double* zeta_bar_out)
+{
+    size_t cb = sizeof(double) * (size_t)(cols ? cols : 1), rb = sizeof(double) * (size_t)(rows ? rows : 1);
+    double *u = malloc(rb), *tu = malloc(rb), *v = malloc(cb), *tv = malloc(cb), *h = malloc(cb),
+           *hb = malloc(cb);
+    memset(x, 0, cb);
+    memcpy(u, b, rb); /* constructor (:236-251) */
+    double beta = decompose(u, rows);
+    or_spmv_t(k, rows, cols, idx, u, v);
+    double alpha = decompose(v, cols);
+    double alpha_bar = alpha, zeta_bar = alpha * beta, rho = 1, rho_bar = 1, c_bar = 1, s_bar = 0;
+    memcpy(h, v, cb);
+    memset(hb, 0, cb);
+    int it = 0;
+    if (check_every <= 0) check_every = 1;
+    for (; it < iterations;) { /* Iterate (:253-282) */
+        double rho_old = rho, rho_bar_old = rho_bar;
+        or_spmv(k, rows, cols, idx, v, tu);
+        for (int64_t i = 0; i < rows; i++) u[i] = tu[i] - alpha * u[i];
+        beta = decompose(u, rows);
+        or_spmv_t(k, rows, cols, idx, u, tv);
+        for (int64_t i = 0; i < cols; i++) v[i] = tv[i] - beta * v[i];
+        alpha = decompose(v, cols);
+        double c_hat, s_hat, alpha_hat;
+        or_givens(alpha_bar, 0, &c_hat, &s_hat, &alpha_hat);
+        double c, s;
+        or_givens(alpha_hat, beta, &c, &s, &rho);
+        double theta_new = s * alpha;
+        alpha_bar = c * alpha;
+        double theta_bar = s_bar * rho;
+        double cb_in = c_bar * rho;
+        or_givens(cb_in, theta_new, &c_bar, &s_bar, &rho_bar);
+        double zeta = c_bar * zeta_bar;
+        zeta_bar *= -s_bar;
+        double f_hb = theta_bar * rho / rho_old / rho_bar_old, f_x = zeta / rho / rho_bar, f_h = theta_new / rho;
+        for (int64_t i = 0; i < cols; i++) {
+            hb[i] = h[i] - f_hb * hb[i];
+            x[i] += f_x * hb[i];
+            h[i] = v[i] - f_h * h[i];
+        }
+        it++;
+        if (tol > 0 && it % check_every == 0 && or_normal_residual(k, rows, cols, idx, b, x) <= tol) break;
+    }
+    *zeta_bar_out = fabs(zeta_bar);
+    free(u); free(tu); free(v); free(tv); free(h); free(hb);
+    return it;
+}

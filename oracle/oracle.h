@@ -39,6 +39,8 @@ double or_normal_residual(int k, int64_t rows, int64_t cols, const uint32_t* idx
 int or_pcg(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int jacobi, int iterations,
            double tol, int check_every, double* x, double* residuum);
 /* Math/Solver.h:128-182 from x0 = 0, FP64; writes x and Residuum() (phi_bar). */
+int or_lsmr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int iterations, double tol,
+            int check_every, double* x, double* zeta_bar);
 int or_lsqr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int iterations, double tol,
             int check_every, double* x, double* residuum);
 

@@ -138,6 +138,34 @@ int ref64_lsqr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const dou
     return it;
 }
 
+// LSMR (Math/Solver.h:222-287) in FP64, same stopping rule as ref64_pcg.
+int ref64_lsmr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int max_iterations,
+               double tol, int check_every, double* x_out, double* rel_res, double* seconds)
+{
+    MatrixCSR m = make_csr(k, rows, cols, idx);
+    Vector score(b, b + rows);
+    double t0 = omp_get_wtime();
+    double excluded = 0;
+    LSMR solver(m, Vector(cols, 0.0), score);
+    int it = 0;
+    while (it < max_iterations) {
+        int n = std::min(check_every, max_iterations - it);
+        solver.Iterate(n);
+        it += n;
+        if (tol > 0) {
+            double c0 = omp_get_wtime();
+            double res = normal_residual(m, score, solver.X());
+            excluded += omp_get_wtime() - c0;
+            if (res <= tol) break;
+        }
+    }
+    *seconds = omp_get_wtime() - t0 - excluded;
+    Vector x = solver.X();
+    std::memcpy(x_out, x.data(), sizeof(double) * cols);
+    *rel_res = normal_residual(m, score, x);
+    return it;
+}
+
 // One PCG iteration's wall time in FP64 on a prebuilt system, averaged over n
 // iterations (the bounded CPU-baseline sample).
 double ref64_pcg_seconds_per_iteration(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b,

@@ -208,6 +208,19 @@ void ref_lsqr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const floa
     *residuum = solver.Residuum();
 }
 
+// LSMR (Math/Solver.h:222-287) from x0 = 0.  Writes x; *residuum receives
+// the reference's Residuum(), which is 0 for LSMR (:284).
+void ref_lsmr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const float* b, int iterations,
+              float* x_out, float* residuum)
+{
+    MatrixCSR m = make_csr(k, rows, cols, idx);
+    LSMR solver(m, Vector(cols, 0.0f), Vector(b, b + rows));
+    solver.Iterate(iterations);
+    Vector x = solver.X();
+    std::memcpy(x_out, x.data(), sizeof(float) * cols);
+    *residuum = solver.Residuum();
+}
+
 // ScoreEstimator(pattern, weights) (Pattern/Evaluator.cpp:11-29) and its
 // Eval (:48-54) on every position.
 void ref_estimator_eval(const uint64_t* masks, int n, const float* weights, int64_t n_weights, const uint64_t* po,

@@ -14,6 +14,8 @@ Outputs (all small, committed):
                    10 FP32 PCG / LSQR iterations on the 5-pattern system of
                    the fuzz positions with seeded targets.
   flips_ref.npz    the four flips of seeded random bitboards.
+  lsmr_ref.npz     10 FP32 LSMR iterations of the reference (Math/Solver.h:
+                   222-287) on the 5-pattern system of math_ref.npz.
   estimator_ref.npz  a PatternBasedEstimator file written by the reference's
                    Save (IO/Binary.cpp:46-63) for ESTIMATOR_MASKS with seeded
                    dense weights (stage size 33: 2 stages; 0xFF00 is stored flipped) and the default
@@ -128,6 +130,7 @@ def main() -> None:
     flips = np.array([[lib.ref_flip(w, int(bb)) for w in range(4)] for bb in boards], dtype=np.uint64)
     np.savez_compressed(OUT / "flips_ref.npz", boards=boards, flips=flips)
     estimator_fixture(lib, pos)
+    lsmr_fixture(lib)
     print("wrote", *(p.name for p in OUT.glob("*.npz")))
 
 
@@ -165,3 +168,12 @@ def estimator_fixture(lib, pos) -> None:
 
 if __name__ == "__main__":
     main()
+
+
+def lsmr_fixture(lib) -> None:
+    g = np.load(OUT / "math_ref.npz")
+    idx, cols, b = g["fit_idx"], int(g["fit_cols"]), g["fit_b"].astype(np.float32)
+    x = np.zeros(cols, np.float32)
+    res = C.c_float()
+    lib.ref_lsmr(idx.shape[1], idx.shape[0], cols, _p(idx), _p(b), 10, _p(x), C.byref(res))
+    np.savez_compressed(OUT / "lsmr_ref.npz", lsmr10_x=x, lsmr10_residuum=np.float32(res.value))

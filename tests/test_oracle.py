@@ -205,6 +205,45 @@ def test_lsqr_matches_reference(orc, ref, golden_math):
     np.testing.assert_allclose(res, g["lsqr10_residuum"], rtol=2e-3)
 
 
+def _ref64_lsmr(ref, idx, cols, b, iters):
+    want = np.empty(cols)
+    rel, sec = np.zeros(1), np.zeros(1)
+    with ref.single_thread():
+        ref.ref64_lib().ref64_lsmr(idx.shape[1], idx.shape[0], cols, _p(idx),
+                                   _p(np.ascontiguousarray(b, np.float64)), iters, 0.0, iters, _p(want), _p(rel),
+                                   _p(sec))
+    return want, rel[0]
+
+
+def test_lsmr_matches_reference(orc, ref):
+    """The oracle's LSMR (Math/Solver.h:222-287 with its Givens rotations)
+    against the reference's own LSMR retyped to FP64, single-threaded:
+    iterates agree to rounding after 5 and 40 steps."""
+    idx, cols, b = _small_system(orc, rows=3000, seed=5)
+    for steps in (5, 40):
+        x, zeta_bar, it = orc.lsmr(idx, cols, b, steps)
+        want, rel = _ref64_lsmr(ref, idx, cols, b, steps)
+        assert it == steps
+        np.testing.assert_allclose(x, want, rtol=0, atol=1e-12 * np.abs(want).max())
+        assert abs(orc.normal_residual(idx, cols, b, x) - rel) <= 1e-9 * rel
+
+
+def test_lsmr_golden(orc):
+    """10 FP32 steps of the reference's LSMR (committed fixture) against the
+    FP64 oracle on the 5-pattern system: FP32 rounding only."""
+    g = np.load("tests/golden/math_ref.npz")
+    lg = np.load("tests/golden/lsmr_ref.npz")
+    x, _, _ = orc.lsmr(g["fit_idx"], int(g["fit_cols"]), g["fit_b"].astype(np.float64), 10)
+    np.testing.assert_allclose(x, lg["lsmr10_x"], rtol=0, atol=1e-3 * np.abs(lg["lsmr10_x"]).max())
+    assert float(lg["lsmr10_residuum"]) == 0.0  # LSMR::Residuum() returns 0 (Math/Solver.h:284)
+
+
+def test_lsmr_reaches_tolerance(orc):
+    idx, cols, b = _small_system(orc, rows=3000, seed=2)
+    x, _, it = orc.lsmr(idx, cols, b, 20000, tol=1e-8, check_every=10)
+    assert orc.normal_residual(idx, cols, b, x) <= 1e-8 and it < 20000
+
+
 def test_pcg_reaches_tolerance(orc):
     idx, cols, b = _small_system(orc, rows=3000, seed=2)
     x, res, it = orc.pcg(idx, cols, b, 5000, tol=1e-8, check_every=10)
