@@ -43,6 +43,7 @@ constexpr int kRingStages = 3;      // A'y FP32 ring schedules: rounds in the pe
 constexpr size_t kRingBytes = sizeof(uint32_t) * kFastThreads * kRingStages * kItemsPerThread;
 constexpr int kMaxScRing = 2;  // widest FP32 accumulator (chunks) that leaves room for the ring
 constexpr int kMaxScRegs = 4;
+constexpr int64_t kBatchItemBlocks = 4;  // most row blocks of one A'y work item in a batched layout
 
 unsigned fgrid(int64_t work, int per)
 {
@@ -815,14 +816,17 @@ __device__ __forceinline__ void warp_round(const uint32_t* __restrict__ g32, uin
     uint32_t last_ent = 1u;  // an empty lane looks like a closed run
     auto step = [&](uint32_t e) {
         sum += y_of<T>(ytile, e);
-        const bool end = (e & 1u) != 0;
-        const int col = static_cast<int>((e >> 16) - c0);
-        const bool close_head = end && open;
-        hs = close_head ? sum : hs;
-        hc = close_head ? col : hc;
-        if (end && !open) acc[col] += sum;  // interior run: only this lane touches col
-        open = open && !end;
-        sum = end ? T(0) : sum;
+        if (e & 1u) {  // the run ends here
+            const int col = static_cast<int>((e >> 16) - c0);
+            if (open) {  // the lane's first run: may continue from the left, closed by the chain
+                hs = sum;
+                hc = col;
+                open = false;
+            } else {
+                acc[col] += sum;  // interior run: only this lane touches col
+            }
+            sum = T(0);
+        }
     };
     if (full) {
 #pragma unroll
@@ -1100,9 +1104,9 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
     __shared__ int s_item;
     __shared__ int pref[kMaxProblems + 1];
     if (done && *(volatile const int*)done) return;
-    T* acc = reinterpret_cast<T*>(smem_raw);
-    T* ytile = acc + kChunkCols * tv.per_sc;
-    uint32_t* ring = reinterpret_cast<uint32_t*>(ytile + kBlockRows);  // RING schedules only
+    T* ytile = reinterpret_cast<T*>(smem_raw);  // first: its entries' byte offsets address it directly
+    T* acc = ytile + kBlockRows;
+    uint32_t* ring = reinterpret_cast<uint32_t*>(acc + kChunkCols * tv.per_sc);  // RING schedules only
     if (!ctr) {
         const int u = static_cast<int>(blockIdx.x);
         aty_item<T, RING>(g, tv, g32, sub_start, y, partial, u / nsplit + item_base, item_base, y_block0,
@@ -1311,6 +1315,10 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
             sc_item0.push_back(static_cast<int>(item_sc.size()));
             if (qnb == 0) continue;
             int64_t n = static_cast<int64_t>(std::llround(sc_entries[static_cast<size_t>(q) * nsc + sc] / per_item));
+            // batched layouts: at most kBatchItemBlocks blocks per item, so
+            // that a problem left alone (or with few others) still has short
+            // units: a unit's blocks run one after another in one CTA
+            if (g.nprob > 1) n = std::max<int64_t>(n, (qnb + kBatchItemBlocks - 1) / kBatchItemBlocks);
             n = std::max<int64_t>(1, std::min<int64_t>(n, qnb));
             for (int64_t i = 0; i < n; i++) {
                 item_sc.push_back(sc);

@@ -110,3 +110,41 @@ def test_fitting_sets_match_reference(cuda, name, stage_size):
     e = cb.MultiStageScoreEstimator(masks, stage_size, w)
     got = e.eval(torch.from_numpy(pos.view(np.int64)).cuda()).cpu().numpy()
     np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["a", "c", "d", "h", "v", "vh", "dc", "vhdc"])
+def test_symmetry_independent_estimator(cuda, orc, name):
+    """PatternTest/Evaluator.cpp:7-31 for every fixture pattern: weights
+    1..N (N = the pattern's configuration count) survive Weights(), and the
+    score of every configuration equals the scores of its 8 symmetric
+    variants."""
+    from tests.golden.make_golden import FIXTURES
+
+    mask = FIXTURES[name]
+    cols = cb.GroupIndexer([mask], "reference").index_space_size
+    w = np.arange(1, cols + 1, dtype=np.float32)[None, :]
+    e = cb.MultiStageScoreEstimator([mask], 65, w)  # one stage
+    np.testing.assert_array_equal(e.weights(0).cpu().numpy(), w[0])
+    sq = [b for b in range(64) if (mask >> b) & 1]
+    cfg = []
+    for code in range(3 ** len(sq)):
+        p = o = 0
+        for b in sq:
+            d = code % 3
+            code //= 3
+            if d == 1:
+                p |= 1 << b
+            elif d == 2:
+                o |= 1 << b
+        cfg.append((p, o))
+    cfg = np.array(cfg, np.uint64)
+    lib = orc.c_lib()
+
+    def flip(wh, a):
+        return np.array([[lib.or_flip(wh, int(p)), lib.or_flip(wh, int(o))] for p, o in a], dtype=np.uint64)
+
+    variants = [cfg, flip(0, cfg), flip(1, cfg), flip(2, cfg), flip(3, cfg), flip(0, flip(2, cfg)),
+                flip(1, flip(2, cfg)), flip(3, flip(2, cfg))]
+    scores = [e.eval(torch.from_numpy(v.view(np.int64)).cuda()).cpu().numpy() for v in variants]
+    for s in scores[1:]:
+        np.testing.assert_array_equal(s, scores[0])

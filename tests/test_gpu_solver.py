@@ -112,6 +112,21 @@ def test_pcg_reaches_tolerance(cuda, orc, precision, mode):
     np.testing.assert_allclose(pred, pw, rtol=0, atol=1e-5 * np.abs(pw).max())
 
 
+def test_cpu_runnable_workload_200_steps(cuda, orc):
+    """The CPU-runnable workload: 100,000 positions of random play to exactly
+    30 empties, the 5 masks in expanded mode (C = 150,903, K = 40), 200
+    Jacobi-PCG steps from x = 0 in plain FP64: the predictions A x equal
+    the FP64 oracle's after the same 200 steps."""
+    a, b, idx, cols, _ = _system(100_000, SET5, "expanded", seed=3, lo=30, hi=30)
+    assert (cols, idx.shape[1]) == (150_903, 40)
+    s = cb.PCG(a, b, check_every=50)
+    s.iterate(200)
+    want, _, _ = orc.pcg(idx, cols, b.cpu().numpy(), 200)
+    pw = orc.spmv(idx, cols, want)
+    got = orc.spmv(idx, cols, s.x().cpu().numpy())
+    np.testing.assert_allclose(got, pw, rtol=0, atol=1e-6 * np.abs(pw).max())
+
+
 def test_lsqr_reaches_tolerance(cuda, orc):
     a, b, idx, cols, _ = _system(3000, SET5, seed=8)
     s = cb.LSQR(a, b, tol=1e-8, max_iterations=50_000, check_every=100)
