@@ -114,17 +114,26 @@ def test_pcg_reaches_tolerance(cuda, orc, precision, mode):
 
 def test_cpu_runnable_workload_200_steps(cuda, orc):
     """The CPU-runnable workload: 100,000 positions of random play to exactly
-    30 empties, the 5 masks in expanded mode (C = 150,903, K = 40), 200
-    Jacobi-PCG steps from x = 0 in plain FP64: the predictions A x equal
-    the FP64 oracle's after the same 200 steps."""
+    30 empties, the 5 masks in expanded mode (C = 150,903 > rows, K = 40),
+    Jacobi-PCG from x = 0 in plain FP64.  This system is underdetermined and
+    the iteration chaotic: a 1e-15 relative change of b moves the predictions
+    by 2e-4 after 30 steps and 1e-3 after 200, and the 200-step normal
+    residual anywhere between 1.7e-5 and 2e-4 (six oracle runs).  So the
+    predictions are pinned after 10 steps and the 200-step iterate through
+    the order of its normal-equation residual."""
     a, b, idx, cols, _ = _system(100_000, SET5, "expanded", seed=3, lo=30, hi=30)
     assert (cols, idx.shape[1]) == (150_903, 40)
-    s = cb.PCG(a, b, check_every=50)
-    s.iterate(200)
-    want, _, _ = orc.pcg(idx, cols, b.cpu().numpy(), 200)
+    bh = b.cpu().numpy()
+    s = cb.PCG(a, b, check_every=10)
+    s.iterate(10)
+    want, _, _ = orc.pcg(idx, cols, bh, 10)
     pw = orc.spmv(idx, cols, want)
-    got = orc.spmv(idx, cols, s.x().cpu().numpy())
-    np.testing.assert_allclose(got, pw, rtol=0, atol=1e-6 * np.abs(pw).max())
+    np.testing.assert_allclose(orc.spmv(idx, cols, s.x().cpu().numpy()), pw, rtol=0, atol=1e-8 * np.abs(pw).max())
+    s.iterate(190)
+    want, _, _ = orc.pcg(idx, cols, bh, 200)
+    res_got = orc.normal_residual(idx, cols, bh, s.x().cpu().numpy())
+    res_want = orc.normal_residual(idx, cols, bh, want)
+    assert 1e-6 < res_got < 1e-3 and res_got <= 20 * res_want, (res_got, res_want)
 
 
 def test_lsqr_reaches_tolerance(cuda, orc):
