@@ -44,6 +44,7 @@ constexpr size_t kRingBytes = sizeof(uint32_t) * kFastThreads * kRingStages * kI
 constexpr int kMaxScRing = 2;  // widest FP32 accumulator (chunks) that leaves room for the ring
 constexpr int kMaxScRegs = 4;
 constexpr int64_t kBatchItemBlocks = 4;  // most row blocks of one A'y work item in a batched layout
+constexpr int64_t kBatchSmallBlocks = 8;  // batched problems this small get one block per A'y item
 
 unsigned fgrid(int64_t work, int per)
 {
@@ -1315,10 +1316,14 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
             sc_item0.push_back(static_cast<int>(item_sc.size()));
             if (qnb == 0) continue;
             int64_t n = static_cast<int64_t>(std::llround(sc_entries[static_cast<size_t>(q) * nsc + sc] / per_item));
-            // batched layouts: at most kBatchItemBlocks blocks per item, so
-            // that a problem left alone (or with few others) still has short
-            // units: a unit's blocks run one after another in one CTA
-            if (g.nprob > 1) n = std::max<int64_t>(n, (qnb + kBatchItemBlocks - 1) / kBatchItemBlocks);
+            // batched layouts: at most kBatchItemBlocks blocks per item, and
+            // one block per item for problems of at most kBatchSmallBlocks
+            // blocks (the small stages that iterate longest), so that a
+            // problem left alone (or with few others) still has short units:
+            // a unit's blocks run one after another in one CTA
+            if (g.nprob > 1)
+                n = std::max<int64_t>(n, qnb <= kBatchSmallBlocks ? qnb
+                                                                  : (qnb + kBatchItemBlocks - 1) / kBatchItemBlocks);
             n = std::max<int64_t>(1, std::min<int64_t>(n, qnb));
             for (int64_t i = 0; i < n; i++) {
                 item_sc.push_back(sc);
