@@ -701,26 +701,30 @@ struct TView {
 // (one column can hold thousands of a block's entries).  Inside a warp each
 // lane owns kItemsPerThread consecutive entries per round.  An entry's bit 0
 // marks the last entry of its column, so a lane sums y over its entries and
-// closes a run at every flagged entry, with no column comparisons.  Every
-// run's sum is added to acc[col] exactly once, in an order fixed by the
-// data, so the result is bitwise reproducible:
-//   1. runs that start and end inside a lane are added to acc directly (no
-//      other lane or warp touches that column);
-//   2. runs cut by lane boundaries are combined by a segmented scan over the
-//      warp's lanes (shuffles); the run still open at the end of the
-//      previous round enters as `carry`;
-//   3. the lane where a cut run ends adds the combined sum, except for the
-//      warp's first and last run, which may continue in the neighbouring
-//      warps: their sums go to the warp's record;
+// closes a run at every flagged entry, with no column comparisons.  A
+// column's entries of a block are one run, so only the lane where a run
+// ends touches its column in a round, and the order of the adds is fixed by
+// the data: the result is bitwise reproducible.
+//   1. at every run end the lane adds its own part of the run to acc[col];
+//   2. the parts of a run in the lanes before (its open tails) are combined
+//      by a segmented scan over the warp's lanes (shuffles; the run still
+//      open at the end of the previous round enters as `carry`) and added
+//      by the lane where the run ends;
+//   3. the run still open at the end of a warp's range goes to the warp's
+//      record;
 //   4. after the block, warp 0 combines the 32 records with the same
-//      segmented scan (one lane per warp) and adds them.
+//      segmented scan (one lane per warp) and adds each chain to the column
+//      where it ends.
 
-// Sums of a warp's first and last run (columns relative to c0).
+// What a warp leaves for the runs that cross warp boundaries (columns
+// relative to the piece's first column).
 template <typename T>
 struct WarpRec {
-    T fs, ls;          // first-run sum, last-run sum (ls unused when fc == lc)
-    int fc, lc;        // first and last column of the warp's range
-    int valid, cp, cn; // range non-empty; first run continues the previous warp; last run continues in the next
+    T ls;        // open sum of the warp's last run (0 when that run ends in the warp)
+    int fc;      // column of the warp's first entry, where its first run ends unless single
+    int valid;   // the warp's range is non-empty
+    int cp;      // the first run continues the previous warp's last run
+    int single;  // no run ends in the warp's range
 };
 
 // y of an entry: its row, already scaled by 4, sits in bits 2..15.
@@ -733,14 +737,15 @@ __device__ __forceinline__ T y_of(const T* __restrict__ ytile, uint32_t e)
         return ytile[(e & 0xFFFCu) >> 2];
 }
 
-// Segmented inclusive scan over the 32 lanes of (any, single, cont_prev,
-// tail sum) and the closing adds of the runs cut by lane boundaries; `sink`
-// receives every such run.  single: no run ends in the lane; tail_open: the
-// lane's last run continues past its last entry.  Lanes without entries pass
-// the chain through.
+// Segmented inclusive scan over the 32 lanes of the open run sums ts.  A
+// chain starts at a lane that ends a run (its tail) or whose first entry
+// starts a column; a lane with no run end that continues the run from its
+// left (single && cont_prev) extends the chain.  The lane whose first run
+// continues from the left and ends in it gets the chain of the lanes before
+// it (carry before lane 0) through `sink`.  Lanes without entries pass the
+// chain through.  Returns the chain leaving lane 31.
 template <typename T, typename Sink>
-__device__ __forceinline__ T lane_chain(bool any, bool single, bool cont_prev, bool cont_next, bool tail_open,
-                                        int hc, int tc, T hs, T ts, T carry, Sink&& sink)
+__device__ __forceinline__ T lane_chain(bool any, bool single, bool cont_prev, int hc, T ts, T carry, Sink&& sink)
 {
     const int lane = threadIdx.x & 31;
     T v = any ? ts : T(0);
@@ -757,15 +762,8 @@ __device__ __forceinline__ T lane_chain(bool any, bool single, bool cont_prev, b
     const T X = f ? v : v + carry;  // chain value ending at this lane
     T Xprev = __shfl_up_sync(0xffffffffu, X, 1);
     if (lane == 0) Xprev = carry;
-    if (any) {
-        if (single) {
-            if (!cont_next) sink(tc, X);
-        } else {
-            sink(hc, cont_prev ? Xprev + hs : hs);
-            if (tail_open && !cont_next) sink(tc, ts);
-        }
-    }
-    return __shfl_sync(0xffffffffu, X, 31);  // open chain leaving the lanes
+    if (any && !single && cont_prev) sink(hc, Xprev);
+    return __shfl_sync(0xffffffffu, X, 31);
 }
 
 constexpr int kLaneVecs = kItemsPerThread / 4;  // 16-byte loads per lane and round
@@ -801,35 +799,30 @@ __device__ __forceinline__ void cp_async_wait()
 // One round of a warp over [w_lo, w_hi): lanes take kItemsPerThread entries
 // each from round_start (a multiple of 4).  A lane whose entries are all in
 // range gets them in `cur` (loaded ahead by the caller); edge lanes load
-// theirs one by one.  prev_end: the last entry before this round ended its
-// run (updated for the next round).
+// theirs one by one.  accc: the accumulator shifted so that an entry's
+// column field indexes it.  carry: the run open before the round (updated);
+// prev_end: the last entry before this round ended its run (updated).
 template <typename T>
 __device__ __forceinline__ void warp_round(const uint32_t* __restrict__ g32, uint32_t round_start, uint32_t w_lo,
-                                           uint32_t w_hi, uint32_t c0, const T* __restrict__ ytile,
-                                           T* __restrict__ acc, T& carry, bool& prev_end, WarpRec<T>& rec,
-                                           const uint4 (&cur)[kLaneVecs], bool full)
+                                           uint32_t w_hi, const T* __restrict__ ytile, T* __restrict__ accc,
+                                           T& carry, bool& prev_end, const uint4 (&cur)[kLaneVecs], bool full)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t e_first = round_start + lane * kItemsPerThread;
-    bool any = false, open = true;
-    T sum = 0, hs = 0;
-    int hc = 0;
-    uint32_t last_ent = 1u;  // an empty lane looks like a closed run
+    T sum = 0;
+    uint32_t ends = 0;
     auto step = [&](uint32_t e) {
         sum += y_of<T>(ytile, e);
-        if (e & 1u) {  // the run ends here
-            const int col = static_cast<int>((e >> 16) - c0);
-            if (open) {  // the lane's first run: may continue from the left, closed by the chain
-                hs = sum;
-                hc = col;
-                open = false;
-            } else {
-                acc[col] += sum;  // interior run: only this lane touches col
-            }
+        ends |= e;
+        if (e & 1u) {  // the run ends here: this lane's part of it
+            accc[e >> 16] += sum;
             sum = T(0);
         }
     };
+    bool any = false;
+    uint32_t first_ent = 1u, last_ent = 1u;  // an empty lane looks like a closed run
     if (full) {
+        first_ent = cur[0].x;
 #pragma unroll
         for (int q = 0; q < kLaneVecs; q++) {
             step(cur[q].x);
@@ -844,44 +837,28 @@ __device__ __forceinline__ void warp_round(const uint32_t* __restrict__ g32, uin
         if (lo < hi) {
             for (uint32_t e = lo; e < hi; e++) step(g32[e]);
             any = true;
+            first_ent = g32[lo];
             last_ent = g32[hi - 1];
         }
     }
-    const bool single = any && open;  // no run ends in this lane
-    const bool tail_open = any && !(last_ent & 1u);
-    const int tc = static_cast<int>((last_ent >> 16) - c0);
-    const uint32_t first_valid = max(e_first, w_lo);
-    const uint32_t last_valid = min(e_first + kItemsPerThread, w_hi) - 1;
+    // no run ends in the lane: one column, its last entry not flagged
+    const bool single = any && !(ends & 1u);
+    const int hc = static_cast<int>(first_ent >> 16);  // the lane's first run
     // the lane continues the run of the entry before it unless that entry
     // ended its run (previous lane's last entry; last round's at lane 0)
+    const uint32_t first_valid = max(e_first, w_lo);
     const uint32_t prev_last = __shfl_up_sync(0xffffffffu, last_ent, 1);
     const bool cont_prev = any && first_valid > w_lo && (lane == 0 ? !prev_end : !(prev_last & 1u));
-    const bool cont_next = tail_open && last_valid + 1 < w_hi;
-    const int fc = rec.fc, lc = rec.lc;
-    auto sink = [&](int col, T val) {
-        if (col == fc)
-            rec.fs = val;
-        else if (col == lc)
-            rec.ls = val;
-        else
-            acc[col] += val;
-    };
+    auto sink = [&](int col, T val) { accc[col] += val; };
     if (__ballot_sync(0xffffffffu, single && cont_prev) == 0) {
-        // no lane is one run continued from its left: every cut run spans at
-        // most two lanes, one shuffle combines them
+        // no lane extends a run from its left: a chain is one lane's tail
         T prev_ts = __shfl_up_sync(0xffffffffu, sum, 1);
         if (lane == 0) prev_ts = carry;
-        if (any) {
-            if (single) {
-                if (!cont_next) sink(tc, sum);
-            } else {
-                sink(hc, cont_prev ? prev_ts + hs : hs);
-                if (tail_open && !cont_next) sink(tc, sum);
-            }
-        }
-        carry = __shfl_sync(0xffffffffu, sum, 31);
+        if (any && !single && cont_prev) sink(hc, prev_ts);
+        const int last = min(31, static_cast<int>((w_hi - 1 - round_start) / kItemsPerThread));  // last lane with entries
+        carry = __shfl_sync(0xffffffffu, sum, last);
     } else {
-        carry = lane_chain<T>(any, single, cont_prev, cont_next, tail_open, hc, tc, hs, sum, carry, sink);
+        carry = lane_chain<T>(any, single, cont_prev, hc, sum, carry, sink);
     }
     prev_end = (__shfl_sync(0xffffffffu, last_ent, 31) & 1u) != 0;
 }
@@ -902,21 +879,7 @@ __device__ __forceinline__ void reduce_block_entries(const uint32_t* __restrict_
         return max(e_lo, (e_lo + static_cast<uint32_t>(n * w / kWarps)) & ~3u);
     };
     const uint32_t w_lo = cut(warp), w_hi = cut(warp + 1);
-    WarpRec<T>& rec = recs[warp];
-    if (lane == 0) {
-        rec.valid = w_lo < w_hi;
-        rec.fs = rec.ls = T(0);
-        rec.fc = rec.lc = -1;
-        rec.cp = rec.cn = 0;
-        if (w_lo < w_hi) {
-            const uint32_t ef = g32[w_lo], el = g32[w_hi - 1];
-            rec.fc = static_cast<int>((ef >> 16) - c0);
-            rec.lc = static_cast<int>((el >> 16) - c0);
-            rec.cp = w_lo > e_lo && !(g32[w_lo - 1] & 1u);
-            rec.cn = !(el & 1u);
-        }
-    }
-    __syncwarp();
+    T* accc = acc - c0;  // indexed by an entry's column field
     T carry = 0;
     bool prev_end = true;
     const uint32_t round_len = 32 * kItemsPerThread;
@@ -950,7 +913,7 @@ __device__ __forceinline__ void reduce_block_entries(const uint32_t* __restrict_
 #pragma unroll
                 for (int q = 0; q < kLaneVecs; q++) cur[q] = src[q];
             }
-            warp_round<T>(g32, rs, w_lo, w_hi, c0, ytile, acc, carry, prev_end, rec, cur, full);
+            warp_round<T>(g32, rs, w_lo, w_hi, ytile, accc, carry, prev_end, cur, full);
         }
         cp_async_wait<0>();
     } else {
@@ -964,23 +927,34 @@ __device__ __forceinline__ void reduce_block_entries(const uint32_t* __restrict_
             uint32_t rn = rs + round_len;
             const bool fb = rn < w_hi && lane_full(rn + lane * kItemsPerThread, w_lo, w_hi);
             if (fb) load_lane(g32, rn + lane * kItemsPerThread, bb);
-            warp_round<T>(g32, rs, w_lo, w_hi, c0, ytile, acc, carry, prev_end, rec, ba, fa);
+            warp_round<T>(g32, rs, w_lo, w_hi, ytile, accc, carry, prev_end, ba, fa);
             rs = rn;
             if (rs >= w_hi) break;
             rn = rs + round_len;
             fa = rn < w_hi && lane_full(rn + lane * kItemsPerThread, w_lo, w_hi);
             if (fa) load_lane(g32, rn + lane * kItemsPerThread, ba);
-            warp_round<T>(g32, rs, w_lo, w_hi, c0, ytile, acc, carry, prev_end, rec, bb, fb);
+            warp_round<T>(g32, rs, w_lo, w_hi, ytile, accc, carry, prev_end, bb, fb);
             rs = rn;
+        }
+    }
+    if (lane == 0) {
+        WarpRec<T>& rec = recs[warp];
+        rec.valid = w_lo < w_hi;
+        rec.ls = carry;  // the chain still open at the range's end (0 if its last run ended)
+        rec.fc = rec.cp = rec.single = 0;
+        if (w_lo < w_hi) {
+            const uint32_t ef = g32[w_lo], el = g32[w_hi - 1];
+            rec.fc = static_cast<int>(ef >> 16);
+            rec.cp = w_lo > e_lo && !(g32[w_lo - 1] & 1u);
+            rec.single = ((ef ^ el) >> 16) == 0 && !(el & 1u);
         }
     }
     __syncthreads();
     if (warp == 0) {
         WarpRec<T> r{};  // lanes past the CTA's warps carry no range
         if (lane < kWarps) r = recs[lane];
-        const bool single = r.fc == r.lc;
-        lane_chain<T>(r.valid != 0, single, r.cp != 0, r.cn != 0, true, r.fc, r.lc, r.fs, single ? r.fs : r.ls, T(0),
-                      [&](int col, T val) { acc[col] += val; });
+        lane_chain<T>(r.valid != 0, r.single != 0, r.cp != 0, r.fc, r.ls, T(0),
+                      [&](int col, T val) { accc[col] += val; });
     }
 }
 
