@@ -68,8 +68,12 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--e2e-steps", type=int, default=None)
-    ap.add_argument("--workload", choices=["single", "batched"], default="single",
-                    help="single: the 20M-row fit; batched: 60 per-empty-count fits in one batched solve")
+    ap.add_argument("--workload", choices=["single", "batched", "evaluator"], default="single",
+                    help="single: the 20M-row fit; batched: 60 per-empty-count fits in one batched solve; "
+                         "evaluator: one training epoch of the differentiable evaluator")
+    ap.add_argument("--eval-rows", type=int, default=8_000_000, help="evaluator: training positions")
+    ap.add_argument("--eval-sample-batches", type=int, default=24,
+                    help="evaluator: minibatches of the bounded CPU sample")
     ap.add_argument("--problems", type=int, default=60, help="batched: problems (empty counts 1..problems)")
     return ap.parse_args(argv)
 
@@ -525,6 +529,157 @@ def run_ours_batched(args) -> dict | None:
     return result if rank == 0 else None
 
 
+EVAL_METRIC = "differentiable evaluator: seconds per training epoch (Huber+L2, Adam, batch 65536)"
+EVAL_EMPTIES = (10, 50)
+EVAL_BATCH = 65536
+EVAL_LR, EVAL_L2, EVAL_DELTA = 1e-2, 1e-4, 4.0
+
+
+def eval_config(rows: int) -> dict:
+    return {"workload": f"differentiable evaluator, 8-pattern expanded, {rows} positions (empties "
+                        f"{EVAL_EMPTIES[0]}..{EVAL_EMPTIES[1]}), one epoch of Adam (lr {EVAL_LR:g}) on mean "
+                        f"Huber (delta {EVAL_DELTA:g}) + L2 {EVAL_L2:g} over shuffled {EVAL_BATCH}-row minibatches",
+            "rows": rows, "batch": EVAL_BATCH, "l2": "inputs larger than L2 (CSR 3 GB; each kernel pass 1-2 GB)"}
+
+
+def run_ours_evaluator(args) -> dict | None:
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    import cassandra_b200 as cb
+    from cassandra_b200 import _lib as L
+    from cassandra_b200 import evaluator as ev
+
+    lib = cb.load()
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    seed = args.seed + 7919 * rank
+    R = args.eval_rows
+
+    pos = cb.generate_positions(seed, R, *EVAL_EMPTIES)
+    model = ev.PatternEvaluator(PATTERNS_8, pos, "expanded")
+    cols, K = model.indexer.index_space_size, model.indexer.nnz_per_row
+    target = cb.generate_targets(model.csr, seed).float()
+    trainer = ev.Trainer(model, target, batch=EVAL_BATCH, lr=EVAL_LR, l2=EVAL_L2, delta=EVAL_DELTA, seed=seed)
+    batches = trainer.batches
+    torch.cuda.synchronize()
+
+    # ---- the two kernels, every minibatch once per pass (a pass reads 1-2 GB > L2)
+    w = model.weight.detach()
+    g = torch.randn(max(r1 - r0 for r0, r1 in batches), dtype=torch.float32, device="cuda")
+    score = torch.empty_like(g)
+    grad = torch.empty(cols, dtype=torch.float32, device="cuda")
+
+    def one_pass(fn):
+        for r0, r1 in batches:
+            L.check(fn(model.csr.handle, r0, r1))
+
+    fwd = lambda h, r0, r1: lib.cas_eval_forward(h, r0, r1, C.c_void_p(w.data_ptr()), C.c_void_p(score.data_ptr()), sp)
+    bwd = lambda h, r0, r1: lib.cas_eval_backward(h, r0, r1, C.c_void_p(g.data_ptr()), C.c_void_p(grad.data_ptr()), sp)
+    kernels = {}
+    for name, fn, idx_bytes in (("eval_forward_f32", fwd, 2), ("eval_backward_f32", bwd, 4)):
+        one_pass(fn)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(3):
+            one_pass(fn)
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3 / (3 * len(batches))
+        by = (idx_bytes * K + 4) * R / len(batches) + 4 * cols  # per launch: entries + rows + the C-vector
+        kernels[name] = {"seconds": t, "bytes": by, "gbs": by / t / 1e9}
+    del g, score, grad
+
+    for _ in range(args.warmup):
+        trainer.epoch()
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.cas_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    losses = [trainer.epoch() for _ in range(args.steps)]
+    e1.record(stream)
+    e1.synchronize()
+    launches_host = lib.cas_kernel_launches() - launches0
+    clk = clocks.stop()
+    elapsed = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        dist.barrier()
+        t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    per_epoch = elapsed / args.steps
+    # graph replays launch the captured kernels without the host counter:
+    # three of ours (forward, A'y partials, partial sum) per minibatch
+    launches = launches_host + 3 * len(batches) * args.steps
+
+    # ---- end to end through the public API with host buffers: copy the
+    # positions and targets in, build the model, one epoch, read the loss
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 2))
+    pos_h = torch.empty((R, 2), dtype=torch.int64, pin_memory=True)
+    pos_h.copy_(pos)
+    tg_h = torch.empty(R, dtype=torch.float32, pin_memory=True)
+    tg_h.copy_(target)
+    del trainer, model, pos, target
+    torch.cuda.synchronize()
+    e2e_times = []
+    for _ in range(e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p_d = pos_h.to("cuda", non_blocking=True)
+        t_d = tg_h.to("cuda", non_blocking=True)
+        m = ev.PatternEvaluator(PATTERNS_8, p_d, "expanded")
+        tr = ev.Trainer(m, t_d, batch=EVAL_BATCH, lr=EVAL_LR, l2=EVAL_L2, delta=EVAL_DELTA, seed=seed)
+        tr.epoch()  # ends with the loss read
+        e2e_times.append(time.perf_counter() - t0)
+        del tr, m, p_d, t_d
+    e2e_val = statistics.mean(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_val], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = float(t.item())
+
+    peak, peak_kind = measured_peaks()
+    dom = max(kernels, key=lambda k: kernels[k]["seconds"])
+    ach = kernels[dom]["gbs"]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_evaluator(args, seed, len(batches))
+    result = {
+        "metric": EVAL_METRIC, "value": per_epoch, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_epoch * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded random-play positions, seeded targets; random-init weights)",
+        "config": {**eval_config(R), "cols": cols, "nnz_per_row": K, "minibatches": len(batches),
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "breakdown": {"epoch_losses": losses, "batch_step_us": per_epoch / len(batches) * 1e6,
+                      "graphs": len(batches)},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": ach / peak, "peak_kind": peak_kind, "traffic": None},
+        "kernels": kernels,
+        "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": int(pos_h.numel() * 8 + tg_h.numel() * 4),
+                "d2h_bytes_per_step": 4, "steps": e2e_steps,
+                "includes": "H2D of positions and targets, model build (indexing, blocked CSR), graph capture, "
+                            "one epoch, loss read"},
+        "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": cpu,
+    }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result if rank == 0 else None
+
+
 # ---------------------------------------------------------------- CPU reference
 
 class ReferenceSample:
@@ -618,6 +773,58 @@ def cpu_baseline_batched(args, seed: int, rows, empties) -> dict | None:
                       f"x{total / done_rows:.3g}"}
 
 
+def cpu_baseline_evaluator(args, seed: int, batches_per_epoch: int) -> dict | None:
+    """The same training step on the host cores with the reference's own
+    products (MatrixCSR * Vector and Vector * MatrixCSR, Math/MatrixCSR.cpp:
+    49-87, OpenMP) on a bounded sample of minibatches, the loss, its
+    gradient and Adam in numpy; the time per minibatch scaled to an epoch.
+    Indexing and the per-minibatch MatrixCSR are prepared untimed, as the
+    GPU arm prepares its CSR before the epoch."""
+    try:
+        import oracle
+
+        if not oracle.ref_available():
+            return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+                    "sample": "unavailable: oracle/_ref not built"}
+    except Exception as e:  # pragma: no cover
+        return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference", "sample": f"error {e}"}
+    nb = max(1, min(args.eval_sample_batches, batches_per_epoch))
+    rows = nb * EVAL_BATCH
+    smp = ReferenceSample(rows, seed, *EVAL_EMPTIES)
+    lib, cols, k = smp.ref, smp.cols, 64
+    target = smp.b.astype(np.float32)
+    mats = [lib.ref_csr_new(k, EVAL_BATCH, cols, smp.idx[i * EVAL_BATCH:].ctypes.data_as(C.c_void_p))
+            for i in range(nb)]
+    w = np.zeros(cols, np.float32)
+    m1, m2 = np.zeros_like(w), np.zeros_like(w)
+    score, grad = np.empty(EVAL_BATCH, np.float32), np.empty(cols, np.float32)
+    b1, b2, eps = 0.9, 0.999, 1e-8
+    order = np.random.default_rng(seed).permutation(nb)
+    try:
+        t0 = time.perf_counter()
+        for step, i in enumerate(order, 1):
+            lib.ref_csr_mul(mats[i], w.ctypes.data_as(C.c_void_p), score.ctypes.data_as(C.c_void_p))
+            d = score - target[i * EVAL_BATCH:(i + 1) * EVAL_BATCH]
+            ad = np.abs(d)
+            _loss = float(np.mean(np.where(ad <= EVAL_DELTA, 0.5 * d * d, EVAL_DELTA * (ad - 0.5 * EVAL_DELTA)))
+                          + EVAL_L2 * np.dot(w, w))
+            dsc = (np.clip(d, -EVAL_DELTA, EVAL_DELTA) / EVAL_BATCH).astype(np.float32)
+            lib.ref_csr_tmul(mats[i], dsc.ctypes.data_as(C.c_void_p), grad.ctypes.data_as(C.c_void_p))
+            grad += (2 * EVAL_L2) * w
+            m1 = b1 * m1 + (1 - b1) * grad
+            m2 = b2 * m2 + (1 - b2) * grad * grad
+            w -= (EVAL_LR / (1 - b1 ** step)) * m1 / (np.sqrt(m2 / (1 - b2 ** step)) + eps)
+        per_batch = (time.perf_counter() - t0) / nb
+    finally:
+        for m in mats:
+            lib.ref_csr_free(m)
+    return {"value": per_batch * batches_per_epoch, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"{nb} of {batches_per_epoch} minibatches of {EVAL_BATCH} rows (same generator; reference "
+                      f"indexing and MatrixCSR built untimed); per minibatch the reference's A*w and g*A plus numpy "
+                      f"Huber/Adam, {per_batch * 1e3:.1f} ms; time scaled to the epoch; OpenMP threads "
+                      f"{os.environ.get('OMP_NUM_THREADS', os.cpu_count())}"}
+
+
 def run_reference(args) -> dict | None:
     world, rank, _ = dist_env()
     if rank != 0:
@@ -627,6 +834,23 @@ def run_reference(args) -> dict | None:
     if not oracle.ref_available():
         return {"impl": "reference", "metric": METRIC,
                 "unavailable": "oracle/_ref (reference sources compiled here) is missing"}
+    if args.workload == "evaluator":
+        nbatch = -(-args.eval_rows // EVAL_BATCH)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            cbl = cpu_baseline_evaluator(args, args.seed, nbatch)
+            if i >= args.warmup:
+                vals.append(cbl["value"])
+        value = statistics.mean(vals)
+        cbl["value"] = value
+        return {
+            "impl": "reference", "metric": EVAL_METRIC, "value": value, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random-play positions, seeded targets)", "config": eval_config(args.eval_rows),
+            "cpu_baseline": cbl,
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
     if args.workload == "batched":
         rows, empties = batched_problems(args.seed, args.problems)
         vals = []
@@ -676,6 +900,8 @@ def main(argv=None) -> int:
         res = run_reference(args)
     elif args.workload == "batched":
         res = run_ours_batched(args)
+    elif args.workload == "evaluator":
+        res = run_ours_evaluator(args)
     else:
         res = run_ours(args)
     if res is not None:

@@ -13,6 +13,13 @@ Minibatches are whole 16384-row blocks (``cas_block_rows``): batch membership
 is fixed and the batch order is shuffled per epoch, so every batch's
 transposed copy exists before training starts.  This is the Python side where
 the reference's NeuralNetwork/ code trains value models.
+
+``Trainer`` runs Adam on the Huber + L2 objective.  By default each batch's
+whole step (forward kernel, loss and its gradient, adjoint kernel, L2 term,
+fused Adam) is captured once as a CUDA graph, and an epoch replays the
+graphs in that epoch's shuffled order with one device-to-host read (the
+epoch's loss) at its end; ``graphs=False`` runs the same step through
+autograd and ``EvaluatorFunction``.
 """
 from __future__ import annotations
 
@@ -81,27 +88,102 @@ def objective(score: torch.Tensor, target: torch.Tensor, w: torch.Tensor, delta:
     return torch.nn.functional.huber_loss(score, target, delta=delta) + l2 * torch.dot(w, w)
 
 
+class Trainer:
+    """Adam (lr, fused) on mean Huber(delta) + l2 ||w||^2 over the model's
+    fixed minibatches of about `batch` rows; every epoch() shuffles the batch
+    order (torch.Generator seeded with `seed`) and returns the mean batch
+    loss.  graphs=True: each batch's step is one CUDA graph (captured at
+    construction; the weights and the optimizer state are left as they were
+    before the capture), replayed in the epoch's order."""
+
+    def __init__(self, model: PatternEvaluator, target: torch.Tensor, batch: int = 65536, lr: float = 1e-2,
+                 l2: float = 1e-4, delta: float = 4.0, seed: int = 0, graphs: bool = True):
+        self.model = model
+        self.target = target.to(torch.float32).contiguous()
+        if self.target.numel() != model.rows:
+            raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+        self.l2, self.delta = float(l2), float(delta)
+        self.batches = model.batches(batch)
+        self.gen = torch.Generator().manual_seed(seed)
+        self.graphs = None
+        w = model.weight
+        if not graphs:
+            self.opt = torch.optim.Adam([w], lr=lr, fused=True)
+            return
+        self.opt = torch.optim.Adam([w], lr=lr, fused=True, capturable=True)
+        dev = w.device
+        nmax = max(r1 - r0 for r0, r1 in self.batches)
+        self._score = torch.empty(nmax, dtype=torch.float32, device=dev)
+        self._grad = torch.zeros_like(w)
+        self._loss_sum = torch.zeros((), dtype=torch.float32, device=dev)
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side), torch.no_grad():
+            # first uses outside the capture: the adjoint's partial buffer for
+            # the largest batch, and Adam's state (a zero-gradient step leaves
+            # the weights as they are; its step count is reset below)
+            big = max(range(len(self.batches)), key=lambda i: self.batches[i][1] - self.batches[i][0])
+            self._step(big)
+            self._grad.zero_()
+            w.grad = self._grad
+            self.opt.step()
+            for st in self.opt.state[w].values():
+                if torch.is_tensor(st):
+                    st.zero_()
+            self._loss_sum.zero_()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        torch.cuda.synchronize(dev)
+        pool = torch.cuda.graph_pool_handle()  # shared: the graphs replay one at a time
+        self.graphs = []
+        with torch.no_grad():
+            for i in range(len(self.batches)):
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, pool=pool):
+                    self._step(i)
+                    w.grad = self._grad
+                    self.opt.step()
+                self.graphs.append(g)
+
+    def _step(self, i: int):
+        """Loss and gradient of batch i into _loss_sum (added) and _grad, on
+        the current stream, without autograd."""
+        r0, r1 = self.batches[i]
+        n = r1 - r0
+        w = self.model.weight
+        score = self._score[:n]
+        stream = _stream()
+        L.check(L.load().cas_eval_forward(self.model.csr.handle, r0, r1, _ptr(w), _ptr(score), stream))
+        t = self.target[r0:r1]
+        self._loss_sum.add_(objective(score, t, w.detach(), self.delta, self.l2))
+        # d/dscore of the mean Huber loss, then the adjoint, then the L2 term
+        dscore = (score - t).clamp_(-self.delta, self.delta).mul_(1.0 / n)
+        L.check(L.load().cas_eval_backward(self.model.csr.handle, r0, r1, _ptr(dscore), _ptr(self._grad), stream))
+        self._grad.add_(w.detach(), alpha=2.0 * self.l2)
+
+    def epoch(self) -> float:
+        order = torch.randperm(len(self.batches), generator=self.gen).tolist()
+        if self.graphs is not None:
+            self._loss_sum.zero_()
+            for i in order:
+                self.graphs[i].replay()
+            return float(self._loss_sum) / len(self.batches)
+        model, total = self.model, torch.zeros((), dtype=torch.float32, device=self.model.weight.device)
+        for i in order:
+            r0, r1 = self.batches[i]
+            self.opt.zero_grad(set_to_none=True)
+            loss = objective(model(r0, r1), self.target[r0:r1], model.weight, self.delta, self.l2)
+            loss.backward()
+            self.opt.step()
+            total += loss.detach()
+        return float(total) / len(self.batches)
+
+
 def train(model: PatternEvaluator, target: torch.Tensor, epochs: int = 5, batch: int = 65536, lr: float = 1e-2,
-          l2: float = 1e-4, delta: float = 4.0, seed: int = 0) -> list[float]:
+          l2: float = 1e-4, delta: float = 4.0, seed: int = 0, graphs: bool = True) -> list[float]:
     """Adam on the Huber + L2 objective over fixed minibatches whose order is
     shuffled every epoch.  Returns the mean batch loss of every epoch."""
-    target = target.to(torch.float32)
-    opt = torch.optim.Adam(model.parameters(), lr=lr)
-    gen = torch.Generator().manual_seed(seed)
-    batches = model.batches(batch)
-    history = []
-    for _ in range(epochs):
-        order = torch.randperm(len(batches), generator=gen).tolist()
-        total = 0.0
-        for i in order:
-            r0, r1 = batches[i]
-            opt.zero_grad(set_to_none=True)
-            loss = objective(model(r0, r1), target[r0:r1], model.weight, delta, l2)
-            loss.backward()
-            opt.step()
-            total += float(loss.detach())
-        history.append(total / len(batches))
-    return history
+    t = Trainer(model, target, batch=batch, lr=lr, l2=l2, delta=delta, seed=seed, graphs=graphs)
+    return [t.epoch() for _ in range(epochs)]
 
 
 def full_objective(model: PatternEvaluator, target: torch.Tensor, w: torch.Tensor | None = None,
@@ -131,6 +213,6 @@ def central_difference(model: PatternEvaluator, target: torch.Tensor, coords: to
     return out
 
 
-__all__ = ["EvaluatorFunction", "PatternEvaluator", "train", "objective", "full_objective", "central_difference",
-           "block_rows"]
+__all__ = ["EvaluatorFunction", "PatternEvaluator", "Trainer", "train", "objective", "full_objective",
+           "central_difference", "block_rows"]
 _ = math

@@ -113,6 +113,13 @@ def ref_lib() -> C.CDLL:
         for n in ("ref_spmv", "ref_spmv_t"):
             getattr(lib, n).restype = None
             getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, _VP]
+        lib.ref_csr_new.restype = _VP
+        lib.ref_csr_new.argtypes = [C.c_int, _I64, _I64, _VP]
+        lib.ref_csr_free.restype = None
+        lib.ref_csr_free.argtypes = [_VP]
+        for n in ("ref_csr_mul", "ref_csr_tmul"):
+            getattr(lib, n).restype = None
+            getattr(lib, n).argtypes = [_VP, _VP, _VP]
         lib.ref_jacobi.restype = None
         lib.ref_jacobi.argtypes = [C.c_int, _I64, _I64, _VP, _VP]
         for n in ("ref_pcg", "ref_lsqr", "ref_lsmr"):

@@ -172,6 +172,31 @@ void ref_spmv_t(int k, int64_t rows, int64_t cols, const uint32_t* idx, const fl
     std::memcpy(x, r.data(), sizeof(float) * cols);
 }
 
+// A MatrixCSR kept across calls (one per minibatch of the evaluator's CPU
+// baseline), and the same two products on it.
+void* ref_csr_new(int k, int64_t rows, int64_t cols, const uint32_t* idx)
+{
+    return new MatrixCSR(make_csr(k, rows, cols, idx));
+}
+
+void ref_csr_free(void* m) { delete static_cast<MatrixCSR*>(m); }
+
+// Math/MatrixCSR.cpp:49-65
+void ref_csr_mul(const void* pm, const float* x, float* y)
+{
+    const MatrixCSR& m = *static_cast<const MatrixCSR*>(pm);
+    Vector r = m * Vector(x, x + m.Cols());
+    std::memcpy(y, r.data(), sizeof(float) * m.Rows());
+}
+
+// Math/MatrixCSR.cpp:67-87
+void ref_csr_tmul(const void* pm, const float* y, float* x)
+{
+    const MatrixCSR& m = *static_cast<const MatrixCSR*>(pm);
+    Vector r = Vector(y, y + m.Rows()) * m;
+    std::memcpy(x, r.data(), sizeof(float) * m.Cols());
+}
+
 // Math/MatrixCSR.cpp:21-47
 void ref_jacobi(int k, int64_t rows, int64_t cols, const uint32_t* idx, float* d)
 {

@@ -106,3 +106,23 @@ def test_training_reduces_loss_towards_least_squares(cuda, orc, setup):
     # Adam on Huber+L2 for 5 epochs lands in the same range as the
     # least-squares optimum evaluated on the same objective
     assert after <= 3.0 * ls_obj + 1.0, (after, ls_obj)
+
+
+def test_graph_trainer_matches_autograd(cuda):
+    """The CUDA-graph training step (manual loss gradient, the same kernels,
+    fused Adam) follows the autograd step through EvaluatorFunction, batch
+    order included; a ragged last batch (a partial block) is part of it."""
+    rows = 6 * BR + 1000
+    pos = cb.generate_positions(46, rows, 10, 50)
+    g = cb.GroupIndexer(SET8, "expanded")
+    target = cb.generate_targets(cb.MatrixCSR.from_positions(g, pos, "rows"), 46).float()
+    m_auto = ev.PatternEvaluator(SET8, pos, "expanded")
+    m_graph = ev.PatternEvaluator(SET8, pos, "expanded")
+    h_auto = ev.train(m_auto, target, epochs=3, batch=2 * BR, seed=3, graphs=False)
+    t = ev.Trainer(m_graph, target, batch=2 * BR, seed=3)
+    assert len(t.graphs) == len(t.batches) == 4
+    assert torch.count_nonzero(m_graph.weight) == 0  # capture changed nothing
+    h_graph = [t.epoch() for _ in range(3)]
+    np.testing.assert_allclose(h_graph, h_auto, rtol=1e-4)
+    torch.testing.assert_close(m_graph.weight.detach(), m_auto.weight.detach(), rtol=1e-3, atol=1e-4)
+    assert h_graph[-1] < h_graph[0]
