@@ -596,7 +596,26 @@ def run_ours_evaluator(args) -> dict | None:
         t = e0.elapsed_time(e1) * 1e-3 / (3 * len(batches))
         by = (idx_bytes * K + 4) * R / len(batches) + 4 * cols  # per launch: entries + rows + the C-vector
         kernels[name] = {"seconds": t, "bytes": by, "gbs": by / t / 1e9}
-    del g, score, grad
+    # the whole training step (three kernels) eagerly, every minibatch once
+    # per pass, on scratch weights and moments
+    ws, ms, vs = w.clone(), torch.zeros_like(w), torch.zeros_like(w)
+    st = torch.zeros((), dtype=torch.int64, device="cuda")
+    ls = torch.zeros((), dtype=torch.float64, device="cuda")
+    step_fn = lambda h, r0, r1: lib.cas_eval_adam_step(
+        h, r0, r1, C.c_void_p(target[r0:r1].data_ptr()), C.c_void_p(ws.data_ptr()), C.c_void_p(ms.data_ptr()),
+        C.c_void_p(vs.data_ptr()), C.c_void_p(st.data_ptr()), C.c_void_p(ls.data_ptr()), C.byref(trainer.opts), sp)
+    one_pass(step_fn)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(3):
+        one_pass(step_fn)
+    e1.record(stream)
+    e1.synchronize()
+    t_step = e0.elapsed_time(e1) * 1e-3 / (3 * len(batches))
+    by_step = (6 * K + 4) * R / len(batches) + 24 * cols  # A16 + G32 + targets; w, m, v read and written
+    train_step = {"seconds": t_step, "bytes": by_step, "gbs": by_step / t_step / 1e9, "kernels": 3}
+    del g, score, grad, ws, ms, vs, st, ls
 
     for _ in range(args.warmup):
         trainer.epoch()
@@ -621,7 +640,7 @@ def run_ours_evaluator(args) -> dict | None:
         elapsed = float(t.item())
     per_epoch = elapsed / args.steps
     # graph replays launch the captured kernels without the host counter:
-    # three of ours (forward, A'y partials, partial sum) per minibatch
+    # three of ours (forward with the loss, A'y partials, Adam epilogue) per minibatch
     launches = launches_host + 3 * len(batches) * args.steps
 
     # ---- end to end through the public API with host buffers: copy the
@@ -664,7 +683,7 @@ def run_ours_evaluator(args) -> dict | None:
         "config": {**eval_config(R), "cols": cols, "nnz_per_row": K, "minibatches": len(batches),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "breakdown": {"epoch_losses": losses, "batch_step_us": per_epoch / len(batches) * 1e6,
-                      "graphs": len(batches)},
+                      "graphs": len(batches), "train_step_eager": train_step},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                      "frac": ach / peak, "peak_kind": peak_kind, "traffic": None},
         "kernels": kernels,

@@ -65,6 +65,18 @@ class SolveReport(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class AdamOpts(C.Structure):
+    """cas_adam_opts: Adam hyperparameters and the objective's L2 weight and Huber threshold."""
+    _fields_ = [
+        ("lr", C.c_float),
+        ("beta1", C.c_float),
+        ("beta2", C.c_float),
+        ("eps", C.c_float),
+        ("l2", C.c_float),
+        ("delta", C.c_float),
+    ]
+
+
 class Schedule(C.Structure):
     _fields_ = [
         ("chunks_per_item", C.c_int),
@@ -116,6 +128,7 @@ SIGNATURES: dict[str, tuple] = {
     "cas_block_rows": (_I64, []),
     "cas_eval_forward": (C.c_int, [_VP, _I64, _I64, _VP, _VP, _VP]),
     "cas_eval_backward": (C.c_int, [_VP, _I64, _I64, _VP, _VP, _VP]),
+    "cas_eval_adam_step": (C.c_int, [_VP, _I64, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "cas_csr_from_indices": (C.c_int, [_VP, C.c_int, _I64, _I64, _VP, _PP]),
     "cas_csr_destroy": (None, [_VP]),
     "cas_csr_rows": (_I64, [_VP]),

@@ -694,6 +694,28 @@ CAS_API cas_status cas_eval_backward(const cas_csr* a, int64_t row0, int64_t row
     return fast_eval_backward(*a->fast, b0, b1, d_g, d_grad, static_cast<cudaStream_t>(stream));
 }
 
+CAS_API cas_status cas_eval_adam_step(const cas_csr* a, int64_t row0, int64_t row1, const float* d_target,
+                                      float* d_w, float* d_m, float* d_v, int64_t* d_step, double* d_loss_sum,
+                                      const cas_adam_opts* opts, void* stream)
+{
+    CAS_REQUIRE(a && a->fast, CAS_ERR_INVALID_ARGUMENT, "cas_eval_adam_step: the CSR needs the blocked layout");
+    CAS_REQUIRE(a->fast->g.nprob == 1, CAS_ERR_INVALID_ARGUMENT,
+                "cas_eval_adam_step: needs the layout of a single fit, not a batch");
+    CAS_REQUIRE(0 <= row0 && row0 <= row1 && row1 <= a->rows, CAS_ERR_SIZE_MISMATCH,
+                "cas_eval_adam_step: row range outside the matrix");
+    CAS_REQUIRE(row0 % kBlockRows == 0 && (row1 % kBlockRows == 0 || row1 == a->rows), CAS_ERR_INVALID_ARGUMENT,
+                "cas_eval_adam_step: the row range must start and end on block boundaries (cas_block_rows())");
+    CAS_REQUIRE(opts, CAS_ERR_INVALID_ARGUMENT, "cas_eval_adam_step: null options");
+    CAS_REQUIRE(row1 == row0 || (d_target && d_w && d_m && d_v && d_step && d_loss_sum), CAS_ERR_INVALID_ARGUMENT,
+                "cas_eval_adam_step: null buffer");
+    CAS_REQUIRE(opts->lr >= 0 && opts->beta1 >= 0 && opts->beta1 < 1 && opts->beta2 >= 0 && opts->beta2 < 1 &&
+                    opts->eps > 0 && opts->l2 >= 0 && opts->delta > 0,
+                CAS_ERR_INVALID_ARGUMENT, "cas_eval_adam_step: bad options");
+    const EvalAdam o{opts->lr, opts->beta1, opts->beta2, opts->eps, opts->l2, opts->delta};
+    return fast_eval_adam_step(*a->fast, row0, row1, d_target, d_w, d_m, d_v, d_step, d_loss_sum, o,
+                               static_cast<cudaStream_t>(stream));
+}
+
 CAS_API cas_status cas_csr_from_indices(const uint32_t* d_indices, int nnz_per_row, int64_t rows, int64_t cols,
                                         void* stream, cas_csr** out)
 {

@@ -1151,6 +1151,89 @@ __global__ void block_partial_sum_kernel(const float* __restrict__ partial, int 
     }
 }
 
+// Forward of a training step fused with its loss: per row the score (as in
+// fast_rows_forward_kernel), d = score - target, the Huber loss of d summed
+// per CTA into red[blockIdx.x] (FP64, deterministic tree), and the loss
+// gradient dscore = clamp(d, -delta, delta) / n for the adjoint.
+__global__ void __launch_bounds__(256) eval_loss_grad_kernel(FastGeometry g, const uint16_t* __restrict__ a16,
+                                                             const float* __restrict__ w,
+                                                             const float* __restrict__ target, int64_t row0,
+                                                             int64_t row1, float delta, float inv_n,
+                                                             float* __restrict__ dscore, double* __restrict__ red)
+{
+    __shared__ double smem[32];
+    double hs = 0;
+    for (int64_t r = row0 + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < row1;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        int64_t b, rb;
+        g.locate_row(r, b, rb);
+        const float* wq = w + g.col_base(b);
+        float acc = 0;
+        for (int p = 0; p < g.npat; p++)
+            gather_row<float>(a16 + g.seg(b, p) + rb * g.slots[p], g.slots[p], wq + g.off[p], wq + g.off[p], 0, false,
+                              acc);
+        const float d = acc - target[r - row0];
+        const float ad = fabsf(d);
+        hs += ad < delta ? 0.5f * d * d : delta * (ad - 0.5f * delta);
+        dscore[r - row0] = fminf(fmaxf(d, -delta), delta) * inv_n;
+    }
+    const double t = block_sum<256>(hs, smem);
+    if (threadIdx.x == 0) red[blockIdx.x] = t;
+}
+
+// Epilogue of a training step, per column c: the gradient g = sum of the
+// adjoint's block partials (block order) + 2 l2 w, then Adam on w, m, v with
+// the step t = *step + 1 (torch.optim.Adam's update: m += (1 - b1)(g - m),
+// v = b2 v + (1 - b2) g^2, w -= lr / (1 - b1^t) * m / (sqrt(v) / sqrt(1 -
+// b2^t) + eps)).  ||w||^2 before the update is summed per CTA; the last CTA
+// (integer counter) adds the step's loss, sum(Huber)/n + l2 ||w||^2, to
+// *loss_sum, stores t and resets the counter.
+__global__ void __launch_bounds__(256) eval_adam_kernel(const float* __restrict__ partial, int nb, int64_t cols,
+                                                        float* __restrict__ w, float* __restrict__ m,
+                                                        float* __restrict__ v, int64_t* __restrict__ step,
+                                                        double* __restrict__ loss_sum, double* __restrict__ red,
+                                                        int nred, int* __restrict__ ctr, EvalAdam o, double inv_n)
+{
+    __shared__ double smem[32];
+    __shared__ int last;
+    const int64_t t = *step + 1;  // read by every CTA before the last one stores t
+    const float step_size = static_cast<float>(o.lr / (1.0 - pow(static_cast<double>(o.beta1), static_cast<double>(t))));
+    const float bc2_sqrt = static_cast<float>(sqrt(1.0 - pow(static_cast<double>(o.beta2), static_cast<double>(t))));
+    double wsq = 0;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cols;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        float gc = 0;
+        for (int j = 0; j < nb; j++) gc += partial[static_cast<int64_t>(j) * cols + c];
+        const float wc = w[c];
+        wsq += static_cast<double>(wc) * wc;
+        gc += (2.0f * o.l2) * wc;
+        float mc = m[c];
+        mc += (1.0f - o.beta1) * (gc - mc);
+        const float vc = o.beta2 * v[c] + (1.0f - o.beta2) * gc * gc;
+        const float denom = sqrtf(vc) / bc2_sqrt + o.eps;
+        w[c] = wc - step_size * (mc / denom);
+        m[c] = mc;
+        v[c] = vc;
+    }
+    const double s = block_sum<256>(wsq, smem);
+    if (threadIdx.x == 0) {
+        red[kEvalRedMax + blockIdx.x] = s;
+        __threadfence();
+        last = atomicAdd(ctr, 1) == static_cast<int>(gridDim.x) - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double hsum = 0, ws = 0;
+        for (int i = 0; i < nred; i++) hsum += __ldcg(red + i);
+        for (int i = 0; i < static_cast<int>(gridDim.x); i++) ws += __ldcg(red + kEvalRedMax + i);
+        *loss_sum += hsum * inv_n + static_cast<double>(o.l2) * ws;
+        *step = t;
+        *ctr = 0;
+        __threadfence();
+    }
+}
+
 template <typename T>
 __global__ void fast_col_sum_kernel(FastCols fc, const T* __restrict__ partial, T* __restrict__ x)
 {
@@ -1583,6 +1666,9 @@ void fast_free(FastLayout& f)
     free_transpose(f.t64);
     free_transpose(f.tb);
     dfree(f.eval_partial);
+    dfree(f.eval_dscore);
+    dfree(f.eval_red);
+    dfree(f.eval_ctr);
     f = FastLayout{};
 }
 
@@ -1798,6 +1884,45 @@ cas_status fast_eval_forward(const FastLayout& f, int64_t row0, int64_t row1, co
     return CAS_OK;
 }
 
+// The evaluator's per-call buffers for adjoints over nb blocks (grown, never
+// shrunk; growing waits for the stream, so the first call of the largest
+// size must come before any graph capture).
+static cas_status eval_buffers(FastLayout& f, int64_t nb, cudaStream_t s)
+{
+    if (nb > f.eval_blocks) {
+        if (f.eval_partial || f.eval_dscore) {
+            CAS_CUDA(cudaStreamSynchronize(s));
+            dfree(f.eval_partial);
+            dfree(f.eval_dscore);
+            f.eval_partial = nullptr;
+            f.eval_dscore = nullptr;
+            f.eval_blocks = 0;
+        }
+        CAS_CUDA(dmalloc(&f.eval_partial, sizeof(float) * nb * f.g.cols));
+        CAS_CUDA(dmalloc(&f.eval_dscore, sizeof(float) * nb * kBlockRows));
+        f.eval_blocks = nb;
+    }
+    if (!f.eval_red) {
+        CAS_CUDA(dmalloc(&f.eval_red, sizeof(double) * 2 * kEvalRedMax));
+        CAS_CUDA(dmalloc(&f.eval_ctr, sizeof(int)));
+        CAS_CUDA(cudaMemsetAsync(f.eval_ctr, 0, sizeof(int), s));
+    }
+    return CAS_OK;
+}
+
+// The adjoint's per-block partials of blocks [b0, b1) on g into eval_partial.
+static cas_status eval_adjoint_partials(FastLayout& f, int64_t b0, int64_t b1, const float* g, cudaStream_t s)
+{
+    const size_t smem = spmv_t_smem<float>(1, false);
+    const int items = static_cast<int>((b1 - b0) * f.g.nchunks);
+    { fast_spmv_t_kernel<float, false><<<items, kFastThreads, smem, s>>>(f.g, tview(f.tb), f.g32, f.sub_start, g,
+                                                                 f.eval_partial, nullptr,
+                                                                 static_cast<int>(b0 * f.g.nchunks), b0, nullptr,
+                                                                 nullptr, nullptr, 1); cas::count_launch(); }
+    CAS_CHECK_LAUNCH();
+    return CAS_OK;
+}
+
 cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float* g, float* grad, cudaStream_t s)
 {
     const int64_t nb = b1 - b0;
@@ -1806,24 +1931,30 @@ cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float
         CAS_CUDA(cudaMemsetAsync(grad, 0, sizeof(float) * f.g.cols, s));
         return CAS_OK;
     }
-    if (nb > f.eval_blocks) {
-        if (f.eval_partial) {
-            CAS_CUDA(cudaStreamSynchronize(s));
-            dfree(f.eval_partial);
-            f.eval_partial = nullptr;
-        }
-        CAS_CUDA(dmalloc(&f.eval_partial, sizeof(float) * nb * f.g.cols));
-        f.eval_blocks = nb;
-    }
-    const size_t smem = spmv_t_smem<float>(1, false);
-    const int items = static_cast<int>(nb * f.g.nchunks);
-    { fast_spmv_t_kernel<float, false><<<items, kFastThreads, smem, s>>>(f.g, tview(f.tb), f.g32, f.sub_start, g,
-                                                                 f.eval_partial, nullptr,
-                                                                 static_cast<int>(b0 * f.g.nchunks), b0, nullptr,
-                                                                 nullptr, nullptr, 1); cas::count_launch(); }
-    CAS_CHECK_LAUNCH();
+    CAS_TRY(eval_buffers(f, nb, s));
+    CAS_TRY(eval_adjoint_partials(f, b0, b1, g, s));
     { block_partial_sum_kernel<<<fgrid(f.g.cols, 256), 256, 0, s>>>(f.eval_partial, static_cast<int>(nb), f.g.cols,
                                                                   grad); cas::count_launch(); }
+    CAS_CHECK_LAUNCH();
+    return CAS_OK;
+}
+
+cas_status fast_eval_adam_step(FastLayout& f, int64_t row0, int64_t row1, const float* target, float* w, float* m,
+                               float* v, int64_t* step, double* loss_sum, const EvalAdam& o, cudaStream_t s)
+{
+    const int64_t n = row1 - row0;
+    const int64_t b0 = row0 / kBlockRows, b1 = (row1 + kBlockRows - 1) / kBlockRows;
+    if (f.g.cols == 0 || n <= 0) return CAS_OK;
+    CAS_TRY(eval_buffers(f, b1 - b0, s));
+    const unsigned g1 = std::min<unsigned>(fgrid(n, 256) * 4, kEvalRedMax);
+    { eval_loss_grad_kernel<<<g1, 256, 0, s>>>(f.g, f.a16, w, target, row0, row1, o.delta, 1.0f / static_cast<float>(n),
+                                               f.eval_dscore, f.eval_red); cas::count_launch(); }
+    CAS_CHECK_LAUNCH();
+    CAS_TRY(eval_adjoint_partials(f, b0, b1, f.eval_dscore, s));
+    const unsigned g3 = std::min<unsigned>(fgrid(f.g.cols, 256), kEvalRedMax);
+    { eval_adam_kernel<<<g3, 256, 0, s>>>(f.eval_partial, static_cast<int>(b1 - b0), f.g.cols, w, m, v, step,
+                                          loss_sum, f.eval_red, static_cast<int>(g1), f.eval_ctr, o,
+                                          1.0 / static_cast<double>(n)); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     return CAS_OK;
 }

@@ -30,6 +30,7 @@ constexpr int kAxAhead = 3;              // index loads in flight per thread in 
 constexpr int kChunkCols = 8192;         // column chunk of the A'y accumulators
 constexpr int kSubCols = 1024;           // column sub-chunk: the finest split of an A'y item
 constexpr int kSubPerChunk = kChunkCols / kSubCols;
+constexpr int kEvalRedMax = 4096;        // CTAs of each reduction of an evaluator training step
 constexpr int kAxSplitMax = 32;          // most CTAs sharing one block's rows in A x
 constexpr int kAxDirectRows = kAxThreads / 2;  // rows of a unit that gathers x without staging (one thread a row)
 static_assert(kBlockRows / kAxSplitMax <= kAxDirectRows, "a block split kAxSplitMax ways must fit the direct path");
@@ -190,7 +191,16 @@ struct FastLayout {
     FastTranspose t32, t64;            // A'y work lists of the solvers (FP32, FP64)
     FastTranspose tb;                  // one item per (block, chunk): adjoints over block ranges
     float* eval_partial = nullptr;     // [blocks][cols] partials of the last adjoint
-    int64_t eval_blocks = 0;
+    float* eval_dscore = nullptr;      // [blocks * kBlockRows] loss gradient of a training step's rows
+    int64_t eval_blocks = 0;           // blocks the two buffers above hold
+    double* eval_red = nullptr;        // [2 * kEvalRedMax] per-CTA loss partials of a training step
+    int* eval_ctr = nullptr;           // last-CTA counter of the training step's epilogue
+};
+
+// Hyperparameters of one training step of the evaluator (Adam as
+// torch.optim.Adam without weight decay; mean Huber loss plus l2 ||w||^2).
+struct EvalAdam {
+    float lr, beta1, beta2, eps, l2, delta;
 };
 
 // Device view used by the column reductions of the solver.
@@ -275,6 +285,12 @@ cas_status fast_diag(const FastLayout& f, uint64_t* diag, cudaStream_t s);
 cas_status fast_eval_forward(const FastLayout& f, int64_t row0, int64_t row1, const float* w, float* score,
                              cudaStream_t s);
 cas_status fast_eval_backward(FastLayout& f, int64_t b0, int64_t b1, const float* g, float* grad, cudaStream_t s);
+// One training step on rows [row0, row1) (block bounds; row1 may be the last
+// row): three kernels — forward with the Huber loss and its gradient, the
+// adjoint's partials, and the epilogue with the L2 term and Adam (w, m, v
+// updated; *step advanced; the step's loss added to *loss_sum).
+cas_status fast_eval_adam_step(FastLayout& f, int64_t row0, int64_t row1, const float* target, float* w, float* m,
+                               float* v, int64_t* step, double* loss_sum, const EvalAdam& o, cudaStream_t s);
 
 // Full A'y into a dense vector (standalone product).
 template <typename T>

@@ -15,11 +15,12 @@ transposed copy exists before training starts.  This is the Python side where
 the reference's NeuralNetwork/ code trains value models.
 
 ``Trainer`` runs Adam on the Huber + L2 objective.  By default each batch's
-whole step (forward kernel, loss and its gradient, adjoint kernel, L2 term,
-fused Adam) is captured once as a CUDA graph, and an epoch replays the
-graphs in that epoch's shuffled order with one device-to-host read (the
-epoch's loss) at its end; ``graphs=False`` runs the same step through
-autograd and ``EvaluatorFunction``.
+whole step is one call of ``cas_eval_adam_step`` (three kernels: forward
+with the loss and its gradient, the adjoint, and an epilogue with the L2
+term and the Adam update), captured once as a CUDA graph; an epoch replays
+the graphs in that epoch's shuffled order with one device-to-host read (the
+epoch's loss) at its end.  ``graphs=False`` runs the same step through
+autograd, ``EvaluatorFunction`` and torch.optim.Adam.
 """
 from __future__ import annotations
 
@@ -89,12 +90,15 @@ def objective(score: torch.Tensor, target: torch.Tensor, w: torch.Tensor, delta:
 
 
 class Trainer:
-    """Adam (lr, fused) on mean Huber(delta) + l2 ||w||^2 over the model's
-    fixed minibatches of about `batch` rows; every epoch() shuffles the batch
-    order (torch.Generator seeded with `seed`) and returns the mean batch
-    loss.  graphs=True: each batch's step is one CUDA graph (captured at
-    construction; the weights and the optimizer state are left as they were
-    before the capture), replayed in the epoch's order."""
+    """Adam (lr; betas 0.9, 0.999; eps 1e-8) on mean Huber(delta) + l2 ||w||^2
+    over the model's fixed minibatches of about `batch` rows; every epoch()
+    shuffles the batch order (torch.Generator seeded with `seed`) and returns
+    the mean batch loss.  graphs=True: each batch's step is one CUDA graph
+    around cas_eval_adam_step (captured at construction; the weights and the
+    Adam state are left as they were), replayed in the epoch's order.
+    graphs=False: autograd through EvaluatorFunction and torch.optim.Adam."""
+
+    BETAS, EPS = (0.9, 0.999), 1e-8
 
     def __init__(self, model: PatternEvaluator, target: torch.Tensor, batch: int = 65536, lr: float = 1e-2,
                  l2: float = 1e-4, delta: float = 4.0, seed: int = 0, graphs: bool = True):
@@ -108,57 +112,37 @@ class Trainer:
         self.graphs = None
         w = model.weight
         if not graphs:
-            self.opt = torch.optim.Adam([w], lr=lr, fused=True)
+            self.opt = torch.optim.Adam([w], lr=lr, betas=self.BETAS, eps=self.EPS, fused=True)
             return
-        self.opt = torch.optim.Adam([w], lr=lr, fused=True, capturable=True)
-        dev = w.device
-        nmax = max(r1 - r0 for r0, r1 in self.batches)
-        self._score = torch.empty(nmax, dtype=torch.float32, device=dev)
-        self._grad = torch.zeros_like(w)
-        self._loss_sum = torch.zeros((), dtype=torch.float32, device=dev)
-        side = torch.cuda.Stream(dev)
-        side.wait_stream(torch.cuda.current_stream(dev))
-        with torch.cuda.stream(side), torch.no_grad():
-            # first uses outside the capture: the adjoint's partial buffer for
-            # the largest batch, and Adam's state (a zero-gradient step leaves
-            # the weights as they are; its step count is reset below)
-            big = max(range(len(self.batches)), key=lambda i: self.batches[i][1] - self.batches[i][0])
-            self._step(big)
-            self._grad.zero_()
-            w.grad = self._grad
-            self.opt.step()
-            for st in self.opt.state[w].values():
-                if torch.is_tensor(st):
-                    st.zero_()
-            self._loss_sum.zero_()
-        torch.cuda.current_stream(dev).wait_stream(side)
-        torch.cuda.synchronize(dev)
-        pool = torch.cuda.graph_pool_handle()  # shared: the graphs replay one at a time
-        self.graphs = []
+        self.opts = L.AdamOpts(lr, self.BETAS[0], self.BETAS[1], self.EPS, self.l2, self.delta)
+        self._m = torch.zeros_like(w.detach())
+        self._v = torch.zeros_like(w.detach())
+        self._step_count = torch.zeros((), dtype=torch.int64, device=w.device)
+        self._loss_sum = torch.zeros((), dtype=torch.float64, device=w.device)
+        # one step outside the capture (it sizes the library's buffers for
+        # the largest batch), then the state as it was before it
+        w0 = w.detach().clone()
+        big = max(range(len(self.batches)), key=lambda i: self.batches[i][1] - self.batches[i][0])
+        self._step(big)
+        torch.cuda.synchronize(w.device)
         with torch.no_grad():
-            for i in range(len(self.batches)):
-                g = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(g, pool=pool):
-                    self._step(i)
-                    w.grad = self._grad
-                    self.opt.step()
-                self.graphs.append(g)
+            w.copy_(w0)
+        for t in (self._m, self._v, self._step_count, self._loss_sum):
+            t.zero_()
+        pool = torch.cuda.graph_pool_handle()
+        self.graphs = []
+        for i in range(len(self.batches)):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, pool=pool):
+                self._step(i)
+            self.graphs.append(g)
 
     def _step(self, i: int):
-        """Loss and gradient of batch i into _loss_sum (added) and _grad, on
-        the current stream, without autograd."""
         r0, r1 = self.batches[i]
-        n = r1 - r0
         w = self.model.weight
-        score = self._score[:n]
-        stream = _stream()
-        L.check(L.load().cas_eval_forward(self.model.csr.handle, r0, r1, _ptr(w), _ptr(score), stream))
-        t = self.target[r0:r1]
-        self._loss_sum.add_(objective(score, t, w.detach(), self.delta, self.l2))
-        # d/dscore of the mean Huber loss, then the adjoint, then the L2 term
-        dscore = (score - t).clamp_(-self.delta, self.delta).mul_(1.0 / n)
-        L.check(L.load().cas_eval_backward(self.model.csr.handle, r0, r1, _ptr(dscore), _ptr(self._grad), stream))
-        self._grad.add_(w.detach(), alpha=2.0 * self.l2)
+        L.check(L.load().cas_eval_adam_step(self.model.csr.handle, r0, r1, _ptr(self.target[r0:r1]), _ptr(w),
+                                            _ptr(self._m), _ptr(self._v), _ptr(self._step_count),
+                                            _ptr(self._loss_sum), C.byref(self.opts), _stream()))
 
     def epoch(self) -> float:
         order = torch.randperm(len(self.batches), generator=self.gen).tolist()

@@ -206,6 +206,26 @@ CAS_API cas_status cas_eval_forward(const cas_csr* a, int64_t row0, int64_t row1
 CAS_API cas_status cas_eval_backward(const cas_csr* a, int64_t row0, int64_t row1, const float* d_g, float* d_grad,
                                      void* stream);
 
+/* One training step of the evaluator on a minibatch.  The reference fits
+ * pattern weights by least squares only; this is the training form of its
+ * score (Pattern/Evaluator.cpp:48-54 over the minibatch's rows) with the
+ * objective mean Huber(score - target; delta) + l2 ||w||^2 and the update of
+ * torch.optim.Adam (betas, eps; no weight decay). */
+typedef struct cas_adam_opts {
+    float lr, beta1, beta2, eps; /* Adam */
+    float l2, delta;             /* L2 weight and Huber threshold of the objective */
+} cas_adam_opts;
+/* Rows [row0, row1) (block boundaries as for cas_eval_backward); d_target has
+ * row1 - row0 entries; d_w, d_m, d_v (cols entries: weights and Adam
+ * moments) are updated in place; *d_step (the Adam step count) is advanced;
+ * the step's loss (weights before the update) is added to *d_loss_sum.  Three
+ * kernels on `stream`, no host synchronisation and no allocation after the
+ * first call of the largest minibatch, so it can be captured in a CUDA graph;
+ * deterministic (fixed reduction orders, integer counters only). */
+CAS_API cas_status cas_eval_adam_step(const cas_csr* a, int64_t row0, int64_t row1, const float* d_target,
+                                      float* d_w, float* d_m, float* d_v, int64_t* d_step, double* d_loss_sum,
+                                      const cas_adam_opts* opts, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Solvers: PCG, LSQR, CG (Math/Solver.h)                                    */
 /* ------------------------------------------------------------------------ */

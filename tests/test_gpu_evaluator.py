@@ -126,3 +126,45 @@ def test_graph_trainer_matches_autograd(cuda):
     np.testing.assert_allclose(h_graph, h_auto, rtol=1e-4)
     torch.testing.assert_close(m_graph.weight.detach(), m_auto.weight.detach(), rtol=1e-3, atol=1e-4)
     assert h_graph[-1] < h_graph[0]
+
+
+def test_fused_adam_step_matches_torch(cuda, setup):
+    """cas_eval_adam_step on one minibatch (the partial last block included)
+    against the same step written in torch: the objective's value, its
+    gradient through the adjoint, and Adam's update of w, m, v."""
+    from cassandra_b200 import _lib as L
+
+    model, _, w0, target = setup
+    r0, r1 = 2 * BR, model.rows
+    w = torch.from_numpy(w0).cuda()
+    m = torch.full_like(w, 0.01)
+    v = torch.full_like(w, 0.02)
+    step = torch.tensor(4, dtype=torch.int64, device="cuda")
+    loss = torch.tensor(1.5, dtype=torch.float64, device="cuda")
+    lr, b1, b2, eps, l2, delta = 1e-2, 0.9, 0.999, 1e-8, 1e-4, 4.0
+    # the reference step in torch, from the same state
+    t = target[r0:r1]
+    score = ev.EvaluatorFunction.apply(w, model.csr, r0, r1)
+    want_loss = float(ev.objective(score, t, w, delta, l2))
+    ds = (score - t).clamp(-delta, delta) / (r1 - r0)
+    g = torch.empty_like(w)
+    L.check(L.load().cas_eval_backward(model.csr.handle, r0, r1, ds.data_ptr(), g.data_ptr(),
+                                       torch.cuda.current_stream().cuda_stream))
+    g = g + 2 * l2 * w
+    m_want = m + (1 - b1) * (g - m)
+    v_want = b2 * v + (1 - b2) * g * g
+    k = 5
+    w_want = w - lr / (1 - b1 ** k) * m_want / (v_want.sqrt() / (1 - b2 ** k) ** 0.5 + eps)
+    opts = L.AdamOpts(lr, b1, b2, eps, l2, delta)
+    L.check(L.load().cas_eval_adam_step(model.csr.handle, r0, r1, t.data_ptr(), w.data_ptr(), m.data_ptr(),
+                                        v.data_ptr(), step.data_ptr(), loss.data_ptr(), C.byref(opts),
+                                        torch.cuda.current_stream().cuda_stream))
+    assert int(step) == k
+    assert float(loss) == pytest.approx(1.5 + want_loss, rel=1e-5)
+    torch.testing.assert_close(m, m_want, rtol=1e-5, atol=1e-8)
+    torch.testing.assert_close(v, v_want, rtol=1e-5, atol=1e-10)
+    torch.testing.assert_close(w, w_want, rtol=1e-5, atol=1e-6)
+    with pytest.raises(cb.CasError):  # an unaligned minibatch is refused
+        L.check(L.load().cas_eval_adam_step(model.csr.handle, 1, BR, t.data_ptr(), w.data_ptr(), m.data_ptr(),
+                                            v.data_ptr(), step.data_ptr(), loss.data_ptr(), C.byref(opts),
+                                            torch.cuda.current_stream().cuda_stream))
