@@ -663,8 +663,8 @@ def run_ours_evaluator(args) -> dict | None:
         tr.epoch()  # ends with the loss read
         e2e_times.append(time.perf_counter() - t0)
         del tr, m, p_d, t_d
-    e2e_val = statistics.mean(e2e_times)
-    if world > 1:
+    e2e_val = statistics.mean(e2e_times) if e2e_times else None
+    if world > 1 and e2e_val is not None:
         t = torch.tensor([e2e_val], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_val = float(t.item())

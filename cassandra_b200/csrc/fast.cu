@@ -1222,15 +1222,19 @@ __global__ void __launch_bounds__(256) eval_adam_kernel(const float* __restrict_
         last = atomicAdd(ctr, 1) == static_cast<int>(gridDim.x) - 1;
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
+    if (last) {  // the whole last CTA: strided sums, then the fixed block tree
         __threadfence();
-        double hsum = 0, ws = 0;
-        for (int i = 0; i < nred; i++) hsum += __ldcg(red + i);
-        for (int i = 0; i < static_cast<int>(gridDim.x); i++) ws += __ldcg(red + kEvalRedMax + i);
-        *loss_sum += hsum * inv_n + static_cast<double>(o.l2) * ws;
-        *step = t;
-        *ctr = 0;
-        __threadfence();
+        double h = 0, q = 0;
+        for (int i = threadIdx.x; i < nred; i += blockDim.x) h += __ldcg(red + i);
+        for (int i = threadIdx.x; i < static_cast<int>(gridDim.x); i += blockDim.x) q += __ldcg(red + kEvalRedMax + i);
+        h = block_sum<256>(h, smem);
+        q = block_sum<256>(q, smem);
+        if (threadIdx.x == 0) {
+            *loss_sum += h * inv_n + static_cast<double>(o.l2) * q;
+            *step = t;
+            *ctr = 0;
+            __threadfence();
+        }
     }
 }
 
@@ -1946,7 +1950,7 @@ cas_status fast_eval_adam_step(FastLayout& f, int64_t row0, int64_t row1, const 
     const int64_t b0 = row0 / kBlockRows, b1 = (row1 + kBlockRows - 1) / kBlockRows;
     if (f.g.cols == 0 || n <= 0) return CAS_OK;
     CAS_TRY(eval_buffers(f, b1 - b0, s));
-    const unsigned g1 = std::min<unsigned>(fgrid(n, 256) * 4, kEvalRedMax);
+    const unsigned g1 = std::min<unsigned>(fgrid(n, 256), kEvalRedMax);  // one thread per row up to 4 CTAs per SM
     { eval_loss_grad_kernel<<<g1, 256, 0, s>>>(f.g, f.a16, w, target, row0, row1, o.delta, 1.0f / static_cast<float>(n),
                                                f.eval_dscore, f.eval_red); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
