@@ -125,6 +125,34 @@ def test_products_match_reference_fp64(orc, ref):
     np.testing.assert_array_equal(orc.jacobi(idx, cols), want)
 
 
+def test_kept_matrix_products_match_reference_calls(ref):
+    """The reference's products on a MatrixCSR kept across calls (the
+    evaluator's CPU baseline) equal the same products on a matrix built for
+    each call; with integer-valued vectors every FP32 sum is exact."""
+    lib = ref.ref_lib()
+    rng = np.random.default_rng(5)
+    rows, k, cols = 2000, 16, 501
+    idx = rng.integers(0, cols, size=(rows, k)).astype(np.uint32)
+    x = rng.integers(-8, 9, cols).astype(np.float32)
+    y = rng.integers(-8, 9, rows).astype(np.float32)
+    m = lib.ref_csr_new(k, rows, cols, _p(idx))
+    try:
+        got, want = np.empty(rows, np.float32), np.empty(rows, np.float32)
+        lib.ref_csr_mul(m, _p(x), _p(got))
+        lib.ref_spmv(k, rows, cols, _p(idx), _p(x), _p(want))
+        np.testing.assert_array_equal(got, want)
+        np.testing.assert_array_equal(got, x[idx].sum(axis=1))
+        got, want = np.empty(cols, np.float32), np.empty(cols, np.float32)
+        lib.ref_csr_tmul(m, _p(y), _p(got))
+        lib.ref_spmv_t(k, rows, cols, _p(idx), _p(y), _p(want))
+        np.testing.assert_array_equal(got, want)
+        exact = np.zeros(cols)
+        np.add.at(exact, idx.ravel(), np.repeat(y.astype(np.float64), k))
+        np.testing.assert_array_equal(got, exact.astype(np.float32))
+    finally:
+        lib.ref_csr_free(m)
+
+
 def _small_system(orc, rows=4000, seed=11):
     import cassandra_b200 as cb
 
