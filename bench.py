@@ -220,6 +220,14 @@ def run_ours(args) -> dict | None:
     measure(ab, "blocked", 2 * nnz, 4 * nnz)
     del ab, x32, y32, yo, xo
     torch.cuda.synchronize()
+    # the indexer alone: positions -> uint32 indices [R, K] (16 B read and
+    # 4 K B written per position; the 5.1 GB output is larger than L2)
+    idx_out = torch.empty((R, K), dtype=torch.int32, device="cuda")
+    t_idx = time_kernel(lambda: L.check(lib.cas_index(g.handle, C.c_void_p(pos.data_ptr()), R,
+                                                      C.c_void_p(idx_out.data_ptr()), sp)), n=3)
+    kernels["index_rows_u32"] = {"seconds": t_idx, "bytes": 16 * R + 4 * nnz, "gbs": (16 * R + 4 * nnz) / t_idx / 1e9}
+    del idx_out
+    torch.cuda.synchronize()
 
     opts_mixed = cb.solve_opts("pcg", "mixed", args.tol, 20000, 50, 50)
     opts_plain = cb.solve_opts("pcg", "fp64", args.tol, 20000, 50, 50)
