@@ -13,6 +13,13 @@ the plain FP64 GPU path on the same system is reported beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
+Other workloads (not the default line): ``--workload batched`` — the 60
+per-empty-count fits (16.6M rows in total) as one batched mixed solve;
+``--workload evaluator`` — one training epoch of the differentiable
+evaluator (8M positions, Adam on Huber + L2 over 65,536-row minibatches, each
+minibatch step one CUDA graph).  ``--impl reference`` times the reference's
+own CPU code for the selected workload.
+
 N > 1 runs under torchrun, one rank per GPU, each rank fitting its own
 independently seeded replica (the fits are independent; no collective on
 the data path).  Rank 0 prints one JSON line.

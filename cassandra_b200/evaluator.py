@@ -25,7 +25,6 @@ autograd, ``EvaluatorFunction`` and torch.optim.Adam.
 from __future__ import annotations
 
 import ctypes as C
-import math
 
 import torch
 
@@ -199,4 +198,3 @@ def central_difference(model: PatternEvaluator, target: torch.Tensor, coords: to
 
 __all__ = ["EvaluatorFunction", "PatternEvaluator", "Trainer", "train", "objective", "full_objective",
            "central_difference", "block_rows"]
-_ = math
