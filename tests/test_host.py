@@ -89,6 +89,10 @@ def test_invalid_arguments_are_reported():
                                                 C.byref(h))
         assert st == L.CAS_ERR_INVALID_ARGUMENT, sizes
     assert lib.cas_solve_batched(None, C.byref(cb.solve_opts()), None, None, None, None) == L.CAS_ERR_INVALID_ARGUMENT
+    # the evaluator's training step needs a blocked CSR
+    opts = L.AdamOpts(1e-2, 0.9, 0.999, 1e-8, 1e-4, 4.0)
+    st = lib.cas_eval_adam_step(None, 0, 0, None, None, None, None, None, None, C.byref(opts), None)
+    assert st == L.CAS_ERR_INVALID_ARGUMENT and "cas_eval_adam_step" in L.last_error()
 
 
 def test_no_cpu_fallback_without_a_device():
@@ -146,3 +150,17 @@ def test_reference_arm_runs_on_cpu(ref):
     assert res["impl"] == "reference" and res["value"] > 0
     assert res["e2e"]["h2d_bytes_per_step"] == 0
     assert res["cpu_baseline"]["kind"] == "reference"
+
+
+def test_reference_arm_runs_the_evaluator_workload_on_cpu(ref):
+    """The evaluator workload's reference arm: the reference's products on
+    kept per-minibatch matrices plus numpy loss and Adam, scaled to the
+    epoch."""
+    import bench
+
+    args = bench.parse_args(["--impl", "reference", "--workload", "evaluator", "--steps", "1", "--warmup", "0",
+                             "--eval-rows", "200000", "--eval-sample-batches", "1"])
+    res = bench.run_reference(args)
+    assert res["impl"] == "reference" and res["value"] > 0 and res["metric"] == bench.EVAL_METRIC
+    assert res["config"]["rows"] == 200000
+    assert "1 of 4 minibatches" in res["cpu_baseline"]["sample"]
