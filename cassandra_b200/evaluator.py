@@ -36,6 +36,22 @@ def block_rows() -> int:
     return int(L.load().cas_block_rows())
 
 
+def _blocks_spanned(r0: int, r1: int, br: int) -> int:
+    return 0 if r1 <= r0 else (r1 + br - 1) // br - r0 // br
+
+
+def _guard_graph_buffers(csr, blocks: int) -> None:
+    """The library sizes its evaluator scratch for the most blocks any call
+    has spanned and reallocates it when a call spans more; CUDA graphs
+    captured by a Trainer hold the old buffers.  Once a Trainer captured on
+    this matrix, a call over more blocks than it sized for is refused."""
+    limit = getattr(csr, "_graph_blocks", None)
+    if limit is not None and blocks > limit:
+        raise RuntimeError(f"a call over {blocks} blocks would reallocate evaluator buffers that CUDA graphs of a "
+                           f"Trainer on this matrix use (sized for {limit}); create the Trainer with the largest "
+                           f"minibatch first or use graphs=False")
+
+
 class EvaluatorFunction(torch.autograd.Function):
     """score = A[row0:row1] w  (A implicit 0/1, FP32)."""
 
@@ -52,6 +68,7 @@ class EvaluatorFunction(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g: torch.Tensor):
+        _guard_graph_buffers(ctx.csr, _blocks_spanned(ctx.row0, ctx.row1, block_rows()))
         g = g.contiguous().to(torch.float32)
         grad = torch.empty(ctx.csr.cols(), dtype=torch.float32, device=g.device)
         L.check(L.load().cas_eval_backward(ctx.csr.handle, ctx.row0, ctx.row1, _ptr(g), _ptr(grad), _stream()))
@@ -113,6 +130,9 @@ class Trainer:
         if not graphs:
             self.opt = torch.optim.Adam([w], lr=lr, betas=self.BETAS, eps=self.EPS, fused=True)
             return
+        br = block_rows()
+        blocks = max(_blocks_spanned(r0, r1, br) for r0, r1 in self.batches)
+        _guard_graph_buffers(model.csr, blocks)
         self.opts = L.AdamOpts(lr, self.BETAS[0], self.BETAS[1], self.EPS, self.l2, self.delta)
         self._m = torch.zeros_like(w.detach())
         self._v = torch.zeros_like(w.detach())
@@ -135,6 +155,7 @@ class Trainer:
             with torch.cuda.graph(g, pool=pool):
                 self._step(i)
             self.graphs.append(g)
+        model.csr._graph_blocks = max(getattr(model.csr, "_graph_blocks", None) or 0, blocks)
 
     def _step(self, i: int):
         r0, r1 = self.batches[i]

@@ -221,7 +221,10 @@ typedef struct cas_adam_opts {
  * the step's loss (weights before the update) is added to *d_loss_sum.  Three
  * kernels on `stream`, no host synchronisation and no allocation after the
  * first call of the largest minibatch, so it can be captured in a CUDA graph;
- * deterministic (fixed reduction orders, integer counters only). */
+ * deterministic (fixed reduction orders, integer counters only).  The scratch
+ * it (and cas_eval_backward) uses belongs to the CSR and grows when a call
+ * spans more blocks than any call before: that frees the old scratch, so
+ * graphs captured earlier must not be replayed after such a call. */
 CAS_API cas_status cas_eval_adam_step(const cas_csr* a, int64_t row0, int64_t row1, const float* d_target,
                                       float* d_w, float* d_m, float* d_v, int64_t* d_step, double* d_loss_sum,
                                       const cas_adam_opts* opts, void* stream);

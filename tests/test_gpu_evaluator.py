@@ -168,3 +168,19 @@ def test_fused_adam_step_matches_torch(cuda, setup):
         L.check(L.load().cas_eval_adam_step(model.csr.handle, 1, BR, t.data_ptr(), w.data_ptr(), m.data_ptr(),
                                             v.data_ptr(), step.data_ptr(), loss.data_ptr(), C.byref(opts),
                                             torch.cuda.current_stream().cuda_stream))
+
+
+def test_graph_trainer_guards_its_buffers(cuda):
+    """After a Trainer captured its graphs for one-block minibatches, calls
+    that would grow (and so reallocate) the matrix's evaluator scratch are
+    refused; calls within the captured size still run."""
+    rows = 4 * BR
+    pos = cb.generate_positions(47, rows, 10, 50)
+    model = ev.PatternEvaluator(SET8, pos, "expanded")
+    target = torch.zeros(rows, dtype=torch.float32, device="cuda")
+    ev.Trainer(model, target, batch=BR)
+    with pytest.raises(RuntimeError, match="reallocate"):
+        ev.Trainer(model, target, batch=2 * BR)
+    with pytest.raises(RuntimeError, match="reallocate"):
+        model(0, rows).sum().backward()
+    assert np.isfinite(ev.Trainer(model, target, batch=BR, graphs=False).epoch())

@@ -164,3 +164,22 @@ def test_reference_arm_runs_the_evaluator_workload_on_cpu(ref):
     assert res["impl"] == "reference" and res["value"] > 0 and res["metric"] == bench.EVAL_METRIC
     assert res["config"]["rows"] == 200000
     assert "1 of 4 minibatches" in res["cpu_baseline"]["sample"]
+
+
+def test_graph_buffer_guard_logic():
+    """The evaluator's guard for buffers that captured CUDA graphs use: once
+    a Trainer captured over n blocks per call, a call over more is refused."""
+    from cassandra_b200 import evaluator as ev
+
+    class Csr:
+        pass
+
+    c = Csr()
+    ev._guard_graph_buffers(c, 100)  # no graphs captured: anything goes
+    c._graph_blocks = 4
+    ev._guard_graph_buffers(c, 4)
+    with pytest.raises(RuntimeError, match="reallocate"):
+        ev._guard_graph_buffers(c, 5)
+    assert ev._blocks_spanned(0, 65536, 16384) == 4
+    assert ev._blocks_spanned(6 * 16384, 6 * 16384 + 1000, 16384) == 1
+    assert ev._blocks_spanned(7, 7, 16384) == 0
