@@ -8,17 +8,26 @@ the 8 board symmetries (expanded layout: 166,212 columns, 64 entries per
 row, 1.28e9 entries), seeded synthetic targets.  A step is FitWeights on
 device-resident positions and targets: indexing, CSR and transposed-copy
 build, Jacobi, and mixed-precision Jacobi-PCG to a relative normal-equation
-residual of 1e-8.  The metric is the time of that step (lower is better);
-the plain FP64 GPU path on the same system is reported beside it.
+residual of 1e-8.  The metric is the time of that step (lower is better).
+
+Beside it on the same line: the plain FP64 GPU path (the fit on the rows
+layout, and FP64 and mixed solves on one blocked CSR, which isolates the
+precision); LSQR solves of the same system (``--lsqr``); the reference's
+own code on the host cores solving the same system (the CPU baseline, one
+full step) and the check of every device solution against it (FP64
+normal-equation residual with the reference's products, largest weight
+difference on the columns with entries); short runs of the batched and
+evaluator workloads (``--no-summaries`` leaves them out).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Other workloads (not the default line): ``--workload batched`` — the 60
-per-empty-count fits (16.6M rows in total) as one batched mixed solve;
-``--workload evaluator`` — one training epoch of the differentiable
-evaluator (8M positions, Adam on Huber + L2 over 65,536-row minibatches, each
-minibatch step one CUDA graph).  ``--impl reference`` times the reference's
-own CPU code for the selected workload.
+Other workloads: ``--workload batched`` — the 60 per-empty-count fits
+(16.6M rows in total) as one batched mixed solve; ``--workload evaluator`` —
+one training epoch of the differentiable evaluator (8M positions, Adam on
+Huber + L2 over 65,536-row minibatches, each minibatch step one CUDA graph).
+``--impl reference`` times the reference's own CPU code on the selected
+workload; for the single fit every step is the whole 20M-row workload, with
+inputs from the oracle's restatement of the seeded generator.
 
 N > 1 runs under torchrun, one rank per GPU, each rank fitting its own
 independently seeded replica (the fits are independent; no collective on
@@ -71,7 +80,12 @@ def parse_args(argv=None):
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample-rows", type=int, default=5_000_000,
-                    help="rows of the bounded sample the CPU baseline runs")
+                    help="batched workload: rows of the bounded sample the CPU baseline runs")
+    ap.add_argument("--lsqr", choices=sorted(LSQ_VARIANTS), default="scaled",
+                    help="LSQR/LSMR solves of the single workload reported beside PCG")
+    ap.add_argument("--lsqr-max-iterations", type=int, default=20000)
+    ap.add_argument("--no-summaries", action="store_true",
+                    help="single workload: leave out the short batched and evaluator runs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -156,6 +170,21 @@ class ClockSampler:
         busy = [r[0] for r in rows]
         return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
                 "samples": len(rows)}
+
+
+def single_config(args) -> dict:
+    """The single-fit workload, as both arms name it."""
+    return {
+        "workload": f"8-pattern expanded fit, {args.rows} rows, empties {args.min_empties}..{args.max_empties}, "
+                    f"Jacobi-PCG to rel. normal-eq. residual {args.tol:g}",
+        "rows": args.rows, "cols": COLS_8, "nnz_per_row": 64, "nnz": args.rows * 64, "method": "pcg",
+        "tol": args.tol, "seed": args.seed,
+        "inputs": f"positions {16 * args.rows / 1e6:.0f} MB, index stream {256 * args.rows / 1e9:.2f} GB per "
+                  f"product ({'larger' if 256 * args.rows > 126e6 else 'smaller'} than the 126 MB L2)",
+    }
+
+
+COLS_8 = sum(3 ** bin(m).count("1") for m in PATTERNS_8)
 
 
 # --------------------------------------------------------------------------- ours
@@ -271,10 +300,48 @@ def run_ours(args) -> dict | None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = float(t.item())
     per_step = elapsed / args.steps
-
-    # plain FP64 GPU path on the same system (the comparison the metric names)
-    plain = None if args.no_plain else fit(opts_plain)
     mixed = reps[-1]
+    solutions = {"mixed_pcg": w.cpu().numpy()}
+
+    # plain FP64 GPU path on the same system, as the fit runs it (rows layout,
+    # the reference's structure)
+    plain = None
+    if not args.no_plain:
+        plain = fit(opts_plain)
+        solutions["plain_fp64_pcg_rows"] = w.cpu().numpy()
+
+    # the same comparison on one layout: FP64 and mixed PCG solves on one
+    # blocked CSR, so the ratio isolates the precision; and LSQR / LSMR
+    same_layout, lsq = None, {}
+    if not args.no_plain or args.lsqr:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        ab = cb.MatrixCSR.from_positions(g, pos, "blocked")
+        ev1.record(stream)
+        ev1.synchronize()
+        build_blocked = ev0.elapsed_time(ev1) * 1e-3
+
+        def solve(opts, key):
+            rep = L.SolveReport()
+            st = lib.cas_solve(ab.handle, C.byref(opts), C.c_void_p(b.data_ptr()), C.c_void_p(w.data_ptr()),
+                               C.byref(rep), sp)
+            if st not in (L.CAS_OK, L.CAS_ERR_NOT_CONVERGED):
+                L.check(st)
+            solutions[key] = w.cpu().numpy()
+            return {"solve_s": rep.seconds, "iterations": rep.iterations, "refinements": rep.refinements,
+                    "rel_residual": rep.rel_residual, "converged": st == L.CAS_OK}
+
+        if not args.no_plain:
+            m = solve(opts_mixed, "mixed_pcg_blocked")
+            pl = solve(opts_plain, "plain_fp64_pcg_blocked")
+            same_layout = {"layout": "blocked", "build_s": build_blocked, "mixed": m, "plain_fp64": pl,
+                           "solve_speedup_mixed_vs_plain": pl["solve_s"] / m["solve_s"] if m["solve_s"] else None}
+        for method, prec, scaled in LSQ_VARIANTS[args.lsqr]:
+            o = cb.solve_opts(method, prec, args.tol, args.lsqr_max_iterations, 50, 100, scale_columns=scaled)
+            key = f"{method}_{prec}{'_scaled' if scaled else ''}"
+            lsq[key] = solve(o, key)
+        del ab
+        torch.cuda.synchronize()
 
     # ---- end to end through the public C ABI with host buffers
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
@@ -300,15 +367,36 @@ def run_ours(args) -> dict | None:
         t = torch.tensor([e2e_val], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_val = float(t.item())
+    e2e = {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": int(pos_h.numel() * 8 + sc_h.numel() * 4),
+           "d2h_bytes_per_step": int(w_h.numel() * 4), "steps": e2e_steps}
 
     peak, peak_kind = measured_peaks()
     blocked = {k: v for k, v in kernels.items() if k.startswith("blocked")}
     dom = max(blocked, key=lambda k: blocked[k]["seconds"])
     ach = kernels[dom]["gbs"]
 
-    cpu = None
+    # ---- the reference's own code on the host cores, on the same system: the
+    # CPU baseline (the whole workload, one step) and the oracle check of
+    # every solution above
+    cpu, check = None, None
+    pos_host = pos.cpu().numpy().view(np.uint64)
+    b_host = b.cpu().numpy()
+    del pos, b, pos_h, sc_h, w_h
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args, seed, mixed.iterations)
+        cpu, check = reference_check(args, pos_host, b_host, solutions)
+
+    summaries = {}
+    if world == 1 and not args.no_summaries:
+        import gc
+
+        gc.collect()
+        torch.cuda.empty_cache()
+        summaries["batched"] = compact(run_ours_batched(summary_args(args)))
+        gc.collect()
+        torch.cuda.empty_cache()
+        summaries["evaluator"] = compact(run_ours_evaluator(summary_args(args)))
 
     result = {
         "metric": METRIC,
@@ -323,37 +411,64 @@ def run_ours(args) -> dict | None:
         "vs_baseline": None,
         "dtype": "f32 products / f64 scalars",
         "data": "synthetic (seeded random-play positions, seeded targets)",
-        "config": {
-            "workload": f"8-pattern expanded fit, {R} rows, empties {args.min_empties}..{args.max_empties}, "
-                        f"mixed Jacobi-PCG to rel. normal-eq. residual {args.tol:g}",
-            "rows": R, "cols": cols, "nnz_per_row": K, "nnz": nnz, "method": "pcg", "precision": "mixed",
-            "refine_every": 50, "tol": args.tol,
-            "l2": "inputs larger than L2 (positions 320 MB, CSR 5.1 GB)",
-            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-        },
+        "config": single_config(args),
+        "precision": "mixed (FP32 products on the blocked layout, FP64 compensated scalars, reliable updating)",
+        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         "breakdown": {
             "build_s": mixed.setup_seconds, "solve_s": mixed.seconds, "iterations": mixed.iterations,
             "refinements": mixed.refinements, "rel_residual": mixed.rel_residual,
         },
         "plain_fp64": None if plain is None else {
-            "step_s": plain.setup_seconds + plain.seconds, "solve_s": plain.seconds, "iterations": plain.iterations,
-            "rel_residual": plain.rel_residual,
+            "layout": "rows", "step_s": plain.setup_seconds + plain.seconds, "solve_s": plain.seconds,
+            "iterations": plain.iterations, "rel_residual": plain.rel_residual,
             "solve_speedup_mixed_vs_plain": plain.seconds / mixed.seconds if mixed.seconds else None,
         },
+        "same_layout": same_layout,
+        "least_squares": lsq or None,
+        "oracle_check": check,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                      "frac": ach / peak, "peak_kind": peak_kind, "traffic": ncu_traffic(dom, nnz),
                      "traffic_unit": "bytes per launch, scaled from ncu at 2M rows"},
         "kernels": kernels,
-        "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": int(pos_h.numel() * 8 + sc_h.numel() * 4),
-                "d2h_bytes_per_step": int(w_h.numel() * 4), "steps": e2e_steps},
+        "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clk,
         "cpu_baseline": cpu,
+        "summaries": summaries or None,
     }
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return result if rank == 0 else None
+
+
+# LSQR / LSMR solves of the single workload: (method, precision, column scaling)
+LSQ_VARIANTS = {
+    "none": [],
+    "scaled": [("lsqr", "mixed", True), ("lsqr", "fp64", True)],
+    "all": [("lsqr", "mixed", True), ("lsqr", "fp64", True), ("lsqr", "mixed", False), ("lsqr", "fp64", False),
+            ("lsmr", "mixed", True), ("lsmr", "mixed", False)],
+}
+
+
+def summary_args(args):
+    """A short run of another workload for the default line: 2 steps after
+    3 warm-ups, no sequential plain comparison, no end-to-end pass, a smaller
+    CPU sample."""
+    d = dict(vars(args))
+    d.update(steps=2, warmup=3, no_plain=True, e2e_steps=0, cpu_sample_rows=1_000_000, eval_sample_batches=8)
+    return argparse.Namespace(**d)
+
+
+def compact(res: dict | None) -> dict | None:
+    if res is None:
+        return None
+    keep = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "config", "roofline", "kernels",
+            "gpu_launches", "cpu_baseline", "clocks")
+    out = {k: res[k] for k in keep if k in res}
+    br = res.get("breakdown", {})
+    out["breakdown"] = {k: v for k, v in br.items() if k != "per_problem"}
+    return out
 
 
 def run_ours_batched(args) -> dict | None:
@@ -716,94 +831,129 @@ def run_ours_evaluator(args) -> dict | None:
 
 # ---------------------------------------------------------------- CPU reference
 
-class ReferenceSample:
-    """A bounded sample of the workload for the host cores, run with the
-    reference's own code: its A_Indexer recipe over FastIndex/Flipped* for the
-    expanded layout (oracle/ref/ref_driver.cpp) and its Math/ PCG retyped to
-    FP64 (oracle/ref/ref64_driver.cpp), to a relative normal-equation residual
-    of 1e-8.  Inputs (positions, targets) are prepared once, untimed."""
+class ReferenceSystem:
+    """One fit's system on the host, run with the reference's own code: its
+    A_Indexer recipe over FastIndex/Flipped* for the expanded layout
+    (oracle/ref/ref_driver.cpp) and its Math/ PCG retyped to FP64
+    (oracle/ref/ref64_driver.cpp, FitWeights' solve, PatternFit/PatternFit.cpp:
+    24-32), to a relative normal-equation residual of tol.  Positions are
+    given, or made by the oracle's restatement of the seeded generator (this
+    process never loads the CUDA library); targets likewise."""
 
-    def __init__(self, rows: int, seed: int, min_e: int, max_e: int):
+    def __init__(self, seed: int, rows: int, min_e: int, max_e: int, pos: np.ndarray | None = None,
+                 b: np.ndarray | None = None, first: int = 0):
         import oracle
-        import cassandra_b200 as cb
 
         self.ref, self.ref64 = oracle.ref_lib(), oracle.ref64_lib()
         self.ref.ref_expanded_index.restype = None
         self.ref.ref_expanded_index.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p]
         self.rows = rows
         self.masks = np.asarray(PATTERNS_8, np.uint64)
-        self.cols = int(sum(3 ** bin(x).count("1") for x in PATTERNS_8))
-        self.pos = cb.generate_positions_host(seed, 0, rows, min_e, max_e)  # same positions as the GPU arm
+        self.cols = COLS_8
+        self.pos = np.ascontiguousarray(pos if pos is not None else
+                                        oracle.generate_positions(seed, first, rows, min_e, max_e), dtype=np.uint64)
         self.idx = np.empty((rows, 64), np.uint32)
-        self._index()
-        rng = np.random.default_rng(seed)
-        wst = rng.normal(0, 0.5, self.cols)
-        aw = np.empty(rows)
-        self.ref64.ref64_spmv(64, rows, self.cols, self.idx.ctypes.data_as(C.c_void_p),
-                              wst.ctypes.data_as(C.c_void_p), aw.ctypes.data_as(C.c_void_p))
-        self.b = np.clip(2 * np.rint((aw + rng.normal(0, 4, rows)) / 2), -64, 64)
+        self.index()
+        self.b = b if b is not None else oracle.generate_targets(self.idx, self.cols, seed)[0]
 
-    def _index(self) -> float:
+    def index(self) -> float:
         t0 = time.perf_counter()
         self.ref.ref_expanded_index(self.masks.ctypes.data_as(C.c_void_p), len(self.masks),
                                     self.pos.ctypes.data_as(C.c_void_p), self.rows,
                                     self.idx.ctypes.data_as(C.c_void_p))
         return time.perf_counter() - t0
 
-    def run(self) -> dict:
-        t_index = self._index()
+    def run(self, tol: float) -> dict:
+        """One step: indexing and the FP64 PCG (Jacobi set-up included; its
+        residual checks every 10 iterations excluded from the time)."""
+        t_index = self.index()
         x = np.empty(self.cols)
         rel, sec = np.zeros(1), np.zeros(1)
         it = self.ref64.ref64_pcg(64, self.rows, self.cols, self.idx.ctypes.data_as(C.c_void_p),
-                                  self.b.ctypes.data_as(C.c_void_p), 20000, 1e-8, 10, x.ctypes.data_as(C.c_void_p),
+                                  self.b.ctypes.data_as(C.c_void_p), 20000, tol, 10, x.ctypes.data_as(C.c_void_p),
                                   rel.ctypes.data_as(C.c_void_p), sec.ctypes.data_as(C.c_void_p))
-        return {"index_s": t_index, "solve_s": float(sec[0]), "iterations": int(it), "rel_residual": float(rel[0])}
+        return {"index_s": t_index, "solve_s": float(sec[0]), "step_s": t_index + float(sec[0]),
+                "iterations": int(it), "rel_residual": float(rel[0]), "x": x}
+
+    def check(self, xs: list[np.ndarray]) -> tuple[list[float], np.ndarray]:
+        """FP64 normal residuals of the given solutions with the reference's
+        products, and the mask of columns with entries."""
+        n = len(xs)
+        flat = np.ascontiguousarray(np.stack(xs) if n else np.zeros((0, self.cols)), dtype=np.float64)
+        out = np.empty(max(n, 1))
+        hit = np.empty(self.cols, np.uint8)
+        self.ref64.ref64_check(64, self.rows, self.cols, self.idx.ctypes.data_as(C.c_void_p),
+                               self.b.ctypes.data_as(C.c_void_p), n, flat.ctypes.data_as(C.c_void_p),
+                               out.ctypes.data_as(C.c_void_p), hit.ctypes.data_as(C.c_void_p))
+        return [float(v) for v in out[:n]], hit.astype(bool)
 
 
-def cpu_baseline(args, seed: int, gpu_iterations: int | None = None) -> dict | None:
+def _threads() -> int:
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+
+
+def reference_check(args, pos: np.ndarray, b: np.ndarray, solutions: dict) -> tuple[dict, dict]:
+    """The reference's FP64 PCG on the benchmarked system (the CPU baseline,
+    one full step) and the check of the device's solutions against it: each
+    solution's FP64 normal-equation residual with the reference's products,
+    and its largest weight difference from the reference's solution on the
+    columns with entries (x0 = 0 and the Jacobi preconditioner in both fix
+    the gauge of the rank-deficient system)."""
     try:
         import oracle
 
         if not oracle.ref_available():
-            return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
-                    "sample": "unavailable: oracle/_ref not built"}
+            return ({"value": None, "unit": "s", "cores": _threads(), "kind": "reference",
+                     "sample": "unavailable: oracle/_ref not built"}, None)
     except Exception as e:  # pragma: no cover
-        return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference", "sample": f"error {e}"}
-    n = min(args.cpu_sample_rows, args.rows)
-    s = ReferenceSample(n, seed, args.min_empties, args.max_empties).run()
-    scale = args.rows / n
-    value = (s["index_s"] + s["solve_s"]) * scale
-    return {"value": value, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
-            "sample": f"{n} of {args.rows} rows (same generator and seed); reference A_Indexer recipe "
-                      f"(FastIndex/Flipped*) + reference Math/ PCG retyped to FP64, run to 1e-8 "
-                      f"({s['iterations']} iterations, rel {s['rel_residual']:.2e}, index {s['index_s']:.3f} s, "
-                      f"solve {s['solve_s']:.2f} s), time scaled by rows x{scale:g}; "
-                      f"OpenMP threads {os.environ.get('OMP_NUM_THREADS', os.cpu_count())}"}
+        return ({"value": None, "unit": "s", "cores": _threads(), "kind": "reference", "sample": f"error {e}"},
+                None)
+    sysm = ReferenceSystem(args.seed, args.rows, args.min_empties, args.max_empties, pos=pos, b=b)
+    r = sysm.run(args.tol)
+    names = list(solutions)
+    rels, hit = sysm.check([solutions[k] for k in names] + [r["x"]])
+    xr = r["x"][hit]
+    scale = float(np.abs(xr).max()) if xr.size else 1.0
+    check = {"reference": {"method": "reference Math/ PCG retyped to FP64, Jacobi, x0 = 0",
+                           "iterations": r["iterations"], "rel_residual_fp64": rels[-1]},
+             "hit_cols": int(hit.sum()), "cols": int(hit.size)}
+    for k, rel in zip(names, rels):
+        d = np.abs(solutions[k][hit] - xr)
+        check[k] = {"rel_residual_fp64": rel, "max_weight_err_hit": float(d.max()) if d.size else 0.0,
+                    "max_weight_err_hit_rel": float(d.max()) / scale if d.size else 0.0}
+    cpu = {"value": r["step_s"], "unit": "s", "cores": _threads(), "kind": "reference",
+           "sample": f"the whole workload ({args.rows} rows), one step on the same system as the GPU arm: reference "
+                     f"A_Indexer recipe (FastIndex/Flipped*) {r['index_s']:.2f} s + reference Math/ PCG retyped to "
+                     f"FP64 to {args.tol:g}, {r['iterations']} iterations, {r['solve_s']:.2f} s "
+                     f"(rel {r['rel_residual']:.2e}); OpenMP threads {_threads()}"}
+    return cpu, check
 
 
 def cpu_baseline_batched(args, seed: int, rows, empties) -> dict | None:
     """The reference fitting the batched workload's problems one after another
     (its training loop's order), on a bounded sample: the first problems in
-    order until about cpu_sample_rows rows, time scaled by total rows."""
+    order until about cpu_sample_rows rows, time scaled by total rows.
+    Positions are the batched workload's (per-problem streams); targets follow
+    the same recipe from per-problem streams."""
     try:
         import oracle
 
         if not oracle.ref_available():
-            return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+            return {"value": None, "unit": "s", "cores": _threads(), "kind": "reference",
                     "sample": "unavailable: oracle/_ref not built"}
     except Exception as e:  # pragma: no cover
-        return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference", "sample": f"error {e}"}
+        return {"value": None, "unit": "s", "cores": _threads(), "kind": "reference", "sample": f"error {e}"}
     total, done_rows, t, its = int(np.sum(rows)), 0, 0.0, []
     for q, (n, e) in enumerate(zip(rows, empties)):
         if done_rows >= args.cpu_sample_rows:
             break
-        s = ReferenceSample(int(n), 1000 * seed + q, int(e), int(e)).run()
-        t += s["index_s"] + s["solve_s"]
+        s = ReferenceSystem(1000 * seed + q, int(n), int(e), int(e)).run(args.tol)
+        t += s["step_s"]
         its.append(s["iterations"])
         done_rows += int(n)
-    return {"value": t * total / done_rows, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+    return {"value": t * total / done_rows, "unit": "s", "cores": _threads(), "kind": "reference",
             "sample": f"first {len(its)} of {len(rows)} problems ({done_rows} of {total} rows), each: reference "
-                      f"indexing + FP64 PCG to 1e-8 ({min(its)}..{max(its)} iterations); time scaled by rows "
+                      f"indexing + FP64 PCG to {args.tol:g} ({min(its)}..{max(its)} iterations); time scaled by rows "
                       f"x{total / done_rows:.3g}"}
 
 
@@ -818,13 +968,13 @@ def cpu_baseline_evaluator(args, seed: int, batches_per_epoch: int) -> dict | No
         import oracle
 
         if not oracle.ref_available():
-            return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+            return {"value": None, "unit": "s", "cores": _threads(), "kind": "reference",
                     "sample": "unavailable: oracle/_ref not built"}
     except Exception as e:  # pragma: no cover
-        return {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference", "sample": f"error {e}"}
+        return {"value": None, "unit": "s", "cores": _threads(), "kind": "reference", "sample": f"error {e}"}
     nb = max(1, min(args.eval_sample_batches, batches_per_epoch))
     rows = nb * EVAL_BATCH
-    smp = ReferenceSample(rows, seed, *EVAL_EMPTIES)
+    smp = ReferenceSystem(seed, rows, *EVAL_EMPTIES)
     lib, cols, k = smp.ref, smp.cols, 64
     target = smp.b.astype(np.float32)
     mats = [lib.ref_csr_new(k, EVAL_BATCH, cols, smp.idx[i * EVAL_BATCH:].ctypes.data_as(C.c_void_p))
@@ -852,7 +1002,7 @@ def cpu_baseline_evaluator(args, seed: int, batches_per_epoch: int) -> dict | No
     finally:
         for m in mats:
             lib.ref_csr_free(m)
-    return {"value": per_batch * batches_per_epoch, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+    return {"value": per_batch * batches_per_epoch, "unit": "s", "cores": _threads(), "kind": "reference",
             "sample": f"{nb} of {batches_per_epoch} minibatches of {EVAL_BATCH} rows (same generator; reference "
                       f"indexing and MatrixCSR built untimed); per minibatch the reference's A*w and g*A plus numpy "
                       f"Huber/Adam, {per_batch * 1e3:.1f} ms; time scaled to the epoch; OpenMP threads "
@@ -904,26 +1054,29 @@ def run_reference(args) -> dict | None:
             "cpu_baseline": cbl,
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
+    # the single fit: the whole workload every step, on the host cores, with
+    # inputs from the oracle's restatement of the seeded generator (the same
+    # system the GPU arm builds; this process loads no CUDA library)
+    sysm = ReferenceSystem(args.seed, args.rows, args.min_empties, args.max_empties)
     times, last = [], None
-    n = min(args.cpu_sample_rows, args.rows)
-    sample = ReferenceSample(n, args.seed, args.min_empties, args.max_empties)
     for i in range(args.warmup + args.steps):
-        s = sample.run()
+        r = sysm.run(args.tol)
         if i >= args.warmup:
-            times.append((s["index_s"] + s["solve_s"]) * args.rows / n)
-            last = s
+            times.append(r["step_s"])
+            last = r
     value = statistics.mean(times)
-    cb = {"value": value, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
-          "sample": f"each step: {n} of {args.rows} rows, reference indexing + FP64 PCG to 1e-8 "
-                    f"({last['iterations']} iterations), time scaled by rows x{args.rows / n:g}"}
+    cbl = {"value": value, "unit": "s", "cores": _threads(), "kind": "reference",
+           "sample": f"the whole workload every step ({args.rows} rows): reference indexing "
+                     f"({last['index_s']:.2f} s) + FP64 PCG to {args.tol:g} ({last['iterations']} iterations, "
+                     f"{last['solve_s']:.2f} s, rel {last['rel_residual']:.2e}); OpenMP threads {_threads()}"}
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random-play positions, seeded targets)",
-        "config": {"workload": f"8-pattern expanded fit, {args.rows} rows, empties {args.min_empties}.."
-                               f"{args.max_empties}, FP64 Jacobi-PCG to rel. normal-eq. residual {args.tol:g}",
-                   "rows": args.rows},
-        "cpu_baseline": cb,
+        "config": single_config(args), "precision": "FP64 (the reference's Math/ retyped from float)",
+        "breakdown": {"index_s": last["index_s"], "solve_s": last["solve_s"], "iterations": last["iterations"],
+                      "rel_residual": last["rel_residual"], "steps_s": times},
+        "cpu_baseline": cbl,
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

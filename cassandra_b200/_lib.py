@@ -48,6 +48,7 @@ class SolveOpts(C.Structure):
         ("refine_every", C.c_int),
         ("check_every", C.c_int),
         ("jacobi", C.c_int),
+        ("scale_columns", C.c_int),
     ]
 
 

@@ -256,7 +256,10 @@ def jacobi_preconditioner_of_ata(a: MatrixCSR, dtype=torch.float64) -> torch.Ten
 
 
 def solve_opts(method: str = "pcg", precision: str = "fp64", tol: float = 1e-8, max_iterations: int = 20000,
-               refine_every: int = 50, check_every: int = 50, jacobi: bool = True) -> L.SolveOpts:
+               refine_every: int = 50, check_every: int = 50, jacobi: bool = True,
+               scale_columns: bool = False) -> L.SolveOpts:
+    """cas_solve_opts.  scale_columns: LSQR/LSMR iterate on A S with S =
+    diag(A'A)^-1/2 (the reference's LSQR/LSMR are unscaled: False)."""
     o = L.SolveOpts()
     L.load().cas_solve_opts_default(C.byref(o))
     o.method = {"pcg": L.CAS_PCG, "lsqr": L.CAS_LSQR, "cg": L.CAS_CG, "lsmr": L.CAS_LSMR}[method]
@@ -266,6 +269,7 @@ def solve_opts(method: str = "pcg", precision: str = "fp64", tol: float = 1e-8, 
     o.refine_every = refine_every
     o.check_every = check_every
     o.jacobi = int(jacobi)
+    o.scale_columns = int(scale_columns)
     return o
 
 
@@ -276,7 +280,7 @@ class _Solver:
 
     def __init__(self, a: MatrixCSR, b: torch.Tensor, x0: torch.Tensor | None = None, precision: str = "fp64",
                  tol: float = 0.0, max_iterations: int = 1 << 30, refine_every: int = 50, check_every: int = 50,
-                 jacobi: bool = True):
+                 jacobi: bool = True, scale_columns: bool = False):
         _require_cuda(b, "b")
         if b.dtype != torch.float64:
             b = b.double()
@@ -289,7 +293,8 @@ class _Solver:
         self._lib = L.load()
         self.a = a
         self.b = b.contiguous()
-        self.opts = solve_opts(self.method, precision, tol, max_iterations, refine_every, check_every, jacobi)
+        self.opts = solve_opts(self.method, precision, tol, max_iterations, refine_every, check_every, jacobi,
+                               scale_columns)
         h = C.c_void_p()
         L.check(self._lib.cas_solver_create(a.handle, C.byref(self.opts), _ptr(self.b), _ptr(x0), _stream(),
                                             C.byref(h)))
@@ -345,7 +350,8 @@ class CG(_Solver):
 
 
 class LSQR(_Solver):
-    """LSQR(A, x0, b) (Math/Solver.h:128-182)."""
+    """LSQR(A, x0, b) (Math/Solver.h:128-182).  scale_columns=True iterates
+    on A S, S = diag(A'A)^-1/2, and returns x = S y (not in the reference)."""
 
     method = "lsqr"
 
@@ -385,7 +391,7 @@ def solve_batched(a: MatrixCSR, b: torch.Tensor, precision: str = "mixed", tol: 
 
 def fit_weights(masks, positions: np.ndarray, scores: np.ndarray, mode: str = "reference", method: str = "pcg",
                 precision: str = "fp64", tol: float = 1e-8, max_iterations: int = 20000,
-                refine_every: int = 50, check_every: int = 50) -> tuple[np.ndarray, dict]:
+                refine_every: int = 50, check_every: int = 50, scale_columns: bool = False) -> tuple[np.ndarray, dict]:
     """FitWeights with host buffers in and out (PatternFit/PatternFit.cpp:7-39).
 
     tol <= 0 runs exactly max_iterations iterations, as the reference's
@@ -401,7 +407,7 @@ def fit_weights(masks, positions: np.ndarray, scores: np.ndarray, mode: str = "r
     cols = int(lib.cas_patterns_cols(h))
     lib.cas_patterns_destroy(h)
     w = np.empty(cols, dtype=np.float32)
-    o = solve_opts(method, precision, tol, max_iterations, refine_every, check_every)
+    o = solve_opts(method, precision, tol, max_iterations, refine_every, check_every, scale_columns=scale_columns)
     rep = L.SolveReport()
     st = lib.cas_fit_weights(m.ctypes.data_as(C.c_void_p), len(m), _REF_MODES[mode], pos.ctypes.data_as(C.c_void_p),
                              sc.ctypes.data_as(C.c_void_p), len(pos), C.byref(o), w.ctypes.data_as(C.c_void_p),

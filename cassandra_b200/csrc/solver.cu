@@ -51,14 +51,17 @@ enum Slot {
     // LSMR (shares kLAlpha, kLBeta, kInvBeta with LSQR)
     kMAlphaBar = 18, kZetaBar = 19, kCBar = 20, kSBar = 21, kMRho = 22, kMRhoBar = 23,
     kFHbar = 24, kFX = 25, kFH = 26,  // coefficients of the h_bar, x, h updates
-    kSlots = 27
+    kArn0 = 27,   // LSQR/LSMR: recursive ||A'r|| estimate at the last (re)start
+    kBn2S = 28,   // LSQR/LSMR with column scaling: ||S A'b||^2 (denominator of the recursive estimate)
+    kSlots = 29
 };
 // kPending: LSQR met its tolerance in the last step; the step's x/w update
 // still has to run, so kDone is raised by the next step's first kernel.
 // kRestart: the last residual replacement found the recursive residual off
 // by more than kRestartDeviation (relative): the search direction restarts.
-// kSkip: no residual replacement is due this iteration (mixed PCG); the
-// replacement step of every iteration returns at entry while it is set.
+// kSkip: no residual replacement is due this iteration (mixed PCG), or no
+// restart from the FP64 residual (mixed LSQR/LSMR); the replacement or
+// restart step of every iteration returns at entry while it is set.
 // kIterRef: iteration count at the last replacement.
 enum Flag {
     kDone = 0, kStatus = 1, kIter = 2, kRefine = 3, kPending = 4, kRestart = 5, kSkip = 6, kIterRef = 7,
@@ -81,6 +84,17 @@ constexpr double kRestartDeviation = 0.1;
 // refine_every iterations at the latest, and whenever it meets the
 // tolerance (convergence is declared on the true residual only).
 constexpr double kReplaceDrop = 1e-4;
+
+// Mixed LSQR/LSMR restart from the FP64 residual b - A x (an outer
+// refinement step on the least-squares correction) once the recursive
+// estimate of ||A'r|| has dropped by this factor since the last (re)start:
+// well above the relative accuracy the FP32 products leave a cycle, so a
+// cycle never iterates on noise, and few enough restarts that little of
+// the Krylov space is thrown away.
+constexpr double kLsqrRestartDrop = 1e-4;
+// A host check at a chunk boundary that finds the true residual this many
+// times above the mixed cycle's recursive estimate restarts the cycle.
+constexpr double kLsqrDrift = 100.0;
 
 __device__ __forceinline__ bool gated(const int* gate) { return gate && *(volatile const int*)gate != 0; }
 
@@ -409,14 +423,17 @@ __global__ void __launch_bounds__(kVecThreads) pcg_residual_kernel(ColSum cs,
 }
 
 // DiagonalPreconditioner (Math/Solver.h:25-38): d = 1/diag(A'A), entries that
-// are not normal (inf from an empty column) become 1.  jacobi == 0: d = 1.
-__global__ void precond_kernel(const uint64_t* __restrict__ diag, int64_t n, int jacobi, double* __restrict__ d)
+// are not normal (inf from an empty column) become 1.  mode 0: d = 1;
+// mode 2: the LSQR/LSMR column scale d = diag(A'A)^-1/2, 1 for an empty
+// column.
+__global__ void precond_kernel(const uint64_t* __restrict__ diag, int64_t n, int mode, double* __restrict__ d)
 {
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         double v = 1.0;
-        if (jacobi) {
-            v = 1.0 / static_cast<double>(diag[c]);
+        if (mode) {
+            const double dg = static_cast<double>(diag[c]);
+            v = 1.0 / (mode == 2 ? sqrt(dg) : dg);
             if (!(isfinite(v) && fabs(v) >= 2.2250738585072014e-308)) v = 1.0;  // not std::isnormal
         }
         d[c] = v;
@@ -433,16 +450,18 @@ __global__ void cast_kernel(int64_t n, const double* __restrict__ in, T* __restr
 
 // ||v||^2 partials of v = bn + (A' q from unit partials); partial may be
 // null (v = bn), bn may be null (v = A' q).  Used for ||A'b||^2 and ||A'r||^2.
+// sc (may be null) scales v column by column first (||S A'b||^2).
 template <bool COMP>
 __global__ void __launch_bounds__(kVecThreads) norm_units_kernel(ColSum cs,
                                                                  double* __restrict__ out, double* __restrict__ part,
-                                                                 const double* __restrict__ bn)
+                                                                 const double* __restrict__ bn,
+                                                                 const double* __restrict__ sc = nullptr)
 {
     __shared__ double smem[64];
     Comp acc;
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cs.a.cols;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const double v = (bn ? bn[c] : 0.0) + cs(c);
+        const double v = ((bn ? bn[c] : 0.0) + cs(c)) * (sc ? sc[c] : 1.0);
         if (out) out[c] = v;
         acc_add<COMP>(acc, v * v);
     }
@@ -464,22 +483,34 @@ __global__ void __launch_bounds__(kRedThreads) store_sum_kernel(const double* __
 // held as device scalars, so no separate scaling pass is needed.
 // ---------------------------------------------------------------------------
 
-// v_hat = (1/beta) A' u_hat - beta v  (v = v_hat_prev / alpha_prev);
-// partial ||v_hat||^2.  init: v_hat = (1/beta) A' u_hat.
+// Column scale of an LSQR/LSMR solve on A S (null: unscaled).
+__device__ __forceinline__ double col_scale(const double* sc, int64_t c) { return sc ? sc[c] : 1.0; }
+
+// The kernels of an LSQR/LSMR step return at entry once the solver is done
+// (init 0 and 2) and, for the restart step, while *gate is set; init 1 is
+// the set-up and always runs.
+__device__ __forceinline__ bool lsqr_skip(const Dev& dv, int init, const int* gate)
+{
+    return (init != 1 && finished(dv.flags)) || gated(gate);
+}
+
+// v_hat = (1/beta) S A' u_hat - beta v  (v = v_hat_prev / alpha_prev);
+// partial ||v_hat||^2.  init: v_hat = (1/beta) S A' u_hat.
 template <bool COMP, typename T>
 __global__ void __launch_bounds__(kVecThreads) lsqr_v_kernel(ColSum cs,
                                                              double* __restrict__ v, double* __restrict__ part,
-                                                             Dev dv, int init)
+                                                             Dev dv, int init, const int* __restrict__ gate,
+                                                             const double* __restrict__ sc)
 {
     __shared__ double smem[64];
-    if (init != 1 && finished(dv.flags)) return;
+    if (lsqr_skip(dv, init, gate)) return;
     const double inv_beta = dv.scal[kInvBeta];
     const double beta = dv.scal[kLBeta];
     const double inv_alpha_prev = dv.scal[kLAlpha] != 0 ? 1.0 / dv.scal[kLAlpha] : 0.0;
     Comp acc;
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cs.a.cols;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        double val = inv_beta * cs(c);
+        double val = inv_beta * col_scale(sc, c) * cs(c);
         if (!init) val -= beta * (v[c] * inv_alpha_prev);
         v[c] = val;
         acc_add<COMP>(acc, val * val);
@@ -487,14 +518,14 @@ __global__ void __launch_bounds__(kVecThreads) lsqr_v_kernel(ColSum cs,
     write_partial<COMP>(part, acc, smem);
 }
 
-// beta = ||u_hat|| (u_hat = A v - alpha u, alpha u = alpha/beta_prev u_hat_prev
+// beta = ||u_hat|| (u_hat = A S v - alpha u, alpha u = alpha/beta_prev u_hat_prev
 // folded into the SpMV's coefficient slot).  Single block.
 template <bool COMP>
 __global__ void __launch_bounds__(kRedThreads) lsqr_beta_kernel(const double* __restrict__ part, int n, Dev dv,
-                                                                int init)
+                                                                int init, const int* __restrict__ gate)
 {
     __shared__ double smem[64];
-    if (init != 1 && finished(dv.flags)) return;
+    if (lsqr_skip(dv, init, gate)) return;
     const double s = reduce_partials<COMP>(part, n, smem);
     if (threadIdx.x == 0) {
         const double beta = sqrt(s);
@@ -505,13 +536,31 @@ __global__ void __launch_bounds__(kRedThreads) lsqr_beta_kernel(const double* __
     }
 }
 
+// Relative recursive residual of an LSQR/LSMR step (against ||S A'b|| when
+// the columns are scaled, the norm the recursion estimates), the tolerance
+// test and, with plan (mixed solves), the restart test: a restart is
+// scheduled (kSkip cleared) when the estimate has dropped by
+// kLsqrRestartDrop since the last (re)start and the tolerance is not met.
+__device__ __forceinline__ void lsqr_step_tests(Dev dv, double arn, int plan, bool scaled)
+{
+    dv.scal[kArNorm] = arn;
+    dv.flags[kIter] += 1;
+    const double bn2 = dv.scal[scaled ? kBn2S : kBn2];
+    const double res = bn2 > 0 ? arn / sqrt(bn2) : arn;
+    dv.scal[kRes] = res;
+    const bool met = dv.scal[kTol] > 0 && res <= dv.scal[kTol];
+    if (met) dv.flags[kPending] = 1;
+    if (plan && !met && arn <= kLsqrRestartDrop * dv.scal[kArn0]) dv.flags[kSkip] = 0;
+}
+
 // alpha = ||v_hat||; Givens step; scalars for the x/w update.  Single block.
 template <bool COMP>
 __global__ void __launch_bounds__(kRedThreads) lsqr_alpha_kernel(const double* __restrict__ part, int n, Dev dv,
-                                                                 int init)
+                                                                 int init, const int* __restrict__ gate, int plan,
+                                                                 int scaled)
 {
     __shared__ double smem[64];
-    if (init != 1 && finished(dv.flags)) return;
+    if (lsqr_skip(dv, init, gate)) return;
     const double s = reduce_partials<COMP>(part, n, smem);
     if (threadIdx.x == 0) {
         const double alpha = sqrt(s);
@@ -519,6 +568,7 @@ __global__ void __launch_bounds__(kRedThreads) lsqr_alpha_kernel(const double* _
             dv.scal[kLAlpha] = alpha;
             dv.scal[kRhoBar] = alpha;  // rho_bar = alpha (Math/Solver.h:150)
             dv.scal[kArNorm] = alpha * dv.scal[kLBeta];
+            dv.scal[kArn0] = alpha * dv.scal[kLBeta];
             return;
         }
         const double beta = dv.scal[kLBeta];
@@ -540,36 +590,45 @@ __global__ void __launch_bounds__(kRedThreads) lsqr_alpha_kernel(const double* _
         dv.scal[kThetaRho] = theta / rho;
         dv.scal[kLAlpha] = alpha;
         // ||A'r_k|| = phi_bar_{k+1} * alpha_{k+1} * |c_k| (Paige & Saunders 1982)
-        const double arn = fabs(sn * phi_bar * alpha * c);
-        dv.scal[kArNorm] = arn;
-        dv.flags[kIter] += 1;
-        const double bn2 = dv.scal[kBn2];
-        const double res = bn2 > 0 ? arn / sqrt(bn2) : arn;
-        dv.scal[kRes] = res;
-        if (dv.scal[kTol] > 0 && res <= dv.scal[kTol]) dv.flags[kPending] = 1;
+        lsqr_step_tests(dv, fabs(sn * phi_bar * alpha * c), plan, scaled != 0);
     }
 }
 
-// x += (phi/rho) w; w = v - (theta/rho) w; gather copy vg = v (normalised).
+// x += (phi/rho) S w; w = v - (theta/rho) w; gather copy vg = S v (v
+// normalised).
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) lsqr_xw_kernel(int64_t n, double* __restrict__ x,
                                                               double* __restrict__ w, const double* __restrict__ v,
-                                                              T* __restrict__ vg, Dev dv, int init)
+                                                              T* __restrict__ vg, Dev dv, int init,
+                                                              const int* __restrict__ gate,
+                                                              const double* __restrict__ sc)
 {
-    if (init != 1 && finished(dv.flags)) return;
+    if (lsqr_skip(dv, init, gate)) return;
     const double inv_alpha = dv.scal[kLAlpha] != 0 ? 1.0 / dv.scal[kLAlpha] : 0.0;
     const double phi_rho = dv.scal[kPhiRho], theta_rho = dv.scal[kThetaRho];
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const double vn = v[c] * inv_alpha;
+        const double scale = col_scale(sc, c);
         if (init) {
             w[c] = vn;
         } else {
-            x[c] += phi_rho * w[c];
+            x[c] += phi_rho * scale * w[c];
             w[c] = vn - theta_rho * w[c];
         }
-        vg[c] = static_cast<T>(vn);
+        vg[c] = static_cast<T>(scale * vn);
     }
+}
+
+// u_hat in FP32 after a restart of the mixed solver computed it in FP64.
+__global__ void __launch_bounds__(kVecThreads) lsqr_round_u_kernel(int64_t n, const double* __restrict__ u,
+                                                                   float* __restrict__ uf, Dev dv,
+                                                                   const int* __restrict__ gate)
+{
+    if (finished(dv.flags) || gated(gate)) return;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        uf[i] = static_cast<float>(u[i]);
 }
 
 // ---------------------------------------------------------------------------
@@ -611,10 +670,11 @@ __device__ __forceinline__ void givens(double a, double b, double& c, double& s,
 // exact): the solver stops.  Single block.
 template <bool COMP>
 __global__ void __launch_bounds__(kRedThreads) lsmr_alpha_kernel(const double* __restrict__ part, int n, Dev dv,
-                                                                 int init)
+                                                                 int init, const int* __restrict__ gate, int plan,
+                                                                 int scaled)
 {
     __shared__ double smem[64];
-    if (init != 1 && finished(dv.flags)) return;
+    if (lsqr_skip(dv, init, gate)) return;
     const double sum = reduce_partials<COMP>(part, n, smem);
     if (threadIdx.x != 0) return;
     const double alpha = sqrt(sum);
@@ -629,6 +689,7 @@ __global__ void __launch_bounds__(kRedThreads) lsmr_alpha_kernel(const double* _
         sc[kCBar] = 1;
         sc[kSBar] = 0;
         sc[kArNorm] = alpha * beta;
+        sc[kArn0] = alpha * beta;
         return;
     }
     const double rho_old = sc[kMRho], rho_bar_old = sc[kMRhoBar];
@@ -658,47 +719,45 @@ __global__ void __launch_bounds__(kRedThreads) lsmr_alpha_kernel(const double* _
     sc[kFX] = zeta / rho / rho_bar;
     sc[kFH] = theta_new / rho;
     sc[kLAlpha] = alpha;
-    const double arn = fabs(zeta_bar);
-    sc[kArNorm] = arn;
-    dv.flags[kIter] += 1;
-    const double bn2 = sc[kBn2];
-    const double res = bn2 > 0 ? arn / sqrt(bn2) : arn;
-    sc[kRes] = res;
-    if (sc[kTol] > 0 && res <= sc[kTol]) dv.flags[kPending] = 1;
+    lsqr_step_tests(dv, fabs(zeta_bar), plan, scaled != 0);
 }
 
-// h_bar = h - f_hbar h_bar; x += f_x h_bar; h = v - f_h h (v normalised);
-// gather copy vg = v.  init: h = v, h_bar = 0.
+// h_bar = h - f_hbar h_bar; x += f_x S h_bar; h = v - f_h h (v normalised);
+// gather copy vg = S v.  init: h = v, h_bar = 0.
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) lsmr_update_kernel(int64_t n, double* __restrict__ x,
                                                                   double* __restrict__ h, double* __restrict__ hbar,
                                                                   const double* __restrict__ v, T* __restrict__ vg,
-                                                                  Dev dv, int init)
+                                                                  Dev dv, int init, const int* __restrict__ gate,
+                                                                  const double* __restrict__ sc)
 {
-    if (init != 1 && finished(dv.flags)) return;
+    if (lsqr_skip(dv, init, gate)) return;
     const double inv_alpha = dv.scal[kLAlpha] != 0 ? 1.0 / dv.scal[kLAlpha] : 0.0;
     const double f_hbar = dv.scal[kFHbar], f_x = dv.scal[kFX], f_h = dv.scal[kFH];
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
          c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const double vn = v[c] * inv_alpha;
+        const double scale = col_scale(sc, c);
         if (init) {
             h[c] = vn;
             hbar[c] = 0;
         } else {
             const double hb = h[c] - f_hbar * hbar[c];
             hbar[c] = hb;
-            x[c] += f_x * hb;
+            x[c] += f_x * scale * hb;
             h[c] = vn - f_h * h[c];
         }
-        vg[c] = static_cast<T>(vn);
+        vg[c] = static_cast<T>(scale * vn);
     }
 }
 
 // coefficient of the u recursion: alpha / beta_prev (u_hat holds beta_prev u).
 // First kernel of an LSQR step: a tolerance met by the previous step stops
-// the solver here, after that step's x/w update has run.
+// the solver here, after that step's x/w update has run.  It also closes
+// the gate of the step's restart, which the step's alpha kernel may open.
 __global__ void lsqr_coef_kernel(Dev dv, int slot)
 {
+    dv.flags[kSkip] = 1;
     if (finished(dv.flags)) return;
     if (dv.flags[kPending]) {
         dv.flags[kDone] = 1;
@@ -730,6 +789,9 @@ struct SolverImpl {
     cas_solve_opts o{};
     // LSQR and LSMR: the bidiagonalisation methods on min ||Ax - b||
     bool least_squares() const { return o.method == CAS_LSQR || o.method == CAS_LSMR; }
+    // LSQR/LSMR on A S, S = diag(A'A)^-1/2 held in d
+    bool scaled() const { return least_squares() && o.scale_columns != 0; }
+    const double* col_scale() const { return scaled() ? d : nullptr; }
     cudaStream_t s = nullptr;
     int device = 0;
     bool mixed = false;
@@ -754,7 +816,6 @@ struct SolverImpl {
     int* host_flags = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_len = 0;
-    int graph_phase = -1;
     long long graph_kernels = 0;
     int launched = 0;  // iterations issued (including no-op tail)
     bool own_stream = false;  // graphs cannot be captured on the legacy default stream
@@ -892,57 +953,69 @@ struct SolverImpl {
     {
         const Dev D = dv();
         T* vg = reinterpret_cast<T*>(std::is_same<T, float>::value ? (void*)pg32 : (void*)p);
-        // u_hat = A v - (alpha / beta_prev) u_hat_prev
+        const double* sc = col_scale();
+        const int plan = mixed ? 1 : 0;
+        const int sd = scaled() ? 1 : 0;
+        // u_hat = A S v - (alpha / beta_prev) u_hat_prev
         { lsqr_coef_kernel<<<1, 1, 0, s>>>(D, kPap); cas::count_launch(); }
         CAS_TRY((product<COMP, T, T>(vg, static_cast<T*>(q), 1, nullptr, kPap, done())));
-        { lsqr_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, 0); cas::count_launch(); }
-        // v_hat = (1/beta) A' u_hat - beta v
+        { lsqr_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, 0, nullptr); cas::count_launch(); }
+        // v_hat = (1/beta) S A' u_hat - beta v
         CAS_TRY(product_t<T>(static_cast<const T*>(q), done()));
-        { lsqr_v_kernel<COMP, T><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<T>(), v, part_a, D, 0); cas::count_launch(); }
+        { lsqr_v_kernel<COMP, T><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<T>(), v, part_a, D, 0, nullptr, sc); cas::count_launch(); }
         if (o.method == CAS_LSMR) {
             // LSMR: h in w, h_bar in z
-            { lsmr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 0); cas::count_launch(); }
-            { lsmr_update_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, z, v, vg, D, 0); cas::count_launch(); }
+            { lsmr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 0, nullptr, plan, sd); cas::count_launch(); }
+            { lsmr_update_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, z, v, vg, D, 0, nullptr, sc); cas::count_launch(); }
         } else {
-            { lsqr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 0); cas::count_launch(); }
-            { lsqr_xw_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, vg, D, 0); cas::count_launch(); }
+            { lsqr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, 0, nullptr, plan, sd); cas::count_launch(); }
+            { lsqr_xw_kernel<T><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, vg, D, 0, nullptr, sc); cas::count_launch(); }
         }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
     }
 
-    // LSQR (re)start from the current x (Math/Solver.h:139-151 with b - A x
-    // for b): beta u = b - A x ; alpha v = A'u ; w = v ; phi_bar = beta ;
-    // rho_bar = alpha.  mode 1 = setup, 2 = restart inside a graph chunk
-    // (the mixed solver's refinement: the true residual replaces b).
-    cas_status issue_lsqr_start(int mode)
+    // LSQR/LSMR (re)start from the current x (Math/Solver.h:139-151 with
+    // b - A x for b): beta u = b - A x ; alpha v = S A'u ; w = v ; phi_bar =
+    // beta ; rho_bar = alpha.  mode 1 = set-up, 2 = the restart step of a
+    // mixed iteration inside a graph chunk (runs only when the step's alpha
+    // kernel opened the kSkip gate), 3 = a restart issued by the host.
+    // The mixed solver computes u and S A'u in FP64 (u is the least-squares
+    // residual, large next to A'u once the solve has progressed, so FP32
+    // would bury A'u under its own rounding) and keeps an FP32 copy of u_hat
+    // for the following steps: a restart is one outer refinement step on the
+    // least-squares correction.
+    cas_status issue_lsqr_start(int mode) { return mixed ? issue_lsqr_start_t<true>(mode) : issue_lsqr_start_t<false>(mode); }
+
+    template <bool COMP>
+    cas_status issue_lsqr_start_t(int mode)
     {
         const Dev D = dv();
-        const bool gate = mode == 2;
+        const int* gate = mode == 2 ? skip() : nullptr;
+        const int init = mode == 1 ? 1 : 2;
+        const double* sc = col_scale();
+        const int sd = scaled() ? 1 : 0;
+        CAS_TRY((product<COMP, double, double>(x, q64, 2, b, 0, gate)));
+        { lsqr_beta_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, init, gate); cas::count_launch(); }
+        CAS_TRY(product_t<double>(q64, gate));
+        { lsqr_v_kernel<COMP, double><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), v, part_a, D, init, gate, sc); cas::count_launch(); }
         if (mixed) {
-            CAS_TRY((product<true, double, float>(x, static_cast<float*>(q), 2, b, 0, gate ? done() : nullptr)));
-            { lsqr_beta_kernel<true><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, mode); cas::count_launch(); }
-            CAS_TRY(product_t<float>(static_cast<const float*>(q), gate ? done() : nullptr));
-            { lsqr_v_kernel<true, float><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<float>(), v, part_a, D, mode); cas::count_launch(); }
-            if (o.method == CAS_LSMR) {
-                { lsmr_alpha_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
-                { lsmr_update_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, z, v, pg32, D, mode); cas::count_launch(); }
-            } else {
-                { lsqr_alpha_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
-                { lsqr_xw_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, pg32, D, mode); cas::count_launch(); }
-            }
+            { lsqr_round_u_kernel<<<row_grid(R), kVecThreads, 0, s>>>(R, q64, static_cast<float*>(q), D, gate); cas::count_launch(); }
         } else {
-            CAS_TRY((product<false, double, double>(x, static_cast<double*>(q), 2, b, 0, gate ? done() : nullptr)));
-            { lsqr_beta_kernel<false><<<1, kRedThreads, 0, s>>>(part_q, n_q_parts, D, mode); cas::count_launch(); }
-            CAS_TRY(product_t<double>(static_cast<const double*>(q), gate ? done() : nullptr));
-            { lsqr_v_kernel<false, double><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), v, part_a, D, mode); cas::count_launch(); }
-            if (o.method == CAS_LSMR) {
-                { lsmr_alpha_kernel<false><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
-                { lsmr_update_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, z, v, p, D, mode); cas::count_launch(); }
-            } else {
-                { lsqr_alpha_kernel<false><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, mode); cas::count_launch(); }
-                { lsqr_xw_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, p, D, mode); cas::count_launch(); }
-            }
+            CAS_CUDA(cudaMemcpyAsync(q, q64, sizeof(double) * R, cudaMemcpyDeviceToDevice, s));
+        }
+        if (o.method == CAS_LSMR) {
+            { lsmr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, init, gate, 0, sd); cas::count_launch(); }
+            if (mixed)
+                { lsmr_update_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, z, v, pg32, D, init, gate, sc); cas::count_launch(); }
+            else
+                { lsmr_update_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, z, v, p, D, init, gate, sc); cas::count_launch(); }
+        } else {
+            { lsqr_alpha_kernel<COMP><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, D, init, gate, 0, sd); cas::count_launch(); }
+            if (mixed)
+                { lsqr_xw_kernel<float><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, pg32, D, init, gate, sc); cas::count_launch(); }
+            else
+                { lsqr_xw_kernel<double><<<n_vec_blocks, kVecThreads, 0, s>>>(C, x, w, v, p, D, init, gate, sc); cas::count_launch(); }
         }
         CAS_CHECK_LAUNCH();
         return CAS_OK;
@@ -952,9 +1025,12 @@ struct SolverImpl {
     {
         const bool lsqr = o.method == CAS_LSQR || o.method == CAS_LSMR;
         if (lsqr) {
-            if (mixed) CAS_TRY((issue_lsqr_iteration<true, float>()));
-            else CAS_TRY((issue_lsqr_iteration<false, double>()));
-            if (mixed && o.refine_every > 0 && (global_index + 1) % o.refine_every == 0) CAS_TRY(issue_lsqr_start(2));
+            if (mixed) {
+                CAS_TRY((issue_lsqr_iteration<true, float>()));
+                CAS_TRY(issue_lsqr_start(2));  // runs only when the step's alpha kernel scheduled it
+            } else {
+                CAS_TRY((issue_lsqr_iteration<false, double>()));
+            }
             return CAS_OK;
         }
         if (mixed) {
@@ -970,11 +1046,8 @@ struct SolverImpl {
     // CUDA graph when the chunk shape allows.
     cas_status issue_chunk(int first, int n)
     {
-        // mixed LSQR restarts at fixed iterations: its graphs depend on the phase
-        const int period = (mixed && least_squares() && o.refine_every > 0) ? o.refine_every : 1;
-        const int phase = first % period;
         if (n > 1) {
-            if (!graph || graph_len != n || graph_phase != phase) {
+            if (!graph || graph_len != n) {
                 if (graph) {
                     cudaGraphExecDestroy(graph);
                     graph = nullptr;
@@ -996,7 +1069,6 @@ struct SolverImpl {
                 cudaGraphDestroy(g);
                 CAS_CUDA(e);
                 graph_len = n;
-                graph_phase = phase;
             }
             CAS_CUDA(cudaGraphLaunch(graph, s));
             count_launch(graph_kernels);
@@ -1071,7 +1143,8 @@ struct SolverImpl {
             CAS_CUDA(cudaMemsetAsync(x, 0, cb, s));
         CAS_CUDA(cudaMemsetAsync(w, 0, cb, s));
         CAS_CUDA(cudaMemsetAsync(v, 0, cb, s));
-        { precond_kernel<<<vec_grid(C), kVecThreads, 0, s>>>(a.diag_int, C, (o.method == CAS_PCG && o.jacobi) ? 1 : 0, d); cas::count_launch(); }
+        const int pmode = (o.method == CAS_PCG && o.jacobi) ? 1 : (scaled() ? 2 : 0);
+        { precond_kernel<<<vec_grid(C), kVecThreads, 0, s>>>(a.diag_int, C, pmode, d); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         const Dev D = dv();
 
@@ -1085,6 +1158,11 @@ struct SolverImpl {
             { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), nullptr, part_a, nullptr); cas::count_launch(); }
         }
         { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kBn2); cas::count_launch(); }
+        if (scaled()) {
+            // ||S A'b||^2: the norm the scaled recursion's residual estimate is relative to
+            { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), nullptr, part_a, nullptr, d); cas::count_launch(); }
+            { store_sum_kernel<true><<<1, kRedThreads, 0, s>>>(part_a, n_vec_blocks, scal + kBn2S); cas::count_launch(); }
+        }
         CAS_CHECK_LAUNCH();
 
         if (least_squares()) {
@@ -1123,6 +1201,8 @@ cas_status validate_opts(const cas_solve_opts* o)
                 "unknown precision mode");
     CAS_REQUIRE(o->max_iterations >= 0 && o->check_every >= 0 && o->refine_every >= 0, CAS_ERR_INVALID_ARGUMENT,
                 "negative iteration counts in solver options");
+    CAS_REQUIRE(o->scale_columns == 0 || o->scale_columns == 1, CAS_ERR_INVALID_ARGUMENT,
+                "scale_columns must be 0 or 1");
     return CAS_OK;
 }
 }  // namespace
@@ -1139,6 +1219,7 @@ CAS_API void cas_solve_opts_default(cas_solve_opts* o)
     o->refine_every = 50;
     o->check_every = 50;
     o->jacobi = 1;
+    o->scale_columns = 0;
 }
 
 }  // extern "C"
@@ -1285,6 +1366,10 @@ CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
             // at every chunk boundary.
             CAS_TRY(m.true_residual(&rel));
             if (rel <= m.o.tol) break;
+            // The mixed solver's cycle has drifted: its estimate is more than
+            // kLsqrDrift times below the true residual (the FP32 products'
+            // noise floor reached before the restart drop): restart now.
+            if (m.mixed && m.host_scal[kRes] * kLsqrDrift < rel && !m.scaled()) CAS_TRY(m.issue_lsqr_start(3));
         }
         if (done) {
             if (m.host_flags[kVerified] && !m.least_squares()) {
@@ -1304,7 +1389,11 @@ CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
             static const int zero = 0;
             CAS_CUDA(cudaMemcpyAsync(m.flags + kDone, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
             CAS_CUDA(cudaMemcpyAsync(m.flags + kPending, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
-            if (m.least_squares()) {
+            if (m.least_squares() && m.mixed) {
+                // the mixed cycle's estimate met the tolerance but the FP64
+                // residual did not: restart from it
+                CAS_TRY(m.issue_lsqr_start(3));
+            } else if (m.least_squares()) {
                 // LSQR / LSMR have no residual to replace: tighten the recursive target
                 double t = m.host_scal[kTol] * 0.5;
                 CAS_CUDA(cudaMemcpyAsync(m.scal + kTol, &t, sizeof t, cudaMemcpyHostToDevice, m.s));

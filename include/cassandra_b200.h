@@ -254,9 +254,15 @@ typedef struct cas_solve_opts {
     cas_precision precision;
     double tol;         /* stop when ||A'(b-Ax)|| / ||A'b|| <= tol; <= 0: run max_iterations */
     int max_iterations;
-    int refine_every;   /* CAS_MIXED: iterations between true-residual replacements (50) */
+    int refine_every;   /* CAS_MIXED PCG: most iterations between true-residual replacements (50).
+                           CAS_MIXED LSQR/LSMR restart from the FP64 residual when their
+                           recursive estimate of ||A'r|| has dropped 1e4-fold since the last
+                           (re)start, or when a host check finds it off the true residual. */
     int check_every;    /* iterations per host-side convergence check (graph chunk) */
     int jacobi;         /* PCG: 1 = Jacobi preconditioner (FitWeights), 0 = none */
+    int scale_columns;  /* LSQR/LSMR: 1 = iterate on A S with S = diag(A'A)^-1/2 (empty columns
+                           scaled by 1) and return x = S y; 0 = the reference's unscaled
+                           method (Math/Solver.h:128-287), the default.  Ignored by PCG/CG. */
 } cas_solve_opts;
 
 typedef struct cas_solve_report {

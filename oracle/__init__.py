@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import contextlib
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -25,7 +26,8 @@ HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liboracle.so"
 REF_SO = HERE / "_ref" / "libcasref.so"
 REF64_SO = HERE / "_ref" / "libcasref64.so"
-REFERENCE_TREE = Path("/root/reference")
+# the reference tree: $CASSANDRA_REFERENCE when set, else its location in the build container
+REFERENCE_TREE = Path(os.environ.get("CASSANDRA_REFERENCE", "/root/reference"))
 
 _VP = C.c_void_p
 _I64 = C.c_int64
@@ -36,7 +38,7 @@ def build(ref: bool = True) -> None:
     targets = ["oracle"]
     if ref and REFERENCE_TREE.is_dir():
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REFERENCE_TREE}", *targets], check=True)
 
 
 def _p(a: np.ndarray):
@@ -76,6 +78,14 @@ def c_lib() -> C.CDLL:
             getattr(lib, n).restype = C.c_int
             getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, C.c_double, C.c_int, _VP,
                                         C.POINTER(C.c_double)]
+        for n in ("or_lsqr_scaled", "or_lsmr_scaled"):
+            getattr(lib, n).restype = C.c_int
+            getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, C.c_int, C.c_double, C.c_int, _VP,
+                                        C.POINTER(C.c_double)]
+        lib.or_generate_positions.restype = C.c_int
+        lib.or_generate_positions.argtypes = [C.c_uint64, _I64, _I64, C.c_int, C.c_int, _VP]
+        lib.or_generate_targets.restype = None
+        lib.or_generate_targets.argtypes = [C.c_int, _I64, _I64, _VP, C.c_uint64, C.c_double, C.c_double, _VP, _VP]
         _c = lib
     return _c
 
@@ -171,6 +181,8 @@ def ref64_lib() -> C.CDLL:
         for n in ("ref64_pcg", "ref64_lsqr", "ref64_lsmr"):
             getattr(lib, n).restype = C.c_int
             getattr(lib, n).argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, C.c_double, C.c_int, _VP, _VP, _VP]
+        lib.ref64_check.restype = None
+        lib.ref64_check.argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int, _VP, _VP, _VP]
         lib.ref64_pcg_seconds_per_iteration.restype = C.c_double
         lib.ref64_pcg_seconds_per_iteration.argtypes = [C.c_int, _I64, _I64, _VP, _VP, C.c_int]
         _ref64 = lib
@@ -238,22 +250,45 @@ def pcg(idx, cols, b, iterations, tol=0.0, check_every=1, jacobi=True):
     return x, res.value, it
 
 
-def lsqr(idx, cols, b, iterations, tol=0.0, check_every=1):
+def lsqr(idx, cols, b, iterations, tol=0.0, check_every=1, scale=False):
+    """LSQR (Math/Solver.h:128-182) in FP64 from x0 = 0: x, phi_bar, steps.
+    scale=True: on A S, S = diag(A'A)^-1/2, x = S y (not in the reference)."""
     idx = np.ascontiguousarray(idx, dtype=np.uint32)
     b = np.ascontiguousarray(b, dtype=np.float64)
     x = np.empty(cols, dtype=np.float64)
     res = C.c_double()
-    it = c_lib().or_lsqr(idx.shape[1], idx.shape[0], cols, _p(idx), _p(b), iterations, tol, check_every, _p(x),
-                         C.byref(res))
+    it = c_lib().or_lsqr_scaled(idx.shape[1], idx.shape[0], cols, _p(idx), _p(b), int(scale), iterations, tol,
+                                check_every, _p(x), C.byref(res))
     return x, res.value, it
 
 
-def lsmr(idx, cols, b, iterations, tol=0.0, check_every=1):
-    """LSMR (Math/Solver.h:222-287) in FP64 from x0 = 0: x, |zeta_bar|, steps."""
+def lsmr(idx, cols, b, iterations, tol=0.0, check_every=1, scale=False):
+    """LSMR (Math/Solver.h:222-287) in FP64 from x0 = 0: x, |zeta_bar|, steps.
+    scale=True: on A S, S = diag(A'A)^-1/2, x = S y (not in the reference)."""
     idx = np.ascontiguousarray(idx, dtype=np.uint32)
     b = np.ascontiguousarray(b, dtype=np.float64)
     x = np.empty(cols, dtype=np.float64)
     res = C.c_double()
-    it = c_lib().or_lsmr(idx.shape[1], idx.shape[0], cols, _p(idx), _p(b), iterations, tol, check_every, _p(x),
-                         C.byref(res))
+    it = c_lib().or_lsmr_scaled(idx.shape[1], idx.shape[0], cols, _p(idx), _p(b), int(scale), iterations, tol,
+                                check_every, _p(x), C.byref(res))
     return x, res.value, it
+
+
+def generate_positions(seed: int, first: int, n: int, min_empties: int, max_empties: int) -> np.ndarray:
+    """The library's seeded random-play positions, restated in C: uint64 [n, 2]
+    rows (P, O) for position indices first .. first + n - 1."""
+    out = np.empty((n, 2), dtype=np.uint64)
+    if c_lib().or_generate_positions(seed, first, n, min_empties, max_empties, _p(out)) != 0:
+        raise ValueError("bad arguments or an unreachable empty count")
+    return out
+
+
+def generate_targets(idx: np.ndarray, cols: int, seed: int, w_sigma: float = 0.5,
+                     noise_sigma: float = 4.0) -> tuple[np.ndarray, np.ndarray]:
+    """The library's seeded targets for the system idx, restated in C:
+    (b, w_true) with b = clamp(2 rint((A w* + e) / 2), -64, 64)."""
+    idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    b = np.empty(idx.shape[0], dtype=np.float64)
+    w = np.empty(cols, dtype=np.float64)
+    c_lib().or_generate_targets(idx.shape[1], idx.shape[0], cols, _p(idx), seed, w_sigma, noise_sigma, _p(b), _p(w))
+    return b, w

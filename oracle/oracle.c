@@ -398,25 +398,61 @@ static double decompose(double* v, int64_t n)
     return len;
 }
 
+/* Column scale of LSQR/LSMR on A S: s_c = diag(A'A)_c^-1/2, 1 for an empty
+ * column (returns NULL when scale == 0: the reference's unscaled methods).
+ * Column scaling is the diagonal right preconditioning that Paige and
+ * Saunders (1982, section 5.4) recommend for LSQR; the reference has none. */
+static double* column_scale(int scale, int k, int64_t rows, int64_t cols, const uint32_t* idx)
+{
+    if (!scale) return NULL;
+    double* s = malloc(sizeof(double) * (size_t)(cols ? cols : 1));
+    or_jacobi(k, rows, cols, idx, s); /* 1/diag, inf for an empty column */
+    for (int64_t c = 0; c < cols; c++) s[c] = isfinite(s[c]) && s[c] > 0 ? sqrt(s[c]) : 1.0;
+    return s;
+}
+
+/* y = A (S v) and v = S (A' y) */
+static void spmv_s(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* s, const double* v,
+                   double* tmp, double* y)
+{
+    if (!s) { or_spmv(k, rows, cols, idx, v, y); return; }
+    for (int64_t c = 0; c < cols; c++) tmp[c] = s[c] * v[c];
+    or_spmv(k, rows, cols, idx, tmp, y);
+}
+static void spmv_t_s(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* s, const double* y,
+                     double* v)
+{
+    or_spmv_t(k, rows, cols, idx, y, v);
+    if (s) for (int64_t c = 0; c < cols; c++) v[c] *= s[c];
+}
+
 int or_lsqr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int iterations, double tol,
             int check_every, double* x, double* residuum)
 {
+    return or_lsqr_scaled(k, rows, cols, idx, b, 0, iterations, tol, check_every, x, residuum);
+}
+
+int or_lsqr_scaled(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int scale,
+                   int iterations, double tol, int check_every, double* x, double* residuum)
+{
     size_t cb = sizeof(double) * (size_t)(cols ? cols : 1), rb = sizeof(double) * (size_t)(rows ? rows : 1);
-    double *u = malloc(rb), *tu = malloc(rb), *v = malloc(cb), *tv = malloc(cb), *w = malloc(cb);
+    double *u = malloc(rb), *tu = malloc(rb), *v = malloc(cb), *tv = malloc(cb), *w = malloc(cb),
+           *tmp = malloc(cb);
+    double* sc = column_scale(scale, k, rows, cols, idx);
     memset(x, 0, cb);
     memcpy(u, b, rb); /* (:139-151) */
     double beta = decompose(u, rows);
-    or_spmv_t(k, rows, cols, idx, u, v);
+    spmv_t_s(k, rows, cols, idx, sc, u, v);
     double alpha = decompose(v, cols);
     memcpy(w, v, cb);
     double phi_bar = beta, rho_bar = alpha;
     int it = 0;
     if (check_every <= 0) check_every = 1;
     for (; it < iterations;) { /* Iterate (:153-177) */
-        or_spmv(k, rows, cols, idx, v, tu);
+        spmv_s(k, rows, cols, idx, sc, v, tmp, tu);
         for (int64_t i = 0; i < rows; i++) u[i] = tu[i] - alpha * u[i];
         beta = decompose(u, rows);
-        or_spmv_t(k, rows, cols, idx, u, tv);
+        spmv_t_s(k, rows, cols, idx, sc, u, tv);
         for (int64_t i = 0; i < cols; i++) v[i] = tv[i] - beta * v[i];
         alpha = decompose(v, cols);
         double rho = sqrt(rho_bar * rho_bar + beta * beta);
@@ -426,13 +462,13 @@ int or_lsqr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double
         rho_bar = -c * alpha;
         double phi = c * phi_bar;
         phi_bar = s * phi_bar;
-        for (int64_t i = 0; i < cols; i++) x[i] += (phi / rho) * w[i];
+        for (int64_t i = 0; i < cols; i++) x[i] += (phi / rho) * (sc ? sc[i] : 1.0) * w[i];
         for (int64_t i = 0; i < cols; i++) w[i] = v[i] - (theta / rho) * w[i];
         it++;
         if (tol > 0 && it % check_every == 0 && or_normal_residual(k, rows, cols, idx, b, x) <= tol) break;
     }
     *residuum = phi_bar; /* Residuum (:179) */
-    free(u); free(tu); free(v); free(tv); free(w);
+    free(u); free(tu); free(v); free(tv); free(w); free(tmp); free(sc);
     return it;
 }
 
@@ -461,13 +497,20 @@ static void or_givens(double a, double b, double* c, double* s, double* r)
 int or_lsmr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int iterations, double tol,
             int check_every, double* x, double* zeta_bar_out)
 {
+    return or_lsmr_scaled(k, rows, cols, idx, b, 0, iterations, tol, check_every, x, zeta_bar_out);
+}
+
+int or_lsmr_scaled(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int scale,
+                   int iterations, double tol, int check_every, double* x, double* zeta_bar_out)
+{
     size_t cb = sizeof(double) * (size_t)(cols ? cols : 1), rb = sizeof(double) * (size_t)(rows ? rows : 1);
     double *u = malloc(rb), *tu = malloc(rb), *v = malloc(cb), *tv = malloc(cb), *h = malloc(cb),
-           *hb = malloc(cb);
+           *hb = malloc(cb), *tmp = malloc(cb);
+    double* sc = column_scale(scale, k, rows, cols, idx);
     memset(x, 0, cb);
     memcpy(u, b, rb); /* constructor (:236-251) */
     double beta = decompose(u, rows);
-    or_spmv_t(k, rows, cols, idx, u, v);
+    spmv_t_s(k, rows, cols, idx, sc, u, v);
     double alpha = decompose(v, cols);
     double alpha_bar = alpha, zeta_bar = alpha * beta, rho = 1, rho_bar = 1, c_bar = 1, s_bar = 0;
     memcpy(h, v, cb);
@@ -476,10 +519,10 @@ int or_lsmr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double
     if (check_every <= 0) check_every = 1;
     for (; it < iterations;) { /* Iterate (:253-282) */
         double rho_old = rho, rho_bar_old = rho_bar;
-        or_spmv(k, rows, cols, idx, v, tu);
+        spmv_s(k, rows, cols, idx, sc, v, tmp, tu);
         for (int64_t i = 0; i < rows; i++) u[i] = tu[i] - alpha * u[i];
         beta = decompose(u, rows);
-        or_spmv_t(k, rows, cols, idx, u, tv);
+        spmv_t_s(k, rows, cols, idx, sc, u, tv);
         for (int64_t i = 0; i < cols; i++) v[i] = tv[i] - beta * v[i];
         alpha = decompose(v, cols);
         double c_hat, s_hat, alpha_hat;
@@ -496,13 +539,141 @@ int or_lsmr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double
         double f_hb = theta_bar * rho / rho_old / rho_bar_old, f_x = zeta / rho / rho_bar, f_h = theta_new / rho;
         for (int64_t i = 0; i < cols; i++) {
             hb[i] = h[i] - f_hb * hb[i];
-            x[i] += f_x * hb[i];
+            x[i] += f_x * (sc ? sc[i] : 1.0) * hb[i];
             h[i] = v[i] - f_h * h[i];
         }
         it++;
         if (tol > 0 && it % check_every == 0 && or_normal_residual(k, rows, cols, idx, b, x) <= tol) break;
     }
     *zeta_bar_out = fabs(zeta_bar);
-    free(u); free(tu); free(v); free(tv); free(h); free(hb);
+    free(u); free(tu); free(v); free(tv); free(h); free(hb); free(tmp); free(sc);
     return it;
+}
+
+/* ------------------------------------------------------------------------
+ * The seeded synthetic inputs of the tests and the benchmark, restated so
+ * that a process that must not load the CUDA library (the benchmark's
+ * reference arm) builds exactly the system the library's generator builds.
+ * Random play follows RandomPlayer (Game/Player.cpp:3-16): a uniform choice
+ * among the legal moves, a pass when the side to move has none; games that
+ * end before the target empty count are replayed with the stream going on.
+ * The stream is SplitMix64 (Steele, Lea and Flood 2014) used as a counter-
+ * based generator: state seeded from (seed, index), advanced by the
+ * golden-ratio increment and mixed on output.
+ * ---------------------------------------------------------------------- */
+static uint64_t sm_mix(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+typedef struct { uint64_t s; } stream_t;
+static stream_t sm_stream(uint64_t seed, uint64_t index)
+{
+    stream_t t = {sm_mix(seed ^ sm_mix(index + 0x632BE59BD9B4E019ULL))};
+    return t;
+}
+static uint64_t sm_next(stream_t* t)
+{
+    t->s += 0x9E3779B97F4A7C15ULL;
+    return sm_mix(t->s);
+}
+/* uniform in [0, n): multiply-high on 32 random bits */
+static uint32_t sm_below(stream_t* t, uint32_t n) { return (uint32_t)(((sm_next(t) >> 32) * n) >> 32); }
+/* uniform in (0, 1) */
+static double sm_unit(stream_t* t) { return ((double)(sm_next(t) >> 11) + 0.5) * (1.0 / 9007199254740992.0); }
+
+/* one square step in direction d of the 8 (bit 63 = A1, x = bit & 7) */
+static uint64_t dir_step(uint64_t b, int d)
+{
+    switch (d) {
+        case 0: return (b << 1) & 0xFEFEFEFEFEFEFEFEULL;
+        case 1: return (b >> 1) & 0x7F7F7F7F7F7F7F7FULL;
+        case 2: return b << 8;
+        case 3: return b >> 8;
+        case 4: return (b << 9) & 0xFEFEFEFEFEFEFEFEULL;
+        case 5: return (b << 7) & 0x7F7F7F7F7F7F7F7FULL;
+        case 6: return (b >> 7) & 0xFEFEFEFEFEFEFEFEULL;
+        default: return (b >> 9) & 0x7F7F7F7F7F7F7F7FULL;
+    }
+}
+static uint64_t moves_of(uint64_t p, uint64_t o)
+{
+    uint64_t m = 0;
+    for (int d = 0; d < 8; d++) {
+        uint64_t t = dir_step(p, d) & o;
+        for (int i = 0; i < 5; i++) t |= dir_step(t, d) & o;
+        m |= dir_step(t, d);
+    }
+    return m & ~(p | o);
+}
+static uint64_t flips_of(uint64_t p, uint64_t o, int sq)
+{
+    uint64_t all = 0;
+    for (int d = 0; d < 8; d++) {
+        uint64_t line = 0, x = dir_step(1ULL << sq, d);
+        while (x & o) { line |= x; x = dir_step(x, d); }
+        if (x & p) all |= line;
+    }
+    return all;
+}
+
+static int random_play(uint64_t seed, uint64_t i, int min_e, int max_e, uint64_t* out_p, uint64_t* out_o)
+{
+    stream_t rng = sm_stream(seed, i);
+    const int target = min_e + (int)sm_below(&rng, (uint32_t)(max_e - min_e + 1));
+    for (int attempt = 0; attempt < (1 << 16); attempt++) {
+        uint64_t p = 0x0000000810000000ULL, o = 0x0000001008000000ULL; /* Position::Start() */
+        int empties = 60, ended = 0;
+        while (empties > target) {
+            uint64_t m = moves_of(p, o);
+            if (!m) {
+                if (!moves_of(o, p)) { ended = 1; break; }
+                uint64_t t = p; p = o; o = t; /* pass */
+                continue;
+            }
+            uint32_t k = sm_below(&rng, (uint32_t)popcount64(m));
+            while (k--) m &= m - 1;
+            int sq = __builtin_ctzll(m);
+            uint64_t f = flips_of(p, o, sq);
+            uint64_t np = o ^ f;
+            o = p ^ f ^ (1ULL << sq);
+            p = np;
+            empties--;
+        }
+        if (!ended) { *out_p = p; *out_o = o; return 1; }
+    }
+    *out_p = 0x0000000810000000ULL;
+    *out_o = 0x0000001008000000ULL;
+    return 0;
+}
+
+int or_generate_positions(uint64_t seed, int64_t first, int64_t n, int min_e, int max_e, uint64_t* po)
+{
+    if (n < 0 || first < 0 || min_e < 0 || min_e > max_e || max_e > 60) return -1;
+    int ok = 1;
+#pragma omp parallel for schedule(static) reduction(&& : ok)
+    for (int64_t i = 0; i < n; i++) ok = random_play(seed, (uint64_t)(first + i), min_e, max_e, po + 2 * i, po + 2 * i + 1) && ok;
+    return ok ? 0 : -1;
+}
+
+void or_generate_targets(int k, int64_t rows, int64_t cols, const uint32_t* idx, uint64_t seed, double w_sigma,
+                         double noise_sigma, double* b, double* w_true)
+{
+    const double two_pi = 6.283185307179586;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < cols; c++) { /* w*_c ~ N(0, sigma^2), Box-Muller */
+        stream_t t = sm_stream(seed ^ 0x5EED0F3EC7ED1ULL, (uint64_t)c);
+        double u1 = sm_unit(&t), u2 = sm_unit(&t);
+        w_true[c] = w_sigma * sqrt(-2.0 * log(u1)) * cos(two_pi * u2);
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < rows; r++) { /* b_r = clamp(2 rint(((A w*)_r + e_r) / 2), -64, 64) */
+        double aw = 0;
+        for (int j = 0; j < k; j++) aw += w_true[idx[r * k + j]];
+        stream_t t = sm_stream(seed ^ 0xB0A5EDD15EA5EULL, (uint64_t)r);
+        double u1 = sm_unit(&t), u2 = sm_unit(&t);
+        double e = noise_sigma * sqrt(-2.0 * log(u1)) * cos(two_pi * u2);
+        b[r] = fmin(64.0, fmax(-64.0, 2.0 * rint((aw + e) * 0.5)));
+    }
 }

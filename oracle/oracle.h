@@ -43,5 +43,20 @@ int or_lsmr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double
             int check_every, double* x, double* zeta_bar);
 int or_lsqr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int iterations, double tol,
             int check_every, double* x, double* residuum);
+/* The same two methods on A S with S = diag(A'A)^-1/2 (1 for an empty
+ * column) when scale != 0, returning x = S y: column scaling, which the
+ * reference does not have. */
+int or_lsqr_scaled(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int scale,
+                   int iterations, double tol, int check_every, double* x, double* residuum);
+int or_lsmr_scaled(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int scale,
+                   int iterations, double tol, int check_every, double* x, double* zeta_bar);
+
+/* The library's seeded random-play positions {P, O} (index first .. first+n)
+ * and targets b = clamp(2 rint((A w* + e) / 2), -64, 64), w* ~ N(0, w_sigma^2),
+ * e ~ N(0, noise_sigma^2), from the same counter-based streams, for a process
+ * that must not load the CUDA library.  0 on success. */
+int or_generate_positions(uint64_t seed, int64_t first, int64_t n, int min_e, int max_e, uint64_t* po);
+void or_generate_targets(int k, int64_t rows, int64_t cols, const uint32_t* idx, uint64_t seed, double w_sigma,
+                         double noise_sigma, double* b, double* w_true);
 
 #endif

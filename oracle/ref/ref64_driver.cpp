@@ -166,6 +166,25 @@ int ref64_lsmr(int k, int64_t rows, int64_t cols, const uint32_t* idx, const dou
     return it;
 }
 
+// The check of solutions computed elsewhere against the reference's own FP64
+// products on one system: out[i] = ||A'(b - A x_i)|| / ||A'b|| for the n
+// vectors x_i (cols doubles each, one after another), and hit[c] = 1 where
+// column c has entries (JacobiPreconditionerOfATA finite).
+void ref64_check(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b, int n, const double* xs,
+                 double* out, uint8_t* hit)
+{
+    MatrixCSR m = make_csr(k, rows, cols, idx);
+    Vector score(b, b + rows);
+    for (int i = 0; i < n; i++) {
+        const double* x = xs + static_cast<int64_t>(i) * cols;
+        out[i] = normal_residual(m, score, Vector(x, x + cols));
+    }
+    if (hit) {
+        Vector d = JacobiPreconditionerOfATA(m);
+        for (int64_t c = 0; c < cols; c++) hit[c] = std::isfinite(d[c]) ? 1 : 0;
+    }
+}
+
 // One PCG iteration's wall time in FP64 on a prebuilt system, averaged over n
 // iterations (the bounded CPU-baseline sample).
 double ref64_pcg_seconds_per_iteration(int k, int64_t rows, int64_t cols, const uint32_t* idx, const double* b,

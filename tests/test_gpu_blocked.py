@@ -128,9 +128,7 @@ def test_solvers_on_blocked_layout(cuda, orc, precision, method):
     idx = orc.group_index(masks, 0 if method == "lsqr" else 1, pos.cpu().numpy().view(np.uint64))
     cols = g.index_space_size
     cls = cb.PCG if method == "pcg" else cb.LSQR
-    # mixed LSQR restarts from the FP64 residual every 50 steps, which costs
-    # convergence speed; it is held to 1e-6 here
-    tol = 1e-6 if (method, precision) == ("lsqr", "mixed") else 1e-8
+    tol = 1e-8
     s = cls(a, b, precision=precision, tol=tol, max_iterations=60_000, check_every=50)
     rep = s.run()
     assert rep["converged"], rep

@@ -100,3 +100,18 @@ def test_generator_device_equals_host(cuda):
     empties = 64 - np.array([bin(int(p) | int(o)).count("1") for p, o in h])
     assert empties.min() >= 20 and empties.max() <= 40
     assert np.all((h[:, 0] & h[:, 1]) == 0)
+
+
+@pytest.mark.parametrize("layout", ["rows", "blocked"])
+def test_device_inputs_equal_oracle_restatement(cuda, orc, layout):
+    """The benchmark's reference arm builds its inputs with the oracle's C
+    restatement of the generator (no CUDA library in that process): the
+    positions and the targets b equal the device generator's bit for bit."""
+    pos = cb.generate_positions(2024, 200_000, 20, 40)
+    np.testing.assert_array_equal(pos.cpu().numpy().view(np.uint64), orc.generate_positions(2024, 0, 200_000, 20, 40))
+    g = cb.GroupIndexer(SET8, "expanded")
+    a = cb.MatrixCSR.from_positions(g, pos, layout)
+    b = cb.generate_targets(a, 2024).cpu().numpy()
+    idx = orc.group_index(SET8, 1, pos.cpu().numpy().view(np.uint64))
+    want, _ = orc.generate_targets(idx, g.index_space_size, 2024)
+    np.testing.assert_array_equal(b, want)

@@ -150,6 +150,43 @@ def test_reference_arm_runs_on_cpu(ref):
     assert res["impl"] == "reference" and res["value"] > 0
     assert res["e2e"]["h2d_bytes_per_step"] == 0
     assert res["cpu_baseline"]["kind"] == "reference"
+    # the same workload description as the GPU arm, the whole workload every step
+    assert res["config"] == bench.single_config(args)
+    assert res["breakdown"]["rel_residual"] <= 1e-8
+    assert "30000 rows" in res["cpu_baseline"]["sample"]
+
+
+def test_reference_arm_loads_no_cuda_library(ref):
+    """The reference arm's process builds its inputs with the oracle's
+    restatement of the generator and maps only the oracle's libraries."""
+    import subprocess
+    import sys
+
+    code = ("import bench; a = bench.parse_args(['--impl', 'reference', '--steps', '1', '--warmup', '0', "
+            "'--rows', '5000']); r = bench.run_reference(a); assert r['value'] > 0; "
+            "print('\\n'.join(sorted({l.split()[-1] for l in open('/proc/self/maps') if '.so' in l})))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=str(ROOT), capture_output=True, text=True, check=True)
+    mine = [l for l in out.stdout.splitlines() if l.startswith(str(ROOT))]
+    assert mine and all("/oracle/_ref/" in l or "/oracle/_build/" in l for l in mine), mine
+
+
+def test_reference_check_pins_a_solution(ref, orc):
+    """The bench's oracle check: the oracle's own PCG solution of the system
+    passes with a residual below the tolerance and weights within rounding
+    of the reference's FP64 PCG on the columns with entries."""
+    import bench
+
+    args = bench.parse_args(["--rows", "20000"])
+    pos = orc.generate_positions(args.seed, 0, args.rows, args.min_empties, args.max_empties)
+    idx = orc.group_index(bench.PATTERNS_8, 1, pos)
+    b, _ = orc.generate_targets(idx, bench.COLS_8, args.seed)
+    x, _, _ = orc.pcg(idx, bench.COLS_8, b, 20000, tol=1e-10, check_every=10)
+    cpu, check = bench.reference_check(args, pos, b, {"oracle_pcg": x})
+    assert cpu["kind"] == "reference" and cpu["value"] > 0
+    assert check["oracle_pcg"]["rel_residual_fp64"] <= 1e-9
+    assert check["reference"]["rel_residual_fp64"] <= 1e-8
+    assert check["oracle_pcg"]["max_weight_err_hit_rel"] < 1e-3
+    assert 0 < check["hit_cols"] < bench.COLS_8
 
 
 def test_reference_arm_runs_the_evaluator_workload_on_cpu(ref):

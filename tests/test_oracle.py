@@ -277,3 +277,78 @@ def test_pcg_reaches_tolerance(orc):
     x, res, it = orc.pcg(idx, cols, b, 5000, tol=1e-8, check_every=10)
     assert it < 5000
     assert orc.normal_residual(idx, cols, b, x) <= 1e-8
+
+
+def _scaled_matrix(orc, idx, cols):
+    """A S as a scipy matrix, S = diag(A'A)^-1/2 (1 for an empty column)."""
+    import scipy.sparse as sp
+
+    d = orc.jacobi(idx, cols)
+    s = np.where(np.isfinite(d) & (d > 0), np.sqrt(np.where(np.isfinite(d), d, 1.0)), 1.0)
+    rows, k = idx.shape
+    a = sp.csr_matrix((np.ones(idx.size), idx.ravel().astype(np.int64), np.arange(0, idx.size + 1, k)),
+                      shape=(rows, cols))
+    return a @ sp.diags(s), s
+
+
+@pytest.mark.parametrize("method", ["lsqr", "lsmr"])
+def test_scaled_least_squares_match_scipy(orc, method):
+    """The column-scaled LSQR/LSMR of the oracle (not in the reference) are
+    the published methods on A S: after 10 steps x = S y equals scipy's
+    lsqr/lsmr on the explicit matrix A S with no stopping test (scipy's
+    LSMR is the Fong-Saunders method whose rotations Math/Solver.h:222-287
+    follow)."""
+    import scipy.sparse.linalg as sla
+
+    idx, cols, b = _small_system(orc, rows=3000, seed=5)
+    a_s, s = _scaled_matrix(orc, idx, cols)
+    fn = orc.lsqr if method == "lsqr" else orc.lsmr
+    x, _, it = fn(idx, cols, b, 10, scale=True)
+    assert it == 10
+    solver = sla.lsqr if method == "lsqr" else sla.lsmr
+    y = solver(a_s, b, atol=0, btol=0, conlim=0, maxiter=10)[0] if method == "lsmr" else \
+        sla.lsqr(a_s, b, atol=0, btol=0, conlim=0, iter_lim=10)[0]
+    np.testing.assert_allclose(x, s * y, rtol=0, atol=1e-9 * np.abs(x).max())
+
+
+@pytest.mark.parametrize("method", ["lsqr", "lsmr"])
+def test_scaled_least_squares_reach_tolerance(orc, method):
+    """Column scaling leaves the least-squares problem unchanged: the scaled
+    solves reach 1e-8 on the normal equations, in fewer steps than the
+    unscaled ones (140 against 290 LSQR steps here), with the predictions
+    A x of the PCG solution."""
+    idx, cols, b = _small_system(orc, rows=3000, seed=2)
+    fn = orc.lsqr if method == "lsqr" else orc.lsmr
+    x, _, it = fn(idx, cols, b, 20000, tol=1e-8, check_every=10, scale=True)
+    assert orc.normal_residual(idx, cols, b, x) <= 1e-8
+    _, _, it_plain = fn(idx, cols, b, 20000, tol=1e-8, check_every=10)
+    assert it < it_plain
+    xp, _, _ = orc.pcg(idx, cols, b, 5000, tol=1e-10, check_every=10)
+    pa, pp = orc.spmv(idx, cols, x), orc.spmv(idx, cols, xp)
+    assert np.abs(pa - pp).max() <= 1e-5 * np.abs(pp).max()
+
+
+@pytest.mark.parametrize("seed,first,n,lo,hi", [(2024, 0, 20_000, 20, 40), (7, 123_456, 5000, 0, 60),
+                                                (1, 0, 3000, 60, 60), (99, 10 ** 9, 2000, 1, 1)])
+def test_generator_restatement_equals_library(orc, seed, first, n, lo, hi):
+    """The oracle's C restatement of the seeded random-play generator (used
+    where the CUDA library must not be loaded) gives the library's host
+    generator's positions bit for bit."""
+    import cassandra_b200 as cb
+
+    want = cb.generate_positions_host(seed, first, n, lo, hi).reshape(-1, 2).view(np.uint64)
+    np.testing.assert_array_equal(orc.generate_positions(seed, first, n, lo, hi), want)
+
+
+def test_generated_targets_follow_their_recipe(orc):
+    """b = clamp(2 rint((A w* + e) / 2), -64, 64): even integers in [-64, 64],
+    correlated with A w*, and w* has the requested spread."""
+    pos = orc.generate_positions(5, 0, 20_000, 20, 40)
+    idx = orc.group_index(SET8, 1, pos)
+    cols, _ = orc.group_info(SET8, 1)
+    b, w = orc.generate_targets(idx, cols, 5)
+    assert np.all(b == 2 * np.rint(b / 2)) and b.min() >= -64 and b.max() <= 64
+    assert abs(w.std() - 0.5) < 0.01 and abs(w.mean()) < 0.01
+    aw = orc.spmv(idx, cols, w)
+    assert np.corrcoef(aw, b)[0, 1] > 0.5
+    assert abs(np.std(b - aw) - 4.0) < 0.2
