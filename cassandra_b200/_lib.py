@@ -22,7 +22,6 @@ CAS_ERR_OUT_OF_MEMORY = 5
 CAS_ERR_NO_DEVICE = 6
 CAS_ERR_BREAKDOWN = 7
 CAS_ERR_NOT_CONVERGED = 8
-CAS_ERR_TIMEOUT = 9
 
 # enums
 CAS_INDEX_REFERENCE = 0
@@ -143,6 +142,7 @@ SIGNATURES: dict[str, tuple] = {
     "cas_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
     "cas_solver_create": (C.c_int, [_VP, C.POINTER(SolveOpts), _VP, _VP, _VP, _PP]),
     "cas_solver_create_normal": (C.c_int, [_VP, C.POINTER(SolveOpts), _VP, _VP, _VP, _PP]),
+    "cas_solver_create_normal_diag": (C.c_int, [_VP, C.POINTER(SolveOpts), _VP, _VP, _VP, _VP, _PP]),
     "cas_solver_destroy": (None, [_VP]),
     "cas_solver_iterate": (C.c_int, [_VP, C.c_int]),
     "cas_solver_residuum": (C.c_int, [_VP, C.POINTER(C.c_double)]),

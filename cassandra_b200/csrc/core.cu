@@ -164,7 +164,6 @@ CAS_API const char* cas_status_name(cas_status s)
         case CAS_ERR_NO_DEVICE: return "CAS_ERR_NO_DEVICE";
         case CAS_ERR_BREAKDOWN: return "CAS_ERR_BREAKDOWN";
         case CAS_ERR_NOT_CONVERGED: return "CAS_ERR_NOT_CONVERGED";
-        case CAS_ERR_TIMEOUT: return "CAS_ERR_TIMEOUT";
     }
     return "CAS_ERR_UNKNOWN";
 }

@@ -1889,13 +1889,25 @@ cas_status fast_eval_forward(const FastLayout& f, int64_t row0, int64_t row1, co
 }
 
 // The evaluator's per-call buffers for adjoints over nb blocks (grown, never
-// shrunk; growing waits for the stream, so the first call of the largest
-// size must come before any graph capture).
+// shrunk).  A call made while `s` is capturing marks them as held by a CUDA
+// graph: from then on a call that would grow them (and so free the buffers
+// the graph's kernels use) is refused, captured or not, and so is growing
+// during a capture.  Growing waits for the whole device, since eager work
+// on other streams may still use the old buffers.
 static cas_status eval_buffers(FastLayout& f, int64_t nb, cudaStream_t s)
 {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CAS_CUDA(cudaStreamIsCapturing(s, &cap));
+    const bool capturing = cap != cudaStreamCaptureStatusNone;
     if (nb > f.eval_blocks) {
+        CAS_REQUIRE(!capturing, CAS_ERR_INVALID_ARGUMENT,
+                    "evaluator step: a captured call may not grow the matrix's evaluator scratch; make one call of "
+                    "the largest minibatch before capturing");
+        CAS_REQUIRE(!f.eval_captured, CAS_ERR_INVALID_ARGUMENT,
+                    "evaluator step: the matrix's evaluator scratch is held by captured CUDA graphs; a call over "
+                    "more blocks than they were captured with would reallocate it (use a new matrix)");
         if (f.eval_partial || f.eval_dscore) {
-            CAS_CUDA(cudaStreamSynchronize(s));
+            CAS_CUDA(cudaDeviceSynchronize());
             dfree(f.eval_partial);
             dfree(f.eval_dscore);
             f.eval_partial = nullptr;
@@ -1907,10 +1919,13 @@ static cas_status eval_buffers(FastLayout& f, int64_t nb, cudaStream_t s)
         f.eval_blocks = nb;
     }
     if (!f.eval_red) {
+        CAS_REQUIRE(!capturing, CAS_ERR_INVALID_ARGUMENT,
+                    "evaluator step: make one call of the largest minibatch before capturing");
         CAS_CUDA(dmalloc(&f.eval_red, sizeof(double) * 2 * kEvalRedMax));
         CAS_CUDA(dmalloc(&f.eval_ctr, sizeof(int)));
         CAS_CUDA(cudaMemsetAsync(f.eval_ctr, 0, sizeof(int), s));
     }
+    if (capturing) f.eval_captured = true;
     return CAS_OK;
 }
 

@@ -193,6 +193,7 @@ struct FastLayout {
     float* eval_partial = nullptr;     // [blocks][cols] partials of the last adjoint
     float* eval_dscore = nullptr;      // [blocks * kBlockRows] loss gradient of a training step's rows
     int64_t eval_blocks = 0;           // blocks the two buffers above hold
+    bool eval_captured = false;        // a CUDA graph captured a call that uses them: they never move again
     double* eval_red = nullptr;        // [2 * kEvalRedMax] per-CTA loss partials of a training step
     int* eval_ctr = nullptr;           // last-CTA counter of the training step's epilogue
 };

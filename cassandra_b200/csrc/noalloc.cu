@@ -14,10 +14,15 @@
 // cannot pass the array's name to a kernel (on the host it is only a
 // stand-in for the device symbol), so the device address is looked up with
 // cudaGetSymbolAddress once per device, on that device's first call; make that
-// first call before any stream capture.  All calls share the array and it
-// keeps the last call's contents; each call overwrites every partial it reads,
-// so nothing has to start at zero, but calls that overlap on the GPU (other
-// streams or threads) race on the array and must be serialised by the caller.
+// first call before any stream capture.  The lookup is cached per device
+// ordinal for the life of the process: it assumes the device's primary
+// context (the one the CUDA runtime uses), and does not survive
+// cudaDeviceReset, after which the library's device image may load elsewhere.
+// All calls share the array and it keeps the last call's contents; each call
+// overwrites every partial it reads, so nothing has to start at zero, but
+// calls that overlap on the GPU (other streams or threads) race on the array
+// and must be serialised by the caller.  A column index >= cols is never
+// read through: it makes its row's y and the norm NaN.
 #include <mutex>
 
 #include "common.cuh"
@@ -34,11 +39,16 @@ constexpr int64_t kNoAllocMaxRows = kNoAllocRowsPerCta * kNoAllocMaxCtas;  // 16
 // Per-CTA (sum, compensation) pairs of ||y||^2.
 static __device__ __align__(256) double g_noalloc_partials[2 * kNoAllocMaxCtas];
 
+// An index >= cols is never read through: it contributes NaN, so that row's
+// y and the norm come out NaN instead of the kernel reading outside x (the
+// call is asynchronous and cannot report the bad index as a status).
 __global__ void __launch_bounds__(kNoAllocThreads) noalloc_spmv_norm_kernel(const uint32_t* __restrict__ idx, int k,
-                                                                            int64_t rows, const double* __restrict__ x,
+                                                                            int64_t rows, int64_t cols,
+                                                                            const double* __restrict__ x,
                                                                             double* __restrict__ y,
                                                                             double* __restrict__ partials)
 {
+    const double kNaN = __longlong_as_double(0x7FF8000000000000LL);
     __shared__ double smem[64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t r0 = static_cast<int64_t>(blockIdx.x) * kNoAllocRowsPerCta;
@@ -47,7 +57,10 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_spmv_norm_kernel(cons
     for (int64_t r = r0 + warp; r < r1; r += kNoAllocThreads / 32) {
         const uint32_t* row = idx + r * k;
         double acc = 0;
-        for (int j = lane; j < k; j += 32) acc += __ldg(x + __ldg(row + j));
+        for (int j = lane; j < k; j += 32) {
+            const uint32_t c = __ldg(row + j);
+            acc += c < cols ? __ldg(x + c) : kNaN;
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) {
@@ -123,7 +136,8 @@ CAS_API cas_status cas_spmv_norm_noalloc(const uint32_t* d_indices, int nnz_per_
     auto s = static_cast<cudaStream_t>(stream);
     const int ctas = static_cast<int>((rows + kNoAllocRowsPerCta - 1) / kNoAllocRowsPerCta);
     if (ctas > 0) {
-        { noalloc_spmv_norm_kernel<<<ctas, kNoAllocThreads, 0, s>>>(d_indices, nnz_per_row, rows, d_x, d_y, scratch); cas::count_launch(); }
+        { noalloc_spmv_norm_kernel<<<ctas, kNoAllocThreads, 0, s>>>(d_indices, nnz_per_row, rows, cols, d_x, d_y,
+                                                                   scratch); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
     }
     { noalloc_norm_finish_kernel<<<1, 1024, 0, s>>>(scratch, ctas, d_norm2); cas::count_launch(); }

@@ -440,6 +440,17 @@ __global__ void precond_kernel(const uint64_t* __restrict__ diag, int64_t n, int
     }
 }
 
+// A caller's DiagonalPreconditioner (Math/Solver.h:25-38): d = the given
+// entries, those that are not normal replaced by 1.
+__global__ void user_precond_kernel(const double* __restrict__ in, int64_t n, double* __restrict__ d)
+{
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double v = in[c];
+        d[c] = (isfinite(v) && fabs(v) >= 2.2250738585072014e-308) ? v : 1.0;
+    }
+}
+
 template <typename T>
 __global__ void cast_kernel(int64_t n, const double* __restrict__ in, T* __restrict__ out)
 {
@@ -806,6 +817,7 @@ struct SolverImpl {
     double* q64 = nullptr;    // FP64 residual b - A x (refinement / true residual)
     const double* b = nullptr;   // rows-length targets (null with a normal RHS)
     const double* bn = nullptr;  // cols-length normal-equation RHS A'b (PCG/CG only)
+    const double* user_d = nullptr;  // a caller's diagonal preconditioner (PCG only; read at set-up)
     double* b_own = nullptr;
     double* partial = nullptr;  // unit partials of the rows layout
     double *part_q = nullptr, *part_a = nullptr, *part_b = nullptr, *part_c = nullptr;
@@ -1144,7 +1156,10 @@ struct SolverImpl {
         CAS_CUDA(cudaMemsetAsync(w, 0, cb, s));
         CAS_CUDA(cudaMemsetAsync(v, 0, cb, s));
         const int pmode = (o.method == CAS_PCG && o.jacobi) ? 1 : (scaled() ? 2 : 0);
-        { precond_kernel<<<vec_grid(C), kVecThreads, 0, s>>>(a.diag_int, C, pmode, d); cas::count_launch(); }
+        if (user_d)
+            { user_precond_kernel<<<vec_grid(C), kVecThreads, 0, s>>>(user_d, C, d); cas::count_launch(); }
+        else
+            { precond_kernel<<<vec_grid(C), kVecThreads, 0, s>>>(a.diag_int, C, pmode, d); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         const Dev D = dv();
 
@@ -1226,7 +1241,7 @@ CAS_API void cas_solve_opts_default(cas_solve_opts* o)
 
 namespace {
 cas_status create_solver(const cas_csr* a, const cas_solve_opts* o, const double* d_b, const double* d_bn,
-                         const double* d_x0, void* stream, cas_solver** out)
+                         const double* d_x0, void* stream, cas_solver** out, const double* d_diag = nullptr)
 {
     CAS_TRY(validate_opts(o));
     *out = nullptr;
@@ -1259,7 +1274,9 @@ cas_status create_solver(const cas_csr* a, const cas_solve_opts* o, const double
         m.bn = m.b_own;
     }
     cudaGetDevice(&m.device);
+    m.user_d = d_diag;
     cas_status st = m.init(d_x0);
+    m.user_d = nullptr;  // copied into the solver's d at set-up
     if (st != CAS_OK) {
         delete sv;
         return st;
@@ -1288,6 +1305,18 @@ CAS_API cas_status cas_solver_create_normal(const cas_csr* a, const cas_solve_op
     CAS_REQUIRE(o && o->method != CAS_LSQR && o->method != CAS_LSMR, CAS_ERR_INVALID_ARGUMENT,
                 "cas_solver_create_normal: LSQR and LSMR need the rows-length right-hand side");
     return create_solver(a, o, nullptr, d_normal_b, d_x0, stream, out);
+}
+
+CAS_API cas_status cas_solver_create_normal_diag(const cas_csr* a, const cas_solve_opts* o, const double* d_normal_b,
+                                                 const double* d_diag, const double* d_x0, void* stream,
+                                                 cas_solver** out)
+{
+    CAS_REQUIRE(a && out, CAS_ERR_INVALID_ARGUMENT, "cas_solver_create_normal_diag: null argument");
+    CAS_REQUIRE((d_normal_b && d_diag) || a->cols == 0, CAS_ERR_INVALID_ARGUMENT,
+                "cas_solver_create_normal_diag: null right-hand side or preconditioner");
+    CAS_REQUIRE(o && o->method == CAS_PCG, CAS_ERR_INVALID_ARGUMENT,
+                "cas_solver_create_normal_diag: the diagonal preconditioner is a PCG argument");
+    return create_solver(a, o, nullptr, d_normal_b, d_x0, stream, out, d_diag);
 }
 
 CAS_API void cas_solver_destroy(cas_solver* s) { delete s; }

@@ -44,8 +44,7 @@ typedef enum cas_status {
     CAS_ERR_OUT_OF_MEMORY = 5,
     CAS_ERR_NO_DEVICE = 6,        /* no usable CUDA device */
     CAS_ERR_BREAKDOWN = 7,        /* solver breakdown: p'A'Ap <= 0, or a non-finite scalar */
-    CAS_ERR_NOT_CONVERGED = 8,    /* tolerance not reached within max_iterations */
-    CAS_ERR_TIMEOUT = 9           /* a bounded device-side wait gave up */
+    CAS_ERR_NOT_CONVERGED = 8     /* tolerance not reached within max_iterations */
 } cas_status;
 
 /* Name of a status code ("CAS_OK", ...).  Never NULL. */
@@ -223,8 +222,13 @@ typedef struct cas_adam_opts {
  * first call of the largest minibatch, so it can be captured in a CUDA graph;
  * deterministic (fixed reduction orders, integer counters only).  The scratch
  * it (and cas_eval_backward) uses belongs to the CSR and grows when a call
- * spans more blocks than any call before: that frees the old scratch, so
- * graphs captured earlier must not be replayed after such a call. */
+ * spans more blocks than any call before.  Once a call has been captured
+ * into a CUDA graph that scratch never moves: a later call (captured or not)
+ * that would grow it returns CAS_ERR_INVALID_ARGUMENT, and so does a call
+ * that would grow it while being captured.  The loss reduction and its
+ * last-CTA counter are also one per CSR: calls on one CSR must be serialised
+ * (one stream, or graphs replayed one after another); overlapping calls on
+ * different streams corrupt each other's loss and counter. */
 CAS_API cas_status cas_eval_adam_step(const cas_csr* a, int64_t row0, int64_t row1, const float* d_target,
                                       float* d_w, float* d_m, float* d_v, int64_t* d_step, double* d_loss_sum,
                                       const cas_adam_opts* opts, void* stream);
@@ -291,6 +295,15 @@ CAS_API cas_status cas_solver_create(const cas_csr* a, const cas_solve_opts* o, 
  * only; residuals are then b' - A'A x. */
 CAS_API cas_status cas_solver_create_normal(const cas_csr* a, const cas_solve_opts* o, const double* d_normal_b,
                                             const double* d_x0, void* stream, cas_solver** out);
+/* PCG given the normal-equation right-hand side and an explicit diagonal
+ * preconditioner d (cols doubles, copied; entries that are not normal act as
+ * 1): PCG(transposed(A) * A, DiagonalPreconditioner(d), x0, b') with any
+ * DiagonalPreconditioner, not only JacobiPreconditionerOfATA
+ * (Math/Solver.h:25-38, :78-117).  o->method must be CAS_PCG; o->jacobi is
+ * ignored. */
+CAS_API cas_status cas_solver_create_normal_diag(const cas_csr* a, const cas_solve_opts* o, const double* d_normal_b,
+                                                 const double* d_diag, const double* d_x0, void* stream,
+                                                 cas_solver** out);
 CAS_API void cas_solver_destroy(cas_solver* s);
 /* IterativeSolver::Iterate(n). */
 CAS_API cas_status cas_solver_iterate(cas_solver* s, int n);
@@ -472,9 +485,12 @@ CAS_API cas_status cas_read_scored_positions(const char* path, uint64_t* h_posit
  * cas_spmv_norm_noalloc_max_rows() = 16,777,216; larger inputs are rejected
  * with CAS_ERR_INVALID_ARGUMENT.  The first call on a device looks up that
  * array's device address (no allocation); make it before any stream capture.
- * Calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller.  The result does not depend on the GPU model
- * (fixed 2048 rows per CTA). */
+ * The lookup assumes the primary context and is not redone after
+ * cudaDeviceReset.  Calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller.  The call is asynchronous, so an index
+ * >= cols cannot be reported as a status: it is never read through, and it
+ * makes its row's y and *d_norm2 NaN.  The result does not depend on the GPU
+ * model (fixed 2048 rows per CTA). */
 CAS_API int64_t cas_spmv_norm_noalloc_max_rows(void);
 CAS_API cas_status cas_spmv_norm_noalloc(const uint32_t* d_indices, int nnz_per_row, int64_t rows, int64_t cols,
                                          const double* d_x, double* d_y, double* d_norm2, void* stream);

@@ -415,24 +415,30 @@ public:
 // PCG as FitWeights builds it (PatternFit/PatternFit.cpp:29-31):
 //   DiagonalPreconditioner P(JacobiPreconditionerOfATA(A));
 //   PCG solver(transposed(A) * A, P, x0, transposed(A) * b);
-// The system matrix must be the lazy transposed(A) * A of a MatrixCSR and P
-// its Jacobi preconditioner (rebuilt on the device from A); b' = A'b is the
-// cols-length right-hand side, as in the reference.
+// The system matrix must be the lazy transposed(A) * A of a MatrixCSR; b' =
+// A'b is the cols-length right-hand side, as in the reference.  P must be a
+// DiagonalPreconditioner (Math/Solver.h:25-38), whatever its diagonal: its
+// d is uploaded and applied on the device.  Any other Preconditioner throws
+// std::invalid_argument (the device applies diagonal preconditioners only).
 template <typename M>
 class PCG;
 
 template <>
 class PCG<TwoMatrix<TransposedMatrix<MatrixCSR>, MatrixCSR>> final : public detail::DeviceSolver {
 public:
-    PCG(const TwoMatrix<TransposedMatrix<MatrixCSR>, MatrixCSR>& ata, const Preconditioner&, Vector x0, Vector b)
+    PCG(const TwoMatrix<TransposedMatrix<MatrixCSR>, MatrixCSR>& ata, const Preconditioner& P, Vector x0, Vector b)
         : DeviceSolver(ata.r, b)
     {
         if (ata.Rows() != ata.Cols()) throw std::runtime_error("Size mismatch.");
         if (ata.Cols() != x0.size()) throw std::runtime_error("Size mismatch.");
         if (ata.Rows() != b.size()) throw std::runtime_error("Size mismatch.");
+        const auto* diag = dynamic_cast<const DiagonalPreconditioner*>(&P);
+        if (!diag) throw std::invalid_argument("PCG: only a DiagonalPreconditioner is applied on the device");
+        if (diag->d.size() != ata.Cols()) throw std::runtime_error("Size mismatch");
         cas_solve_opts o = opts(CAS_PCG, 1);
         auto dx0 = detail::to_device_f64(x0);
-        check(cas_solver_create_normal(a.device(), &o, rhs.p, dx0.p, nullptr, &s));
+        auto dd = detail::to_device_f64(diag->d);
+        check(cas_solver_create_normal_diag(a.device(), &o, rhs.p, dd.p, dx0.p, nullptr, &s));
     }
     // Error() = b' - A'A x (Math/Solver.h:115).
     Vector Error() const override

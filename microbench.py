@@ -1,6 +1,6 @@
 """Timing of the two sparse products on one layout, for profiling and tuning.
 
-    python -m cassandra_b200.microbench --rows 2000000 --layout blocked --reps 3
+    python microbench.py --rows 2000000 --layout blocked --reps 3
 
 Builds the 8-pattern expanded matrix of `rows` random-play positions (empty
 counts 20..40) on the requested layout, runs A x and A'y `reps` times each
@@ -13,11 +13,14 @@ import argparse
 import ctypes as C
 import json
 import sys
+from pathlib import Path
 
 import torch
 
-from . import PATTERNS_8, GroupIndexer, MatrixCSR, generate_positions
-from . import _lib as L
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+
+from cassandra_b200 import PATTERNS_8, GroupIndexer, MatrixCSR, generate_positions  # noqa: E402
+from cassandra_b200 import _lib as L  # noqa: E402
 
 
 def main(argv=None) -> int:

@@ -1,7 +1,8 @@
 // The reference's own usage of its fitting API, compiled unchanged in shape
 // against the drop-in header: MatrixCSR known answers
 // (MathTest/MatrixCSR.cpp:3-55), the FitWeights sequence
-// (PatternFit/PatternFit.cpp:12-38) and LSQR (Math/Solver.h:128-182).
+// (PatternFit/PatternFit.cpp:12-38), PCG with another DiagonalPreconditioner
+// and LSQR (Math/Solver.h:78-182).
 // Prints "OK <name>" per check and exits non-zero on the first failure.
 #include <cmath>
 #include <cstdio>
@@ -87,6 +88,34 @@ int main()
         EXPECT(diff <= 1e-4f * mx, "FitWeights equals the explicit PCG sequence");
         Vector err = solver.Error();
         EXPECT(err.size() == cols, "PCG Error size");
+
+        // A DiagonalPreconditioner other than Jacobi is honoured: with d = 1 the
+        // PCG iterates are CG's (Math/Solver.h:40-76 and :78-117 with P = I).
+        PCG pcg_identity(transposed(matrix) * matrix, DiagonalPreconditioner(Vector(cols, 1.0f)), weights,
+                         transposed(matrix) * score);
+        CG cg(transposed(matrix) * matrix, weights, transposed(matrix) * score);
+        pcg_identity.Iterate(4);
+        cg.Iterate(4);
+        Vector xp = pcg_identity.X(), xc = cg.X();
+        float dpc = 0, mpc = 0;
+        for (std::size_t i = 0; i < cols; i++) {
+            dpc = std::max(dpc, std::fabs(xp[i] - xc[i]));
+            mpc = std::max(mpc, std::fabs(xc[i]));
+        }
+        EXPECT(dpc <= 1e-5f * mpc && mpc > 0, "PCG honours its DiagonalPreconditioner");
+        EXPECT(std::fabs(pcg_identity.Residuum() - cg.Residuum()) <= 1e-4f * cg.Residuum(),
+               "PCG with P = I has CG's residuum");
+        struct Other : Preconditioner {
+            Vector apply(const Vector& v) const override { return v; }
+            Vector revert(const Vector& v) const override { return v; }
+        };
+        bool refused = false;
+        try {
+            PCG other(transposed(matrix) * matrix, Other{}, weights, transposed(matrix) * score);
+        } catch (const std::invalid_argument&) {
+            refused = true;
+        }
+        EXPECT(refused, "PCG refuses a preconditioner it cannot apply");
 
         LSQR lsqr(matrix, Vector(cols, 0.0f), score);
         lsqr.Iterate(5);

@@ -109,3 +109,19 @@ def test_empty_matrix(cuda):
     x = torch.ones(a.cols(), dtype=torch.float64, device="cuda")
     assert (a @ x).numel() == 0
     assert torch.count_nonzero(torch.empty(0, dtype=torch.float64, device="cuda") @ a) == 0
+
+
+def test_from_indices_rejects_out_of_range_columns(cuda):
+    """Caller-supplied indices are checked (one pass over them) before any
+    kernel uses them as addresses: an index >= cols is refused with
+    CAS_ERR_INVALID_ARGUMENT, at the first and at the last entry alike."""
+    from cassandra_b200 import _lib as L
+
+    for where in (0, -1):
+        idx = np.zeros((5000, 7), np.uint32)
+        idx.flat[where] = 11
+        with pytest.raises(cb.CasError) as e:
+            cb.MatrixCSR.from_indices(torch.from_numpy(idx.view(np.int32)).cuda(), 11)
+        assert e.value.status == L.CAS_ERR_INVALID_ARGUMENT
+    idx[:] = 10
+    assert cb.MatrixCSR.from_indices(torch.from_numpy(idx.view(np.int32)).cuda(), 11).cols() == 11

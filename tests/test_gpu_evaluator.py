@@ -184,3 +184,53 @@ def test_graph_trainer_guards_its_buffers(cuda):
     with pytest.raises(RuntimeError, match="reallocate"):
         model(0, rows).sum().backward()
     assert np.isfinite(ev.Trainer(model, target, batch=BR, graphs=False).epoch())
+
+
+def test_captured_scratch_never_moves(cuda):
+    """The rule behind the graph trainer, enforced in the library itself
+    (direct C calls, no Python guard): once a training step has been
+    captured into a CUDA graph, a call that would grow (and so free) the
+    matrix's evaluator scratch is refused, eager or captured; growing it
+    during a capture is refused too; calls within the size run and the
+    captured graph still replays."""
+    from cassandra_b200 import _lib as L
+
+    lib = L.load()
+    rows = 3 * BR
+    pos = cb.generate_positions(48, rows, 10, 50)
+    opts = L.AdamOpts(1e-2, 0.9, 0.999, 1e-8, 1e-4, 4.0)
+
+    def state(cols):
+        return [torch.zeros(cols, dtype=torch.float32, device="cuda") for _ in range(3)] + \
+               [torch.zeros((), dtype=torch.int64, device="cuda"), torch.zeros((), dtype=torch.float64, device="cuda")]
+
+    def step(model, r0, r1, st, target):
+        w, m, v, n, loss = st
+        return lib.cas_eval_adam_step(model.csr.handle, r0, r1, target.data_ptr(), w.data_ptr(), m.data_ptr(),
+                                      v.data_ptr(), n.data_ptr(), loss.data_ptr(), C.byref(opts),
+                                      torch.cuda.current_stream().cuda_stream)
+
+    model = ev.PatternEvaluator(SET8, pos, "expanded")
+    target = torch.ones(rows, dtype=torch.float32, device="cuda")
+    st = state(model.weight.numel())
+    L.check(step(model, 0, BR, st, target))  # sizes the scratch for one block
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            L.check(step(model, BR, 2 * BR, st, target))
+    torch.cuda.current_stream().wait_stream(s)
+    assert step(model, 0, 2 * BR, st, target) == L.CAS_ERR_INVALID_ARGUMENT
+    assert "captured" in L.last_error()
+    L.check(step(model, 2 * BR, 3 * BR, st, target))
+    g.replay()
+    torch.cuda.synchronize()
+    assert int(st[3]) == 3 and np.isfinite(float(st[4]))
+
+    fresh = ev.PatternEvaluator(SET8, pos, "expanded")
+    st2 = state(fresh.weight.numel())
+    g2 = torch.cuda.CUDAGraph()
+    with pytest.raises(cb.CasError, match="before capturing"):
+        with torch.cuda.graph(g2):
+            L.check(step(fresh, 0, BR, st2, target))
