@@ -158,6 +158,7 @@ SIGNATURES: dict[str, tuple] = {
     "cas_generate_positions": (C.c_int, [_U64, _I64, C.c_int, C.c_int, _VP, _VP]),
     "cas_generate_positions_host": (C.c_int, [_U64, _I64, _I64, C.c_int, C.c_int, _VP]),
     "cas_generate_targets": (C.c_int, [_VP, _U64, C.c_double, C.c_double, _VP, _VP, _VP]),
+    "cas_generate_targets_rows": (C.c_int, [_VP, _U64, C.c_double, C.c_double, _I64, _VP, _VP, _VP]),
     "cas_csr_schedules": (C.c_int, [_VP, _VP, C.c_int, _VP]),
     "cas_cached_memory": (C.c_size_t, []),
     "cas_release_cached_memory": (None, []),

@@ -434,10 +434,13 @@ def generate_positions_host(seed: int, first: int, n: int, min_empties: int, max
 
 
 def generate_targets(a: MatrixCSR, seed: int, w_sigma: float = 0.5, noise_sigma: float = 4.0,
-                     return_true_weights: bool = False):
+                     return_true_weights: bool = False, first_row: int = 0):
+    """Seeded targets b = clamp(2 rint((A w* + e) / 2), -64, 64); the rows of
+    `a` are rows first_row.. of the whole system (a rank's block)."""
     b = torch.empty(a.rows(), dtype=torch.float64, device="cuda")
     w = torch.empty(a.cols(), dtype=torch.float64, device="cuda") if return_true_weights else None
-    L.check(L.load().cas_generate_targets(a.handle, seed, w_sigma, noise_sigma, _ptr(b), _ptr(w), _stream()))
+    L.check(L.load().cas_generate_targets_rows(a.handle, seed, w_sigma, noise_sigma, first_row, _ptr(b), _ptr(w),
+                                               _stream()))
     return (b, w) if return_true_weights else b
 
 

@@ -179,7 +179,7 @@ CAS_API size_t cas_last_error(char* buf, size_t cap)
     return m.size();
 }
 
-CAS_API int cas_version(void) { return 10000; }
+CAS_API int cas_version(void) { return 20000; }  // 2.0.0: cas_solve_opts.scale_columns; no timeout status
 
 CAS_API long long cas_kernel_launches(void) { return launch_count(); }
 

@@ -33,16 +33,11 @@ namespace {
 
 constexpr int kSortThreads = 1024;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kItemsPerThread = 8;  // A'y entries per lane and round (a multiple of 4)
-constexpr int kRingStages = 3;      // A'y FP32 ring schedules: rounds in the per-lane cp.async ring
-
-// A'y streams its entries either one round ahead in registers or, for FP32
-// schedules with narrow accumulators, through a per-lane ring of cp.async
-// copies in shared memory (kRingStages rounds in flight).  The build-time
-// autotuner picks the schedule (accumulator width, streaming, items per SM).
-constexpr size_t kRingBytes = sizeof(uint32_t) * kFastThreads * kRingStages * kItemsPerThread;
-constexpr int kMaxScRing = 2;  // widest FP32 accumulator (chunks) that leaves room for the ring
-constexpr int kMaxScRegs = 4;
+// The A'y accumulator of a work item holds at most kMaxSc column chunks
+// (with the y tile, the FP32 kernel's dynamic shared memory: 192 KB).  The
+// build-time autotuner picks the schedule (accumulator width, items per SM,
+// packing of narrow patterns, persistent CTAs).
+constexpr int kMaxSc = 4;
 constexpr int64_t kBatchItemBlocks = 4;  // most row blocks of one A'y work item in a batched layout
 constexpr int64_t kBatchSmallBlocks = 8;  // batched problems this small get one block per A'y item
 
@@ -133,7 +128,11 @@ __device__ void block_exclusive_scan_256(uint32_t* hist, uint32_t* out)
     __syncthreads();
 }
 
-template <bool FROM_A16>
+// One stable 8-bit counting-sort pass of a group's n items.  FROM_A16: the
+// items are made from the A16 segment (local column << 16 | row << 2).
+// ROUNDS: the output is written in G32's round order (round_phys of the
+// sorted position; out starts on a round boundary).
+template <bool FROM_A16, bool ROUNDS>
 __device__ void sort_pass(const uint16_t* __restrict__ a16_in, const uint32_t* __restrict__ in, int n, int slots,
                           int shift, uint32_t* __restrict__ out, SortSmem& sm)
 {
@@ -171,7 +170,10 @@ __device__ void sort_pass(const uint16_t* __restrict__ a16_in, const uint32_t* _
             sm.total[t] = acc;
         }
         __syncthreads();
-        if (valid) out[sm.base[d] + sm.running[d] + sm.wcount[warp][d] + rank] = item;
+        if (valid) {
+            const uint32_t pos = sm.base[d] + sm.running[d] + sm.wcount[warp][d] + rank;
+            out[ROUNDS ? round_phys(pos) : pos] = item;
+        }
         __syncthreads();
         if (t < 256) {
             sm.running[t] += sm.total[t];
@@ -193,18 +195,19 @@ __global__ void __launch_bounds__(kSortThreads, 1) fast_sort_kernel(FastGeometry
         const int p = static_cast<int>(grp - b * g.npat);
         const int n = static_cast<int>(g.seg_len(b, p));
         const int64_t seg = g.seg(b, p);
-        sort_pass<true>(a16 + seg, nullptr, n, g.slots[p], 16, mine, sm);
-        sort_pass<false>(nullptr, mine, n, g.slots[p], 24, g32 + seg, sm);
+        sort_pass<true, false>(a16 + seg, nullptr, n, g.slots[p], 16, mine, sm);
+        sort_pass<false, true>(nullptr, mine, n, g.slots[p], 24, g32 + seg, sm);
         __syncthreads();
         // run-end flags: bit 0 marks the last entry of each column (found
         // first for all of a thread's entries, then set)
         uint32_t* out = g32 + seg;
         uint32_t ends[kBlockRows * 8 / kSortThreads / 32] = {};
         for (int e = threadIdx.x, k = 0; e < n; e += kSortThreads, k++)
-            if (e + 1 == n || (out[e + 1] >> 16) != (out[e] >> 16)) ends[k >> 5] |= 1u << (k & 31);
+            if (e + 1 == n || (out[round_phys(e + 1)] >> 16) != (out[round_phys(e)] >> 16))
+                ends[k >> 5] |= 1u << (k & 31);
         __syncthreads();
         for (int e = threadIdx.x, k = 0; e < n; e += kSortThreads, k++)
-            if ((ends[k >> 5] >> (k & 31)) & 1u) out[e] |= 1u;
+            if ((ends[k >> 5] >> (k & 31)) & 1u) out[round_phys(e)] |= 1u;
         __syncthreads();
     }
 }
@@ -228,7 +231,7 @@ __global__ void fast_sub_kernel(FastGeometry g, const uint32_t* __restrict__ g32
         int64_t lo = 0, hi = g.seg_len(b, p);
         while (lo < hi) {
             const int64_t mid = (lo + hi) >> 1;
-            if ((g32[seg + mid] >> 16) < c0)
+            if ((g32[seg + round_phys(static_cast<uint32_t>(mid))] >> 16) < c0)
                 lo = mid + 1;
             else
                 hi = mid;
@@ -271,9 +274,11 @@ __global__ void fast_diag_kernel(FastGeometry g, const uint32_t* __restrict__ g3
             const int64_t e = e0 + threadIdx.x;
             uint32_t col = 0xFFFFFFFFu, contrib = 0;
             if (e < n) {
-                const uint32_t v = g32[seg + e];
+                const uint32_t v = g32[seg + round_phys(static_cast<uint32_t>(e))];
                 int64_t j = 0;
-                while (e - j - 1 >= 0 && (g32[seg + e - j - 1] >> 2) == (v >> 2)) j++;  // same (column, row)
+                while (e - j - 1 >= 0 &&
+                       (g32[seg + round_phys(static_cast<uint32_t>(e - j - 1))] >> 2) == (v >> 2))
+                    j++;  // same (column, row)
                 col = v >> 16;
                 contrib = static_cast<uint32_t>(2 * j + 1);
             }
@@ -347,6 +352,21 @@ __device__ __forceinline__ void store_vec(double* d, uint4 u)
 {
     d[0] = __hiloint2double(static_cast<int>(u.y), static_cast<int>(u.x));
     d[1] = __hiloint2double(static_cast<int>(u.w), static_cast<int>(u.z));
+}
+
+// Asks L2 to fetch [p, p + bytes) (the 16-byte words wholly inside it), in
+// 4 KB bulk prefetches spread over the CTA's threads.  A hint: the data is
+// read later with ordinary loads.
+__device__ __forceinline__ void prefetch_l2(const void* p, int64_t bytes)
+{
+    if (bytes <= 0) return;
+    const uintptr_t a = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + static_cast<uintptr_t>(bytes)) & ~uintptr_t(15);
+    for (uintptr_t c = a + static_cast<uintptr_t>(threadIdx.x) * 4096; c < e;
+         c += static_cast<uintptr_t>(blockDim.x) * 4096) {
+        const unsigned n = static_cast<unsigned>(min(static_cast<uint64_t>(e - c), static_cast<uint64_t>(4096)));
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c), "r"(n) : "memory");
+    }
 }
 
 // Copies a pattern's slice of x (cap entries) into shared memory with
@@ -529,12 +549,19 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
         Acc acc[kAxRows];
 #pragma unroll
         for (int j = 0; j < kAxRows; j++) acc[j] = 0;
+        // the index stream of a pattern is fetched into L2 one phase ahead,
+        // so that HBM keeps streaming while x's next slice is staged
+        prefetch_l2(a16 + g.seg(blk, 0) + static_cast<int64_t>(r0) * g.slots[0],
+                    static_cast<int64_t>(nb) * g.slots[0] * 2);
         for (int p = 0; p < g.npat; p++) {
             const int cap = min(g.space[p], kCap);
             const T* xg = xq + g.off[p];
             __syncthreads();
             load_table<T>(table, xg, cap);
             __syncthreads();
+            if (p + 1 < g.npat)
+                prefetch_l2(a16 + g.seg(blk, p + 1) + static_cast<int64_t>(r0) * g.slots[p + 1],
+                            static_cast<int64_t>(nb) * g.slots[p + 1] * 2);
             const int ns = g.slots[p];
             const uint16_t* base = a16 + g.seg(blk, p) + static_cast<int64_t>(r0) * ns;
             const bool all_in = g.space[p] <= kCap;
@@ -695,36 +722,52 @@ struct TView {
     int nitems;
 };
 
-// Column-sorted entries are reduced warp by warp.  The (block, chunk range)
-// entry list is cut into 32 nearly equal pieces, one per warp, so warps
-// stream their entries without block barriers whatever the run lengths
-// (one column can hold thousands of a block's entries).  Inside a warp each
-// lane owns kItemsPerThread consecutive entries per round.  An entry's bit 0
+// Column-sorted entries are reduced lane by lane.  For one block of an item,
+// the entry ranges of all the item's pieces (their shares of columns) are
+// cut into G32 rounds: piece k covers the rounds that overlap its range
+// [lo_k, hi_k), and the pieces' round lists, one after another, form the
+// block's list of virtual rounds, which the 32 warps split into contiguous
+// stretches of nearly equal length.  In a round each lane owns 32
+// consecutive entries (one round is read with 8 coalesced 16-byte loads per
+// lane; entries outside the piece's range are masked).  An entry's bit 0
 // marks the last entry of its column, so a lane sums y over its entries and
 // closes a run at every flagged entry, with no column comparisons.  A
-// column's entries of a block are one run, so only the lane where a run
-// ends touches its column in a round, and the order of the adds is fixed by
-// the data: the result is bitwise reproducible.
+// column's entries of a block are one run, so only the lane where a run ends
+// touches its column, and the order of the adds is fixed by the data: the
+// result is bitwise reproducible.
 //   1. at every run end the lane adds its own part of the run to acc[col];
-//   2. the parts of a run in the lanes before (its open tails) are combined
+//   2. the parts of a run in the lanes before (their open tails) are combined
 //      by a segmented scan over the warp's lanes (shuffles; the run still
-//      open at the end of the previous round enters as `carry`) and added
-//      by the lane where the run ends;
-//   3. the run still open at the end of a warp's range goes to the warp's
+//      open at the end of the warp's previous round enters as `carry`) and
+//      added by the lane where the run ends;
+//   3. the run still open at the end of a warp's stretch goes to the warp's
 //      record;
 //   4. after the block, warp 0 combines the 32 records with the same
 //      segmented scan (one lane per warp) and adds each chain to the column
 //      where it ends.
+// A run never crosses pieces (a piece holds whole columns), so the chain is
+// reset where a warp's stretch moves on to the next piece.
 
-// What a warp leaves for the runs that cross warp boundaries (columns
-// relative to the piece's first column).
+constexpr int kMaxPieces = kMaxFastPatterns;  // pieces of one super-chunk: at most one per pattern
+
+// The pieces of one (item, block): logical entry ranges, the accumulator
+// index of column field 0, and the first virtual round of each piece.
+struct BlockPieces {
+    uint32_t lo[kMaxPieces];
+    uint32_t hi[kMaxPieces];
+    int acc_off[kMaxPieces];
+    int round0[kMaxPieces + 1];
+    int n;
+};
+
+// What a warp leaves for the runs that cross warp boundaries.
 template <typename T>
 struct WarpRec {
     T ls;        // open sum of the warp's last run (0 when that run ends in the warp)
-    int fc;      // column of the warp's first entry, where its first run ends unless single
-    int valid;   // the warp's range is non-empty
+    int fc;      // accumulator index of the warp's first entry's column
+    int valid;   // the warp's stretch is non-empty
     int cp;      // the first run continues the previous warp's last run
-    int single;  // no run ends in the warp's range
+    int single;  // no run ends in the warp's stretch
 };
 
 // y of an entry: its row, already scaled by 4, sits in bits 2..15.
@@ -766,195 +809,145 @@ __device__ __forceinline__ T lane_chain(bool any, bool single, bool cont_prev, i
     return __shfl_sync(0xffffffffu, X, 31);
 }
 
-constexpr int kLaneVecs = kItemsPerThread / 4;  // 16-byte loads per lane and round
-
-// A lane's entries of a round are all inside the warp's range.
-__device__ __forceinline__ bool lane_full(uint32_t e_first, uint32_t w_lo, uint32_t w_hi)
+__device__ __forceinline__ uint32_t word_of(const uint4& u, int j)
 {
-    return e_first >= w_lo && e_first + kItemsPerThread <= w_hi;
+    return j == 0 ? u.x : (j == 1 ? u.y : (j == 2 ? u.z : u.w));
 }
 
-// Streaming loads of a lane's entries (read once per product: evict first,
-// so that the y and x slices stay in L2).
-__device__ __forceinline__ void load_lane(const uint32_t* __restrict__ g32, uint32_t e_first, uint4 (&u)[kLaneVecs])
+// A lane's entries of one round: slots [k0, k1) of its 32 (all of them when
+// FULL), read from src (the lane's first 16-byte word of the round) in two
+// halves of 16.  Runs that end here are added to accc (indexed by an entry's
+// column field); returns the open tail, the OR of the entries (bit 0: some
+// run ended) and the first and last entries in range.
+template <typename T, bool FULL>
+__device__ __forceinline__ T lane_entries(const uint4* __restrict__ src, int k0, int k1, const T* __restrict__ ytile,
+                                          T* __restrict__ accc, uint32_t& eor, uint32_t& first_e, uint32_t& last_e)
 {
-#pragma unroll
-    for (int q = 0; q < kLaneVecs; q++) u[q] = __ldcs(reinterpret_cast<const uint4*>(g32 + e_first) + q);
-}
-
-// 16-byte asynchronous global -> shared copy (L2 only) and its group
-// bookkeeping; wait_group waits for this thread's own copies only.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
-{
-    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// One round of a warp over [w_lo, w_hi): lanes take kItemsPerThread entries
-// each from round_start (a multiple of 4).  A lane whose entries are all in
-// range gets them in `cur` (loaded ahead by the caller); edge lanes load
-// theirs one by one.  accc: the accumulator shifted so that an entry's
-// column field indexes it.  carry: the run open before the round (updated);
-// prev_end: the last entry before this round ended its run (updated).
-template <typename T>
-__device__ __forceinline__ void warp_round(const uint32_t* __restrict__ g32, uint32_t round_start, uint32_t w_lo,
-                                           uint32_t w_hi, const T* __restrict__ ytile, T* __restrict__ accc,
-                                           T& carry, bool& prev_end, const uint4 (&cur)[kLaneVecs], bool full)
-{
-    const int lane = threadIdx.x & 31;
-    const uint32_t e_first = round_start + lane * kItemsPerThread;
     T sum = 0;
-    uint32_t ends = 0;
-    auto step = [&](uint32_t e) {
-        sum += y_of<T>(ytile, e);
-        ends |= e;
-        if (e & 1u) {  // the run ends here: this lane's part of it
-            accc[e >> 16] += sum;
-            sum = T(0);
-        }
-    };
-    bool any = false;
-    uint32_t first_ent = 1u, last_ent = 1u;  // an empty lane looks like a closed run
-    if (full) {
-        first_ent = cur[0].x;
+    uint32_t o = 0, fe = 1u, le = 1u;
 #pragma unroll
-        for (int q = 0; q < kLaneVecs; q++) {
-            step(cur[q].x);
-            step(cur[q].y);
-            step(cur[q].z);
-            step(cur[q].w);
-        }
-        any = true;
-        last_ent = cur[kLaneVecs - 1].w;
-    } else {
-        const uint32_t lo = max(e_first, w_lo), hi = min(e_first + kItemsPerThread, w_hi);
-        if (lo < hi) {
-            for (uint32_t e = lo; e < hi; e++) step(g32[e]);
-            any = true;
-            first_ent = g32[lo];
-            last_ent = g32[hi - 1];
+    for (int h = 0; h < 2; h++) {
+        uint4 u[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) u[q] = __ldcs(src + 32 * (4 * h + q));
+#pragma unroll
+        for (int t = 0; t < kLaneRun / 2; t++) {
+            const int s = (kLaneRun / 2) * h + t;
+            const uint32_t e = word_of(u[t >> 2], t & 3);
+            if (FULL || (s >= k0 && s < k1)) {
+                sum += y_of<T>(ytile, e);
+                o |= e;
+                if (e & 1u) {  // the run ends here: this lane's part of it
+                    accc[e >> 16] += sum;
+                    sum = T(0);
+                }
+                if (FULL) {
+                    if (s == 0) fe = e;
+                } else if (s == k0) {
+                    fe = e;
+                }
+                le = e;
+            }
         }
     }
-    // no run ends in the lane: one column, its last entry not flagged
-    const bool single = any && !(ends & 1u);
-    const int hc = static_cast<int>(first_ent >> 16);  // the lane's first run
-    // the lane continues the run of the entry before it unless that entry
-    // ended its run (previous lane's last entry; last round's at lane 0)
-    const uint32_t first_valid = max(e_first, w_lo);
-    const uint32_t prev_last = __shfl_up_sync(0xffffffffu, last_ent, 1);
-    const bool cont_prev = any && first_valid > w_lo && (lane == 0 ? !prev_end : !(prev_last & 1u));
-    auto sink = [&](int col, T val) { accc[col] += val; };
-    if (__ballot_sync(0xffffffffu, single && cont_prev) == 0) {
-        // no lane extends a run from its left: a chain is one lane's tail
-        T prev_ts = __shfl_up_sync(0xffffffffu, sum, 1);
-        if (lane == 0) prev_ts = carry;
-        if (any && !single && cont_prev) sink(hc, prev_ts);
-        const int last = min(31, static_cast<int>((w_hi - 1 - round_start) / kItemsPerThread));  // last lane with entries
-        carry = __shfl_sync(0xffffffffu, sum, last);
-    } else {
-        carry = lane_chain<T>(any, single, cont_prev, hc, sum, carry, sink);
-    }
-    prev_end = (__shfl_sync(0xffffffffu, last_ent, 31) & 1u) != 0;
+    eor = o;
+    first_e = fe;
+    last_e = le;
+    return sum;
 }
 
-// The warp-range reduction of one block's entries [e_lo, e_hi) into acc.
-// Ends with a block barrier; the next block may restage ytile after it.
-template <typename T, bool RING>
-__device__ __forceinline__ void reduce_block_entries(const uint32_t* __restrict__ g32, uint32_t e_lo, uint32_t e_hi,
-                                                     uint32_t c0, const T* __restrict__ ytile, T* __restrict__ acc,
-                                                     WarpRec<T>* recs, uint32_t* __restrict__ ring)
+// The reduction of one block's entries of every piece in `bp` into acc.
+// Ends with a block barrier and warp 0's record combination; the next block
+// may restage ytile after the next barrier.
+template <typename T>
+__device__ __forceinline__ void reduce_block(const uint32_t* __restrict__ g32, const BlockPieces& bp,
+                                             const T* __restrict__ ytile, T* __restrict__ acc, WarpRec<T>* recs)
 {
     constexpr int kWarps = kFastThreads / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t n = e_hi - e_lo;
-    auto cut = [&](int w) -> uint32_t {
-        if (w == 0) return e_lo;
-        if (w == kWarps) return e_hi;
-        return max(e_lo, (e_lo + static_cast<uint32_t>(n * w / kWarps)) & ~3u);
-    };
-    const uint32_t w_lo = cut(warp), w_hi = cut(warp + 1);
-    T* accc = acc - c0;  // indexed by an entry's column field
+    const int nrounds = bp.round0[bp.n];
+    const int vr0 = nrounds * warp / kWarps, vr1 = nrounds * (warp + 1) / kWarps;
     T carry = 0;
     bool prev_end = true;
-    const uint32_t round_len = 32 * kItemsPerThread;
-    const uint32_t rs0 = w_lo & ~3u;
-    if (w_lo >= w_hi) {
-        // empty range (its start need not be 4-aligned): no rounds
-    } else if constexpr (RING) {
-        // round r of this lane lands in ring slot r % kRingStages; the copies
-        // of rounds r+1 .. r+kRingStages-1 are in flight while r is reduced
-        uint32_t* mine = ring + (static_cast<size_t>(warp) * kRingStages * 32 + lane) * kItemsPerThread;
-        const uint32_t nrounds = w_hi > rs0 ? (w_hi - rs0 + round_len - 1) / round_len : 0;
-        auto issue = [&](uint32_t r) {
-            const uint32_t ef = rs0 + r * round_len + lane * kItemsPerThread;
-            if (r < nrounds && lane_full(ef, w_lo, w_hi)) {
-                uint32_t* d = mine + (r % kRingStages) * 32 * kItemsPerThread;
-#pragma unroll
-                for (int q = 0; q < kLaneVecs; q++) cp_async16(d + 4 * q, g32 + ef + 4 * q);
-            }
-            cp_async_commit();
-        };
-#pragma unroll
-        for (int j = 0; j < kRingStages - 1; j++) issue(j);
-        for (uint32_t r = 0; r < nrounds; r++) {
-            issue(r + kRingStages - 1);
-            cp_async_wait<kRingStages - 1>();
-            const uint32_t rs = rs0 + r * round_len;
-            const bool full = lane_full(rs + lane * kItemsPerThread, w_lo, w_hi);
-            uint4 cur[kLaneVecs];
-            if (full) {
-                const uint4* src = reinterpret_cast<const uint4*>(mine + (r % kRingStages) * 32 * kItemsPerThread);
-#pragma unroll
-                for (int q = 0; q < kLaneVecs; q++) cur[q] = src[q];
-            }
-            warp_round<T>(g32, rs, w_lo, w_hi, ytile, accc, carry, prev_end, cur, full);
+    bool w_end = false, w_cp = false;
+    int w_fc = 0;
+    int k = 0;
+    while (k < bp.n && bp.round0[k + 1] <= vr0) k++;
+    for (int vr = vr0; vr < vr1; vr++) {
+        if (vr >= bp.round0[k + 1]) {  // the stretch moves on to the next piece
+            do {
+                k++;
+            } while (vr >= bp.round0[k + 1]);
+            carry = T(0);
+            prev_end = true;
         }
-        cp_async_wait<0>();
-    } else {
-        // two register buffers that swap roles every round: the next round's
-        // entries load while this round is reduced
-        uint4 ba[kLaneVecs], bb[kLaneVecs];
-        uint32_t rs = rs0;
-        bool fa = rs < w_hi && lane_full(rs + lane * kItemsPerThread, w_lo, w_hi);
-        if (fa) load_lane(g32, rs + lane * kItemsPerThread, ba);
-        while (rs < w_hi) {
-            uint32_t rn = rs + round_len;
-            const bool fb = rn < w_hi && lane_full(rn + lane * kItemsPerThread, w_lo, w_hi);
-            if (fb) load_lane(g32, rn + lane * kItemsPerThread, bb);
-            warp_round<T>(g32, rs, w_lo, w_hi, ytile, accc, carry, prev_end, ba, fa);
-            rs = rn;
-            if (rs >= w_hi) break;
-            rn = rs + round_len;
-            fa = rn < w_hi && lane_full(rn + lane * kItemsPerThread, w_lo, w_hi);
-            if (fa) load_lane(g32, rn + lane * kItemsPerThread, ba);
-            warp_round<T>(g32, rs, w_lo, w_hi, ytile, accc, carry, prev_end, bb, fb);
-            rs = rn;
+        const uint32_t lo = bp.lo[k], hi = bp.hi[k];
+        const uint32_t rbase = ((lo / kRound) + static_cast<uint32_t>(vr - bp.round0[k])) * kRound;
+        T* accc = acc + bp.acc_off[k];
+        if (lane == 0 && vr + 1 < bp.round0[k + 1]) {
+            // the next round of this piece into L2 while this one is reduced
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g32 + rbase + kRound),
+                         "r"(static_cast<unsigned>(kRound * sizeof(uint32_t)))
+                         : "memory");
         }
+        const uint4* src = reinterpret_cast<const uint4*>(g32 + rbase) + lane;
+        const uint32_t lb = rbase + kLaneRun * lane;  // the lane's first slot
+        const int k0 = lo > lb ? static_cast<int>(min(lo - lb, static_cast<uint32_t>(kLaneRun))) : 0;
+        const int k1 = hi > lb ? static_cast<int>(min(hi - lb, static_cast<uint32_t>(kLaneRun))) : 0;
+        const bool any = k0 < k1;
+        uint32_t eor, first_e, last_e;
+        T sum;
+        if (__all_sync(0xffffffffu, k0 == 0 && k1 == kLaneRun))
+            sum = lane_entries<T, true>(src, 0, kLaneRun, ytile, accc, eor, first_e, last_e);
+        else
+            sum = lane_entries<T, false>(src, k0, k1, ytile, accc, eor, first_e, last_e);
+        // no run ends in the lane: one column, its last entry not flagged
+        const bool single = any && !(eor & 1u);
+        const int hc = static_cast<int>(first_e >> 16);  // the lane's first run
+        // the lane continues the run of the entry before it unless that entry
+        // ended its run (previous lane's last entry; at lane 0 the warp's
+        // previous round, and none in the warp's first round: the record
+        // chain joins runs across warps)
+        const uint32_t f = lb + static_cast<uint32_t>(k0);
+        const uint32_t prev_last = __shfl_up_sync(0xffffffffu, last_e, 1);
+        const bool cont_prev = any && f > lo && (lane == 0 ? (vr != vr0 && !prev_end) : !(prev_last & 1u));
+        auto sink = [&](int col, T val) { accc[col] += val; };
+        const unsigned anyb = __ballot_sync(0xffffffffu, any);
+        const int lastl = 31 - __clz(anyb);  // a round holds at least one entry of its piece
+        if (__ballot_sync(0xffffffffu, single && cont_prev) == 0) {
+            // no lane extends a run from its left: a chain is one lane's tail
+            T prev_ts = __shfl_up_sync(0xffffffffu, sum, 1);
+            if (lane == 0) prev_ts = carry;
+            if (any && !single && cont_prev) sink(hc, prev_ts);
+            carry = __shfl_sync(0xffffffffu, sum, lastl);
+        } else {
+            carry = lane_chain<T>(any, single, cont_prev, hc, sum, carry, sink);
+        }
+        prev_end = (__shfl_sync(0xffffffffu, last_e, lastl) & 1u) != 0;
+        if (vr == vr0) {
+            // the stretch's first entry: its column, and whether it continues
+            // the run that ends the previous warp's stretch
+            const int fl = __ffs(anyb) - 1;
+            const uint32_t f0 = __shfl_sync(0xffffffffu, f, fl);
+            w_fc = bp.acc_off[k] + static_cast<int>(__shfl_sync(0xffffffffu, first_e, fl) >> 16);
+            w_cp = f0 > lo && !(g32[round_phys(f0 - 1)] & 1u);
+        }
+        w_end = w_end || __ballot_sync(0xffffffffu, any && !single) != 0;
     }
     if (lane == 0) {
         WarpRec<T>& rec = recs[warp];
-        rec.valid = w_lo < w_hi;
-        rec.ls = carry;  // the chain still open at the range's end (0 if its last run ended)
-        rec.fc = rec.cp = rec.single = 0;
-        if (w_lo < w_hi) {
-            const uint32_t ef = g32[w_lo], el = g32[w_hi - 1];
-            rec.fc = static_cast<int>(ef >> 16);
-            rec.cp = w_lo > e_lo && !(g32[w_lo - 1] & 1u);
-            rec.single = ((ef ^ el) >> 16) == 0 && !(el & 1u);
-        }
+        rec.valid = vr0 < vr1;
+        rec.ls = carry;  // the chain still open at the stretch's end (0 if its last run ended)
+        rec.fc = w_fc;
+        rec.cp = w_cp;
+        rec.single = !w_end;
     }
     __syncthreads();
     if (warp == 0) {
-        WarpRec<T> r{};  // lanes past the CTA's warps carry no range
+        WarpRec<T> r{};  // lanes past the CTA's warps carry no stretch
         if (lane < kWarps) r = recs[lane];
         lane_chain<T>(r.valid != 0, r.single != 0, r.cp != 0, r.fc, r.ls, T(0),
-                      [&](int col, T val) { accc[col] += val; });
+                      [&](int col, T val) { acc[col] += val; });
     }
 }
 
@@ -977,13 +970,12 @@ __device__ __forceinline__ void piece_share(const FastGeometry& g, const TView& 
 // written to those columns of partial + item_part[item] -
 // item_part[item_base].  A column's entries of a block are one run of the
 // sorted group, so splitting at sub-chunk bounds splits no run.
-template <typename T, bool RING>
+template <typename T>
 __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv, const uint32_t* __restrict__ g32,
                                          const uint32_t* __restrict__ sub_start, const T* __restrict__ y,
                                          T* __restrict__ partial, int item, int item_base, int64_t y_block0,
                                          int split, int nsplit, T* __restrict__ acc, T* __restrict__ ytile,
-                                         uint32_t* __restrict__ ring, WarpRec<T> (*recs)[kFastThreads / 32],
-                                         const int* __restrict__ pdone)
+                                         WarpRec<T>* recs, BlockPieces& bp, const int* __restrict__ pdone)
 {
     if (pdone && pdone[g.prob_of_block(tv.item_b0[item])]) return;  // retired problem: partials unused
     const int sc = tv.item_sc[item];
@@ -998,7 +990,7 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
         for (int i = a0 + threadIdx.x; i < a1; i += kFastThreads) ap[i] = 0;
     }
     if (!any) return;  // more splits than sub-chunks: nothing here
-    int flip = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int64_t blk = tv.item_b0[item]; blk < tv.item_b1[item]; blk++) {
         const int nb = static_cast<int>(g.block_rows(blk));
         __syncthreads();
@@ -1009,38 +1001,65 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
             constexpr int kPer = 16 / sizeof(T);
             constexpr int kInFlight = sizeof(T) == 4 ? 2 : 1;
             const int nvec = nb / kPer;
-            const uint4* src = reinterpret_cast<const uint4*>(yb);
+            const uint4* srcv = reinterpret_cast<const uint4*>(yb);
             uint4* dst = reinterpret_cast<uint4*>(ytile);
             for (int i0 = threadIdx.x; i0 < nvec; i0 += kInFlight * kFastThreads) {
-                uint4 u[kInFlight];
+                uint4 v[kInFlight];
 #pragma unroll
-                for (int k = 0; k < kInFlight; k++)
-                    if (i0 + k * kFastThreads < nvec) u[k] = __ldg(src + i0 + k * kFastThreads);
+                for (int kk = 0; kk < kInFlight; kk++)
+                    if (i0 + kk * kFastThreads < nvec) v[kk] = __ldg(srcv + i0 + kk * kFastThreads);
 #pragma unroll
-                for (int k = 0; k < kInFlight; k++)
-                    if (i0 + k * kFastThreads < nvec) dst[i0 + k * kFastThreads] = u[k];
+                for (int kk = 0; kk < kInFlight; kk++)
+                    if (i0 + kk * kFastThreads < nvec) dst[i0 + kk * kFastThreads] = v[kk];
             }
             for (int i = nvec * kPer + threadIdx.x; i < nb; i += kFastThreads) ytile[i] = yb[i];
         } else {
             for (int i = threadIdx.x; i < nb; i += kFastThreads) ytile[i] = yb[i];
         }
-        __syncthreads();
-        for (int pc = pc0; pc < pc1; pc++) {
-            int a0, a1;
-            piece_share(g, tv, pc, split, nsplit, a0, a1);
-            if (a0 >= a1) continue;
-            const int p = tv.piece_pat[pc];
-            const int ch0 = tv.piece_ch0[pc];
-            const int pat_sub_end = (p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks) * kSubPerChunk;
-            const int j0 = ch0 * kSubPerChunk + a0 / kSubCols;
-            const int j1 = ch0 * kSubPerChunk + (a1 + kSubCols - 1) / kSubCols;
-            const uint32_t e_lo = sub_start[blk * nsub + j0];
-            const uint32_t e_hi = j1 < pat_sub_end ? sub_start[blk * nsub + j1]
-                                                   : static_cast<uint32_t>(g.seg(blk, p) + g.seg_len(blk, p));
-            const uint32_t c0 = static_cast<uint32_t>(ch0 - g.chunk0[p]) * kChunkCols;
-            reduce_block_entries<T, RING>(g32, e_lo, e_hi, c0, ytile, acc + tv.piece_acc[pc], recs[flip], ring);
-            flip ^= 1;
+        if (blk + 1 < tv.item_b1[item])  // the next block's y slice into L2
+            prefetch_l2(y + (g.block_row0(blk + 1) - g.block_row0(y_block0)),
+                        static_cast<int64_t>(g.block_rows(blk + 1)) * static_cast<int64_t>(sizeof(T)));
+        if (warp == 0) {
+            // the block's pieces: entry ranges and their virtual rounds
+            const int npc = pc1 - pc0;
+            uint32_t lo = 0, hi = 0;
+            int off = 0, nr = 0;
+            if (lane < npc) {
+                const int pc = pc0 + lane;
+                int a0, a1;
+                piece_share(g, tv, pc, split, nsplit, a0, a1);
+                if (a0 < a1) {
+                    const int p = tv.piece_pat[pc];
+                    const int ch0 = tv.piece_ch0[pc];
+                    const int pat_sub_end = (p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks) * kSubPerChunk;
+                    const int j0 = ch0 * kSubPerChunk + a0 / kSubCols;
+                    const int j1 = ch0 * kSubPerChunk + (a1 + kSubCols - 1) / kSubCols;
+                    lo = sub_start[blk * nsub + j0];
+                    hi = j1 < pat_sub_end ? sub_start[blk * nsub + j1]
+                                          : static_cast<uint32_t>(g.seg(blk, p) + g.seg_len(blk, p));
+                    off = tv.piece_acc[pc] - (ch0 - g.chunk0[p]) * kChunkCols;
+                    if (lo < hi) nr = static_cast<int>((hi - 1) / kRound - lo / kRound) + 1;
+                }
+            }
+            int incl = nr;  // inclusive scan of the rounds over the pieces
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += v;
+            }
+            if (lane < npc) {
+                bp.lo[lane] = lo;
+                bp.hi[lane] = hi;
+                bp.acc_off[lane] = off;
+                bp.round0[lane + 1] = incl;
+            }
+            if (lane == 0) {
+                bp.round0[0] = 0;
+                bp.n = npc;
+            }
         }
+        __syncthreads();
+        reduce_block<T>(g32, bp, ytile, acc, recs);
     }
     __syncthreads();
     T* out = partial + (tv.item_part[item] - tv.item_part[item_base]);
@@ -1061,7 +1080,7 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
 // must therefore be stream-ordered).  Without ctr, CTA i runs unit i of the
 // items from item_base on.  With act (and ctr) the units are those of the
 // listed problems' items, split by a factor derived from their number.
-template <typename T, bool RING>
+template <typename T>
 __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeometry g, TView tv,
                                                                        const uint32_t* __restrict__ g32,
                                                                        const uint32_t* __restrict__ sub_start,
@@ -1073,19 +1092,17 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
                                                                        const FastActive* __restrict__ act, int nsplit)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    // two record sets, alternating per piece: warp 0 may still combine one
-    // piece's records while the other warps start on the next piece
-    __shared__ WarpRec<T> recs[2][kFastThreads / 32];
+    __shared__ WarpRec<T> recs[kFastThreads / 32];
+    __shared__ BlockPieces bp;
     __shared__ int s_item;
     __shared__ int pref[kMaxProblems + 1];
     if (done && *(volatile const int*)done) return;
     T* ytile = reinterpret_cast<T*>(smem_raw);  // first: its entries' byte offsets address it directly
     T* acc = ytile + kBlockRows;
-    uint32_t* ring = reinterpret_cast<uint32_t*>(acc + kChunkCols * tv.per_sc);  // RING schedules only
     if (!ctr) {
         const int u = static_cast<int>(blockIdx.x);
-        aty_item<T, RING>(g, tv, g32, sub_start, y, partial, u / nsplit + item_base, item_base, y_block0,
-                          u % nsplit, nsplit, acc, ytile, ring, recs, pdone);
+        aty_item<T>(g, tv, g32, sub_start, y, partial, u / nsplit + item_base, item_base, y_block0, u % nsplit,
+                    nsplit, acc, ytile, recs, bp, pdone);
         return;
     }
     int K = nsplit, units = tv.nitems * nsplit;
@@ -1107,7 +1124,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
             const int slot = active_slot(pref, act->n, item);
             item = tv.sc_item0[act->list[slot] * tv.nsc] + (item - pref[slot]);
         }
-        aty_item<T, RING>(g, tv, g32, sub_start, y, partial, item, 0, 0, u % K, K, acc, ytile, ring, recs, pdone);
+        aty_item<T>(g, tv, g32, sub_start, y, partial, item, 0, 0, u % K, K, acc, ytile, recs, bp, pdone);
     }
     if (threadIdx.x == 0) {
         __threadfence();
@@ -1476,9 +1493,9 @@ const FastTranspose& transpose_of(const FastLayout& f)
 }
 
 template <typename T>
-size_t spmv_t_smem(int per_sc, bool ring)
+size_t spmv_t_smem(int per_sc)
 {
-    return sizeof(T) * (static_cast<size_t>(kChunkCols) * per_sc + kBlockRows) + (ring ? kRingBytes : 0);
+    return sizeof(T) * (static_cast<size_t>(kChunkCols) * per_sc + kBlockRows);
 }
 
 void free_transpose(FastTranspose& t)
@@ -1507,9 +1524,8 @@ cas_status fast_set_attributes()
 cas_status fast_set_attributes_now()
 {
     const int s32 = static_cast<int>(sizeof(float) * kTable32), s64 = static_cast<int>(sizeof(double) * kTable64);
-    const int t32 = static_cast<int>(spmv_t_smem<float>(kMaxScRegs, false));
-    const int t32r = static_cast<int>(spmv_t_smem<float>(kMaxScRing, true));
-    const int t64 = static_cast<int>(spmv_t_smem<double>(1, false));
+    const int t32 = static_cast<int>(spmv_t_smem<float>(kMaxSc));
+    const int t64 = static_cast<int>(spmv_t_smem<double>(1));
     const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 0, true>, attr, s32));
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<float, float, 0, false>, attr, s32));
@@ -1529,9 +1545,8 @@ cas_status fast_set_attributes_now()
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 1, false>, attr, s64));
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 2, true>, attr, s64));
     CAS_CUDA(cudaFuncSetAttribute(fast_spmv_kernel<double, float, 2, false>, attr, s64));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<float, false>, attr, t32));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<float, true>, attr, t32r));
-    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<double, false>, attr, t64));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<float>, attr, t32));
+    CAS_CUDA(cudaFuncSetAttribute(fast_spmv_t_kernel<double>, attr, t64));
     return CAS_OK;
 }
 
@@ -1540,8 +1555,9 @@ cas_status fast_set_attributes_now()
 // is built and timed (partials + column sums, CUDA events, one warm-up
 // launch) on this layout; the fastest is kept and remembered per geometry
 // for the rest of the process, so later builds of the same shape skip the
-// timing.  CAS_ATY_SCHEDULE="chunks,ring,items_per_sm,pack,persistent"
-// forces a schedule.
+// timing.  CAS_ATY_SCHEDULE="chunks,0,items_per_sm,pack,persistent"
+// forces a schedule (the second field, entries streamed through a shared-
+// memory ring, is kept for the format of the schedule table and must be 0).
 // ---------------------------------------------------------------------------
 struct Sched {
     int per_sc;
@@ -1554,8 +1570,8 @@ constexpr Sched kSchedDefault = {4, false, 2, false, false};
 constexpr Sched kSchedCandidates[] = {
     {4, false, 2, false, false}, {4, false, 3, false, false}, {3, false, 2, false, false},
     {4, false, 2, true, false},  {4, false, 2, true, true},   {4, false, 4, true, true},
-    {4, false, 4, false, true},  {2, false, 2, true, false},  {2, true, 3, true, false},
-    {2, true, 4, true, true},    {2, true, 2, false, false},  {4, false, 6, false, true}};
+    {4, false, 4, false, true},  {2, false, 2, true, false},  {2, false, 3, true, false},
+    {2, false, 4, true, true},   {4, false, 1, false, false}, {4, false, 6, false, true}};
 static_assert(sizeof(kSchedCandidates) / sizeof(Sched) <= kMaxTune, "tune table");
 constexpr int64_t kTuneMinBlocks = 64;  // smaller layouts take the default schedule
 
@@ -1572,7 +1588,7 @@ std::string tune_key(const FastGeometry& g)
 
 bool valid_sched(const Sched& c)
 {
-    return c.per_sc >= 1 && c.per_sc <= (c.ring ? kMaxScRing : kMaxScRegs) && c.ips >= 1 && c.ips <= 16;
+    return c.per_sc >= 1 && c.per_sc <= kMaxSc && !c.ring && c.ips >= 1 && c.ips <= 16;
 }
 
 cas_status tune_transpose(FastLayout& f, const std::vector<int64_t>& entries, cudaStream_t s)
@@ -1588,7 +1604,7 @@ cas_status tune_transpose(FastLayout& f, const std::vector<int64_t>& entries, cu
         const int n = std::sscanf(env, "%d,%d,%d,%d,%d", &a, &b, &c, &d, &e);
         const Sched forced{a, b != 0, c, d != 0, e != 0};
         CAS_REQUIRE(n == 5 && valid_sched(forced), CAS_ERR_INVALID_ARGUMENT,
-                    "CAS_ATY_SCHEDULE must be \"chunks,ring,items_per_sm,pack,persistent\" within limits");
+                    "CAS_ATY_SCHEDULE must be \"chunks,0,items_per_sm,pack,persistent\" within limits");
         return build(forced);
     }
     if (g.nblocks < kTuneMinBlocks) return build(kSchedDefault);
@@ -1825,7 +1841,7 @@ cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag,
 {
     const FastTranspose& t = transpose_of<T>(f);
     if (t.nitems == 0) return CAS_OK;
-    const size_t smem = spmv_t_smem<T>(t.per_sc, t.ring);
+    const size_t smem = spmv_t_smem<T>(t.per_sc);
     // with an active list the kernel splits the units itself (persistent);
     // else the items are split so that a short list still fills the GPU
     const int nsplit = act ? 1 : unit_splits(t.nitems, sm_count(), kAtySplitMax);
@@ -1834,16 +1850,7 @@ cas_status fast_spmv_t_partials(const FastLayout& f, const T* y, int* done_flag,
     const unsigned grid = static_cast<unsigned>(persistent ? std::min(units, sm_count()) : units);
     const unsigned pgrid = act ? static_cast<unsigned>(sm_count()) : grid;
     int* ctr = persistent ? t.ctr : nullptr;
-    if constexpr (sizeof(T) == 4) {
-        if (t.ring) {
-            { fast_spmv_t_kernel<T, true><<<pgrid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.sub_start, y,
-                                                                         static_cast<T*>(t.partial), done_flag, 0, 0,
-                                                                         ctr, pdone, act, nsplit); cas::count_launch(); }
-            CAS_CHECK_LAUNCH();
-            return CAS_OK;
-        }
-    }
-    { fast_spmv_t_kernel<T, false><<<pgrid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.sub_start, y,
+    { fast_spmv_t_kernel<T><<<pgrid, kFastThreads, smem, s>>>(f.g, tview(t), f.g32, f.sub_start, y,
                                                                   static_cast<T*>(t.partial), done_flag, 0, 0,
                                                                   ctr, pdone, act, nsplit); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
@@ -1932,9 +1939,9 @@ static cas_status eval_buffers(FastLayout& f, int64_t nb, cudaStream_t s)
 // The adjoint's per-block partials of blocks [b0, b1) on g into eval_partial.
 static cas_status eval_adjoint_partials(FastLayout& f, int64_t b0, int64_t b1, const float* g, cudaStream_t s)
 {
-    const size_t smem = spmv_t_smem<float>(1, false);
+    const size_t smem = spmv_t_smem<float>(1);
     const int items = static_cast<int>((b1 - b0) * f.g.nchunks);
-    { fast_spmv_t_kernel<float, false><<<items, kFastThreads, smem, s>>>(f.g, tview(f.tb), f.g32, f.sub_start, g,
+    { fast_spmv_t_kernel<float><<<items, kFastThreads, smem, s>>>(f.g, tview(f.tb), f.g32, f.sub_start, g,
                                                                  f.eval_partial, nullptr,
                                                                  static_cast<int>(b0 * f.g.nchunks), b0, nullptr,
                                                                  nullptr, nullptr, 1); cas::count_launch(); }

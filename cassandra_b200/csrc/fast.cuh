@@ -10,6 +10,13 @@
 //                                              transposed copy); end marks the
 //                                              last entry of each column
 //
+// G32 is stored in rounds of kRound entries: the sorted order is cut into
+// rounds from each group's start (every group starts on a round boundary),
+// and inside a round the 32 consecutive entries a lane reduces (lane L:
+// entries 32L .. 32L+31) lie in 8 rows of 512 bytes, one 16-byte word per
+// lane and row, so that a warp reads a round with 8 coalesced loads.
+// round_phys() maps an entry's position in the sorted order to its place.
+//
 // so that a CTA touches one pattern's columns at a time.  A x stages that
 // pattern's slice of x in shared memory and gathers from there; A'y stages
 // the block's slice of y in shared memory and reduces the column-sorted
@@ -23,6 +30,8 @@
 namespace cas {
 
 constexpr int kBlockRows = 16384;        // rows per block (and per A'y tile)
+constexpr int kRound = 1024;             // G32 entries of one A'y round (32 lanes x 32)
+constexpr int kLaneRun = kRound / 32;    // consecutive entries a lane reduces per round
 constexpr int kFastThreads = 1024;       // threads of the A'y kernel
 constexpr int kAxThreads = 1024;         // threads of the A x kernel
 constexpr int kAxRows = kBlockRows / kAxThreads;  // rows per thread in A x
@@ -109,8 +118,12 @@ struct FastGeometry {
         b = pblk0[q] + local / kBlockRows;
         rb = local - (local / kBlockRows) * kBlockRows;
     }
-    // Rows of a block rounded up to 8 so that every segment is 16-byte aligned.
-    __host__ __device__ int64_t padded_rows(int64_t b) const { return (block_rows(b) + 7) & ~int64_t(7); }
+    // Rows of a block rounded up to kRound, so that every (block, pattern)
+    // segment starts on a G32 round (and on a 16-byte boundary).
+    __host__ __device__ int64_t padded_rows(int64_t b) const
+    {
+        return (block_rows(b) + kRound - 1) & ~int64_t(kRound - 1);
+    }
     // Element offset of (block, pattern) in A16 / G32.
     __host__ __device__ int64_t seg(int64_t b, int p) const
     {
@@ -122,6 +135,15 @@ struct FastGeometry {
         return nblocks == 0 ? 0 : (nblocks - 1) * int64_t(kBlockRows) * k + padded_rows(nblocks - 1) * k;
     }
 };
+
+// Place in G32 of the entry at position i of the sorted order (i counted
+// from any round boundary): offset o = 32 L + 4 q + j inside the round goes
+// to 128 q + 4 L + j.
+__host__ __device__ __forceinline__ uint32_t round_phys(uint32_t i)
+{
+    return (i & ~uint32_t(kRound - 1)) | ((i & 0x1Cu) << 5) | ((i & 0x3E0u) >> 3) | (i & 3u);
+}
+static_assert(kRound == 1024 && kLaneRun == 32, "round_phys assumes 32 lanes x 32 entries");
 
 // The problems a batched step works on (those not retired), in problem
 // order, rebuilt on the device before each iteration.  Given to the

@@ -37,11 +37,11 @@ __global__ void true_weights_kernel(uint64_t seed, int64_t cols, double sigma, d
 // b_r = clamp(2 rint(((A w*)_r + e_r) / 2), -64, 64), e_r ~ N(0, noise^2);
 // aw holds (A w*)_r, computed on whichever layout the CSR has.
 __global__ void targets_kernel(const double* __restrict__ aw, int64_t rows, uint64_t seed, double noise,
-                               double* __restrict__ b)
+                               int64_t first_row, double* __restrict__ b)
 {
     for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < rows;
          r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        Stream rng(seed ^ 0xB0A5EDD15EA5EULL, static_cast<uint64_t>(r));
+        Stream rng(seed ^ 0xB0A5EDD15EA5EULL, static_cast<uint64_t>(first_row + r));
         const double u1 = rng.unit(), u2 = rng.unit();
         const double e = noise * sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
         b[r] = fmin(64.0, fmax(-64.0, 2.0 * rint((aw[r] + e) * 0.5)));
@@ -121,7 +121,14 @@ CAS_API cas_status cas_generate_positions_host(uint64_t seed, int64_t first, int
 CAS_API cas_status cas_generate_targets(const cas_csr* a, uint64_t seed, double w_sigma, double noise_sigma,
                                         double* d_b, double* d_w_true, void* stream)
 {
-    CAS_REQUIRE(a && (d_b || a->rows == 0), CAS_ERR_INVALID_ARGUMENT, "cas_generate_targets: bad argument");
+    return cas_generate_targets_rows(a, seed, w_sigma, noise_sigma, 0, d_b, d_w_true, stream);
+}
+
+CAS_API cas_status cas_generate_targets_rows(const cas_csr* a, uint64_t seed, double w_sigma, double noise_sigma,
+                                             int64_t first_row, double* d_b, double* d_w_true, void* stream)
+{
+    CAS_REQUIRE(a && (d_b || a->rows == 0) && first_row >= 0, CAS_ERR_INVALID_ARGUMENT,
+                "cas_generate_targets: bad argument");
     auto s = static_cast<cudaStream_t>(stream);
     double* w = d_w_true;
     if (!w) CAS_CUDA(cudaMallocAsync(&w, sizeof(double) * std::max<int64_t>(a->cols, 1), s));
@@ -130,7 +137,7 @@ CAS_API cas_status cas_generate_targets(const cas_csr* a, uint64_t seed, double 
     if (a->rows) {
         // A w* into d_b first (FP64 product on the CSR's layout), then noise and rounding in place
         CAS_TRY(cas_spmv(a, CAS_F64, w, d_b, stream));
-        { targets_kernel<<<grid(a->rows), 256, 0, s>>>(d_b, a->rows, seed, noise_sigma, d_b); cas::count_launch(); }
+        { targets_kernel<<<grid(a->rows), 256, 0, s>>>(d_b, a->rows, seed, noise_sigma, first_row, d_b); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
     }
     if (!d_w_true) cudaFreeAsync(w, s);

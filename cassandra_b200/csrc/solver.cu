@@ -93,8 +93,10 @@ constexpr double kReplaceDrop = 1e-4;
 // the Krylov space is thrown away.
 constexpr double kLsqrRestartDrop = 1e-4;
 // A host check at a chunk boundary that finds the true residual this many
-// times above the mixed cycle's recursive estimate restarts the cycle.
-constexpr double kLsqrDrift = 100.0;
+// times above the mixed cycle's recursive estimate restarts the cycle: the
+// cycle has reached the floor its FP32 products leave (on the unscaled
+// systems the two agree within 2x until then, measured).
+constexpr double kLsqrDrift = 4.0;
 
 __device__ __forceinline__ bool gated(const int* gate) { return gate && *(volatile const int*)gate != 0; }
 

@@ -397,6 +397,12 @@ CAS_API cas_status cas_generate_positions_host(uint64_t seed, int64_t first, int
  * returns w* (cols doubles, may be NULL). */
 CAS_API cas_status cas_generate_targets(const cas_csr* a, uint64_t seed, double w_sigma, double noise_sigma,
                                         double* d_b, double* d_w_true, void* stream);
+/* The same targets for a block of rows of a larger system: row r of `a` is
+ * row first_row + r of the whole system (its noise is drawn from that row's
+ * stream), so ranks that each hold a block of rows generate the whole
+ * system's targets between them.  first_row = 0 is cas_generate_targets. */
+CAS_API cas_status cas_generate_targets_rows(const cas_csr* a, uint64_t seed, double w_sigma, double noise_sigma,
+                                             int64_t first_row, double* d_b, double* d_w_true, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Pattern-based score estimators (Pattern/Evaluator.h, IO/Binary.cpp)       */

@@ -49,8 +49,15 @@ def test_blocked_products_match_oracle(cuda, orc, rows, masks, mode):
         np.testing.assert_array_equal(cb.jacobi_preconditioner_of_ata(a).cpu().numpy(), orc.jacobi(idx, cols))
 
 
-SCHEDULES = ["4,0,2,0,0", "4,0,1,1,0", "3,0,2,1,1", "2,0,2,0,1", "2,1,2,1,0", "1,1,2,0,0", "2,1,3,1,1",
+SCHEDULES = ["4,0,2,0,0", "4,0,1,1,0", "3,0,2,1,1", "2,0,2,0,1", "2,0,2,1,0", "1,0,2,0,0", "2,0,3,1,1",
              "1,0,5,1,1"]
+
+
+def test_aty_schedule_rejects_the_retired_ring_form(cuda, monkeypatch):
+    """The schedule format keeps its second field; only 0 is accepted."""
+    monkeypatch.setenv("CAS_ATY_SCHEDULE", "2,1,2,1,0")
+    with pytest.raises(cb.CasError):
+        _build(3 * 16384, SET8, "expanded", "blocked", seed=31)
 
 
 @pytest.mark.parametrize("sched", SCHEDULES)
