@@ -29,9 +29,11 @@ Huber + L2 over 65,536-row minibatches, each minibatch step one CUDA graph).
 workload; for the single fit every step is the whole 20M-row workload, with
 inputs from the oracle's restatement of the seeded generator.
 
-N > 1 runs under torchrun, one rank per GPU, each rank fitting its own
-independently seeded replica (the fits are independent; no collective on
-the data path).  Rank 0 prints one JSON line.
+N > 1 runs under torchrun, one rank per GPU: the single workload becomes one
+fit sharded by rows (each rank holds a block range of the 20M rows; one
+all-reduce per PCG iteration; strong scaling), the batched and evaluator
+workloads run one independently seeded replica per rank (their fits are
+independent; no collective on the data path).  Rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -86,6 +88,8 @@ def parse_args(argv=None):
     ap.add_argument("--lsqr-max-iterations", type=int, default=20000)
     ap.add_argument("--no-summaries", action="store_true",
                     help="single workload: leave out the short batched and evaluator runs")
+    ap.add_argument("--sharded", action="store_true",
+                    help="single workload: the row-sharded fit even on one GPU (always with N > 1)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -313,7 +317,7 @@ def run_ours(args) -> dict | None:
     # the same comparison on one layout: FP64 and mixed PCG solves on one
     # blocked CSR, so the ratio isolates the precision; and LSQR / LSMR
     same_layout, lsq = None, {}
-    if not args.no_plain or args.lsqr:
+    if not args.no_plain or LSQ_VARIANTS[args.lsqr]:
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         ab = cb.MatrixCSR.from_positions(g, pos, "blocked")
@@ -439,6 +443,106 @@ def run_ours(args) -> dict | None:
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    return result if rank == 0 else None
+
+
+def run_ours_sharded(args) -> dict | None:
+    """The single workload on N GPUs as one fit sharded by rows: rank k holds
+    the rows of its block range of the 20M-row system (positions from the
+    seeded generator at those row numbers, the system's targets for them),
+    and every step builds its blocked CSR and runs the row-sharded mixed PCG
+    (cassandra_b200.parallel: one all-reduce of cols + 1 doubles per
+    iteration, FP64 residual replacement at chunk boundaries) to the
+    tolerance.  Total work is fixed: strong scaling."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world == 1:  # --sharded on one GPU: a process group of one rank
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29511")
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    import cassandra_b200 as cb
+    from cassandra_b200 import parallel as par
+
+    lib = cb.load()
+    stream = torch.cuda.current_stream()
+    R = args.rows
+    lo, hi = par.split_rows(R, world, rank, int(lib.cas_block_rows()))
+    n = hi - lo
+    g = cb.GroupIndexer(PATTERNS_8, "expanded")
+    pos_h = torch.from_numpy(cb.generate_positions_host(args.seed, lo, n, args.min_empties, args.max_empties)
+                             .view(np.int64).reshape(n, 2)).pin_memory()
+    pos = pos_h.to("cuda")
+    b = cb.generate_targets(cb.MatrixCSR.from_positions(g, pos, "rows"), args.seed, first_row=lo)
+    torch.cuda.synchronize()
+
+    def step():
+        a = cb.MatrixCSR.from_positions(g, pos, "blocked")
+        return par.sharded_pcg(par.GpuShard(a, b, "mixed"), tol=args.tol, max_iterations=20000)
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.cas_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    results = [step() for _ in range(args.steps)]
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    launches = lib.cas_kernel_launches() - launches0
+    clk = clocks.stop()
+    t = torch.tensor([e0.elapsed_time(e1) * 1e-3], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    per_step = float(t.item()) / args.steps
+    last = results[-1]
+
+    # end to end: the rank's positions and targets from pinned host memory,
+    # the fit, the weights back
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 2))
+    b_h = b.cpu().pin_memory()
+    w_h = torch.empty(COLS_8, dtype=torch.float64).pin_memory()
+    times = []
+    for _ in range(e2e_steps):
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p_d, b_d = pos_h.to("cuda", non_blocking=True), b_h.to("cuda", non_blocking=True)
+        a = cb.MatrixCSR.from_positions(g, p_d, "blocked")
+        res = par.sharded_pcg(par.GpuShard(a, b_d, "mixed"), tol=args.tol, max_iterations=20000)
+        w_h.copy_(res.x)
+        times.append(time.perf_counter() - t0)
+    te = torch.tensor([statistics.mean(times)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    peak, peak_kind = measured_peaks()
+    result = {
+        "metric": METRIC, "value": per_step, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": False, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32 products / f64 scalars",
+        "data": "synthetic (seeded random-play positions, seeded targets)",
+        "config": single_config(args),
+        "precision": "mixed (FP32 products, FP64 replicated state, FP64 residual replacement on a 1e3 drop or "
+                     "every 50 iterations)",
+        "parallelism": f"row-sharded x{world}: one all-reduce of {COLS_8 + 1} doubles per iteration (NCCL)",
+        "breakdown": {"iterations": last.iterations, "replacements": last.replacements,
+                      "allreduces": last.allreduces, "rel_residual": last.rel_residual,
+                      "rows_per_rank": n},
+        "roofline": None, "peak_hbm_gbs": peak, "peak_kind": peak_kind,
+        "e2e": {"value": float(te.item()), "unit": "s", "h2d_bytes_per_step": int(n * 16 + n * 8),
+                "d2h_bytes_per_step": COLS_8 * 8, "steps": e2e_steps},
+        "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": None,
+    }
+    dist.barrier()
+    dist.destroy_process_group()
     return result if rank == 0 else None
 
 
@@ -1089,6 +1193,8 @@ def main(argv=None) -> int:
         res = run_ours_batched(args)
     elif args.workload == "evaluator":
         res = run_ours_evaluator(args)
+    elif dist_env()[0] > 1 or args.sharded:
+        res = run_ours_sharded(args)
     else:
         res = run_ours(args)
     if res is not None:

@@ -31,8 +31,9 @@ namespace cas {
 
 namespace {
 
-constexpr int kSortThreads = 1024;
+constexpr int kSortThreads = 256;  // a sort pass's round is kSortThreads items (at least 256: one thread per digit)
 constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortCtasPerSm = 4;  // groups sorted at once per SM: their barriers and scans overlap
 // The A'y accumulator of a work item holds at most kMaxSc column chunks
 // (with the y tile, the FP32 kernel's dynamic shared memory: 192 KB).  The
 // build-time autotuner picks the schedule (accumulator width, items per SM,
@@ -183,7 +184,8 @@ __device__ void sort_pass(const uint16_t* __restrict__ a16_in, const uint32_t* _
     }
 }
 
-__global__ void __launch_bounds__(kSortThreads, 1) fast_sort_kernel(FastGeometry g, const uint16_t* __restrict__ a16,
+__global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm) fast_sort_kernel(FastGeometry g,
+                                                                                const uint16_t* __restrict__ a16,
                                                                    uint32_t* __restrict__ g32,
                                                                    uint32_t* __restrict__ scratch)
 {
@@ -399,27 +401,26 @@ __device__ __forceinline__ void load_table(T* __restrict__ table, const T* __res
 }
 
 // Rows of one 8-slot pattern segment (the expanded layout): each thread owns
-// kAxRows rows (stride kAxThreads); the 16-byte index word of row j+kAxAhead
-// is loaded while row j is gathered, so kAxAhead loads per thread stay in
-// flight.
-template <typename T, bool ALL_IN>
+// ROWS rows (stride kAxThreads); the 16-byte index word of row j+AHEAD is
+// loaded while row j is gathered, so AHEAD loads per thread stay in flight.
+template <typename T, bool ALL_IN, int ROWS, int AHEAD>
 __device__ __forceinline__ void gather_segment8(const uint16_t* __restrict__ base, int nb,
                                                 const T* __restrict__ table, const T* __restrict__ xg, int cap,
-                                                typename AccOf<T>::type (&acc)[kAxRows])
+                                                typename AccOf<T>::type (&acc)[ROWS])
 {
-    uint4 w[kAxAhead];
+    uint4 w[AHEAD];
 #pragma unroll
-    for (int j = 0; j < kAxAhead; j++) {
+    for (int j = 0; j < AHEAD; j++) {
         const int r = threadIdx.x + j * kAxThreads;
         w[j] = r < nb ? *reinterpret_cast<const uint4*>(base + static_cast<int64_t>(r) * 8) : make_uint4(0, 0, 0, 0);
     }
 #pragma unroll
-    for (int j = 0; j < kAxRows; j++) {
-        const uint4 cur = w[j % kAxAhead];
-        if (j + kAxAhead < kAxRows) {
-            const int rn = threadIdx.x + (j + kAxAhead) * kAxThreads;
-            w[j % kAxAhead] = rn < nb ? *reinterpret_cast<const uint4*>(base + static_cast<int64_t>(rn) * 8)
-                                      : make_uint4(0, 0, 0, 0);
+    for (int j = 0; j < ROWS; j++) {
+        const uint4 cur = w[j % AHEAD];
+        if (j + AHEAD < ROWS) {
+            const int rn = threadIdx.x + (j + AHEAD) * kAxThreads;
+            w[j % AHEAD] = rn < nb ? *reinterpret_cast<const uint4*>(base + static_cast<int64_t>(rn) * 8)
+                                   : make_uint4(0, 0, 0, 0);
         }
         const int r = threadIdx.x + j * kAxThreads;
         if (r < nb) {
@@ -494,7 +495,9 @@ __host__ __device__ __forceinline__ int unit_splits(int64_t units, int64_t ctas,
 // split for `ctas` CTAs, partials [block][kAxSplitMax] (splits past the one
 // in use written 0); a split of kAxSplitMax is left to
 // fast_spmv_direct_kernel.
-template <typename T, typename Y, int MODE, bool ALL8>
+// ROWS: rows per thread (a unit holds at most kAxThreads * ROWS rows: a
+// whole block), AHEAD: index loads in flight per thread.
+template <typename T, typename Y, int MODE, bool ALL8, int ROWS = kAxRows, int AHEAD = kAxAhead>
 __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g, const uint16_t* __restrict__ a16,
                                                                    const T* __restrict__ x, Y* __restrict__ y,
                                                                    const double* __restrict__ b,
@@ -546,9 +549,9 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
         const int64_t row0 = g.block_row0(blk) + r0;
         const T* xq = x + q * g.pcols;
         Comp mine;
-        Acc acc[kAxRows];
+        Acc acc[ROWS];
 #pragma unroll
-        for (int j = 0; j < kAxRows; j++) acc[j] = 0;
+        for (int j = 0; j < ROWS; j++) acc[j] = 0;
         // the index stream of a pattern is fetched into L2 one phase ahead,
         // so that HBM keeps streaming while x's next slice is staged
         prefetch_l2(a16 + g.seg(blk, 0) + static_cast<int64_t>(r0) * g.slots[0],
@@ -567,19 +570,19 @@ __global__ void __launch_bounds__(kAxThreads, 1) fast_spmv_kernel(FastGeometry g
             const bool all_in = g.space[p] <= kCap;
             if (ALL8 || ns == 8) {
                 if (all_in)
-                    gather_segment8<T, true>(base, nb, table, xg, cap, acc);
+                    gather_segment8<T, true, ROWS, AHEAD>(base, nb, table, xg, cap, acc);
                 else
-                    gather_segment8<T, false>(base, nb, table, xg, cap, acc);
+                    gather_segment8<T, false, ROWS, AHEAD>(base, nb, table, xg, cap, acc);
             } else if (!ALL8) {
 #pragma unroll
-                for (int j = 0; j < kAxRows; j++) {
+                for (int j = 0; j < ROWS; j++) {
                     const int r = threadIdx.x + j * kAxThreads;
                     if (r < nb) gather_row<T>(base + static_cast<int64_t>(r) * ns, ns, table, xg, cap, all_in, acc[j]);
                 }
             }
         }
 #pragma unroll
-        for (int j = 0; j < kAxRows; j++) {
+        for (int j = 0; j < ROWS; j++) {
             const int r = threadIdx.x + j * kAxThreads;
             if (r < nb) {
                 const int64_t row = row0 + r;
@@ -716,7 +719,7 @@ struct TView {
     const int* piece_ch0;
     const int* piece_ch1;
     const int* piece_acc;
-    const int* sc_item0;  // [nprob * nsc + 1] first item of each (problem, super-chunk)
+    const int* sc_item0;  // [nprob * nsc + 1]: items of problem q are [sc_item0[q * nsc], sc_item0[(q + 1) * nsc])
     int nsc;
     int per_sc;
     int nitems;
@@ -856,12 +859,31 @@ __device__ __forceinline__ T lane_entries(const uint4* __restrict__ src, int k0,
     return sum;
 }
 
+// Lane 0 of each warp asks L2 for the first round of the warp's stretch in
+// the block whose table is bp (issued a block ahead, before its barrier).
+__device__ __forceinline__ void prefetch_first_round(const uint32_t* __restrict__ g32, const BlockPieces& bp)
+{
+    constexpr int kWarps = kFastThreads / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane != 0) return;
+    const int nrounds = bp.round0[bp.n];
+    const int v = nrounds * warp / kWarps;
+    if (v >= nrounds * (warp + 1) / kWarps) return;  // no stretch
+    int k = 0;
+    while (bp.round0[k + 1] <= v) k++;
+    const uint32_t rbase = ((bp.lo[k] / kRound) + static_cast<uint32_t>(v - bp.round0[k])) * kRound;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g32 + rbase),
+                 "r"(static_cast<unsigned>(kRound * sizeof(uint32_t)))
+                 : "memory");
+}
+
 // The reduction of one block's entries of every piece in `bp` into acc.
 // Ends with a block barrier and warp 0's record combination; the next block
 // may restage ytile after the next barrier.
 template <typename T>
 __device__ __forceinline__ void reduce_block(const uint32_t* __restrict__ g32, const BlockPieces& bp,
-                                             const T* __restrict__ ytile, T* __restrict__ acc, WarpRec<T>* recs)
+                                             const BlockPieces* next, const T* __restrict__ ytile,
+                                             T* __restrict__ acc, WarpRec<T>* recs)
 {
     constexpr int kWarps = kFastThreads / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -934,6 +956,7 @@ __device__ __forceinline__ void reduce_block(const uint32_t* __restrict__ g32, c
         }
         w_end = w_end || __ballot_sync(0xffffffffu, any && !single) != 0;
     }
+    if (next) prefetch_first_round(g32, *next);  // while the other warps finish this block
     if (lane == 0) {
         WarpRec<T>& rec = recs[warp];
         rec.valid = vr0 < vr1;
@@ -951,6 +974,164 @@ __device__ __forceinline__ void reduce_block(const uint32_t* __restrict__ g32, c
     }
 }
 
+// ---------------------------------------------------------------------------
+// The same reduction for items whose blocks hold few rounds (the FP64
+// products, whose accumulator holds one chunk): each (block, piece) entry
+// range is cut into 32 nearly equal stretches of whole 4-entry words, one
+// per warp, so every warp works whatever the number of rounds; a warp's
+// stretch is reduced in steps of kStretchRun entries per lane (consecutive
+// in the sorted order, two 16-byte words of G32 each), with the same lane
+// chain and warp records.
+// ---------------------------------------------------------------------------
+constexpr int kStretchRun = 8;                  // entries per lane and step
+constexpr int kStretchVecs = kStretchRun / 4;   // 16-byte words per lane and step
+
+// The 16-byte word of G32 that holds sorted positions e .. e+3 (e a
+// multiple of 4).
+__device__ __forceinline__ uint4 word_at(const uint32_t* __restrict__ g32, uint32_t e)
+{
+    return __ldcs(reinterpret_cast<const uint4*>(g32 + round_phys(e)));
+}
+
+// A lane's entries of a step are all inside the warp's stretch.
+__device__ __forceinline__ bool lane_full(uint32_t e_first, uint32_t w_lo, uint32_t w_hi)
+{
+    return e_first >= w_lo && e_first + kStretchRun <= w_hi;
+}
+
+__device__ __forceinline__ void load_lane(const uint32_t* __restrict__ g32, uint32_t e_first,
+                                          uint4 (&u)[kStretchVecs])
+{
+#pragma unroll
+    for (int q = 0; q < kStretchVecs; q++) u[q] = word_at(g32, e_first + 4 * q);
+}
+
+// One step of a warp over [w_lo, w_hi): lanes take kStretchRun entries
+// each from step_start (a multiple of 4).  A lane whose entries are all in
+// range gets them in `cur` (loaded ahead by the caller); edge lanes load
+// theirs one by one.  accc: the accumulator shifted so that an entry's
+// column field indexes it.  carry: the run open before the step (updated);
+// prev_end: the last entry before this step ended its run (updated).
+template <typename T>
+__device__ __forceinline__ void stretch_step(const uint32_t* __restrict__ g32, uint32_t step_start, uint32_t w_lo,
+                                             uint32_t w_hi, const T* __restrict__ ytile, T* __restrict__ accc,
+                                             T& carry, bool& prev_end, const uint4 (&cur)[kStretchVecs], bool full)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t e_first = step_start + lane * kStretchRun;
+    T sum = 0;
+    uint32_t ends = 0;
+    auto step = [&](uint32_t e) {
+        sum += y_of<T>(ytile, e);
+        ends |= e;
+        if (e & 1u) {  // the run ends here: this lane's part of it
+            accc[e >> 16] += sum;
+            sum = T(0);
+        }
+    };
+    bool any = false;
+    uint32_t first_ent = 1u, last_ent = 1u;  // an empty lane looks like a closed run
+    if (full) {
+        first_ent = cur[0].x;
+#pragma unroll
+        for (int q = 0; q < kStretchVecs; q++) {
+            step(cur[q].x);
+            step(cur[q].y);
+            step(cur[q].z);
+            step(cur[q].w);
+        }
+        any = true;
+        last_ent = cur[kStretchVecs - 1].w;
+    } else {
+        const uint32_t lo = max(e_first, w_lo), hi = min(e_first + kStretchRun, w_hi);
+        if (lo < hi) {
+            for (uint32_t e = lo; e < hi; e++) step(g32[round_phys(e)]);
+            any = true;
+            first_ent = g32[round_phys(lo)];
+            last_ent = g32[round_phys(hi - 1)];
+        }
+    }
+    const bool single = any && !(ends & 1u);
+    const int hc = static_cast<int>(first_ent >> 16);
+    const uint32_t first_valid = max(e_first, w_lo);
+    const uint32_t prev_last = __shfl_up_sync(0xffffffffu, last_ent, 1);
+    const bool cont_prev = any && first_valid > w_lo && (lane == 0 ? !prev_end : !(prev_last & 1u));
+    auto sink = [&](int col, T val) { accc[col] += val; };
+    if (__ballot_sync(0xffffffffu, single && cont_prev) == 0) {
+        T prev_ts = __shfl_up_sync(0xffffffffu, sum, 1);
+        if (lane == 0) prev_ts = carry;
+        if (any && !single && cont_prev) sink(hc, prev_ts);
+        const int last = min(31, static_cast<int>((w_hi - 1 - step_start) / kStretchRun));  // last lane with entries
+        carry = __shfl_sync(0xffffffffu, sum, last);
+    } else {
+        carry = lane_chain<T>(any, single, cont_prev, hc, sum, carry, sink);
+    }
+    prev_end = (__shfl_sync(0xffffffffu, last_ent, 31) & 1u) != 0;
+}
+
+// The stretch reduction of one block's entries [e_lo, e_hi) of one piece
+// into accc (indexed by column field).  Ends with a block barrier; warp 0
+// then combines the records (recs: the set of this piece; the caller
+// alternates two sets so that the next piece may start meanwhile).
+template <typename T>
+__device__ __forceinline__ void reduce_stretch(const uint32_t* __restrict__ g32, uint32_t e_lo, uint32_t e_hi,
+                                               const T* __restrict__ ytile, T* __restrict__ accc, WarpRec<T>* recs)
+{
+    constexpr int kWarps = kFastThreads / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t n = e_hi - e_lo;
+    auto cut = [&](int w) -> uint32_t {
+        if (w == 0) return e_lo;
+        if (w == kWarps) return e_hi;
+        return max(e_lo, (e_lo + static_cast<uint32_t>(n * w / kWarps)) & ~3u);
+    };
+    const uint32_t w_lo = cut(warp), w_hi = cut(warp + 1);
+    T carry = 0;
+    bool prev_end = true;
+    const uint32_t step_len = 32 * kStretchRun;
+    const uint32_t rs0 = w_lo & ~3u;
+    if (w_lo < w_hi) {
+        // two register buffers that swap roles every step: the next step's
+        // entries load while this one is reduced
+        uint4 ba[kStretchVecs], bb[kStretchVecs];
+        uint32_t rs = rs0;
+        bool fa = rs < w_hi && lane_full(rs + lane * kStretchRun, w_lo, w_hi);
+        if (fa) load_lane(g32, rs + lane * kStretchRun, ba);
+        while (rs < w_hi) {
+            uint32_t rn = rs + step_len;
+            const bool fb = rn < w_hi && lane_full(rn + lane * kStretchRun, w_lo, w_hi);
+            if (fb) load_lane(g32, rn + lane * kStretchRun, bb);
+            stretch_step<T>(g32, rs, w_lo, w_hi, ytile, accc, carry, prev_end, ba, fa);
+            rs = rn;
+            if (rs >= w_hi) break;
+            rn = rs + step_len;
+            fa = rn < w_hi && lane_full(rn + lane * kStretchRun, w_lo, w_hi);
+            if (fa) load_lane(g32, rn + lane * kStretchRun, ba);
+            stretch_step<T>(g32, rs, w_lo, w_hi, ytile, accc, carry, prev_end, bb, fb);
+            rs = rn;
+        }
+    }
+    if (lane == 0) {
+        WarpRec<T>& rec = recs[warp];
+        rec.valid = w_lo < w_hi;
+        rec.ls = carry;  // the chain still open at the stretch's end (0 if its last run ended)
+        rec.fc = rec.cp = rec.single = 0;
+        if (w_lo < w_hi) {
+            const uint32_t ef = g32[round_phys(w_lo)], el = g32[round_phys(w_hi - 1)];
+            rec.fc = static_cast<int>(ef >> 16);
+            rec.cp = w_lo > e_lo && !(g32[round_phys(w_lo - 1)] & 1u);
+            rec.single = ((ef ^ el) >> 16) == 0 && !(el & 1u);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        WarpRec<T> r{};  // lanes past the CTA's warps carry no stretch
+        if (lane < kWarps) r = recs[lane];
+        lane_chain<T>(r.valid != 0, r.single != 0, r.cp != 0, r.fc, r.ls, T(0),
+                      [&](int col, T val) { accc[col] += val; });
+    }
+}
+
 // Accumulator columns [a0, a1) of piece pc that split `split` of `nsplit`
 // covers: its share of the piece's column sub-chunks.
 __device__ __forceinline__ void piece_share(const FastGeometry& g, const TView& tv, int pc, int split, int nsplit,
@@ -964,18 +1145,66 @@ __device__ __forceinline__ void piece_share(const FastGeometry& g, const TView& 
     a1 = min(w, ns * (split + 1) / nsplit * kSubCols);
 }
 
+// The table of one block's pieces (entry ranges of their shares, the
+// accumulator offsets, the virtual rounds), by one warp.
+__device__ __forceinline__ void fill_pieces(const FastGeometry& g, const TView& tv, const uint32_t* __restrict__ sub_start,
+                                            int pc0, int pc1, int split, int nsplit, int64_t blk, BlockPieces& bp)
+{
+    const int lane = threadIdx.x & 31;
+    const int nsub = g.nchunks * kSubPerChunk;
+    const int npc = pc1 - pc0;
+    uint32_t lo = 0, hi = 0;
+    int off = 0, nr = 0;
+    if (lane < npc) {
+        const int pc = pc0 + lane;
+        int a0, a1;
+        piece_share(g, tv, pc, split, nsplit, a0, a1);
+        if (a0 < a1) {
+            const int p = tv.piece_pat[pc];
+            const int ch0 = tv.piece_ch0[pc];
+            const int pat_sub_end = (p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks) * kSubPerChunk;
+            const int j0 = ch0 * kSubPerChunk + a0 / kSubCols;
+            const int j1 = ch0 * kSubPerChunk + (a1 + kSubCols - 1) / kSubCols;
+            lo = sub_start[blk * nsub + j0];
+            hi = j1 < pat_sub_end ? sub_start[blk * nsub + j1]
+                                  : static_cast<uint32_t>(g.seg(blk, p) + g.seg_len(blk, p));
+            off = tv.piece_acc[pc] - (ch0 - g.chunk0[p]) * kChunkCols;
+            if (lo < hi) nr = static_cast<int>((hi - 1) / kRound - lo / kRound) + 1;
+        }
+    }
+    int incl = nr;  // inclusive scan of the rounds over the pieces
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    if (lane < npc) {
+        bp.lo[lane] = lo;
+        bp.hi[lane] = hi;
+        bp.acc_off[lane] = off;
+        bp.round0[lane + 1] = incl;
+    }
+    if (lane == 0) {
+        bp.round0[0] = 0;
+        bp.n = npc;
+    }
+}
+
 // One work unit: split `split` of `nsplit` of item `item`, i.e. the partial
 // column sums of its share of super-chunk item_sc[item]'s columns (a share
 // of every piece's column sub-chunks) over the blocks [item_b0, item_b1),
 // written to those columns of partial + item_part[item] -
 // item_part[item_base].  A column's entries of a block are one run of the
 // sorted group, so splitting at sub-chunk bounds splits no run.
-template <typename T>
+// STRETCH: each (block, piece) range is reduced on its own by the stretch
+// reduction (the FP64 items); else the block's pieces share one round list.
+template <typename T, bool STRETCH>
 __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv, const uint32_t* __restrict__ g32,
                                          const uint32_t* __restrict__ sub_start, const T* __restrict__ y,
                                          T* __restrict__ partial, int item, int item_base, int64_t y_block0,
                                          int split, int nsplit, T* __restrict__ acc, T* __restrict__ ytile,
-                                         WarpRec<T>* recs, BlockPieces& bp, const int* __restrict__ pdone)
+                                         WarpRec<T> (*recs)[kFastThreads / 32], BlockPieces* bp,
+                                         const int* __restrict__ pdone)
 {
     if (pdone && pdone[g.prob_of_block(tv.item_b0[item])]) return;  // retired problem: partials unused
     const int sc = tv.item_sc[item];
@@ -990,10 +1219,14 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
         for (int i = a0 + threadIdx.x; i < a1; i += kFastThreads) ap[i] = 0;
     }
     if (!any) return;  // more splits than sub-chunks: nothing here
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int64_t blk = tv.item_b0[item]; blk < tv.item_b1[item]; blk++) {
+    const int warp = threadIdx.x >> 5;
+    const int64_t b0 = tv.item_b0[item], b1 = tv.item_b1[item];
+    if (!STRETCH && warp == 0) fill_pieces(g, tv, sub_start, pc0, pc1, split, nsplit, b0, bp[0]);
+    for (int64_t blk = b0; blk < b1; blk++) {
         const int nb = static_cast<int>(g.block_rows(blk));
+        const int i = static_cast<int>(blk - b0);
         __syncthreads();
+        if (!STRETCH && i == 0) prefetch_first_round(g32, bp[0]);
         const T* yb = y + (g.block_row0(blk) - g.block_row0(y_block0));
         if ((reinterpret_cast<uintptr_t>(yb) & 15) == 0) {
             // 16-byte loads, kInFlight per thread issued before their stores
@@ -1019,47 +1252,31 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
         if (blk + 1 < tv.item_b1[item])  // the next block's y slice into L2
             prefetch_l2(y + (g.block_row0(blk + 1) - g.block_row0(y_block0)),
                         static_cast<int64_t>(g.block_rows(blk + 1)) * static_cast<int64_t>(sizeof(T)));
-        if (warp == 0) {
-            // the block's pieces: entry ranges and their virtual rounds
-            const int npc = pc1 - pc0;
-            uint32_t lo = 0, hi = 0;
-            int off = 0, nr = 0;
-            if (lane < npc) {
-                const int pc = pc0 + lane;
+        if constexpr (STRETCH) {
+            __syncthreads();
+            int flip = 0;
+            for (int pc = pc0; pc < pc1; pc++) {
                 int a0, a1;
                 piece_share(g, tv, pc, split, nsplit, a0, a1);
-                if (a0 < a1) {
-                    const int p = tv.piece_pat[pc];
-                    const int ch0 = tv.piece_ch0[pc];
-                    const int pat_sub_end = (p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks) * kSubPerChunk;
-                    const int j0 = ch0 * kSubPerChunk + a0 / kSubCols;
-                    const int j1 = ch0 * kSubPerChunk + (a1 + kSubCols - 1) / kSubCols;
-                    lo = sub_start[blk * nsub + j0];
-                    hi = j1 < pat_sub_end ? sub_start[blk * nsub + j1]
-                                          : static_cast<uint32_t>(g.seg(blk, p) + g.seg_len(blk, p));
-                    off = tv.piece_acc[pc] - (ch0 - g.chunk0[p]) * kChunkCols;
-                    if (lo < hi) nr = static_cast<int>((hi - 1) / kRound - lo / kRound) + 1;
-                }
+                if (a0 >= a1) continue;
+                const int p = tv.piece_pat[pc];
+                const int ch0 = tv.piece_ch0[pc];
+                const int pat_sub_end = (p + 1 < g.npat ? g.chunk0[p + 1] : g.nchunks) * kSubPerChunk;
+                const int j0 = ch0 * kSubPerChunk + a0 / kSubCols;
+                const int j1 = ch0 * kSubPerChunk + (a1 + kSubCols - 1) / kSubCols;
+                const uint32_t e_lo = sub_start[blk * nsub + j0];
+                const uint32_t e_hi = j1 < pat_sub_end ? sub_start[blk * nsub + j1]
+                                                       : static_cast<uint32_t>(g.seg(blk, p) + g.seg_len(blk, p));
+                T* accc = acc + tv.piece_acc[pc] - (ch0 - g.chunk0[p]) * kChunkCols;
+                reduce_stretch<T>(g32, e_lo, e_hi, ytile, accc, recs[flip]);
+                flip ^= 1;
             }
-            int incl = nr;  // inclusive scan of the rounds over the pieces
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, incl, d);
-                if (lane >= d) incl += v;
-            }
-            if (lane < npc) {
-                bp.lo[lane] = lo;
-                bp.hi[lane] = hi;
-                bp.acc_off[lane] = off;
-                bp.round0[lane + 1] = incl;
-            }
-            if (lane == 0) {
-                bp.round0[0] = 0;
-                bp.n = npc;
-            }
+            continue;
         }
+        if (warp == 0 && blk + 1 < b1)  // the next block's table, a block ahead
+            fill_pieces(g, tv, sub_start, pc0, pc1, split, nsplit, blk + 1, bp[(i + 1) & 1]);
         __syncthreads();
-        reduce_block<T>(g32, bp, ytile, acc, recs);
+        reduce_block<T>(g32, bp[i & 1], blk + 1 < b1 ? &bp[(i + 1) & 1] : nullptr, ytile, acc, recs[0]);
     }
     __syncthreads();
     T* out = partial + (tv.item_part[item] - tv.item_part[item_base]);
@@ -1092,8 +1309,12 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
                                                                        const FastActive* __restrict__ act, int nsplit)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ WarpRec<T> recs[kFastThreads / 32];
-    __shared__ BlockPieces bp;
+    // two record sets: the stretch reduction alternates them per piece, so
+    // that warp 0 may still combine one piece's records while the other
+    // warps start on the next piece
+    __shared__ WarpRec<T> recs[2][kFastThreads / 32];
+    __shared__ BlockPieces bp[2];  // this block's piece table and the next one's
+    constexpr bool kStretch = sizeof(T) == 8;  // FP64 items hold one chunk: few rounds per block
     __shared__ int s_item;
     __shared__ int pref[kMaxProblems + 1];
     if (done && *(volatile const int*)done) return;
@@ -1101,8 +1322,8 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
     T* acc = ytile + kBlockRows;
     if (!ctr) {
         const int u = static_cast<int>(blockIdx.x);
-        aty_item<T>(g, tv, g32, sub_start, y, partial, u / nsplit + item_base, item_base, y_block0, u % nsplit,
-                    nsplit, acc, ytile, recs, bp, pdone);
+        aty_item<T, kStretch>(g, tv, g32, sub_start, y, partial, u / nsplit + item_base, item_base, y_block0,
+                              u % nsplit, nsplit, acc, ytile, recs, bp, pdone);
         return;
     }
     int K = nsplit, units = tv.nitems * nsplit;
@@ -1124,7 +1345,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) fast_spmv_t_kernel(FastGeomet
             const int slot = active_slot(pref, act->n, item);
             item = tv.sc_item0[act->list[slot] * tv.nsc] + (item - pref[slot]);
         }
-        aty_item<T>(g, tv, g32, sub_start, y, partial, item, 0, 0, u % K, K, acc, ytile, recs, bp, pdone);
+        aty_item<T, kStretch>(g, tv, g32, sub_start, y, partial, item, 0, 0, u % K, K, acc, ytile, recs, bp, pdone);
     }
     if (threadIdx.x == 0) {
         __threadfence();
@@ -1388,6 +1609,50 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
     std::vector<int> item_sc, item_b0, item_b1, sc_item0;
     std::vector<int64_t> item_part;
     int64_t part_elems = 0;
+    if (g.nprob == 1 && nsc > 1) {
+        // One fit: every super-chunk shares one partition of the blocks into
+        // ranges, and the items run range by range (within a range the
+        // heaviest super-chunks first), so that the CTAs at work at one time
+        // stage the y slices of the same few blocks: a slice comes from HBM
+        // once and from L2 for the other super-chunks.  Items of one
+        // super-chunk stay contiguous in the partial buffer, in range order,
+        // which is the order its column sums add them in.
+        const int64_t nb = g.pblk0[1] - g.pblk0[0];
+        const int64_t nr = std::max<int64_t>(1, std::min<int64_t>(nb, (target_items + nsc - 1) / nsc));
+        std::vector<int> order(nsc);
+        for (int sc = 0; sc < nsc; sc++) order[sc] = sc;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sc_entries[a] > sc_entries[b]; });
+        // partials in item order; each super-chunk's items listed for the
+        // column sums in range order
+        std::vector<std::vector<int64_t>> by_sc(nsc);
+        for (int64_t r = 0; r < nr; r++)
+            for (int sc : order) {
+                item_sc.push_back(sc);
+                item_b0.push_back(static_cast<int>(g.pblk0[0] + nb * r / nr));
+                item_b1.push_back(static_cast<int>(g.pblk0[0] + nb * (r + 1) / nr));
+                item_part.push_back(part_elems);
+                by_sc[sc].push_back(part_elems);
+                part_elems += pc.sc_width[sc];
+            }
+        std::vector<int64_t> part_by_sc;
+        part_by_sc.reserve(item_sc.size());
+        for (int sc = 0; sc < nsc; sc++) {
+            sc_item0.push_back(static_cast<int>(part_by_sc.size()));
+            part_by_sc.insert(part_by_sc.end(), by_sc[sc].begin(), by_sc[sc].end());
+        }
+        sc_item0.push_back(static_cast<int>(part_by_sc.size()));
+        t.nitems = static_cast<int>(item_sc.size());
+        mp.add(item_sc, &t.item_sc);
+        mp.add(item_b0, &t.item_b0);
+        mp.add(item_b1, &t.item_b1);
+        mp.add(item_part, &t.item_part);
+        mp.add(sc_item0, &t.sc_item0);
+        mp.add(part_by_sc, &t.sc_part);
+        mp.add(std::vector<int>{0, 0}, &t.ctr);
+        CAS_TRY(mp.upload(&t.meta));
+        CAS_CUDA(dmalloc(&t.partial, elem * std::max<int64_t>(part_elems, 1)));
+        return CAS_OK;
+    }
     for (int q = 0; q < g.nprob; q++) {
         const int64_t qb0 = g.pblk0[q], qnb = g.pblk0[q + 1] - g.pblk0[q];
         for (int sc = 0; sc < nsc; sc++) {
@@ -1419,6 +1684,7 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
     mp.add(item_b1, &t.item_b1);
     mp.add(item_part, &t.item_part);
     mp.add(sc_item0, &t.sc_item0);
+    mp.add(item_part, &t.sc_part);  // items are listed super-chunk by super-chunk already
     mp.add(std::vector<int>{0, 0}, &t.ctr);
     CAS_TRY(mp.upload(&t.meta));
     CAS_CUDA(dmalloc(&t.partial, elem * std::max<int64_t>(part_elems, 1)));
@@ -1746,7 +2012,8 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
             dp.instances, dp.k, dp.tables, reinterpret_cast<const ulonglong2*>(d_pos), g, f.a16); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
         const int64_t groups = g.nblocks * g.npat;
-        const unsigned sgrid = static_cast<unsigned>(std::min<int64_t>(groups, static_cast<int64_t>(sm_count())));
+        const unsigned sgrid =
+            static_cast<unsigned>(std::min<int64_t>(groups, static_cast<int64_t>(sm_count()) * kSortCtasPerSm));
         uint32_t* scratch = nullptr;
         CAS_CUDA(dmalloc(&scratch, sizeof(uint32_t) * kBlockRows * 8 * sgrid));
         { fast_sort_kernel<<<sgrid, kSortThreads, 0, s>>>(g, f.a16, f.g32, scratch); cas::count_launch(); }
@@ -1867,7 +2134,7 @@ FastCols fast_cols(const FastLayout& f)
     c.chunk_sc = t.chunk_sc;
     c.chunk_acc = t.chunk_acc;
     c.sc_item0 = t.sc_item0;
-    c.item_part = t.item_part;
+    c.sc_part = t.sc_part;
     return c;
 }
 

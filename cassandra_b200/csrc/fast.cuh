@@ -184,7 +184,9 @@ struct FastTranspose {
     int* item_b0 = nullptr;    // [nitems]
     int* item_b1 = nullptr;    // [nitems]
     int64_t* item_part = nullptr;  // [nitems] offset of the item's partials
-    int* sc_item0 = nullptr;       // [nprob * nsc + 1] first item of each (problem, super-chunk)
+    int* sc_item0 = nullptr;       // [nprob * nsc + 1] first entry of each (problem, super-chunk) in sc_part
+    int64_t* sc_part = nullptr;    // [nitems] partial offsets of the items, listed super-chunk by super-chunk
+                                   // (block ranges in order): the order the column sums add them in
     void* partial = nullptr;       // float or double partials
     int* ctr = nullptr;            // [2] work counter and finished CTAs of the persistent schedule (reset by the kernel)
     void* meta = nullptr;          // one device block holding every array above except partial
@@ -233,7 +235,7 @@ struct FastCols {
     const int* chunk_sc;
     const int* chunk_acc;
     const int* sc_item0;
-    const int64_t* item_part;
+    const int64_t* sc_part;
 };
 
 // Builds the blocked layout from positions (indexes them itself).  Returns
@@ -295,7 +297,7 @@ __device__ __forceinline__ double fast_col_sum(const FastCols& fc, const T* part
     const int sc = static_cast<int>(q) * fc.nsc + fc.chunk_sc[ch];
     const int pos = fc.chunk_acc[ch] + local % kChunkCols;
     double acc = 0;
-    for (int it = fc.sc_item0[sc]; it < fc.sc_item0[sc + 1]; it++) acc += static_cast<double>(partial[fc.item_part[it] + pos]);
+    for (int it = fc.sc_item0[sc]; it < fc.sc_item0[sc + 1]; it++) acc += static_cast<double>(partial[fc.sc_part[it] + pos]);
     return acc;
 }
 

@@ -14,10 +14,12 @@ the device: an iteration reads nothing back to the host, and the residual is
 read once per chunk of `check_every` iterations.
 
 With FP32 products (a GpuShard of precision "mixed") the recursive residual
-drifts from the true one, so at every chunk boundary the true residual
-A'(b - A x) is computed in FP64 (one more all-reduce of a cols-length
-vector) and replaces the recursive one; a replacement that finds the
-recursive residual more than 10 % off restarts the direction, and
+drifts from the true one, so it is replaced by the true residual
+A'(b - A x), computed in FP64 (one more all-reduce of a cols-length
+vector), once it has dropped by REPLACE_DROP since the last replacement,
+after refine_every iterations, or when it meets the tolerance (checked at
+chunk boundaries, every check_every iterations); a replacement that finds
+the recursive residual more than 10 % off restarts the direction, and
 convergence is declared on the true residual only -- the single-GPU mixed
 solver's reliable updating, at chunk granularity.
 
@@ -103,6 +105,9 @@ class ShardedResult:
 
 # a replacement that finds the recursive residual this far off restarts the direction
 RESTART_DEVIATION = 0.1
+# FP32 products: the recursive residual is replaced once it has dropped this
+# much since the last replacement (before FP32 drift relative to it grows)
+REPLACE_DROP = 1e-3
 
 
 def _allreduce(t: torch.Tensor, group) -> torch.Tensor:
@@ -111,7 +116,7 @@ def _allreduce(t: torch.Tensor, group) -> torch.Tensor:
 
 
 def sharded_pcg(shard: Shard, tol: float = 1e-8, max_iterations: int = 20000, jacobi: bool = True,
-                group=None, check_every: int = 50) -> ShardedResult:
+                group=None, check_every: int = 10, refine_every: int = 50) -> ShardedResult:
     """Jacobi-PCG on sum_k A_k'A_k x = sum_k A_k'b_k from x0 = 0.  Every rank
     calls it with its shard; all ranks return the same x.  tol <= 0 runs
     exactly max_iterations iterations with no checks (one all-reduce per
@@ -145,6 +150,7 @@ def sharded_pcg(shard: Shard, tol: float = 1e-8, max_iterations: int = 20000, ja
     rel = rel_of(r)
     if tol > 0 and rel <= tol:
         return ShardedResult(x=x, iterations=0, rel_residual=rel, allreduces=n_ar)
+    rel_ref, it_ref = rel, 0  # the residual and iteration of the last replacement
     while it < max_iterations:
         for _ in range(min(chunk, max_iterations - it)):
             s_loc, qq = shard.normal_product(p)
@@ -165,9 +171,11 @@ def sharded_pcg(shard: Shard, tol: float = 1e-8, max_iterations: int = 20000, ja
         if tol <= 0:
             break
         rel = rel_of(r)
-        if shard.mixed or rel <= tol:
-            # the FP64 true residual decides; with FP32 products it also
-            # replaces the recursive one
+        due = rel <= tol
+        if shard.mixed:
+            due = due or rel <= REPLACE_DROP * rel_ref or it - it_ref >= refine_every
+        if due:
+            # the FP64 true residual decides; it replaces the recursive one
             rt = _allreduce(shard.residual_product(x).to(torch.float64).clone(), group)
             n_ar += 1
             rel_true = rel_of(rt)
@@ -181,7 +189,8 @@ def sharded_pcg(shard: Shard, tol: float = 1e-8, max_iterations: int = 20000, ja
             replacements += 1
             if dev > RESTART_DEVIATION * float(torch.linalg.vector_norm(rt)):
                 p.copy_(z)
-            rel = rel_true
+            rel = rel_ref = rel_true
+            it_ref = it
     if tol <= 0:
         rel = rel_of(r)
     return ShardedResult(x=x, iterations=it, rel_residual=rel, allreduces=n_ar, replacements=replacements)

@@ -6,7 +6,10 @@ pieces' entry ranges cut into virtual rounds that 32 warps split into
 stretches, 32 entries per lane and round with the entries outside a piece's
 range masked, every run end adding the lane's part of its run to the
 accumulator, the segmented scan over lanes whose runs continue from their
-left, and the warp records combined after the block.
+left, and the warp records combined after the block.  The FP64 items use
+the stretch reduction instead (reduce_stretch, stretch_step): each piece's
+range cut into 32 stretches of whole 4-entry words, 8 entries per lane and
+step, read through round_phys; it is modelled the same way.
 
 On random blocks (several pieces in different groups, runs of one entry up
 to runs spanning many warps, piece ranges starting and ending anywhere in a
@@ -266,3 +269,93 @@ def test_model_few_rounds_and_empty_pieces():
     want = _expect(logical, pieces, y)
     for col, val in want.items():
         assert acc.v.get(col, 0) == val
+
+
+STEP = 8  # kStretchRun
+
+
+def reduce_stretch(g32, y, e_lo, e_hi, acc, off, col_lo, col_hi):
+    """reduce_stretch / stretch_step over sorted positions [e_lo, e_hi) of a
+    group stored in round order."""
+    n = e_hi - e_lo
+
+    def cut(w):
+        if w == 0:
+            return e_lo
+        if w == WARPS:
+            return e_hi
+        return max(e_lo, (e_lo + n * w // WARPS) & ~3)
+
+    def at(e):
+        return g32[round_phys(e)]
+
+    recs = []
+    for warp in range(WARPS):
+        w_lo, w_hi = cut(warp), cut(warp + 1)
+        carry, prev_end = 0, True
+        rs, rnd = w_lo & ~3, 0
+        while w_lo < w_hi and rs < w_hi:
+            step = ("step", warp, rnd)
+            sums, any_, first, last, ends = [0] * LANES, [False] * LANES, [1] * LANES, [1] * LANES, [0] * LANES
+            for lane in range(LANES):
+                ef = rs + lane * STEP
+                full = ef >= w_lo and ef + STEP <= w_hi
+                if full:  # two 16-byte words: round_phys of ef and ef + 4, 4 entries each
+                    words = [g32[round_phys(ef + 4 * q) + j] for q in range(2) for j in range(4)]
+                    assert words == [at(e) for e in range(ef, ef + STEP)]
+                lo, hi = max(ef, w_lo), min(ef + STEP, w_hi)
+                s = 0
+                for e in range(lo, hi):
+                    v = at(e)
+                    s += int(y[(v & 0xFFFC) >> 2])
+                    ends[lane] |= v
+                    if v & 1:
+                        acc.add(off + (v >> 16), s, step + ("end", e - ef), lane, col_lo, col_hi)
+                        s = 0
+                if lo < hi:
+                    any_[lane], first[lane], last[lane] = True, at(lo), at(hi - 1)
+                sums[lane] = s
+            single = [any_[i] and not (ends[i] & 1) for i in range(LANES)]
+            hc = [first[i] >> 16 for i in range(LANES)]
+            cont_prev = []
+            for i in range(LANES):
+                fv = max(rs + i * STEP, w_lo)
+                prev_open = (not prev_end) if i == 0 else not (last[i - 1] & 1)
+                cont_prev.append(any_[i] and fv > w_lo and prev_open)
+            sink = lambda i, col, val: acc.add(off + col, val, step + ("sink",), i, col_lo, col_hi)  # noqa: E731
+            if not any(single[i] and cont_prev[i] for i in range(LANES)):
+                for i in range(LANES):
+                    prev_ts = carry if i == 0 else sums[i - 1]
+                    if any_[i] and not single[i] and cont_prev[i]:
+                        sink(i, hc[i], prev_ts)
+                carry = sums[min(31, (w_hi - 1 - rs) // STEP)]
+            else:
+                carry = lane_chain(any_, single, cont_prev, hc, sums, carry, sink)
+            prev_end = (last[31] & 1) != 0
+            rs += LANES * STEP
+            rnd += 1
+        if w_lo < w_hi:
+            ef, el = at(w_lo), at(w_hi - 1)
+            recs.append((True, w_lo > e_lo and not (at(w_lo - 1) & 1), ((ef ^ el) >> 16) == 0 and not (el & 1),
+                         ef >> 16, carry))
+        else:
+            recs.append((False, False, False, 0, carry))
+    lane_chain([r[0] for r in recs], [r[2] for r in recs], [r[1] for r in recs], [r[3] for r in recs],
+               [r[4] for r in recs], 0,
+               lambda i, col, val: acc.add(off + col, val, ("records",), i, col_lo, col_hi))
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_stretch_model_sums_columns(mode):
+    rng = np.random.default_rng(200 + mode)
+    y = rng.integers(-5, 6, 16384)
+    for trial in range(6):
+        g32, logical, pieces, width = _block(rng, mode, 1 + trial % 3)
+        acc = Acc(width)
+        for lo, hi, off, seg, seg_end, col_lo, col_hi in pieces:
+            if lo < hi:
+                reduce_stretch(g32, y, lo, hi, acc, off, col_lo, col_hi)
+        want = _expect(logical, pieces, y)
+        assert set(acc.v) <= set(want)
+        for col, val in want.items():
+            assert acc.v.get(col, 0) == val, (mode, trial, col)

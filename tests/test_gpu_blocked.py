@@ -167,3 +167,21 @@ def test_mixed_solution_matches_plain(cuda):
     pm = (plain @ m.x()).cpu().numpy()
     pp = (plain @ p.x()).cpu().numpy()
     np.testing.assert_allclose(pm, pp, rtol=0, atol=1e-5 * np.abs(pp).max())
+
+
+def test_products_on_a_layout_of_one_unit_per_block(cuda):
+    """A layout of more blocks than SMs runs A x with one unit per 16384-row
+    block (16 rows per thread) and A'y on its range-major work list: both
+    products against the same products on the rows layout, FP32 and FP64,
+    over every row and column."""
+    rows = 160 * 16384 + 4321
+    pos = cb.generate_positions(91, rows, 20, 40)
+    g = cb.GroupIndexer(SET8, "expanded")
+    fast = cb.MatrixCSR.from_positions(g, pos, "blocked")
+    plain = cb.MatrixCSR.from_positions(g, pos, "rows")
+    gen = torch.Generator("cuda").manual_seed(3)
+    x = torch.randint(-40, 40, (g.index_space_size,), device="cuda", generator=gen).double()
+    y = torch.randint(-40, 40, (rows,), device="cuda", generator=gen).double()
+    for dt in (torch.float32, torch.float64):
+        assert torch.equal((fast @ x.to(dt)).double(), (plain @ x).double())  # integer values: exact
+        assert torch.equal((y.to(dt) @ fast).double(), (y @ plain).double())
