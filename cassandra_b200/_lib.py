@@ -80,7 +80,7 @@ class AdamOpts(C.Structure):
 class Schedule(C.Structure):
     _fields_ = [
         ("chunks_per_item", C.c_int),
-        ("ring", C.c_int),
+        ("range_major", C.c_int),
         ("items_per_sm", C.c_int),
         ("pack", C.c_int),
         ("persistent", C.c_int),

@@ -651,20 +651,20 @@ CAS_API int cas_csr_schedules(const cas_csr* a, cas_schedule* out, int max, cas_
     const FastLayout& f = *a->fast;
     if (in_use) {
         in_use->chunks_per_item = f.t32.per_sc;
-        in_use->ring = f.t32.ring ? 1 : 0;
+        in_use->range_major = f.t32.range_major ? 1 : 0;
         in_use->items_per_sm = f.t32.items_per_sm;
         in_use->pack = f.t32.pack ? 1 : 0;
         in_use->persistent = f.t32.persistent ? 1 : 0;
         in_use->ms = 0;
         for (int i = 0; i < f.ntune; i++)
-            if (f.tune[i].per_sc == f.t32.per_sc && f.tune[i].ring == in_use->ring &&
+            if (f.tune[i].per_sc == f.t32.per_sc && f.tune[i].range_major == in_use->range_major &&
                 f.tune[i].items_per_sm == f.t32.items_per_sm && f.tune[i].pack == in_use->pack &&
                 f.tune[i].persistent == in_use->persistent)
                 in_use->ms = f.tune[i].ms;
     }
     int n = 0;
     for (int i = 0; i < f.ntune && out && n < max; i++, n++)
-        out[n] = cas_schedule{f.tune[i].per_sc, f.tune[i].ring, f.tune[i].items_per_sm, f.tune[i].pack,
+        out[n] = cas_schedule{f.tune[i].per_sc, f.tune[i].range_major, f.tune[i].items_per_sm, f.tune[i].pack,
                               f.tune[i].persistent, f.tune[i].ms};
     return n;
 }

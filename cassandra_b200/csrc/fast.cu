@@ -1584,10 +1584,10 @@ void pack_pieces(const Pieces& pc, FastTranspose& t, MetaPack& mp)
 // chunk): super-chunks of at most per_sc chunks of columns, each split into
 // block ranges so that items carry about equal numbers of entries.
 cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entries_bc, int per_sc, int items_per_sm,
-                       bool ring, bool pack, bool persistent, size_t elem, FastTranspose& t)
+                       bool range_major, bool pack, bool persistent, size_t elem, FastTranspose& t)
 {
     t.per_sc = per_sc;
-    t.ring = ring;
+    t.range_major = range_major;
     t.items_per_sm = items_per_sm;
     t.pack = pack;
     t.persistent = persistent;
@@ -1609,7 +1609,7 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
     std::vector<int> item_sc, item_b0, item_b1, sc_item0;
     std::vector<int64_t> item_part;
     int64_t part_elems = 0;
-    if (g.nprob == 1 && nsc > 1) {
+    if (range_major && g.nprob == 1 && nsc > 1) {
         // One fit: every super-chunk shares one partition of the blocks into
         // ranges, and the items run range by range (within a range the
         // heaviest super-chunks first), so that the CTAs at work at one time
@@ -1821,23 +1821,21 @@ cas_status fast_set_attributes_now()
 // is built and timed (partials + column sums, CUDA events, one warm-up
 // launch) on this layout; the fastest is kept and remembered per geometry
 // for the rest of the process, so later builds of the same shape skip the
-// timing.  CAS_ATY_SCHEDULE="chunks,0,items_per_sm,pack,persistent"
-// forces a schedule (the second field, entries streamed through a shared-
-// memory ring, is kept for the format of the schedule table and must be 0).
+// timing.  CAS_ATY_SCHEDULE="chunks,range_major,items_per_sm,pack,persistent"
+// forces a schedule.
 // ---------------------------------------------------------------------------
 struct Sched {
     int per_sc;
-    bool ring;
+    bool range_major;
     int ips;
     bool pack;
     bool persistent;
 };
 constexpr Sched kSchedDefault = {4, false, 2, false, false};
 constexpr Sched kSchedCandidates[] = {
-    {4, false, 2, false, false}, {4, false, 3, false, false}, {3, false, 2, false, false},
-    {4, false, 2, true, false},  {4, false, 2, true, true},   {4, false, 4, true, true},
-    {4, false, 4, false, true},  {2, false, 2, true, false},  {2, false, 3, true, false},
-    {2, false, 4, true, true},   {4, false, 1, false, false}, {4, false, 6, false, true}};
+    {4, false, 2, false, false}, {4, false, 3, false, false}, {4, false, 2, true, true}, {4, false, 4, true, true},
+    {4, false, 4, false, true},  {2, false, 4, true, true},   {4, false, 6, false, true}, {4, true, 2, false, false},
+    {4, true, 4, false, true},   {4, true, 6, false, true},   {4, true, 4, true, true},   {2, true, 4, true, true}};
 static_assert(sizeof(kSchedCandidates) / sizeof(Sched) <= kMaxTune, "tune table");
 constexpr int64_t kTuneMinBlocks = 64;  // smaller layouts take the default schedule
 
@@ -1854,7 +1852,7 @@ std::string tune_key(const FastGeometry& g)
 
 bool valid_sched(const Sched& c)
 {
-    return c.per_sc >= 1 && c.per_sc <= kMaxSc && !c.ring && c.ips >= 1 && c.ips <= 16;
+    return c.per_sc >= 1 && c.per_sc <= kMaxSc && c.ips >= 1 && c.ips <= 16;
 }
 
 cas_status tune_transpose(FastLayout& f, const std::vector<int64_t>& entries, cudaStream_t s)
@@ -1863,14 +1861,14 @@ cas_status tune_transpose(FastLayout& f, const std::vector<int64_t>& entries, cu
     f.ntune = 0;
     f.tune_cached = 0;
     auto build = [&](const Sched& c) {
-        return build_items(g, entries, c.per_sc, c.ips, c.ring, c.pack, c.persistent, sizeof(float), f.t32);
+        return build_items(g, entries, c.per_sc, c.ips, c.range_major, c.pack, c.persistent, sizeof(float), f.t32);
     };
     if (const char* env = std::getenv("CAS_ATY_SCHEDULE")) {
         int a = 0, b = 0, c = 0, d = 0, e = 0;
         const int n = std::sscanf(env, "%d,%d,%d,%d,%d", &a, &b, &c, &d, &e);
         const Sched forced{a, b != 0, c, d != 0, e != 0};
         CAS_REQUIRE(n == 5 && valid_sched(forced), CAS_ERR_INVALID_ARGUMENT,
-                    "CAS_ATY_SCHEDULE must be \"chunks,0,items_per_sm,pack,persistent\" within limits");
+                    "CAS_ATY_SCHEDULE must be \"chunks,range_major,items_per_sm,pack,persistent\" within limits");
         return build(forced);
     }
     if (g.nblocks < kTuneMinBlocks) return build(kSchedDefault);
@@ -1913,7 +1911,8 @@ cas_status tune_transpose(FastLayout& f, const std::vector<int64_t>& entries, cu
         free_transpose(f.t32);
         if (st != CAS_OK) break;
         ms *= 0.5f;
-        f.tune[f.ntune++] = FastTuneEntry{c.per_sc, c.ring ? 1 : 0, c.ips, c.pack ? 1 : 0, c.persistent ? 1 : 0, ms};
+        f.tune[f.ntune++] =
+            FastTuneEntry{c.per_sc, c.range_major ? 1 : 0, c.ips, c.pack ? 1 : 0, c.persistent ? 1 : 0, ms};
         if (ms < best_ms) {
             best_ms = ms;
             best = c;
@@ -2042,7 +2041,9 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
     }
     if (g.nblocks > 0) {
         CAS_TRY(tune_transpose(f, entries, s));
-        CAS_TRY(build_items(g, entries, 1, 2, false, true, false, sizeof(double), f.t64));
+        // FP64 items hold one chunk, so the y slices would be read once per
+        // chunk: always range by range
+        CAS_TRY(build_items(g, entries, 1, 2, true, true, false, sizeof(double), f.t64));
         if (g.nprob == 1) CAS_TRY(build_block_items(g, f.tb));  // evaluator minibatches: single fits only
     }
     return CAS_OK;

@@ -165,7 +165,7 @@ struct FastActive {
 // of its super-chunk's items in item order.
 struct FastTranspose {
     int per_sc = 1;        // accumulator capacity in chunks
-    bool ring = false;     // FP32 only: entries streamed through a cp.async ring in shared memory
+    bool range_major = false;  // single fits: items run block range by block range (y slices shared in L2)
     int items_per_sm = 2;  // work items per SM the entries are balanced over
     bool pack = true;      // super-chunks may hold pieces of several patterns
     bool persistent = false;  // one CTA per SM taking items from a counter (else one CTA per item)
@@ -195,7 +195,7 @@ struct FastTranspose {
 // One measured A'y schedule of the build-time autotuner.
 struct FastTuneEntry {
     int per_sc;
-    int ring;
+    int range_major;
     int items_per_sm;
     int pack;
     int persistent;

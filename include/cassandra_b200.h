@@ -157,8 +157,9 @@ CAS_API cas_status cas_csr_transposed(const cas_csr* a, const int64_t** d_col_pt
 
 /* No counterpart in the reference: the schedules of the FP32 transposed
  * product on the BLOCKED layout that the build-time autotuner timed for this
- * matrix (accumulator width in 8192-column chunks per work item, entries
- * streamed through a shared-memory cp.async ring or in registers, work items
+ * matrix (accumulator width in 8192-column chunks per work item, work items
+ * run block range by block range so that concurrent items share y slices
+ * through L2 or balanced by entries super-chunk by super-chunk, work items
  * per SM, accumulators shared by several patterns, persistent CTAs taking
  * items from a counter; mean milliseconds per product), and the schedule in
  * use.  Returns
@@ -168,7 +169,7 @@ CAS_API cas_status cas_csr_transposed(const cas_csr* a, const int64_t** d_col_pt
  * under 64 blocks; -1 without a blocked layout. */
 typedef struct cas_schedule {
     int chunks_per_item;
-    int ring;
+    int range_major; /* items run block range by block range (super-chunks share y slices through L2) */
     int items_per_sm;
     int pack;
     int persistent;

@@ -49,15 +49,8 @@ def test_blocked_products_match_oracle(cuda, orc, rows, masks, mode):
         np.testing.assert_array_equal(cb.jacobi_preconditioner_of_ata(a).cpu().numpy(), orc.jacobi(idx, cols))
 
 
-SCHEDULES = ["4,0,2,0,0", "4,0,1,1,0", "3,0,2,1,1", "2,0,2,0,1", "2,0,2,1,0", "1,0,2,0,0", "2,0,3,1,1",
-             "1,0,5,1,1"]
-
-
-def test_aty_schedule_rejects_the_retired_ring_form(cuda, monkeypatch):
-    """The schedule format keeps its second field; only 0 is accepted."""
-    monkeypatch.setenv("CAS_ATY_SCHEDULE", "2,1,2,1,0")
-    with pytest.raises(cb.CasError):
-        _build(3 * 16384, SET8, "expanded", "blocked", seed=31)
+SCHEDULES = ["4,0,2,0,0", "4,0,1,1,0", "3,0,2,1,1", "2,0,2,0,1", "2,1,2,1,0", "1,1,2,0,0", "2,1,3,1,1",
+             "4,1,6,0,1", "1,0,5,1,1"]
 
 
 @pytest.mark.parametrize("sched", SCHEDULES)
@@ -70,7 +63,7 @@ def test_aty_schedules_match_oracle(cuda, orc, monkeypatch, sched):
     a, pos, g = _build(rows, SET8, "expanded", "blocked", seed=31)
     want = tuple(int(v) for v in sched.split(","))
     cur = a.schedules()["in_use"]
-    assert (cur["chunks_per_item"], cur["ring"], cur["items_per_sm"], cur["pack"], cur["persistent"]) == want
+    assert (cur["chunks_per_item"], cur["range_major"], cur["items_per_sm"], cur["pack"], cur["persistent"]) == want
     idx = orc.group_index(SET8, 1, pos.cpu().numpy().view(np.uint64))
     yi = np.random.default_rng(5).integers(-50, 50, rows).astype(np.float32)
     np.testing.assert_array_equal((torch.from_numpy(yi).cuda() @ a).cpu().numpy(),
@@ -88,7 +81,7 @@ def test_autotuner_times_candidates_and_caches(cuda, monkeypatch):
     assert len(timed) == 12 and all(t["ms"] > 0 for t in timed)
     best = min(timed, key=lambda t: t["ms"])
     cur = sch["in_use"]
-    keys = ("chunks_per_item", "ring", "items_per_sm", "pack", "persistent")
+    keys = ("chunks_per_item", "range_major", "items_per_sm", "pack", "persistent")
     assert tuple(cur[k] for k in keys) == tuple(best[k] for k in keys)
     b = cb.MatrixCSR.from_positions(g, pos, "blocked")  # same shape: cached, not re-timed
     sb = b.schedules()
