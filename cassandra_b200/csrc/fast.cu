@@ -90,20 +90,41 @@ __global__ void __launch_bounds__(256) fast_index_kernel(const Instance* __restr
 
 // ---------------------------------------------------------------------------
 // Per-(block, pattern) stable sort of entries by local column: two 8-bit LSD
-// passes inside one CTA, through a per-CTA scratch slice (L2 resident).
-// Items are (column << 16) | (row-in-block << 2) | end, end (bit 0) set on
-// the last entry of each column; the input order is row-major (row, slot),
-// so equal columns keep ascending rows.
+// passes inside one CTA, the first into a per-CTA scratch slice.  Items are
+// (column << 16) | (row-in-block << 2) | end, end (bit 0) set on the last
+// entry of each column; the input order is row-major (row, slot), so equal
+// columns keep ascending rows.
+//
+// A pass moves its items in tiles of kSortTile: each warp ranks its 512
+// items by digit (match_any, in item order, counts per digit in shared
+// memory), one scan per tile turns the warps' counts into offsets, the tile
+// is scattered digit by digit into a shared buffer and written out from
+// there, so that consecutive threads write the consecutive output positions
+// of a digit's run.  The final pass writes G32's round order and the end
+// flags: an entry ends its run when the next entry of its digit in the tile
+// has another column; the last entry of a digit in a tile waits (position
+// and column kept per digit) for the digit's first entry in a later tile,
+// or for the pass's end (the next entry then has another digit).
 // ---------------------------------------------------------------------------
+constexpr int kSortPerThread = 16;                           // items per thread and tile
+constexpr int kSortTile = kSortThreads * kSortPerThread;     // items per tile
+constexpr int kSortWarpItems = 32 * kSortPerThread;          // items a warp ranks per tile
+constexpr uint32_t kNoPend = 0xFFFFFFFFu;
+
 struct SortSmem {
-    uint32_t hist[256];
-    uint32_t base[256];
-    uint32_t running[256];
-    uint32_t total[256];
-    uint32_t wcount[kSortWarps][256];
+    uint32_t hist[256];     // digit counts of the first pass (counted from the input)
+    uint32_t hist2[256];    // digit counts of the final pass (counted by the first pass's write-out)
+    uint32_t base[256];     // first output position of each digit
+    uint32_t running[256];  // entries of each digit written by earlier tiles
+    uint32_t tcount[256];   // the tile's entries of each digit
+    uint32_t tbase[256];    // the digit's first slot in the tile buffer
+    uint32_t pend_pos[256]; // final pass: the digit's last entry so far (kNoPend: none)
+    uint32_t pend_col[256]; //   and its column
+    uint32_t wcnt[kSortWarps][256];
+    uint32_t buf[kSortTile];
 };
 
-__device__ void block_exclusive_scan_256(uint32_t* hist, uint32_t* out)
+__device__ void block_exclusive_scan_256(const uint32_t* hist, uint32_t* out)
 {
     // 256 values scanned by the first 8 warps; others idle.
     __shared__ uint32_t warp_tot[8];
@@ -129,59 +150,110 @@ __device__ void block_exclusive_scan_256(uint32_t* hist, uint32_t* out)
     __syncthreads();
 }
 
-// One stable 8-bit counting-sort pass of a group's n items.  FROM_A16: the
-// items are made from the A16 segment (local column << 16 | row << 2).
-// ROUNDS: the output is written in G32's round order (round_phys of the
-// sorted position; out starts on a round boundary).
-template <bool FROM_A16, bool ROUNDS>
+// One stable 8-bit counting-sort pass of a group's n items by the digit at
+// `shift`.  FROM_A16: the first pass, items made from the A16 segment
+// (local column << 16 | row << 2), written to out in sorted order while the
+// final pass's digit counts are gathered.  !FROM_A16: the final pass, items
+// read from `in`, written in G32's round order (round_phys of the sorted
+// position; out starts on a round boundary) with their end flags.
+template <bool FROM_A16>
 __device__ void sort_pass(const uint16_t* __restrict__ a16_in, const uint32_t* __restrict__ in, int n, int slots,
                           int shift, uint32_t* __restrict__ out, SortSmem& sm)
 {
+    constexpr bool FINAL = !FROM_A16;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const unsigned lt_mask = (1u << lane) - 1;
     auto item_at = [&](int e) -> uint32_t {
         if (FROM_A16) return (static_cast<uint32_t>(a16_in[e]) << 16) | (static_cast<uint32_t>(e / slots) << 2);
         return in[e];
     };
-    if (t < 256) sm.hist[t] = 0;
-    for (int w = 0; w < kSortWarps; w++)
-        if (t < 256) sm.wcount[w][t] = 0;
-    __syncthreads();
-    for (int e = t; e < n; e += kSortThreads) atomicAdd(&sm.hist[(item_at(e) >> shift) & 255u], 1u);
-    __syncthreads();
-    block_exclusive_scan_256(sm.hist, sm.base);
-    if (t < 256) sm.running[t] = 0;
-    __syncthreads();
-    for (int r0 = 0; r0 < n; r0 += kSortThreads) {
-        const int e = r0 + t;
-        const bool valid = e < n;
-        const uint32_t item = valid ? item_at(e) : 0u;
-        const uint32_t d = valid ? (item >> shift) & 255u : 0xFFFFu;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        const int rank = __popc(peers & lt_mask);
-        if (valid && rank == 0) sm.wcount[warp][d] = __popc(peers);
+    if (FROM_A16) {
+        if (t < 256) sm.hist[t] = 0;
         __syncthreads();
+        for (int e = t; e < n; e += kSortThreads) atomicAdd(&sm.hist[(item_at(e) >> shift) & 255u], 1u);
+        __syncthreads();
+    }
+    block_exclusive_scan_256(FROM_A16 ? sm.hist : sm.hist2, sm.base);
+    if (t < 256) {
+        sm.running[t] = 0;
+        if (FROM_A16) sm.hist2[t] = 0;
+        sm.pend_pos[t] = kNoPend;
+    }
+    for (int t0 = 0; t0 < n; t0 += kSortTile) {
+        // 1. rank: the warp's items t0 + warp * 512 + 32 k + lane, in item order
+        for (int i = lane; i < 256; i += 32) sm.wcnt[warp][i] = 0;
+        __syncwarp();
+        uint32_t item[kSortPerThread];
+        uint32_t rk[kSortPerThread];  // rank among the warp's items of the same digit
+#pragma unroll
+        for (int k = 0; k < kSortPerThread; k++) {
+            const int e = t0 + warp * kSortWarpItems + k * 32 + lane;
+            const bool valid = e < n;
+            item[k] = valid ? item_at(e) : 0u;
+            const uint32_t d = valid ? (item[k] >> shift) & 255u : 0xFFFFu;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const int leader = __ffs(peers) - 1;
+            uint32_t before = 0;
+            if (valid && lane == leader) {
+                before = sm.wcnt[warp][d];
+                sm.wcnt[warp][d] = before + __popc(peers);
+            }
+            before = __shfl_sync(0xffffffffu, before, leader);
+            rk[k] = before + __popc(peers & lt_mask);
+            __syncwarp();
+        }
+        __syncthreads();
+        // 2. per digit: each warp's offset inside the tile's run of the digit
         if (t < 256) {
             uint32_t acc = 0;
             for (int w = 0; w < kSortWarps; w++) {
-                const uint32_t c = sm.wcount[w][t];
-                sm.wcount[w][t] = acc;
+                const uint32_t c = sm.wcnt[w][t];
+                sm.wcnt[w][t] = acc;
                 acc += c;
             }
-            sm.total[t] = acc;
+            sm.tcount[t] = acc;
         }
         __syncthreads();
-        if (valid) {
-            const uint32_t pos = sm.base[d] + sm.running[d] + sm.wcount[warp][d] + rank;
-            out[ROUNDS ? round_phys(pos) : pos] = item;
+        block_exclusive_scan_256(sm.tcount, sm.tbase);
+        // 3. the tile into the buffer, digit by digit
+#pragma unroll
+        for (int k = 0; k < kSortPerThread; k++) {
+            const int e = t0 + warp * kSortWarpItems + k * 32 + lane;
+            if (e < n) {
+                const uint32_t d = (item[k] >> shift) & 255u;
+                sm.buf[sm.tbase[d] + sm.wcnt[warp][d] + rk[k]] = item[k];
+            }
         }
         __syncthreads();
-        if (t < 256) {
-            sm.running[t] += sm.total[t];
-            for (int w = 0; w < kSortWarps; w++) sm.wcount[w][t] = 0;
+        // 4. out: consecutive buffer slots of a digit are consecutive positions
+        const int tn = min(kSortTile, n - t0);
+        for (int j = t; j < tn; j += kSortThreads) {
+            uint32_t it = sm.buf[j];
+            const uint32_t d = (it >> shift) & 255u;
+            const uint32_t pos = sm.base[d] + sm.running[d] + static_cast<uint32_t>(j) - sm.tbase[d];
+            if (FINAL) {
+                const bool last_in_tile = static_cast<uint32_t>(j) + 1 == sm.tbase[d] + sm.tcount[d];
+                if (!last_in_tile && (sm.buf[j + 1] >> 16) != (it >> 16)) it |= 1u;
+                out[round_phys(pos)] = it;
+            } else {
+                out[pos] = it;
+                atomicAdd(&sm.hist2[it >> 24], 1u);
+            }
+        }
+        if (FINAL && t < 256 && sm.tcount[t] > 0) {
+            // the digit's entry waiting from an earlier tile ends its run
+            // unless this tile's first entry of the digit continues its column
+            const uint32_t first = sm.buf[sm.tbase[t]];
+            if (sm.pend_pos[t] != kNoPend && (first >> 16) != sm.pend_col[t]) out[round_phys(sm.pend_pos[t])] |= 1u;
+            sm.pend_pos[t] = sm.base[t] + sm.running[t] + sm.tcount[t] - 1;
+            sm.pend_col[t] = sm.buf[sm.tbase[t] + sm.tcount[t] - 1] >> 16;
         }
         __syncthreads();
+        if (t < 256) sm.running[t] += sm.tcount[t];
     }
+    // the last entry of every digit ends its run (the next has another digit)
+    if (FINAL && t < 256 && sm.pend_pos[t] != kNoPend) out[round_phys(sm.pend_pos[t])] |= 1u;
+    __syncthreads();
 }
 
 __global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm) fast_sort_kernel(FastGeometry g,
@@ -197,20 +269,8 @@ __global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm) fast_sort_kernel
         const int p = static_cast<int>(grp - b * g.npat);
         const int n = static_cast<int>(g.seg_len(b, p));
         const int64_t seg = g.seg(b, p);
-        sort_pass<true, false>(a16 + seg, nullptr, n, g.slots[p], 16, mine, sm);
-        sort_pass<false, true>(nullptr, mine, n, g.slots[p], 24, g32 + seg, sm);
-        __syncthreads();
-        // run-end flags: bit 0 marks the last entry of each column (found
-        // first for all of a thread's entries, then set)
-        uint32_t* out = g32 + seg;
-        uint32_t ends[kBlockRows * 8 / kSortThreads / 32] = {};
-        for (int e = threadIdx.x, k = 0; e < n; e += kSortThreads, k++)
-            if (e + 1 == n || (out[round_phys(e + 1)] >> 16) != (out[round_phys(e)] >> 16))
-                ends[k >> 5] |= 1u << (k & 31);
-        __syncthreads();
-        for (int e = threadIdx.x, k = 0; e < n; e += kSortThreads, k++)
-            if ((ends[k >> 5] >> (k & 31)) & 1u) out[round_phys(e)] |= 1u;
-        __syncthreads();
+        sort_pass<true>(a16 + seg, nullptr, n, g.slots[p], 16, mine, sm);
+        sort_pass<false>(nullptr, mine, n, g.slots[p], 24, g32 + seg, sm);
     }
 }
 
