@@ -150,6 +150,9 @@ SIGNATURES: dict[str, tuple] = {
     "cas_solver_rel_residual": (C.c_int, [_VP, C.POINTER(C.c_double)]),
     "cas_solver_run": (C.c_int, [_VP, C.POINTER(SolveReport)]),
     "cas_solver_iterations": (C.c_int, [_VP]),
+    "cas_solver_state_size": (C.c_int, [_VP, C.POINTER(C.c_size_t)]),
+    "cas_solver_save_state": (C.c_int, [_VP, _VP, C.c_size_t]),
+    "cas_solver_load_state": (C.c_int, [_VP, _VP, C.c_size_t]),
     "cas_solve": (C.c_int, [_VP, C.POINTER(SolveOpts), _VP, _VP, C.POINTER(SolveReport), _VP]),
     "cas_fit_weights": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP, _I64, C.POINTER(SolveOpts), _VP,
                                   C.POINTER(SolveReport)]),

@@ -327,6 +327,22 @@ class _Solver:
     def iterations(self) -> int:
         return int(self._lib.cas_solver_iterations(self._h))
 
+    def save_state(self) -> np.ndarray:
+        """The solver's state as a host byte array (cas_solver_save_state):
+        a checkpoint that load_state() resumes from."""
+        n = C.c_size_t()
+        L.check(self._lib.cas_solver_state_size(self._h, C.byref(n)))
+        buf = np.empty(n.value, dtype=np.uint8)
+        L.check(self._lib.cas_solver_save_state(self._h, buf.ctypes.data_as(C.c_void_p), n.value))
+        return buf
+
+    def load_state(self, state) -> None:
+        """Resumes from a checkpoint of save_state() (same method, precision,
+        column scaling, matrix and right-hand side)."""
+        buf = np.ascontiguousarray(np.frombuffer(state, dtype=np.uint8) if isinstance(state, (bytes, bytearray))
+                                   else state, dtype=np.uint8)
+        L.check(self._lib.cas_solver_load_state(self._h, buf.ctypes.data_as(C.c_void_p), buf.nbytes))
+
     def run(self) -> dict:
         rep = L.SolveReport()
         st = self._lib.cas_solver_run(self._h, C.byref(rep))

@@ -871,6 +871,7 @@ extern "C" {
 CAS_API cas_status cas_solve_batched(const cas_csr* a, const cas_solve_opts* o, const double* d_b, double* d_x,
                                      cas_solve_report* reports, void* stream)
 {
+    cas::NvtxRange nvtx_range("cas_solve_batched");
     CAS_REQUIRE(a && o && (a->rows == 0 || d_b) && (a->cols == 0 || d_x), CAS_ERR_INVALID_ARGUMENT,
                 "cas_solve_batched: null argument");
     CAS_REQUIRE(a->fast, CAS_ERR_INVALID_ARGUMENT,

@@ -7,9 +7,21 @@
 #include <cstdio>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/cassandra_b200.h"
 
 namespace cas {
+
+// An NVTX range over a scope: the library's long host calls (fits, layout
+// builds, solves) show as named ranges in a profiler timeline.  Header-only
+// NVTX 3: without a profiler attached a push/pop is a few instructions.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Thread-local message of the last failing call (read by cas_last_error).
 void set_error(const std::string& msg);

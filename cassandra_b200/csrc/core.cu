@@ -179,7 +179,7 @@ CAS_API size_t cas_last_error(char* buf, size_t cap)
     return m.size();
 }
 
-CAS_API int cas_version(void) { return 20000; }  // 2.0.0: cas_solve_opts.scale_columns; no timeout status
+CAS_API int cas_version(void) { return 20100; }  // 2.1.0: solver checkpoints (cas_solver_*_state)
 
 CAS_API long long cas_kernel_launches(void) { return launch_count(); }
 
@@ -245,6 +245,7 @@ CAS_API cas_status cas_patterns_indexer(const cas_patterns* p, int i, uint64_t* 
 CAS_API cas_status cas_index(const cas_patterns* p, const uint64_t* d_positions, int64_t n, uint32_t* d_out,
                              void* stream)
 {
+    cas::NvtxRange nvtx_range("cas_index");
     CAS_REQUIRE(p && n >= 0, CAS_ERR_INVALID_ARGUMENT, "cas_index: null handle or negative count");
     CAS_REQUIRE(n == 0 || (d_positions && d_out), CAS_ERR_INVALID_ARGUMENT, "cas_index: null buffer");
     CAS_REQUIRE((reinterpret_cast<uintptr_t>(d_positions) & 15) == 0, CAS_ERR_INVALID_ARGUMENT,

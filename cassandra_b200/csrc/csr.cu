@@ -503,6 +503,7 @@ extern "C" {
 CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const uint64_t* d_positions, int64_t rows,
                                                  int layouts, void* stream, cas_csr** out)
 {
+    cas::NvtxRange nvtx_range("cas_csr_from_positions");
     CAS_REQUIRE(p && out && rows >= 0, CAS_ERR_INVALID_ARGUMENT, "cas_csr_from_positions: bad argument");
     CAS_REQUIRE(rows == 0 || d_positions, CAS_ERR_INVALID_ARGUMENT, "cas_csr_from_positions: null positions");
     CAS_REQUIRE((reinterpret_cast<uintptr_t>(d_positions) & 15) == 0, CAS_ERR_INVALID_ARGUMENT,
@@ -569,6 +570,7 @@ CAS_API cas_status cas_csr_from_positions_batched(const cas_patterns* p, const u
                                                   const int64_t* h_problem_rows, int problems, void* stream,
                                                   cas_csr** out)
 {
+    cas::NvtxRange nvtx_range("cas_csr_from_positions_batched");
     CAS_REQUIRE(p && out && h_problem_rows && problems >= 1 && problems <= kMaxProblems, CAS_ERR_INVALID_ARGUMENT,
                 "cas_csr_from_positions_batched: bad argument (1 to 64 problems)");
     CAS_REQUIRE(fast_supported(pattern_set(p)), CAS_ERR_INVALID_ARGUMENT,

@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(256) fast_index_kernel(const Instance* __restr
 // columns keep ascending rows.
 //
 // A pass moves its items in tiles of kSortTile: each warp ranks its 512
-// items by digit (match_any, in item order, counts per digit in shared
+// items by digit (peers from ballots, in item order, counts per digit in shared
 // memory), one scan per tile turns the warps' counts into offsets, the tile
 // is scattered digit by digit into a shared buffer and written out from
 // there, so that consecutive threads write the consecutive output positions
@@ -120,6 +120,8 @@ struct SortSmem {
     uint32_t tbase[256];    // the digit's first slot in the tile buffer
     uint32_t pend_pos[256]; // final pass: the digit's last entry so far (kNoPend: none)
     uint32_t pend_col[256]; //   and its column
+    uint32_t dst[256];      // output position of the tile buffer's slot 0 for the digit (mod 2^32)
+    uint32_t tend[256];     // end of the digit's slots in the tile buffer
     uint32_t wcnt[kSortWarps][256];
     uint32_t buf[kSortTile];
 };
@@ -150,6 +152,21 @@ __device__ void block_exclusive_scan_256(const uint32_t* hist, uint32_t* out)
     __syncthreads();
 }
 
+// The lanes of the warp whose valid 8-bit digit equals this lane's (from
+// eight ballots: no match instruction, which costs far more here).  Only
+// meaningful on valid lanes.
+__device__ __forceinline__ unsigned digit_peers(uint32_t d, bool valid)
+{
+    unsigned peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        const bool bit = (d >> b) & 1u;
+        const unsigned m = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? m : ~m;
+    }
+    return peers;
+}
+
 // One stable 8-bit counting-sort pass of a group's n items by the digit at
 // `shift`.  FROM_A16: the first pass, items made from the A16 segment
 // (local column << 16 | row << 2), written to out in sorted order while the
@@ -168,9 +185,19 @@ __device__ void sort_pass(const uint16_t* __restrict__ a16_in, const uint32_t* _
         return in[e];
     };
     if (FROM_A16) {
+        // the digits (low column bytes) of the group, 8 columns per 16-byte
+        // load (segments start on 1024-entry rounds), the last n % 8 one by
+        // one
         if (t < 256) sm.hist[t] = 0;
         __syncthreads();
-        for (int e = t; e < n; e += kSortThreads) atomicAdd(&sm.hist[(item_at(e) >> shift) & 255u], 1u);
+        const uint4* v = reinterpret_cast<const uint4*>(a16_in);
+        for (int e = (n & ~7) + t; e < n; e += kSortThreads) atomicAdd(&sm.hist[a16_in[e] & 255u], 1u);
+        for (int i = t; i < n / 8; i += kSortThreads) {
+            const uint4 u = __ldcs(v + i);
+            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int q = 0; q < 8; q++) atomicAdd(&sm.hist[(w[q >> 1] >> (16 * (q & 1))) & 255u], 1u);
+        }
         __syncthreads();
     }
     block_exclusive_scan_256(FROM_A16 ? sm.hist : sm.hist2, sm.base);
@@ -186,12 +213,16 @@ __device__ void sort_pass(const uint16_t* __restrict__ a16_in, const uint32_t* _
         uint32_t item[kSortPerThread];
         uint32_t rk[kSortPerThread];  // rank among the warp's items of the same digit
 #pragma unroll
+        for (int k = 0; k < kSortPerThread; k++) {  // all loads first: one memory latency per tile
+            const int e = t0 + warp * kSortWarpItems + k * 32 + lane;
+            item[k] = e < n ? item_at(e) : 0u;
+        }
+#pragma unroll
         for (int k = 0; k < kSortPerThread; k++) {
             const int e = t0 + warp * kSortWarpItems + k * 32 + lane;
             const bool valid = e < n;
-            item[k] = valid ? item_at(e) : 0u;
-            const uint32_t d = valid ? (item[k] >> shift) & 255u : 0xFFFFu;
-            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const uint32_t d = (item[k] >> shift) & 255u;
+            const unsigned peers = digit_peers(d, valid);
             const int leader = __ffs(peers) - 1;
             uint32_t before = 0;
             if (valid && lane == leader) {
@@ -215,7 +246,12 @@ __device__ void sort_pass(const uint16_t* __restrict__ a16_in, const uint32_t* _
         }
         __syncthreads();
         block_exclusive_scan_256(sm.tcount, sm.tbase);
-        // 3. the tile into the buffer, digit by digit
+        // 3. the tile into the buffer, digit by digit; per digit, the output
+        // position of buffer slot 0 and the end of its slots
+        if (t < 256) {
+            sm.dst[t] = sm.base[t] + sm.running[t] - sm.tbase[t];
+            sm.tend[t] = sm.tbase[t] + sm.tcount[t];
+        }
 #pragma unroll
         for (int k = 0; k < kSortPerThread; k++) {
             const int e = t0 + warp * kSortWarpItems + k * 32 + lane;
@@ -230,9 +266,9 @@ __device__ void sort_pass(const uint16_t* __restrict__ a16_in, const uint32_t* _
         for (int j = t; j < tn; j += kSortThreads) {
             uint32_t it = sm.buf[j];
             const uint32_t d = (it >> shift) & 255u;
-            const uint32_t pos = sm.base[d] + sm.running[d] + static_cast<uint32_t>(j) - sm.tbase[d];
+            const uint32_t pos = sm.dst[d] + static_cast<uint32_t>(j);
             if (FINAL) {
-                const bool last_in_tile = static_cast<uint32_t>(j) + 1 == sm.tbase[d] + sm.tcount[d];
+                const bool last_in_tile = static_cast<uint32_t>(j) + 1 == sm.tend[d];
                 if (!last_in_tile && (sm.buf[j + 1] >> 16) != (it >> 16)) it |= 1u;
                 out[round_phys(pos)] = it;
             } else {
@@ -2020,6 +2056,7 @@ void fast_free(FastLayout& f)
 cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint64_t* d_pos, int64_t rows,
                       const int64_t* prob_rows, int nprob, uint64_t* diag_int, FastLayout& f, cudaStream_t s)
 {
+    cas::NvtxRange nvtx_range("blocked layout build");
     CAS_REQUIRE(fast_supported(ps), CAS_ERR_INVALID_ARGUMENT, "pattern set does not fit the blocked layout");
     CAS_REQUIRE(nprob >= 1 && nprob <= kMaxProblems, CAS_ERR_INVALID_ARGUMENT,
                 "blocked layout: 1 to 64 problems per batch");

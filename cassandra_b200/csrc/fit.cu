@@ -148,6 +148,7 @@ CAS_API cas_status cas_fit_weights_device(const cas_patterns* p, const uint64_t*
                                           int64_t rows, const cas_solve_opts* o, double* d_weights,
                                           cas_solve_report* rep, void* stream)
 {
+    cas::NvtxRange nvtx_range("cas_fit_weights_device");
     CAS_REQUIRE(p && o && d_weights, CAS_ERR_INVALID_ARGUMENT, "cas_fit_weights_device: null argument");
     CAS_REQUIRE(rows >= 0 && (rows == 0 || (d_positions && d_scores)), CAS_ERR_INVALID_ARGUMENT,
                 "cas_fit_weights_device: bad rows or buffers");
@@ -183,6 +184,7 @@ CAS_API cas_status cas_fit_weights(const uint64_t* masks, int n_masks, cas_index
                                    const uint64_t* h_positions, const float* h_scores, int64_t rows,
                                    const cas_solve_opts* o, float* h_weights, cas_solve_report* rep)
 {
+    cas::NvtxRange nvtx_range("cas_fit_weights");
     CAS_REQUIRE(masks && o && h_weights && rows >= 0, CAS_ERR_INVALID_ARGUMENT, "cas_fit_weights: bad argument");
     CAS_REQUIRE(rows == 0 || (h_positions && h_scores), CAS_ERR_INVALID_ARGUMENT, "cas_fit_weights: null input");
     CAS_TRY(require_device());
@@ -234,6 +236,7 @@ CAS_API cas_status cas_fit_weights_batched_device(const cas_patterns* p, const u
                                                   int problems, const cas_solve_opts* o, double* d_weights,
                                                   cas_solve_report* reports, void* stream)
 {
+    cas::NvtxRange nvtx_range("cas_fit_weights_batched_device");
     CAS_REQUIRE(p && o && d_weights && h_problem_rows, CAS_ERR_INVALID_ARGUMENT,
                 "cas_fit_weights_batched_device: null argument");
     auto s = static_cast<cudaStream_t>(stream);
@@ -266,6 +269,7 @@ CAS_API cas_status cas_fit_weights_batched(const uint64_t* masks, int n_masks, c
                                            const int64_t* h_problem_rows, int problems, const cas_solve_opts* o,
                                            float* h_weights, cas_solve_report* reports)
 {
+    cas::NvtxRange nvtx_range("cas_fit_weights_batched");
     CAS_REQUIRE(masks && o && h_weights && h_problem_rows && problems >= 1, CAS_ERR_INVALID_ARGUMENT,
                 "cas_fit_weights_batched: bad argument");
     int64_t rows = 0;

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <vector>
+#include <cstring>
 
 #include "common.cuh"
 #include "fast.cuh"
@@ -1093,6 +1094,22 @@ struct SolverImpl {
         return CAS_OK;
     }
 
+    // The device buffers that hold an iteration's state, in checkpoint order
+    // (vectors, the rows-length products LSQR/LSMR keep their u in, device
+    // scalars and flags); the partial sums are scratch and not included.
+    std::vector<std::pair<void*, size_t>> state_buffers() const
+    {
+        const size_t cb = sizeof(double) * std::max<int64_t>(C, 1), rb8 = sizeof(double) * std::max<int64_t>(R, 1);
+        std::vector<std::pair<void*, size_t>> v_;
+        for (double* ptr : {x, r, z, p, d, w, v}) v_.push_back({ptr, cb});
+        if (mixed) v_.push_back({pg32, sizeof(float) * std::max<int64_t>(C, 1)});
+        v_.push_back({q, mixed ? sizeof(float) * std::max<int64_t>(R, 1) : rb8});
+        v_.push_back({q64, rb8});
+        v_.push_back({scal, sizeof(double) * kSlots});
+        v_.push_back({flags, sizeof(int) * kFlags});
+        return v_;
+    }
+
     cas_status read_state()
     {
         CAS_CUDA(cudaMemcpyAsync(host_scal, scal, sizeof(double) * kSlots, cudaMemcpyDeviceToHost, s));
@@ -1323,6 +1340,83 @@ CAS_API cas_status cas_solver_create_normal_diag(const cas_csr* a, const cas_sol
 
 CAS_API void cas_solver_destroy(cas_solver* s) { delete s; }
 
+namespace {
+// Header of a solver checkpoint (cas_solver_save_state).
+struct StateHeader {
+    uint64_t magic;
+    uint32_t version;
+    int32_t method, precision, scaled;
+    int64_t cols, rows;
+    uint64_t bytes;  // the whole checkpoint, header included
+};
+constexpr uint64_t kStateMagic = 0x5453564c4f534143ull;  // "CASOLVST"
+constexpr uint32_t kStateVersion = 1;
+
+StateHeader state_header(const SolverImpl& m)
+{
+    StateHeader h{};
+    h.magic = kStateMagic;
+    h.version = kStateVersion;
+    h.method = m.o.method;
+    h.precision = m.o.precision;
+    h.scaled = m.scaled() ? 1 : 0;
+    h.cols = m.C;
+    h.rows = m.R;
+    h.bytes = sizeof(StateHeader);
+    for (const auto& b : m.state_buffers()) h.bytes += b.second;
+    return h;
+}
+}  // namespace
+
+CAS_API cas_status cas_solver_state_size(const cas_solver* sv, size_t* bytes)
+{
+    CAS_REQUIRE(sv && bytes, CAS_ERR_INVALID_ARGUMENT, "cas_solver_state_size: null argument");
+    *bytes = state_header(sv->impl).bytes;
+    return CAS_OK;
+}
+
+CAS_API cas_status cas_solver_save_state(cas_solver* sv, void* h_buf, size_t bytes)
+{
+    CAS_REQUIRE(sv && h_buf, CAS_ERR_INVALID_ARGUMENT, "cas_solver_save_state: null argument");
+    SolverImpl& m = sv->impl;
+    const StateHeader h = state_header(m);
+    CAS_REQUIRE(bytes >= h.bytes, CAS_ERR_INVALID_ARGUMENT, "cas_solver_save_state: buffer smaller than cas_solver_state_size");
+    char* out = static_cast<char*>(h_buf);
+    std::memcpy(out, &h, sizeof h);
+    size_t off = sizeof h;
+    for (const auto& b : m.state_buffers()) {
+        CAS_CUDA(cudaMemcpyAsync(out + off, b.first, b.second, cudaMemcpyDeviceToHost, m.s));
+        off += b.second;
+    }
+    CAS_CUDA(cudaStreamSynchronize(m.s));
+    return CAS_OK;
+}
+
+CAS_API cas_status cas_solver_load_state(cas_solver* sv, const void* h_buf, size_t bytes)
+{
+    CAS_REQUIRE(sv && h_buf, CAS_ERR_INVALID_ARGUMENT, "cas_solver_load_state: null argument");
+    SolverImpl& m = sv->impl;
+    CAS_REQUIRE(bytes >= sizeof(StateHeader), CAS_ERR_INVALID_ARGUMENT, "cas_solver_load_state: buffer too small");
+    StateHeader h;
+    std::memcpy(&h, h_buf, sizeof h);
+    const StateHeader want = state_header(m);
+    CAS_REQUIRE(h.magic == kStateMagic && h.version == kStateVersion, CAS_ERR_INVALID_ARGUMENT,
+                "cas_solver_load_state: not a solver checkpoint of this version");
+    CAS_REQUIRE(h.method == want.method && h.precision == want.precision && h.scaled == want.scaled &&
+                    h.cols == want.cols && h.rows == want.rows && h.bytes == want.bytes && bytes >= h.bytes,
+                CAS_ERR_INVALID_ARGUMENT,
+                "cas_solver_load_state: the checkpoint was saved by a solver of another method, precision, "
+                "column scaling or matrix shape");
+    const char* in = static_cast<const char*>(h_buf);
+    size_t off = sizeof h;
+    for (const auto& b : m.state_buffers()) {
+        CAS_CUDA(cudaMemcpyAsync(b.first, in + off, b.second, cudaMemcpyHostToDevice, m.s));
+        off += b.second;
+    }
+    CAS_TRY(m.read_state());  // also waits for the copies: the caller may free its buffer
+    return CAS_OK;
+}
+
 CAS_API cas_status cas_solver_iterate(cas_solver* sv, int n)
 {
     CAS_REQUIRE(sv && n >= 0, CAS_ERR_INVALID_ARGUMENT, "cas_solver_iterate: bad argument");
@@ -1371,6 +1465,7 @@ CAS_API int cas_solver_iterations(const cas_solver* sv)
 
 CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
 {
+    cas::NvtxRange nvtx_range("cas_solver_run");
     CAS_REQUIRE(sv, CAS_ERR_INVALID_ARGUMENT, "cas_solver_run: null solver");
     SolverImpl& m = sv->impl;
     const int chunk = m.o.check_every > 0 ? m.o.check_every : 50;

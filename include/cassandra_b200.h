@@ -318,6 +318,24 @@ CAS_API cas_status cas_solver_rel_residual(cas_solver* s, double* h_out);
 CAS_API cas_status cas_solver_run(cas_solver* s, cas_solve_report* rep);
 CAS_API int cas_solver_iterations(const cas_solver* s);
 
+/* Checkpoint and resume of an iterative solve (no counterpart in the
+ * reference, whose solvers keep their state in host Vectors for one run):
+ * the solver's device state -- the iterate, residual, preconditioned
+ * residual and direction vectors, the bidiagonalisation vectors of
+ * LSQR/LSMR (rows-length u included), the device scalars and flags -- as
+ * one host byte buffer of cas_solver_state_size bytes (a header, then the
+ * buffers).  A checkpoint loads into a solver created with the same method,
+ * precision, column scaling and matrix shape (checked:
+ * CAS_ERR_INVALID_ARGUMENT otherwise) on the same matrix and right-hand side
+ * (not checked).  Iterating on from a loaded checkpoint gives bitwise the
+ * iterates the saved solver would have produced, provided the products
+ * run the same kernels: in one process, or, for FP32 products on the
+ * blocked layout, with the same A'y schedule (CAS_ATY_SCHEDULE).  Both
+ * calls synchronise the solver's stream. */
+CAS_API cas_status cas_solver_state_size(const cas_solver* s, size_t* bytes);
+CAS_API cas_status cas_solver_save_state(cas_solver* s, void* h_buf, size_t bytes);
+CAS_API cas_status cas_solver_load_state(cas_solver* s, const void* h_buf, size_t bytes);
+
 /* ------------------------------------------------------------------------ */
 /* Batched fits: one problem per empty-count stage                           */
 /* ------------------------------------------------------------------------ */

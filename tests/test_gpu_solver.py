@@ -230,3 +230,36 @@ def test_least_squares_reach_1e8_on_fit_system(cuda, orc, method, scale, layout,
     xp, _, _ = orc.pcg(idx, cols, bh, 5000, tol=1e-10, check_every=10)
     pp = orc.spmv(idx, cols, xp)
     assert np.abs(orc.spmv(idx, cols, x) - pp).max() <= 1e-4 * np.abs(pp).max()
+
+
+@pytest.mark.parametrize("method,layout,precision", [("pcg", "rows", "fp64"), ("pcg", "blocked", "mixed"),
+                                                     ("lsqr", "blocked", "mixed"), ("lsmr", "rows", "fp64")])
+def test_checkpoint_resumes_bitwise(cuda, method, layout, precision):
+    """cas_solver_save_state / cas_solver_load_state: a solver created on the
+    same system that loads a checkpoint taken after 30 iterations produces,
+    over 40 more (FP64 residual replacements or restarts of the mixed solvers
+    included), bitwise the iterate of the solver that was never stopped; the
+    checkpoint does not load into a solver of another method or precision."""
+    pos = cb.generate_positions(23, 20_000, 20, 40)
+    g = cb.GroupIndexer(SET8, "expanded")
+    a = cb.MatrixCSR.from_positions(g, pos, layout)
+    b = cb.generate_targets(a, 23)
+    cls = {"pcg": cb.PCG, "lsqr": cb.LSQR, "lsmr": cb.LSMR}[method]
+    kw = dict(precision=precision, tol=1e-12, check_every=10)
+    s1 = cls(a, b, **kw)
+    s1.iterate(30)
+    state = s1.save_state()
+    s1.iterate(40)
+    want = s1.x()
+    s2 = cls(a, b, **kw)
+    s2.iterate(3)  # a different state, overwritten by the load
+    s2.load_state(bytes(state))
+    assert s2.iterations() == 30
+    s2.iterate(40)
+    assert s2.iterations() == s1.iterations() == 70
+    assert torch.equal(s2.x(), want)
+    other = cb.CG(a, b, precision=precision) if method != "pcg" else cb.PCG(a, b, precision="fp64" if precision == "mixed" else "mixed")
+    with pytest.raises(cb.CasError):
+        other.load_state(state)
+    with pytest.raises(cb.CasError):
+        s2.load_state(state[:100])
