@@ -60,7 +60,7 @@ FALLBACK_HBM_GBS = 6650.0
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on a
 # 2M-row launch of the same kernels, 128M entries; traffic grows with the
 # entries, so a full launch's traffic is this times its entries.
-NCU_DRAM_BYTES_PER_ENTRY = {"aty_f32": (521.47e6 + 6.35e6) / 128e6, "ax_f32": (256.89e6 + 7.29e6) / 128e6}
+NCU_DRAM_BYTES_PER_ENTRY = {"aty_f32": (563.91e6 + 33.30e6) / 128e6, "ax_f32": (288.12e6 + 4.19e6) / 128e6}
 
 
 def ncu_traffic(kernel: str, entries: int):

@@ -17,6 +17,7 @@ from .api import (  # noqa: F401
     MultiStageScoreEstimator,
     estimator_stages,
     fit_weights,
+    fit_weights_batched,
     generate_positions,
     generate_positions_host,
     generate_targets,

@@ -405,6 +405,41 @@ def solve_batched(a: MatrixCSR, b: torch.Tensor, precision: str = "mixed", tol: 
     return x.view(n, -1), out, st == L.CAS_OK
 
 
+def fit_weights_batched(indexer: GroupIndexer, positions: torch.Tensor, scores: torch.Tensor, sizes,
+                        method: str = "pcg", precision: str = "mixed", tol: float = 1e-8,
+                        max_iterations: int = 20000, refine_every: int = 50, check_every: int = 50,
+                        jacobi: bool = True, scale_columns: bool = False) -> tuple[torch.Tensor, list[dict], bool]:
+    """The per-stage fits of the training loop in one call
+    (cas_fit_weights_batched_device): problem q is the next sizes[q]
+    positions (device {P, O} int64 pairs) and scores.  PCG/CG run as one
+    batched solve on a block-diagonal layout; LSQR/LSMR as one solver per
+    problem, all run together.  Returns the weights as [problems, cols], one
+    report per problem and whether all reached the tolerance."""
+    _require_cuda(positions, "positions")
+    _require_cuda(scores, "scores")
+    sizes = np.ascontiguousarray(sizes, dtype=np.int64)
+    if positions.shape[0] != int(sizes.sum()) or scores.numel() != int(sizes.sum()):
+        raise L.SizeMismatch(L.CAS_ERR_SIZE_MISMATCH, "Size mismatch.")
+    pos = positions.contiguous()
+    sc = scores.double().contiguous()
+    lib = L.load()
+    n = len(sizes)
+    opts = solve_opts(method, precision, tol, max_iterations, refine_every, check_every, jacobi, scale_columns)
+    x = torch.empty(n * indexer.index_space_size, dtype=torch.float64, device="cuda")
+    reps = (L.SolveReport * n)()
+    st = lib.cas_fit_weights_batched_device(indexer.handle, _ptr(pos), _ptr(sc),
+                                            sizes.ctypes.data_as(C.c_void_p), n, C.byref(opts), _ptr(x), reps,
+                                            _stream())
+    if st not in (L.CAS_OK, L.CAS_ERR_NOT_CONVERGED):
+        L.check(st)
+    out = []
+    for r in reps:
+        d = r.as_dict()
+        d["converged"] = bool(tol <= 0 or d["rel_residual"] <= tol)
+        out.append(d)
+    return x.view(n, -1), out, st == L.CAS_OK
+
+
 def fit_weights(masks, positions: np.ndarray, scores: np.ndarray, mode: str = "reference", method: str = "pcg",
                 precision: str = "fp64", tol: float = 1e-8, max_iterations: int = 20000,
                 refine_every: int = 50, check_every: int = 50, scale_columns: bool = False) -> tuple[np.ndarray, dict]:

@@ -1079,7 +1079,7 @@ __device__ __forceinline__ void reduce_block(const uint32_t* __restrict__ g32, c
 // in the sorted order, two 16-byte words of G32 each), with the same lane
 // chain and warp records.
 // ---------------------------------------------------------------------------
-constexpr int kStretchRun = 8;                  // entries per lane and step
+constexpr int kStretchRun = 16;                 // entries per lane and step
 constexpr int kStretchVecs = kStretchRun / 4;   // 16-byte words per lane and step
 
 // The 16-byte word of G32 that holds sorted positions e .. e+3 (e a

@@ -231,6 +231,88 @@ CAS_API cas_status cas_fit_weights(const uint64_t* masks, int n_masks, cas_index
     return st;
 }
 
+namespace {
+// The per-stage fits by LSQR or LSMR: one CSR (the layout a single fit of
+// that precision uses) and one solver per stage, each on its own stream,
+// run to tolerance together -- the host steps the unfinished solvers in
+// turn, so that one stage's chunk of iterations runs while another's state
+// is read.  A stage without rows gets zero weights.  Each stage's result is
+// the single fit's of that stage.
+cas_status batched_least_squares(const cas_patterns* p, const uint64_t* d_positions, const double* d_scores,
+                                 const int64_t* h_rows, int problems, const cas_solve_opts* o, double* d_weights,
+                                 cas_solve_report* reports, cudaStream_t s)
+{
+    const int64_t cols = cas_patterns_cols(p);
+    const int layouts =
+        (o->precision == CAS_MIXED && fast_supported(pattern_set(p))) ? CAS_LAYOUT_BLOCKED : CAS_LAYOUT_ROWS;
+    std::vector<cudaStream_t> streams(problems, nullptr);
+    std::vector<cas_csr*> csrs(problems, nullptr);
+    std::vector<cas_solver*> solvers(problems, nullptr);
+    std::vector<cas_status> sts(problems, CAS_OK);
+    std::vector<cas_solve_report> reps(problems, cas_solve_report{});
+    cudaEvent_t ready = nullptr, e0 = nullptr, e1 = nullptr;
+    cas_status st = CAS_OK;
+    auto cuda = [&](cudaError_t e) {
+        if (e != cudaSuccess && st == CAS_OK) {
+            set_error(std::string("batched least squares: ") + cudaGetErrorString(e));
+            st = e == cudaErrorMemoryAllocation ? CAS_ERR_OUT_OF_MEMORY : CAS_ERR_CUDA;
+        }
+    };
+    cuda(cudaEventCreate(&ready));
+    cuda(cudaEventCreate(&e0));
+    cuda(cudaEventCreate(&e1));
+    if (st == CAS_OK) cuda(cudaEventRecord(ready, s));  // the inputs are written on s
+    if (st == CAS_OK) cuda(cudaEventRecord(e0, s));
+    int64_t row0 = 0;
+    for (int q = 0; q < problems && st == CAS_OK; q++) {
+        const int64_t rq = std::max<int64_t>(h_rows[q], 0);
+        if (rq == 0) {
+            cuda(cudaMemsetAsync(d_weights + q * cols, 0, sizeof(double) * cols, s));
+            continue;
+        }
+        cuda(cudaStreamCreateWithFlags(&streams[q], cudaStreamNonBlocking));
+        if (st == CAS_OK) cuda(cudaStreamWaitEvent(streams[q], ready, 0));
+        if (st == CAS_OK) st = cas_csr_from_positions_layout(p, d_positions + 2 * row0, rq, layouts, streams[q], &csrs[q]);
+        if (st == CAS_OK) st = cas_solver_create(csrs[q], o, d_scores + row0, nullptr, streams[q], &solvers[q]);
+        row0 += rq;
+    }
+    // set-up time: from the first build to the last solver's set-up
+    float setup_ms = 0;
+    for (int q = 0; q < problems && st == CAS_OK; q++)
+        if (streams[q]) {
+            cuda(cudaEventRecord(e1, streams[q]));
+            if (st == CAS_OK) cuda(cudaStreamWaitEvent(s, e1, 0));
+        }
+    if (st == CAS_OK) cuda(cudaEventRecord(e1, s));
+    if (st == CAS_OK) cuda(cudaEventSynchronize(e1));
+    if (st == CAS_OK) cuda(cudaEventElapsedTime(&setup_ms, e0, e1));
+    if (st == CAS_OK) st = solvers_run_all(solvers.data(), problems, reps.data(), sts.data());
+    for (int q = 0; q < problems && st == CAS_OK; q++) {
+        if (!solvers[q]) continue;
+        if (sts[q] == CAS_OK || sts[q] == CAS_ERR_NOT_CONVERGED) st = cas_solver_x(solvers[q], d_weights + q * cols);
+    }
+    for (int q = 0; q < problems; q++)
+        if (streams[q]) cuda(cudaStreamSynchronize(streams[q]));
+    for (int q = 0; q < problems; q++) {
+        if (solvers[q]) cas_solver_destroy(solvers[q]);
+        if (csrs[q]) cas_csr_destroy(csrs[q]);
+        if (streams[q]) cudaStreamDestroy(streams[q]);
+    }
+    if (ready) cudaEventDestroy(ready);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (reports)
+        for (int q = 0; q < problems; q++) {
+            reports[q] = reps[q];
+            reports[q].setup_seconds = setup_ms * 1e-3;
+        }
+    if (st != CAS_OK) return st;
+    for (int q = 0; q < problems; q++)
+        if (sts[q] != CAS_OK) return sts[q];  // the first stage that did not converge
+    return CAS_OK;
+}
+}  // namespace
+
 CAS_API cas_status cas_fit_weights_batched_device(const cas_patterns* p, const uint64_t* d_positions,
                                                   const double* d_scores, const int64_t* h_problem_rows,
                                                   int problems, const cas_solve_opts* o, double* d_weights,
@@ -240,6 +322,8 @@ CAS_API cas_status cas_fit_weights_batched_device(const cas_patterns* p, const u
     CAS_REQUIRE(p && o && d_weights && h_problem_rows, CAS_ERR_INVALID_ARGUMENT,
                 "cas_fit_weights_batched_device: null argument");
     auto s = static_cast<cudaStream_t>(stream);
+    if (o->method == CAS_LSQR || o->method == CAS_LSMR)
+        return batched_least_squares(p, d_positions, d_scores, h_problem_rows, problems, o, d_weights, reports, s);
     cudaEvent_t e0, e1;
     CAS_CUDA(cudaEventCreate(&e0));
     CAS_CUDA(cudaEventCreate(&e1));

@@ -20,6 +20,10 @@ cas_status patterns_on_device(const cas_patterns* p, const DevicePatterns** out)
 const PatternSet& pattern_set(const cas_patterns* p);
 cas_status launch_index(const DevicePatterns& dp, const uint64_t* d_pos, int64_t n, uint32_t* d_out,
                         cudaStream_t stream);
+// Several solvers to tolerance at once, each on its own stream; per-solver
+// statuses in sts, reports in reps (may be null).  Returns the first failed
+// CUDA call's status (solver.cu).
+cas_status solvers_run_all(cas_solver* const* svs, int n, cas_solve_report* reps, cas_status* sts);
 
 // Entries of one A'y work unit: a column's row list is cut into units of at
 // most kUnit entries, one warp each.

@@ -1463,101 +1463,193 @@ CAS_API int cas_solver_iterations(const cas_solver* sv)
     return m.host_flags[kIter];
 }
 
+}  // extern "C"
+
+namespace cas {
+// The host side of one solve to tolerance, as a sequence of steps: each
+// step reads the device state once, takes the decisions of a chunk
+// boundary (convergence on the FP64 true residual, restarts and
+// replacements requested by the host) and issues the next chunk of
+// iterations without waiting for it.  cas_solver_run steps one solver; the
+// batched LSQR/LSMR fit steps several, each on its own stream, in turn, so
+// that one solver's chunk runs while the host reads another's state.
+struct RunLoop {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    double rel = 0;
+    int extra_checks = 0;
+    cas_status st = CAS_OK;
+    bool finished = false;
+    float ms = 0;
+};
+
+cas_status run_begin(SolverImpl& m, RunLoop& L)
+{
+    CAS_CUDA(cudaEventCreate(&L.e0));
+    CAS_CUDA(cudaEventCreate(&L.e1));
+    CAS_CUDA(cudaEventRecord(L.e0, m.s));
+    return CAS_OK;
+}
+
+cas_status run_step(SolverImpl& m, RunLoop& L)
+{
+    const int chunk = m.o.check_every > 0 ? m.o.check_every : 50;
+    CAS_TRY(m.read_state());
+    const int it = m.host_flags[kIter];
+    if (m.host_flags[kStatus] != 0) {
+        L.st = static_cast<cas_status>(m.host_flags[kStatus]);
+        L.finished = true;
+        return CAS_OK;
+    }
+    const bool done = m.host_flags[kDone] || m.host_flags[kPending];
+    if (m.least_squares() && m.o.tol > 0 && !done && it > 0) {
+        // LSQR's recursive residual estimates lose their meaning once the
+        // bidiagonalisation loses orthogonality, and iterating past
+        // convergence can diverge (the reference's LSQR has no stopping
+        // test), so its stopping test is the true FP64 residual, checked
+        // at every chunk boundary.
+        CAS_TRY(m.true_residual(&L.rel));
+        if (L.rel <= m.o.tol) {
+            L.finished = true;
+            return CAS_OK;
+        }
+        // The mixed solver's cycle has drifted: its estimate is more than
+        // kLsqrDrift times below the true residual (the FP32 products'
+        // noise floor reached before the restart drop): restart now.
+        if (m.mixed && m.host_scal[kRes] * kLsqrDrift < L.rel && !m.scaled()) CAS_TRY(m.issue_lsqr_start(3));
+    }
+    if (done) {
+        if (m.host_flags[kVerified] && !m.least_squares()) {
+            // a residual replacement met the tolerance on the FP64 true residual
+            L.rel = m.host_scal[kRes];
+            L.finished = true;
+            return CAS_OK;
+        }
+        // verify with the true FP64 residual
+        CAS_TRY(m.true_residual(&L.rel));
+        if (m.o.tol <= 0 || L.rel <= m.o.tol || it >= m.o.max_iterations) {
+            L.finished = true;
+            return CAS_OK;
+        }
+        if (L.extra_checks > 20) {
+            L.st = CAS_ERR_NOT_CONVERGED;
+            L.finished = true;
+            return CAS_OK;
+        }
+        // recursive residual drifted: replace it and continue
+        L.extra_checks++;
+        static const int zero = 0;
+        CAS_CUDA(cudaMemcpyAsync(m.flags + kDone, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
+        CAS_CUDA(cudaMemcpyAsync(m.flags + kPending, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
+        if (m.least_squares() && m.mixed) {
+            // the mixed cycle's estimate met the tolerance but the FP64
+            // residual did not: restart from it
+            CAS_TRY(m.issue_lsqr_start(3));
+        } else if (m.least_squares()) {
+            // LSQR / LSMR have no residual to replace: tighten the recursive target
+            double t = m.host_scal[kTol] * 0.5;
+            CAS_CUDA(cudaMemcpyAsync(m.scal + kTol, &t, sizeof t, cudaMemcpyHostToDevice, m.s));
+        } else if (m.mixed) {
+            // the converged step skipped p = z + beta p: restart p = z
+            CAS_TRY(m.issue_pcg_refine<true>(true));
+        } else {
+            CAS_TRY(m.issue_pcg_refine<false>(true));
+        }
+        return CAS_OK;  // the next step reads the state again
+    }
+    if (it >= m.o.max_iterations) {
+        CAS_TRY(m.true_residual(&L.rel));
+        if (m.o.tol > 0 && L.rel > m.o.tol) L.st = CAS_ERR_NOT_CONVERGED;
+        L.finished = true;
+        return CAS_OK;
+    }
+    const int n = std::min(chunk, m.o.max_iterations - it);
+    CAS_TRY(m.issue_chunk(m.launched, n));
+    return CAS_OK;
+}
+
+// Ends a solve: its device time, the report, the status.
+cas_status run_end(SolverImpl& m, RunLoop& L, cas_solve_report* rep)
+{
+    CAS_CUDA(cudaEventRecord(L.e1, m.s));
+    CAS_CUDA(cudaEventSynchronize(L.e1));
+    cudaEventElapsedTime(&L.ms, L.e0, L.e1);
+    cudaEventDestroy(L.e0);
+    cudaEventDestroy(L.e1);
+    L.e0 = L.e1 = nullptr;
+    CAS_TRY(m.read_state());
+    if (rep) {
+        rep->iterations = m.host_flags[kIter];
+        rep->refinements = m.host_flags[kRefine];
+        rep->rel_residual = L.rel;
+        rep->residuum = m.o.method == CAS_LSQR ? m.host_scal[kPhiBar] : (m.o.method == CAS_LSMR ? 0.0 : m.host_scal[kRr]);
+        rep->seconds = L.ms * 1e-3;
+        rep->setup_seconds = 0;
+    }
+    if (L.st == CAS_ERR_NOT_CONVERGED) set_error("solver did not reach the tolerance within max_iterations");
+    if (L.st == CAS_ERR_BREAKDOWN) set_error("solver breakdown (p'A'Ap <= 0 or non-finite scalar)");
+    return L.st;
+}
+
+void run_abandon(RunLoop& L)
+{
+    if (L.e0) cudaEventDestroy(L.e0);
+    if (L.e1) cudaEventDestroy(L.e1);
+    L.e0 = L.e1 = nullptr;
+}
+}  // namespace cas
+
+extern "C" {
+
 CAS_API cas_status cas_solver_run(cas_solver* sv, cas_solve_report* rep)
 {
     cas::NvtxRange nvtx_range("cas_solver_run");
     CAS_REQUIRE(sv, CAS_ERR_INVALID_ARGUMENT, "cas_solver_run: null solver");
     SolverImpl& m = sv->impl;
-    const int chunk = m.o.check_every > 0 ? m.o.check_every : 50;
-    cudaEvent_t e0, e1;
-    CAS_CUDA(cudaEventCreate(&e0));
-    CAS_CUDA(cudaEventCreate(&e1));
-    CAS_CUDA(cudaEventRecord(e0, m.s));
-    cas_status st = CAS_OK;
-    double rel = 0;
-    int extra_checks = 0;
-    while (true) {
-        CAS_TRY(m.read_state());
-        const int it = m.host_flags[kIter];
-        if (m.host_flags[kStatus] != 0) {
-            st = static_cast<cas_status>(m.host_flags[kStatus]);
-            break;
+    RunLoop L;
+    cas_status st = run_begin(m, L);
+    while (st == CAS_OK && !L.finished) st = run_step(m, L);
+    if (st != CAS_OK) {
+        run_abandon(L);
+        return st;
+    }
+    return run_end(m, L, rep);
+}
+
+}  // extern "C"
+
+namespace cas {
+// Several solvers to tolerance at once, each on its own stream (the batched
+// LSQR/LSMR fit): the host steps the unfinished ones in turn.  Returns the
+// first error of a CUDA call; per-solver statuses go to sts.
+cas_status solvers_run_all(cas_solver* const* svs, int n, cas_solve_report* reps, cas_status* sts)
+{
+    std::vector<RunLoop> loops(n);
+    for (int i = 0; i < n; i++) {
+        sts[i] = CAS_OK;
+        if (svs[i]) CAS_TRY(run_begin(svs[i]->impl, loops[i]));
+    }
+    cas_status err = CAS_OK;
+    for (bool any = true; any && err == CAS_OK;) {
+        any = false;
+        for (int i = 0; i < n && err == CAS_OK; i++) {
+            if (!svs[i] || loops[i].finished) continue;
+            err = run_step(svs[i]->impl, loops[i]);
+            any = true;
         }
-        const bool done = m.host_flags[kDone] || m.host_flags[kPending];
-        if (m.least_squares() && m.o.tol > 0 && !done && it > 0) {
-            // LSQR's recursive residual estimates lose their meaning once the
-            // bidiagonalisation loses orthogonality, and iterating past
-            // convergence can diverge (the reference's LSQR has no stopping
-            // test), so its stopping test is the true FP64 residual, checked
-            // at every chunk boundary.
-            CAS_TRY(m.true_residual(&rel));
-            if (rel <= m.o.tol) break;
-            // The mixed solver's cycle has drifted: its estimate is more than
-            // kLsqrDrift times below the true residual (the FP32 products'
-            // noise floor reached before the restart drop): restart now.
-            if (m.mixed && m.host_scal[kRes] * kLsqrDrift < rel && !m.scaled()) CAS_TRY(m.issue_lsqr_start(3));
-        }
-        if (done) {
-            if (m.host_flags[kVerified] && !m.least_squares()) {
-                // a residual replacement met the tolerance on the FP64 true residual
-                rel = m.host_scal[kRes];
-                break;
-            }
-            // verify with the true FP64 residual
-            CAS_TRY(m.true_residual(&rel));
-            if (m.o.tol <= 0 || rel <= m.o.tol || it >= m.o.max_iterations) break;
-            if (extra_checks > 20) {
-                st = CAS_ERR_NOT_CONVERGED;
-                break;
-            }
-            // recursive residual drifted: replace it and continue
-            extra_checks++;
-            static const int zero = 0;
-            CAS_CUDA(cudaMemcpyAsync(m.flags + kDone, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
-            CAS_CUDA(cudaMemcpyAsync(m.flags + kPending, &zero, sizeof zero, cudaMemcpyHostToDevice, m.s));
-            if (m.least_squares() && m.mixed) {
-                // the mixed cycle's estimate met the tolerance but the FP64
-                // residual did not: restart from it
-                CAS_TRY(m.issue_lsqr_start(3));
-            } else if (m.least_squares()) {
-                // LSQR / LSMR have no residual to replace: tighten the recursive target
-                double t = m.host_scal[kTol] * 0.5;
-                CAS_CUDA(cudaMemcpyAsync(m.scal + kTol, &t, sizeof t, cudaMemcpyHostToDevice, m.s));
-            } else if (m.mixed) {
-                // the converged step skipped p = z + beta p: restart p = z
-                CAS_TRY(m.issue_pcg_refine<true>(true));
-            } else {
-                CAS_TRY(m.issue_pcg_refine<false>(true));
-            }
+    }
+    for (int i = 0; i < n; i++) {
+        if (!svs[i]) continue;
+        if (err != CAS_OK) {
+            run_abandon(loops[i]);
             continue;
         }
-        if (it >= m.o.max_iterations) {
-            CAS_TRY(m.true_residual(&rel));
-            if (m.o.tol > 0 && rel > m.o.tol) st = CAS_ERR_NOT_CONVERGED;
-            break;
-        }
-        const int n = std::min(chunk, m.o.max_iterations - it);
-        CAS_TRY(m.issue_chunk(m.launched, n));
+        sts[i] = run_end(svs[i]->impl, loops[i], reps ? &reps[i] : nullptr);
     }
-    CAS_CUDA(cudaEventRecord(e1, m.s));
-    CAS_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    CAS_TRY(m.read_state());
-    if (rep) {
-        rep->iterations = m.host_flags[kIter];
-        rep->refinements = m.host_flags[kRefine];
-        rep->rel_residual = rel;
-        rep->residuum = m.o.method == CAS_LSQR ? m.host_scal[kPhiBar] : (m.o.method == CAS_LSMR ? 0.0 : m.host_scal[kRr]);
-        rep->seconds = ms * 1e-3;
-        rep->setup_seconds = 0;
-    }
-    if (st == CAS_ERR_NOT_CONVERGED) set_error("solver did not reach the tolerance within max_iterations");
-    if (st == CAS_ERR_BREAKDOWN) set_error("solver breakdown (p'A'Ap <= 0 or non-finite scalar)");
-    return st;
+    return err;
 }
+}  // namespace cas
+
+extern "C" {
 
 CAS_API cas_status cas_solve(const cas_csr* a, const cas_solve_opts* o, const double* d_b, double* d_x,
                              cas_solve_report* rep, void* stream)

@@ -385,9 +385,14 @@ CAS_API cas_status cas_fit_weights_device(const cas_patterns* p, const uint64_t*
 
 /* The per-stage fits of the training loop (PatternFit/PatternFit.cpp:53-84:
  * one FitWeights per empty-count stage, one after another) as one batched
- * solve (cas_csr_from_positions_batched + cas_solve_batched): problem q is
- * the next h_problem_rows[q] positions and scores; weights out are
- * problems * cols floats (problem-major), reports one per problem. */
+ * solve: problem q is the next h_problem_rows[q] positions and scores;
+ * weights out are problems * cols floats (problem-major), reports one per
+ * problem.  PCG and CG: one block-diagonal layout and one batched solve
+ * (cas_csr_from_positions_batched + cas_solve_batched).  LSQR and LSMR: one
+ * CSR and one solver per problem, each on its own stream, all run to
+ * tolerance together (the host steps them in turn); each problem's result
+ * is its single fit's.  A problem without rows gets zero weights.  The
+ * first problem that did not converge sets the returned status. */
 CAS_API cas_status cas_fit_weights_batched(const uint64_t* masks, int n_masks, cas_index_mode mode,
                                            const uint64_t* h_positions, const float* h_scores,
                                            const int64_t* h_problem_rows, int problems, const cas_solve_opts* o,

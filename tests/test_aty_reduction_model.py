@@ -8,7 +8,7 @@ range masked, every run end adding the lane's part of its run to the
 accumulator, the segmented scan over lanes whose runs continue from their
 left, and the warp records combined after the block.  The FP64 items use
 the stretch reduction instead (reduce_stretch, stretch_step): each piece's
-range cut into 32 stretches of whole 4-entry words, 8 entries per lane and
+range cut into 32 stretches of whole 4-entry words, 16 entries per lane and
 step, read through round_phys; it is modelled the same way.
 
 On random blocks (several pieces in different groups, runs of one entry up
@@ -271,7 +271,7 @@ def test_model_few_rounds_and_empty_pieces():
         assert acc.v.get(col, 0) == val
 
 
-STEP = 8  # kStretchRun
+STEP = 16  # kStretchRun
 
 
 def reduce_stretch(g32, y, e_lo, e_hi, acc, off, col_lo, col_hi):
@@ -300,8 +300,8 @@ def reduce_stretch(g32, y, e_lo, e_hi, acc, off, col_lo, col_hi):
             for lane in range(LANES):
                 ef = rs + lane * STEP
                 full = ef >= w_lo and ef + STEP <= w_hi
-                if full:  # two 16-byte words: round_phys of ef and ef + 4, 4 entries each
-                    words = [g32[round_phys(ef + 4 * q) + j] for q in range(2) for j in range(4)]
+                if full:  # STEP / 4 16-byte words: round_phys of ef, ef + 4, ..., 4 entries each
+                    words = [g32[round_phys(ef + 4 * q) + j] for q in range(STEP // 4) for j in range(4)]
                     assert words == [at(e) for e in range(ef, ef + STEP)]
                 lo, hi = max(ef, w_lo), min(ef + STEP, w_hi)
                 s = 0

@@ -189,3 +189,40 @@ def test_single_solver_on_identical_rows(cuda, orc):
         assert rep["converged"], (layout, rep)
         idx = orc.group_index(SET8, 1, pos.cpu().numpy().view(np.uint64))
         assert orc.normal_residual(idx, g.index_space_size, b.cpu().numpy(), s.x().cpu().numpy()) <= 1.5e-8
+
+
+@pytest.mark.parametrize("method,precision,scale", [("lsqr", "mixed", True), ("lsmr", "fp64", True),
+                                                    ("lsqr", "fp64", False)])
+def test_batched_least_squares_fits(cuda, orc, method, precision, scale):
+    """LSQR/LSMR through cas_fit_weights_batched_device: one solver per stage,
+    run together on their own streams.  Each stage's weights are bitwise the
+    single fit's of that stage with the same options, reach 1e-8 by the
+    oracle's FP64 residual, and a stage without rows gets zero weights."""
+    sizes = [20000, 0, 9000, 3000]
+    empties = [24, 30, 36, 18]
+    g = cb.GroupIndexer(SET8, "expanded")
+    parts = [cb.generate_positions(90 + q, n, empties[q], empties[q]) for q, n in enumerate(sizes) if n]
+    pos = torch.cat(parts)
+    a_all = cb.MatrixCSR.from_positions(g, pos, "rows")
+    b = cb.generate_targets(a_all, 90)
+    kw = dict(method=method, precision=precision, tol=1e-8, max_iterations=40_000, check_every=50,
+              scale_columns=scale)
+    x, reps, ok = cb.fit_weights_batched(g, pos, b, sizes, **kw)
+    assert ok, reps
+    assert torch.count_nonzero(x[1]) == 0 and reps[1]["iterations"] == 0
+    layout = "blocked" if precision == "mixed" else "rows"
+    cls = cb.LSQR if method == "lsqr" else cb.LSMR
+    row0 = np.concatenate([[0], np.cumsum(sizes)])
+    ph = pos.cpu().numpy().view(np.uint64)
+    for q, n in enumerate(sizes):
+        if not n:
+            continue
+        rs = slice(int(row0[q]), int(row0[q + 1]))
+        single = cb.MatrixCSR.from_positions(g, pos[rs].contiguous(), layout)
+        s = cls(single, b[rs].contiguous(), precision=precision, tol=1e-8, max_iterations=40_000, check_every=50,
+                scale_columns=scale)
+        rep = s.run()
+        assert rep["converged"] and rep["iterations"] == reps[q]["iterations"]
+        assert torch.equal(s.x(), x[q])
+        idx = orc.group_index(SET8, 1, ph[rs])
+        assert orc.normal_residual(idx, g.index_space_size, b[rs].cpu().numpy(), x[q].cpu().numpy()) <= 1.5e-8
