@@ -568,7 +568,7 @@ def compact(res: dict | None) -> dict | None:
     if res is None:
         return None
     keep = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "config", "roofline", "kernels",
-            "gpu_launches", "cpu_baseline", "clocks")
+            "gpu_launches", "cpu_baseline", "clocks", "least_squares")
     out = {k: res[k] for k in keep if k in res}
     br = res.get("breakdown", {})
     out["breakdown"] = {k: v for k, v in br.items() if k != "per_problem"}
@@ -579,7 +579,8 @@ def run_ours_batched(args) -> dict | None:
     """60 per-empty-count fits (empty counts 1..60, rows log-uniform in
     [20k, 1.5M], seeded) as one step: batched layout build + one batched
     mixed-precision PCG to 1e-8 for every problem.  The plain FP64 GPU path
-    fits the same problems one after another on the rows layout."""
+    fits the same problems one after another on the rows layout; the LSQR
+    variants of --lsqr fit them with one solver per problem, run together."""
     import torch
     import torch.distributed as dist
 
@@ -703,6 +704,36 @@ def run_ours_batched(args) -> dict | None:
                  "speedup_batched_mixed_vs_sequential_plain": p0.elapsed_time(p1) * 1e-3 / per_step,
                  "per_problem": [[int(i), round(t, 5)] for i, t in zip(plain_its, plain_t)]}
 
+    # the same fits by LSQR (--lsqr variants), one solver per problem, all
+    # run together on their own streams (cas_fit_weights_batched_device with
+    # method LSQR): one untimed warm-up, then one step on the host clock (the
+    # call returns when every problem has finished)
+    least_squares = {}
+    for method, prec, scaled in LSQ_VARIANTS[args.lsqr]:
+        o = cb.solve_opts(method, prec, args.tol, args.lsqr_max_iterations, 50, 100, scale_columns=scaled)
+        wl = torch.empty(P * cols, dtype=torch.float64, device="cuda")
+
+        def fit_lsq():
+            lreps = (L.SolveReport * P)()
+            st = lib.cas_fit_weights_batched_device(g.handle, C.c_void_p(pos.data_ptr()), C.c_void_p(b.data_ptr()),
+                                                    rows_c.ctypes.data_as(C.c_void_p), P, C.byref(o),
+                                                    C.c_void_p(wl.data_ptr()), lreps, sp)
+            if st not in (L.CAS_OK, L.CAS_ERR_NOT_CONVERGED):
+                L.check(st)
+            return st, lreps
+
+        fit_lsq()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st, lreps = fit_lsq()
+        torch.cuda.synchronize()
+        least_squares[f"{method}_{prec}{'_scaled' if scaled else ''}"] = {
+            "step_s": time.perf_counter() - t0, "converged": st == L.CAS_OK,
+            "iterations_max": max(r.iterations for r in lreps),
+            "iterations_sum": int(sum(r.iterations for r in lreps)),
+            "rel_residual_max": max(r.rel_residual for r in lreps)}
+        del wl
+
     # end to end through the public C ABI with host buffers
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
     pos_h = torch.empty((R, 2), dtype=torch.int64, pin_memory=True)
@@ -749,6 +780,7 @@ def run_ours_batched(args) -> dict | None:
                       "per_problem": [[int(n), int(e), int(r.iterations), int(r.refinements)]
                                       for n, e, r in zip(rows, empties, last)]},
         "plain_fp64": plain,
+        "least_squares": least_squares or None,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                      "frac": ach / peak, "peak_kind": peak_kind, "traffic": ncu_traffic(dom, nnz),
                      "traffic_unit": "bytes per launch, scaled from ncu at 2M rows"},

@@ -503,6 +503,13 @@ extern "C" {
 CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const uint64_t* d_positions, int64_t rows,
                                                  int layouts, void* stream, cas_csr** out)
 {
+    return cas::csr_from_positions(p, d_positions, rows, layouts, static_cast<cudaStream_t>(stream), out, nullptr);
+}
+}  // extern "C"
+
+cas_status cas::csr_from_positions(const cas_patterns* p, const uint64_t* d_positions, int64_t rows, int layouts,
+                                   cudaStream_t s, cas_csr** out, const PositionChunks* chunks)
+{
     cas::NvtxRange nvtx_range("cas_csr_from_positions");
     CAS_REQUIRE(p && out && rows >= 0, CAS_ERR_INVALID_ARGUMENT, "cas_csr_from_positions: bad argument");
     CAS_REQUIRE(rows == 0 || d_positions, CAS_ERR_INVALID_ARGUMENT, "cas_csr_from_positions: null positions");
@@ -517,7 +524,6 @@ CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const ui
     *out = nullptr;
     const DevicePatterns* dp = nullptr;
     CAS_TRY(patterns_on_device(p, &dp));
-    auto s = static_cast<cudaStream_t>(stream);
     auto* a = new cas_csr;
     CAS_CUDA(cudaGetDevice(&a->device));
     a->rows = rows;
@@ -536,7 +542,7 @@ CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const ui
         a->fast = new FastLayout;
         // diag(A'A) comes from the blocked copy unless the row layout builds it
         st = fast_build(*dp, pattern_set(p), d_positions, rows, nullptr, 1,
-                        (layouts & CAS_LAYOUT_ROWS) ? nullptr : a->diag_int, *a->fast, s);
+                        (layouts & CAS_LAYOUT_ROWS) ? nullptr : a->diag_int, *a->fast, s, chunks);
         if (st != CAS_OK) {
             free_csr(a);
             return st;
@@ -549,6 +555,8 @@ CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const ui
             set_error("cas_csr_from_positions: cannot allocate the index array");
             return CAS_ERR_OUT_OF_MEMORY;
         }
+        if (chunks && !(layouts & CAS_LAYOUT_BLOCKED))  // the row layout indexes all rows at once
+            for (int c = 0; c < chunks->n; c++) CAS_CUDA(cudaStreamWaitEvent(s, chunks->ready[c], 0));
         st = launch_index(*dp, d_positions, rows, a->idx, s);
         if (st != CAS_OK) {
             free_csr(a);
@@ -565,6 +573,8 @@ CAS_API cas_status cas_csr_from_positions_layout(const cas_patterns* p, const ui
     *out = a;
     return CAS_OK;
 }
+
+extern "C" {
 
 CAS_API cas_status cas_csr_from_positions_batched(const cas_patterns* p, const uint64_t* d_positions,
                                                   const int64_t* h_problem_rows, int problems, void* stream,

@@ -54,12 +54,12 @@ unsigned fgrid(int64_t work, int per)
 __global__ void __launch_bounds__(256) fast_index_kernel(const Instance* __restrict__ g_inst, int k,
                                                          const uint32_t* __restrict__ tables,
                                                          const ulonglong2* __restrict__ pos, FastGeometry g,
-                                                         uint16_t* __restrict__ a16)
+                                                         uint16_t* __restrict__ a16, int64_t r_begin, int64_t r_end)
 {
     extern __shared__ Instance s_inst[];
     for (int i = threadIdx.x; i < k; i += blockDim.x) s_inst[i] = g_inst[i];
     __syncthreads();
-    for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < g.rows;
+    for (int64_t r = r_begin + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < r_end;
          r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const ulonglong2 ps = pos[r];
         const uint32_t plo = static_cast<uint32_t>(ps.x), phi = static_cast<uint32_t>(ps.x >> 32);
@@ -2054,7 +2054,8 @@ void fast_free(FastLayout& f)
 }
 
 cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint64_t* d_pos, int64_t rows,
-                      const int64_t* prob_rows, int nprob, uint64_t* diag_int, FastLayout& f, cudaStream_t s)
+                      const int64_t* prob_rows, int nprob, uint64_t* diag_int, FastLayout& f, cudaStream_t s,
+                      const PositionChunks* chunks)
 {
     cas::NvtxRange nvtx_range("blocked layout build");
     CAS_REQUIRE(fast_supported(ps), CAS_ERR_INVALID_ARGUMENT, "pattern set does not fit the blocked layout");
@@ -2103,10 +2104,27 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
     CAS_CUDA(dmalloc(&f.sub_start, sizeof(uint32_t) * std::max<int64_t>(nsub, 1)));
     if (rows > 0) {
         const int threads = 256;
-        const unsigned grid = fgrid(rows, threads);
-        { fast_index_kernel<<<grid * 4, threads, sizeof(Instance) * dp.k, s>>>(
-            dp.instances, dp.k, dp.tables, reinterpret_cast<const ulonglong2*>(d_pos), g, f.a16); cas::count_launch(); }
-        CAS_CHECK_LAUNCH();
+        // one launch over all rows, or one per arriving chunk behind its copy
+        const int nch = chunks ? chunks->n : 1;
+        int64_t r0 = 0;
+        for (int c = 0; c < nch; c++) {
+            const int64_t r1 = chunks ? std::min(chunks->row_end[c], rows) : rows;
+            if (chunks) CAS_CUDA(cudaStreamWaitEvent(s, chunks->ready[c], 0));
+            if (r1 > r0) {
+                const unsigned grid = fgrid(r1 - r0, threads);
+                { fast_index_kernel<<<grid * 4, threads, sizeof(Instance) * dp.k, s>>>(
+                    dp.instances, dp.k, dp.tables, reinterpret_cast<const ulonglong2*>(d_pos), g, f.a16, r0, r1);
+                  cas::count_launch(); }
+                CAS_CHECK_LAUNCH();
+            }
+            r0 = std::max(r0, r1);
+        }
+        if (r0 < rows) {  // rows past the last chunk (all chunks are waited for above)
+            { fast_index_kernel<<<fgrid(rows - r0, threads) * 4, threads, sizeof(Instance) * dp.k, s>>>(
+                dp.instances, dp.k, dp.tables, reinterpret_cast<const ulonglong2*>(d_pos), g, f.a16, r0, rows);
+              cas::count_launch(); }
+            CAS_CHECK_LAUNCH();
+        }
         const int64_t groups = g.nblocks * g.npat;
         const unsigned sgrid =
             static_cast<unsigned>(std::min<int64_t>(groups, static_cast<int64_t>(sm_count()) * kSortCtasPerSm));

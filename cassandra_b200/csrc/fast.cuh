@@ -244,8 +244,10 @@ struct FastCols {
 // or a slot count other than 1, 2, 4, 8).
 // prob_rows (host, nprob entries) splits the rows into independent problems
 // (a batch of fits, in row order); null with nprob == 1 is a single fit.
+// chunks (may be null): positions still arriving, indexed chunk by chunk.
 cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint64_t* d_pos, int64_t rows,
-                      const int64_t* prob_rows, int nprob, uint64_t* diag_int, FastLayout& out, cudaStream_t s);
+                      const int64_t* prob_rows, int nprob, uint64_t* diag_int, FastLayout& out, cudaStream_t s,
+                      const PositionChunks* chunks = nullptr);
 bool fast_supported(const PatternSet& ps);
 void fast_free(FastLayout& f);
 
@@ -297,6 +299,9 @@ __device__ __forceinline__ double fast_col_sum(const FastCols& fc, const T* part
     const int sc = static_cast<int>(q) * fc.nsc + fc.chunk_sc[ch];
     const int pos = fc.chunk_acc[ch] + local % kChunkCols;
     double acc = 0;
+    // unrolled so that the partials' loads are issued ahead of the adds,
+    // which keep their order
+#pragma unroll 8
     for (int it = fc.sc_item0[sc]; it < fc.sc_item0[sc + 1]; it++) acc += static_cast<double>(partial[fc.sc_part[it] + pos]);
     return acc;
 }

@@ -144,15 +144,15 @@ CAS_API cas_status cas_generate_targets_rows(const cas_csr* a, uint64_t seed, do
     return CAS_OK;
 }
 
-CAS_API cas_status cas_fit_weights_device(const cas_patterns* p, const uint64_t* d_positions, const double* d_scores,
-                                          int64_t rows, const cas_solve_opts* o, double* d_weights,
-                                          cas_solve_report* rep, void* stream)
+namespace {
+// FitWeights on device buffers.  chunks (may be null): the positions are
+// still arriving in row chunks (the build indexes each behind its copy);
+// scores_ready (may be null): the solve waits for it before reading the
+// scores.
+cas_status fit_weights_device(const cas_patterns* p, const uint64_t* d_positions, const double* d_scores, int64_t rows,
+                              const cas_solve_opts* o, double* d_weights, cas_solve_report* rep, cudaStream_t s,
+                              const PositionChunks* chunks, cudaEvent_t scores_ready)
 {
-    cas::NvtxRange nvtx_range("cas_fit_weights_device");
-    CAS_REQUIRE(p && o && d_weights, CAS_ERR_INVALID_ARGUMENT, "cas_fit_weights_device: null argument");
-    CAS_REQUIRE(rows >= 0 && (rows == 0 || (d_positions && d_scores)), CAS_ERR_INVALID_ARGUMENT,
-                "cas_fit_weights_device: bad rows or buffers");
-    auto s = static_cast<cudaStream_t>(stream);
     cudaEvent_t e0, e1;
     CAS_CUDA(cudaEventCreate(&e0));
     CAS_CUDA(cudaEventCreate(&e1));
@@ -162,7 +162,7 @@ CAS_API cas_status cas_fit_weights_device(const cas_patterns* p, const uint64_t*
     int layouts = CAS_LAYOUT_ROWS;
     if (o->precision == CAS_MIXED && fast_supported(pattern_set(p))) layouts = CAS_LAYOUT_BLOCKED;
     cas_csr* a = nullptr;
-    cas_status st = cas_csr_from_positions_layout(p, d_positions, rows, layouts, stream, &a);
+    cas_status st = csr_from_positions(p, d_positions, rows, layouts, s, &a, chunks);
     if (st != CAS_OK) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -174,10 +174,30 @@ CAS_API cas_status cas_fit_weights_device(const cas_patterns* p, const uint64_t*
     cudaEventElapsedTime(&setup_ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    st = cas_solve(a, o, d_scores, d_weights, rep, stream);
+    if (scores_ready) {
+        const cudaError_t e = cudaStreamWaitEvent(s, scores_ready, 0);
+        if (e != cudaSuccess) {
+            cas_csr_destroy(a);
+            CAS_CUDA(e);
+        }
+    }
+    st = cas_solve(a, o, d_scores, d_weights, rep, s);
     if (rep) rep->setup_seconds = setup_ms * 1e-3;
     cas_csr_destroy(a);
     return st;
+}
+}  // namespace
+
+CAS_API cas_status cas_fit_weights_device(const cas_patterns* p, const uint64_t* d_positions, const double* d_scores,
+                                          int64_t rows, const cas_solve_opts* o, double* d_weights,
+                                          cas_solve_report* rep, void* stream)
+{
+    cas::NvtxRange nvtx_range("cas_fit_weights_device");
+    CAS_REQUIRE(p && o && d_weights, CAS_ERR_INVALID_ARGUMENT, "cas_fit_weights_device: null argument");
+    CAS_REQUIRE(rows >= 0 && (rows == 0 || (d_positions && d_scores)), CAS_ERR_INVALID_ARGUMENT,
+                "cas_fit_weights_device: bad rows or buffers");
+    return fit_weights_device(p, d_positions, d_scores, rows, o, d_weights, rep, static_cast<cudaStream_t>(stream),
+                              nullptr, nullptr);
 }
 
 CAS_API cas_status cas_fit_weights(const uint64_t* masks, int n_masks, cas_index_mode mode,
@@ -202,17 +222,40 @@ CAS_API cas_status cas_fit_weights(const uint64_t* masks, int n_masks, cas_index
         set_error(std::string("cas_fit_weights: ") + cudaGetErrorString(e));
         st = e == cudaErrorMemoryAllocation ? CAS_ERR_OUT_OF_MEMORY : CAS_ERR_CUDA;
     };
+    // The inputs go up on a copy stream: the positions in kInputChunks row
+    // chunks, each indexed as soon as it has landed (while the next one is
+    // copied), then the scores, converted to FP64 there and waited for by the
+    // solve only.
+    constexpr int kInputChunks = 8;
+    cudaStream_t cs = nullptr;
+    cudaEvent_t ready[kInputChunks] = {};
+    cudaEvent_t scores_ready = nullptr;
+    int64_t row_end[kInputChunks];
     cudaError_t e = dmalloc(&d_pos, 16 * std::max<int64_t>(rows, 1));
     if (e == cudaSuccess) e = dmalloc(&d_s32, sizeof(float) * std::max<int64_t>(rows, 1));
     if (e == cudaSuccess) e = dmalloc(&d_s, sizeof(double) * std::max<int64_t>(rows, 1));
     if (e == cudaSuccess) e = dmalloc(&d_w, sizeof(double) * std::max<int64_t>(cols, 1));
     if (e == cudaSuccess) e = dmalloc(&d_w32, sizeof(float) * std::max<int64_t>(cols, 1));
-    if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_pos, h_positions, 16 * rows, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_s32, h_scores, sizeof(float) * rows, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    for (int c = 0; c < kInputChunks && e == cudaSuccess; c++) {
+        const int64_t r0 = rows * c / kInputChunks, r1 = rows * (c + 1) / kInputChunks;
+        row_end[c] = r1;
+        e = cudaEventCreateWithFlags(&ready[c], cudaEventDisableTiming);
+        if (e == cudaSuccess && r1 > r0)
+            e = cudaMemcpyAsync(d_pos + 2 * r0, h_positions + 2 * r0, 16 * (r1 - r0), cudaMemcpyHostToDevice, cs);
+        if (e == cudaSuccess) e = cudaEventRecord(ready[c], cs);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&scores_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess && rows) e = cudaMemcpyAsync(d_s32, h_scores, sizeof(float) * rows, cudaMemcpyHostToDevice, cs);
+    if (e == cudaSuccess && rows) {
+        { f32_to_f64_kernel<<<grid(rows), 256, 0, cs>>>(d_s32, rows, d_s); cas::count_launch(); }
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(scores_ready, cs);
     if (e != cudaSuccess) fail(e);
     if (st == CAS_OK) {
-        { f32_to_f64_kernel<<<grid(rows), 256, 0, s>>>(d_s32, rows, d_s); cas::count_launch(); }
-        st = cas_fit_weights_device(p, d_pos, d_s, rows, o, d_w, rep, s);
+        const PositionChunks chunks{kInputChunks, row_end, ready};
+        st = fit_weights_device(p, d_pos, d_s, rows, o, d_w, rep, s, &chunks, scores_ready);
     }
     if (st == CAS_OK || st == CAS_ERR_NOT_CONVERGED) {
         { f64_to_f32_kernel<<<grid(cols), 256, 0, s>>>(d_w, cols, d_w32); cas::count_launch(); }
@@ -221,6 +264,13 @@ CAS_API cas_status cas_fit_weights(const uint64_t* masks, int n_masks, cas_index
         if (e != cudaSuccess) fail(e);
     }
     cudaStreamSynchronize(s);
+    if (cs) {
+        cudaStreamSynchronize(cs);
+        cudaStreamDestroy(cs);
+    }
+    for (cudaEvent_t ev : ready)
+        if (ev) cudaEventDestroy(ev);
+    if (scores_ready) cudaEventDestroy(scores_ready);
     dfree(d_pos);
     dfree(d_s32);
     dfree(d_s);

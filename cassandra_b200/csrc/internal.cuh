@@ -15,6 +15,16 @@ struct DevicePatterns {
     int64_t cols = 0;
 };
 
+// Positions still arriving on another stream, in row chunks: chunk i (rows
+// [row_end[i-1], row_end[i]), row_end[-1] = 0) is on the device once
+// ready[i] has completed.  A build given this launches the indexing of each
+// chunk behind its event, so that the copy of the next chunk overlaps it.
+struct PositionChunks {
+    int n = 0;
+    const int64_t* row_end = nullptr;
+    const cudaEvent_t* ready = nullptr;
+};
+
 cas_status require_device();
 cas_status patterns_on_device(const cas_patterns* p, const DevicePatterns** out);
 const PatternSet& pattern_set(const cas_patterns* p);
@@ -24,6 +34,10 @@ cas_status launch_index(const DevicePatterns& dp, const uint64_t* d_pos, int64_t
 // statuses in sts, reports in reps (may be null).  Returns the first failed
 // CUDA call's status (solver.cu).
 cas_status solvers_run_all(cas_solver* const* svs, int n, cas_solve_report* reps, cas_status* sts);
+// cas_csr_from_positions_layout with positions that may still be arriving
+// (chunks may be null: all on the device) (csr.cu).
+cas_status csr_from_positions(const cas_patterns* p, const uint64_t* d_positions, int64_t rows, int layouts,
+                              cudaStream_t s, cas_csr** out, const PositionChunks* chunks);
 
 // Entries of one A'y work unit: a column's row list is cut into units of at
 // most kUnit entries, one warp each.
