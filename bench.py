@@ -401,6 +401,9 @@ def run_ours(args) -> dict | None:
         gc.collect()
         torch.cuda.empty_cache()
         summaries["evaluator"] = compact(run_ours_evaluator(summary_args(args)))
+        gc.collect()
+        torch.cuda.empty_cache()
+        summaries["config0"] = run_config0(args)
 
     result = {
         "metric": METRIC,
@@ -793,6 +796,101 @@ def run_ours_batched(args) -> dict | None:
         dist.barrier()
         dist.destroy_process_group()
     return result if rank == 0 else None
+
+
+CONFIG0_METRIC = "seconds for FitWeights(pattern, positions, 200): index, CSR, Jacobi, 200 PCG iterations"
+PATTERNS_5 = PATTERNS_8[:5]
+
+
+def run_config0(args) -> dict:
+    """The reference's CPU-runnable case: 100,000 positions at exactly 30
+    empties, the 5-pattern set expanded (150,903 columns, 40 entries per
+    row), targets by the seeded recipe, Jacobi-PCG from x0 = 0 for exactly
+    200 iterations (FitWeights(pattern, positions, 200),
+    PatternFit/PatternFit.cpp:7-39).  GPU: one step = cas_fit_weights_device
+    (indexing, the layout, Jacobi and the 200 iterations) on the plain FP64
+    path (rows layout) and on the mixed path, CUDA events; e2e through
+    cas_fit_weights with host buffers; CPU: the reference compiled from its
+    sources (FP32 as shipped), indexing and the 200 iterations on the host
+    cores."""
+    import torch
+
+    import cassandra_b200 as cb
+    import oracle
+    from cassandra_b200 import _lib as L
+
+    lib = cb.load()
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    rows, iters, seed = 100_000, 200, args.seed
+    pos = cb.generate_positions(seed, rows, 30, 30)
+    g = cb.GroupIndexer(PATTERNS_5, "expanded")
+    cols, K = g.index_space_size, g.nnz_per_row
+    b = cb.generate_targets(cb.MatrixCSR.from_positions(g, pos, "rows"), seed)
+    w = torch.empty(cols, dtype=torch.float64, device="cuda")
+    out = {}
+    for precision in ("fp64", "mixed"):
+        opts = cb.solve_opts("pcg", precision, 0.0, iters, 50, 50)
+
+        def step():
+            rep = L.SolveReport()
+            L.check(lib.cas_fit_weights_device(g.handle, C.c_void_p(pos.data_ptr()), C.c_void_p(b.data_ptr()), rows,
+                                               C.byref(opts), C.c_void_p(w.data_ptr()), C.byref(rep), sp))
+            return rep
+
+        for _ in range(2):
+            step()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        n = 5
+        e0.record(stream)
+        for _ in range(n):
+            rep = step()
+        e1.record(stream)
+        e1.synchronize()
+        out[precision] = {"step_s": e0.elapsed_time(e1) * 1e-3 / n, "iterations": int(rep.iterations),
+                          "rel_residual": rep.rel_residual}
+    # end to end with host buffers (plain FP64 path)
+    pos_h = np.ascontiguousarray(pos.cpu().numpy().view(np.uint64))
+    sc_h = np.ascontiguousarray(b.cpu().numpy().astype(np.float32))
+    w_h = np.empty(cols, np.float32)
+    masks = np.asarray(PATTERNS_5, np.uint64)
+    opts = cb.solve_opts("pcg", "fp64", 0.0, iters, 50, 50)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rep = L.SolveReport()
+    L.check(lib.cas_fit_weights(masks.ctypes.data_as(C.c_void_p), len(masks), L.CAS_INDEX_EXPANDED,
+                                pos_h.ctypes.data_as(C.c_void_p), sc_h.ctypes.data_as(C.c_void_p), rows,
+                                C.byref(opts), w_h.ctypes.data_as(C.c_void_p), C.byref(rep)))
+    e2e = time.perf_counter() - t0
+    # the reference on the host cores: its indexing (A_Indexer recipe) and its
+    # FP32 PCG, 200 iterations
+    cpu = {"value": None, "unit": "s", "cores": _threads(), "kind": "reference",
+           "sample": f"the whole workload: reference indexing + FP32 PCG, {iters} iterations"}
+    if not args.no_cpu_baseline:
+        try:
+            ref = oracle.ref_lib()
+        except (OSError, FileNotFoundError) as e:
+            cpu["sample"] = f"reference library unavailable: {e}"
+        else:
+            ref.ref_expanded_index.restype = None
+            ref.ref_expanded_index.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p]
+            idx = np.empty((rows, K), np.uint32)
+            x = np.empty(cols, np.float32)
+            res = C.c_float()
+            t0 = time.perf_counter()
+            ref.ref_expanded_index(masks.ctypes.data_as(C.c_void_p), len(masks), pos_h.ctypes.data_as(C.c_void_p),
+                                   rows, idx.ctypes.data_as(C.c_void_p))
+            ref.ref_pcg(K, rows, cols, idx.ctypes.data_as(C.c_void_p), sc_h.ctypes.data_as(C.c_void_p), iters,
+                        x.ctypes.data_as(C.c_void_p), C.byref(res))
+            cpu["value"] = time.perf_counter() - t0
+    return {
+        "metric": CONFIG0_METRIC, "value": out["fp64"]["step_s"], "unit": "s", "higher_is_better": False,
+        "config": {"workload": f"5-pattern expanded fit, {rows} positions at 30 empties, Jacobi-PCG x0 = 0, "
+                               f"{iters} iterations", "rows": rows, "cols": cols, "nnz_per_row": K},
+        "plain_fp64": out["fp64"], "mixed": out["mixed"], "e2e": {"value": e2e, "unit": "s"},
+        "cpu_baseline": cpu,
+    }
 
 
 EVAL_METRIC = "differentiable evaluator: seconds per training epoch (Huber+L2, Adam, batch 65536)"

@@ -263,3 +263,33 @@ def test_checkpoint_resumes_bitwise(cuda, method, layout, precision):
         other.load_state(state)
     with pytest.raises(cb.CasError):
         s2.load_state(state[:100])
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_host_fit_equals_device_fit(cuda, precision):
+    """cas_fit_weights (host buffers: positions uploaded in row chunks, each
+    indexed as soon as it lands; scores uploaded while the layout builds)
+    returns bitwise the weights of cas_fit_weights_device on the same inputs,
+    on a row count that splits into neither whole chunks nor whole blocks."""
+    import ctypes as C
+
+    from cassandra_b200 import _lib as L
+
+    rows = 3 * 16384 + 4099
+    pos = cb.generate_positions_host(29, 0, rows, 20, 40)
+    g = cb.GroupIndexer(SET8, "expanded")
+    d_pos = torch.from_numpy(pos.view(np.int64).reshape(-1, 2)).cuda()
+    scores = cb.generate_targets(cb.MatrixCSR.from_positions(g, d_pos, "rows"), 29).cpu().numpy().astype(np.float32)
+    w_host, rep = cb.fit_weights(SET8, pos, scores, mode="expanded", precision=precision, tol=1e-8)
+    lib = L.load()
+    d_sc = torch.from_numpy(scores.astype(np.float64)).cuda()
+    w = torch.empty(g.index_space_size, dtype=torch.float64, device="cuda")
+    drep = L.SolveReport()
+    opts = cb.solve_opts("pcg", precision, 1e-8)
+    L.check(lib.cas_fit_weights_device(g.handle, C.c_void_p(d_pos.data_ptr()), C.c_void_p(d_sc.data_ptr()), rows,
+                                       C.byref(opts), C.c_void_p(w.data_ptr()), C.byref(drep),
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    assert drep.iterations == rep["iterations"]
+    np.testing.assert_array_equal(w_host, w.cpu().numpy().astype(np.float32))
+    assert rep["converged"], rep
