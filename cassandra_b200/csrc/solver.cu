@@ -937,12 +937,17 @@ struct SolverImpl {
     // the direction when the drift exceeds kRestartDeviation and declares
     // convergence on the true residual.
     template <bool COMP>
-    cas_status issue_pcg_refine(bool restart)
+    // reuse_atb: x is zero and the FP64 partials of the last transposed
+    // product are those of A'b (the set-up's), so A'(b - A x) = A'b is read
+    // from them instead of recomputed.
+    cas_status issue_pcg_refine(bool restart, bool reuse_atb = false)
     {
         const Dev D = dv();
         const int* gate = restart ? nullptr : skip();
-        CAS_TRY((product<COMP, double, double>(x, q64, 2, b, 0, gate)));
-        CAS_TRY(product_t<double>(q64, gate));
+        if (!reuse_atb) {
+            CAS_TRY((product<COMP, double, double>(x, q64, 2, b, 0, gate)));
+            CAS_TRY(product_t<double>(q64, gate));
+        }
         double* pdev = restart ? nullptr : part_c;
         if (mixed)
             { pcg_residual_kernel<COMP, float><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), r, z, p, pg32, d,
@@ -1202,8 +1207,11 @@ struct SolverImpl {
         if (least_squares()) {
             CAS_TRY(issue_lsqr_start(1));
         } else {
-            if (mixed) CAS_TRY(issue_pcg_refine<true>(true));
-            else CAS_TRY(issue_pcg_refine<false>(true));
+            // from x0 = 0 the first residual is A'b, whose partials the norm
+            // above has just read
+            const bool reuse_atb = !x0 && !bn;
+            if (mixed) CAS_TRY(issue_pcg_refine<true>(true, reuse_atb));
+            else CAS_TRY(issue_pcg_refine<false>(true, reuse_atb));
         }
         CAS_TRY(read_state());
         // the initial residual replacement counted as a refinement; reset
