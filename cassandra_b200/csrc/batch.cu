@@ -522,10 +522,12 @@ struct BatchSolver {
     // the recursive residual's drift and restarts the direction of the
     // problems whose drift exceeds kBRestartDeviation; retires the problems
     // whose true residual meets the tolerance.
+    // reuse_atb (set-up): x is zero and the FP64 partials hold A'b, which is
+    // then the residual A'(b - A x) itself.
     template <bool COMP>
-    cas_status refine(Sel sel)
+    cas_status refine(Sel sel, bool reuse_atb = false)
     {
-        CAS_TRY(residual_products(sel));
+        if (!reuse_atb) CAS_TRY(residual_products(sel));
         const BDev d = dev();
         const FastCols fc = fast_cols<double>(*f);
         const double* t64 = static_cast<const double*>(f->t64.partial);
@@ -758,11 +760,12 @@ struct BatchSolver {
                                                                 part_a, all); cas::count_launch(); }
         { bstore_kernel<<<B, kBRedThreads, 0, s>>>(part_a, G, all, d, bBn2); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
-        // r = A'b, z = D r, p = z (x = 0); no replacement due yet
+        // r = A'b (the partials just summed), z = D r, p = z (x = 0); no
+        // replacement due yet
         if (mixed)
-            CAS_TRY(refine<true>(Sel::All));
+            CAS_TRY(refine<true>(Sel::All, true));
         else
-            CAS_TRY(refine<false>(Sel::All));
+            CAS_TRY(refine<false>(Sel::All, true));
         CAS_TRY(read_state());
         // the initial residual counted as a refinement: reset the counters;
         // no replacement is due before the first iteration's schedule
