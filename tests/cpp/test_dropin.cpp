@@ -1,8 +1,8 @@
 // The reference's own usage of its fitting API, compiled unchanged in shape
 // against the drop-in header: MatrixCSR known answers
 // (MathTest/MatrixCSR.cpp:3-55), the FitWeights sequence
-// (PatternFit/PatternFit.cpp:12-38), PCG with another DiagonalPreconditioner
-// and LSQR (Math/Solver.h:78-182).
+// (PatternFit/PatternFit.cpp:12-38), PCG with another DiagonalPreconditioner,
+// LSQR and LSMR (Math/Solver.h:78-287).
 // Prints "OK <name>" per check and exits non-zero on the first failure.
 #include <cmath>
 #include <cstdio>
@@ -126,6 +126,16 @@ int main()
             b2 += double(score[i]) * score[i];
         }
         EXPECT(std::fabs(std::sqrt(n2) - lsqr.Residuum()) <= 1e-3 * std::sqrt(b2), "LSQR Residuum is ||b - Ax||");
+
+        // LSMR (Math/Solver.h:184-287): Residuum() is 0 as in the reference;
+        // its residual ||b - Ax|| decreases from ||b||
+        LSMR lsmr(matrix, Vector(cols, 0.0f), score);
+        lsmr.Iterate(5);
+        Vector el = lsmr.Error();
+        double nl2 = 0;
+        for (int i = 0; i < rows; i++) nl2 += double(el[i]) * el[i];
+        EXPECT(lsmr.Residuum() == 0.0f, "LSMR Residuum is 0");
+        EXPECT(std::sqrt(nl2) < std::sqrt(b2), "LSMR reduces ||b - Ax||");
     }
     std::printf(failures ? "FAILED %d\n" : "ALL OK\n", failures);
     return failures ? 1 : 0;
