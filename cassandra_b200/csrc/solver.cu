@@ -445,6 +445,14 @@ __global__ void precond_kernel(const uint64_t* __restrict__ diag, int64_t n, int
 
 // A caller's DiagonalPreconditioner (Math/Solver.h:25-38): d = the given
 // entries, those that are not normal replaced by 1.
+// out = in rounded to FP32 (the gather copy of a rows-length vector).
+__global__ void to_f32_kernel(const double* __restrict__ in, int64_t n, float* __restrict__ out)
+{
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        out[i] = static_cast<float>(in[i]);
+}
+
 __global__ void user_precond_kernel(const double* __restrict__ in, int64_t n, double* __restrict__ d)
 {
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
@@ -937,10 +945,10 @@ struct SolverImpl {
     // the direction when the drift exceeds kRestartDeviation and declares
     // convergence on the true residual.
     template <bool COMP>
-    // reuse_atb: x is zero and the FP64 partials of the last transposed
-    // product are those of A'b (the set-up's), so A'(b - A x) = A'b is read
-    // from them instead of recomputed.
-    cas_status issue_pcg_refine(bool restart, bool reuse_atb = false)
+    // reuse_atb: x is zero and the partials of the last transposed product
+    // are those of A'b (the set-up's), so A'(b - A x) = A'b is read from them
+    // instead of recomputed; FP32 ones when atb32 (the mixed set-up).
+    cas_status issue_pcg_refine(bool restart, bool reuse_atb = false, bool atb32 = false)
     {
         const Dev D = dv();
         const int* gate = restart ? nullptr : skip();
@@ -950,7 +958,8 @@ struct SolverImpl {
         }
         double* pdev = restart ? nullptr : part_c;
         if (mixed)
-            { pcg_residual_kernel<COMP, float><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), r, z, p, pg32, d,
+            { pcg_residual_kernel<COMP, float><<<n_vec_blocks, kVecThreads, 0, s>>>(
+                  atb32 ? colsum<float>() : colsum<double>(), r, z, p, pg32, d,
                                                                                 part_a, part_b, restart ? 1 : 0, D,
                                                                                 gate, bn, pdev); cas::count_launch(); }
         else
@@ -1187,11 +1196,20 @@ struct SolverImpl {
         CAS_CHECK_LAUNCH();
         const Dev D = dv();
 
-        // ||A'b||^2 (denominator of the relative residual)
+        // ||A'b||^2 (denominator of the relative residual).  The mixed PCG
+        // from x0 = 0 forms A'b with its FP32 products: its first residual
+        // then carries FP32 rounding like every recursive residual of that
+        // solver, and the FP64 replacements and the final FP64 check decide
+        // convergence.
+        const bool atb32 = !bn && !x0 && mixed && fast32 && !least_squares();
         if (bn) {
             ColSum none;
             none.a = a;
             { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(none, nullptr, part_a, bn); cas::count_launch(); }
+        } else if (atb32) {
+            { to_f32_kernel<<<row_grid(R), kVecThreads, 0, s>>>(b, R, static_cast<float*>(q)); cas::count_launch(); }
+            CAS_TRY(product_t<float>(static_cast<const float*>(q), nullptr));
+            { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<float>(), nullptr, part_a, nullptr); cas::count_launch(); }
         } else {
             CAS_TRY(product_t<double>(b, nullptr));
             { norm_units_kernel<true><<<n_vec_blocks, kVecThreads, 0, s>>>(colsum<double>(), nullptr, part_a, nullptr); cas::count_launch(); }
@@ -1210,7 +1228,7 @@ struct SolverImpl {
             // from x0 = 0 the first residual is A'b, whose partials the norm
             // above has just read
             const bool reuse_atb = !x0 && !bn;
-            if (mixed) CAS_TRY(issue_pcg_refine<true>(true, reuse_atb));
+            if (mixed) CAS_TRY(issue_pcg_refine<true>(true, reuse_atb, atb32));
             else CAS_TRY(issue_pcg_refine<false>(true, reuse_atb));
         }
         CAS_TRY(read_state());
