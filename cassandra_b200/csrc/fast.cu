@@ -388,6 +388,109 @@ __global__ void fast_diag_kernel(FastGeometry g, const uint32_t* __restrict__ g3
     }
 }
 
+// The column counts A'1 from the FP32 A'y partials of a vector of ones:
+// every partial (and every sum the A'y kernel forms on the way) counts
+// entries of one column inside one item, so it is an exact float integer
+// while the item holds fewer than 2^24 entries; the column sums add the
+// partials in FP64.
+__global__ void fast_count_kernel(FastCols fc, const float* __restrict__ partial, uint64_t* __restrict__ diag)
+{
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < fc.g.cols;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        diag[c] = static_cast<uint64_t>(fast_col_sum<float>(fc, partial, c));
+}
+
+constexpr int kRepeatRounds = 16;  // G32 rounds of one warp's stretch
+
+// The repeats' share of diag(A'A): a row holding a column m times adds
+// m^2 = m + 2 (1 + 2 + ... + (m - 1)), and the count A'1 holds the m.
+// Equal (column, row) pairs are adjacent in a sorted group and number at
+// most the pattern's slots (<= 8).  A warp takes a stretch of kRepeatRounds
+// rounds of one group; per round each lane holds its 32 consecutive sorted
+// entries (the lane run of the round: eight 16-byte words 512 bytes apart)
+// and counts copies along them, starting from the entry before its run and
+// the number of equal entries that end there (the previous lane's, carried
+// from lane 31 across rounds, and walked back in G32 at the stretch's
+// start).  A lane adds a column's repeats once per run of that column.
+__global__ void __launch_bounds__(256, 4) fast_repeat_kernel(FastGeometry g, const uint32_t* __restrict__ g32,
+                                                             uint64_t* __restrict__ diag, int stretches)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    const int64_t units = g.nblocks * g.npat * stretches;
+    for (int64_t u = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; u < units; u += nwarps) {
+        const int64_t grp = u / stretches;
+        const int st = static_cast<int>(u - grp * stretches);
+        const int64_t b = grp / g.npat;
+        const int p = static_cast<int>(grp - b * g.npat);
+        const int64_t seg = g.seg(b, p), n = g.seg_len(b, p);
+        const int64_t r_begin = static_cast<int64_t>(st) * kRepeatRounds * kRound;
+        if (r_begin >= n) continue;  // uniform over the warp
+        const int64_t r_end = n < r_begin + kRepeatRounds * kRound ? n : r_begin + kRepeatRounds * kRound;
+        uint64_t* dcol = diag + g.col_base(b) + g.off[p];
+        // the entry before the stretch and the equal entries ending there
+        uint32_t carry_last = 0;
+        int carry_tail = 0;  // 0: none before
+        if (r_begin > 0) {
+            carry_last = g32[seg + round_phys(static_cast<uint32_t>(r_begin - 1))];
+            carry_tail = 1;
+            while (carry_tail < r_begin &&
+                   (g32[seg + round_phys(static_cast<uint32_t>(r_begin - 1 - carry_tail))] >> 2) == (carry_last >> 2))
+                carry_tail++;
+        }
+        for (int64_t r0 = r_begin; r0 < r_end; r0 += kRound) {
+            const int64_t lb = r0 + kLaneRun * lane;  // the lane's first sorted position
+            const int64_t rem = r_end - lb;
+            const int cnt = rem <= 0 ? 0 : (rem >= kLaneRun ? kLaneRun : static_cast<int>(rem));
+            uint32_t e[kLaneRun];
+            const uint4* src = reinterpret_cast<const uint4*>(g32 + seg + r0) + lane;
+#pragma unroll
+            for (int q = 0; q < kLaneRun / 4; q++) {
+                uint4 w = make_uint4(0, 0, 0, 0);
+                if (4 * q < cnt) w = src[32 * q];
+                e[4 * q] = w.x, e[4 * q + 1] = w.y, e[4 * q + 2] = w.z, e[4 * q + 3] = w.w;
+            }
+            // the run's last entry and the equal entries ending it (a full
+            // run holds more than 8 entries, so this needs nothing before it)
+            int tail = 0;
+            uint32_t last = 0;
+#pragma unroll
+            for (int k = 0; k < kLaneRun; k++) {
+                if (k < cnt) {
+                    tail = (k > 0 && (e[k] >> 2) == (e[k - 1] >> 2)) ? tail + 1 : 1;
+                    last = e[k];
+                }
+            }
+            uint32_t before = __shfl_up_sync(0xffffffffu, last, 1);
+            int m = __shfl_up_sync(0xffffffffu, tail, 1);
+            if (lane == 0) before = carry_last, m = carry_tail;
+            carry_last = __shfl_sync(0xffffffffu, last, 31);
+            carry_tail = __shfl_sync(0xffffffffu, tail, 31);
+            uint64_t acc = 0;
+            uint32_t acc_col = cnt > 0 ? e[0] >> 16 : 0;
+#pragma unroll
+            for (int k = 0; k < kLaneRun; k++) {
+                if (k < cnt) {
+                    const uint32_t col = e[k] >> 16;
+                    if (col != acc_col) {
+                        if (acc) atomicAdd(reinterpret_cast<unsigned long long*>(dcol + acc_col), acc);
+                        acc = 0;
+                        acc_col = col;
+                    }
+                    if (m > 0 && (e[k] >> 2) == (before >> 2)) {  // copy number m (from 0) of (column, row)
+                        acc += 2 * static_cast<uint64_t>(m);
+                        m++;
+                    } else {
+                        m = 1;
+                    }
+                    before = e[k];
+                }
+            }
+            if (acc) atomicAdd(reinterpret_cast<unsigned long long*>(dcol + acc_col), acc);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // A x on the blocked layout.
 // ---------------------------------------------------------------------------
@@ -1324,8 +1427,10 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
         const int i = static_cast<int>(blk - b0);
         __syncthreads();
         if (!STRETCH && i == 0) prefetch_first_round(g32, bp[0]);
-        const T* yb = y + (g.block_row0(blk) - g.block_row0(y_block0));
-        if ((reinterpret_cast<uintptr_t>(yb) & 15) == 0) {
+        const T* yb = y ? y + (g.block_row0(blk) - g.block_row0(y_block0)) : nullptr;
+        if (!yb) {  // no y: a vector of ones (the column counts A'1)
+            for (int i = threadIdx.x; i < nb; i += kFastThreads) ytile[i] = T(1);
+        } else if ((reinterpret_cast<uintptr_t>(yb) & 15) == 0) {
             // 16-byte loads, kInFlight per thread issued before their stores
             // (FP32: the whole tile in two rounds; FP64 keeps its registers)
             constexpr int kPer = 16 / sizeof(T);
@@ -1346,7 +1451,7 @@ __device__ __forceinline__ void aty_item(const FastGeometry& g, const TView& tv,
         } else {
             for (int i = threadIdx.x; i < nb; i += kFastThreads) ytile[i] = yb[i];
         }
-        if (blk + 1 < tv.item_b1[item])  // the next block's y slice into L2
+        if (y && blk + 1 < tv.item_b1[item])  // the next block's y slice into L2
             prefetch_l2(y + (g.block_row0(blk + 1) - g.block_row0(y_block0)),
                         static_cast<int64_t>(g.block_rows(blk + 1)) * static_cast<int64_t>(sizeof(T)));
         if constexpr (STRETCH) {
@@ -1680,6 +1785,25 @@ void pack_pieces(const Pieces& pc, FastTranspose& t, MetaPack& mp)
 // Builds the work list of one A'y variant from the entry counts per (block,
 // chunk): super-chunks of at most per_sc chunks of columns, each split into
 // block ranges so that items carry about equal numbers of entries.
+// The most G32 entries of any item: its super-chunk's chunks over its blocks.
+int64_t max_item_entries(const FastGeometry& g, const std::vector<int64_t>& entries_bc, const Pieces& pc,
+                         const std::vector<int>& item_sc, const std::vector<int>& item_b0,
+                         const std::vector<int>& item_b1)
+{
+    const int nsc = pc.sc_width.empty() ? 0 : static_cast<int>(pc.sc_width.size());
+    // prefix over blocks of every super-chunk's entries
+    std::vector<int64_t> pre(static_cast<size_t>(g.nblocks + 1) * nsc, 0);
+    for (int64_t b = 0; b < g.nblocks; b++) {
+        for (int sc = 0; sc < nsc; sc++) pre[(b + 1) * nsc + sc] = pre[b * nsc + sc];
+        for (int ch = 0; ch < g.nchunks; ch++) pre[(b + 1) * nsc + pc.chunk_sc[ch]] += entries_bc[b * g.nchunks + ch];
+    }
+    int64_t most = 0;
+    for (size_t i = 0; i < item_sc.size(); i++)
+        most = std::max(most, pre[static_cast<size_t>(item_b1[i]) * nsc + item_sc[i]] -
+                                  pre[static_cast<size_t>(item_b0[i]) * nsc + item_sc[i]]);
+    return most;
+}
+
 cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entries_bc, int per_sc, int items_per_sm,
                        bool range_major, bool pack, bool persistent, size_t elem, FastTranspose& t)
 {
@@ -1739,6 +1863,7 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
         }
         sc_item0.push_back(static_cast<int>(part_by_sc.size()));
         t.nitems = static_cast<int>(item_sc.size());
+        t.max_item_entries = max_item_entries(g, entries_bc, pc, item_sc, item_b0, item_b1);
         mp.add(item_sc, &t.item_sc);
         mp.add(item_b0, &t.item_b0);
         mp.add(item_b1, &t.item_b1);
@@ -1776,6 +1901,7 @@ cas_status build_items(const FastGeometry& g, const std::vector<int64_t>& entrie
     }
     sc_item0.push_back(static_cast<int>(item_sc.size()));
     t.nitems = static_cast<int>(item_sc.size());
+    t.max_item_entries = max_item_entries(g, entries_bc, pc, item_sc, item_b0, item_b1);
     mp.add(item_sc, &t.item_sc);
     mp.add(item_b0, &t.item_b0);
     mp.add(item_b1, &t.item_b1);
@@ -2136,11 +2262,6 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
         dfree(scratch);
         { fast_sub_kernel<<<fgrid(nsub, 256), 256, 0, s>>>(g, f.g32, f.sub_start); cas::count_launch(); }
         CAS_CHECK_LAUNCH();
-        if (diag_int) {
-            { fast_diag_kernel<<<std::min<unsigned>(static_cast<unsigned>(groups), sm_count() * 8), 256, 0, s>>>(
-                g, f.g32, diag_int); cas::count_launch(); }
-            CAS_CHECK_LAUNCH();
-        }
     }
     // entries per (block, chunk) -> work items
     std::vector<int64_t> entries(static_cast<size_t>(g.nblocks * g.nchunks), 0);
@@ -2161,6 +2282,7 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
         // chunk: always range by range
         CAS_TRY(build_items(g, entries, 1, 2, true, true, false, sizeof(double), f.t64));
         if (g.nprob == 1) CAS_TRY(build_block_items(g, f.tb));  // evaluator minibatches: single fits only
+        if (diag_int && rows > 0) CAS_TRY(fast_diag(f, diag_int, s));
     }
     return CAS_OK;
 }
@@ -2168,8 +2290,32 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
 cas_status fast_diag(const FastLayout& f, uint64_t* diag, cudaStream_t s)
 {
     const int64_t groups = f.g.nblocks * f.g.npat;
-    if (groups == 0) return CAS_OK;
-    { fast_diag_kernel<<<std::min<unsigned>(static_cast<unsigned>(groups), sm_count() * 8), 256, 0, s>>>(f.g, f.g32, diag); cas::count_launch(); }
+    if (f.g.cols == 0) return CAS_OK;
+    if (groups == 0) {
+        CAS_CUDA(cudaMemsetAsync(diag, 0, sizeof(uint64_t) * f.g.cols, s));
+        return CAS_OK;
+    }
+    const unsigned grid = std::min<unsigned>(static_cast<unsigned>(groups), sm_count() * 8);
+    int max_slots = 0;
+    for (int p = 0; p < f.g.npat; p++) max_slots = std::max(max_slots, f.g.slots[p]);
+    // a column's count inside an item is at most the item's entries;
+    // CAS_DIAG_FROM_G32=1 takes the direct count whatever the items
+    const char* direct = std::getenv("CAS_DIAG_FROM_G32");
+    const bool exact32 = f.t32.nitems > 0 && f.t32.partial && !(direct && std::strcmp(direct, "1") == 0) &&
+                         f.t32.max_item_entries < (int64_t(1) << 24);
+    if (!exact32) {
+        CAS_CUDA(cudaMemsetAsync(diag, 0, sizeof(uint64_t) * f.g.cols, s));
+        { fast_diag_kernel<<<grid, 256, 0, s>>>(f.g, f.g32, diag); cas::count_launch(); }
+        CAS_CHECK_LAUNCH();
+        return CAS_OK;
+    }
+    CAS_TRY(fast_spmv_t_partials<float>(f, nullptr, nullptr, s));  // no y: ones
+    { fast_count_kernel<<<fgrid(f.g.cols, 256), 256, 0, s>>>(fast_cols<float>(f), static_cast<const float*>(f.t32.partial), diag); cas::count_launch(); }
+    CAS_CHECK_LAUNCH();
+    const int stretches = (kBlockRows * max_slots + kRepeatRounds * kRound - 1) / (kRepeatRounds * kRound);
+    const int64_t warps = groups * stretches;
+    const unsigned rgrid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((warps + 7) / 8, sm_count() * 8)));
+    { fast_repeat_kernel<<<rgrid, 256, 0, s>>>(f.g, f.g32, diag, stretches); cas::count_launch(); }
     CAS_CHECK_LAUNCH();
     return CAS_OK;
 }

@@ -17,7 +17,8 @@
 // lane and row, so that a warp reads a round with 8 coalesced loads.
 // round_phys() maps an entry's position in the sorted order to its place.
 //
-// so that a CTA touches one pattern's columns at a time.  A x stages that
+// Both copies group a block's entries by pattern, so that a CTA touches one
+// pattern's columns at a time.  A x stages that
 // pattern's slice of x in shared memory and gathers from there; A'y stages
 // the block's slice of y in shared memory and reduces the column-sorted
 // entries of one column chunk into a shared-memory accumulator.  Local
@@ -172,6 +173,7 @@ struct FastTranspose {
     int nsc = 0;
     int npieces = 0;
     int nitems = 0;
+    int64_t max_item_entries = 0;  // most G32 entries any item reduces
     int* sc_piece0 = nullptr;  // [nsc + 1] first piece of each super-chunk
     int* sc_width = nullptr;   // [nsc] accumulator columns in use
     int* piece_pat = nullptr;  // [npieces] pattern of the piece
@@ -271,7 +273,8 @@ cas_status fast_spmv(const FastLayout& f, const T* x, Y* y, const double* b, con
 int fast_ax_splits(int64_t nblocks);
 
 // Partials of A' y on the blocked layout (FP32: float partials, FP64:
-// double partials); columns are summed by fast_col_sum().  Items of
+// double partials; a null y stands for a vector of ones); columns are
+// summed by fast_col_sum().  Items of
 // problems whose pdone flag is set are skipped.  An item's columns may be
 // split over several CTAs (column sub-chunks), each writing its columns of
 // the item's partials, so the partial layout does not depend on the split.
@@ -306,7 +309,11 @@ __device__ __forceinline__ double fast_col_sum(const FastCols& fc, const T* part
     return acc;
 }
 
-// Jacobi diagonal from G32 (integer, deterministic).
+// Jacobi diagonal diag(A'A) as integers (deterministic), written over diag:
+// the column counts from the FP32 A'y of a vector of ones (exact while every
+// item holds fewer than 2^24 entries, else counted from G32 directly) plus
+// the share of rows that hold a column more than once.  Needs the FP32 work
+// list.
 cas_status fast_diag(const FastLayout& f, uint64_t* diag, cudaStream_t s);
 
 // Evaluator forward over rows [row0, row1) (FP32 scores) and its adjoint

@@ -70,6 +70,28 @@ def test_aty_schedules_match_oracle(cuda, orc, monkeypatch, sched):
                                   orc.spmv_t(idx, g.index_space_size, yi.astype(np.float64)).astype(np.float32))
     y = torch.randn(rows, dtype=torch.float32, device="cuda")
     assert (y @ a).cpu().numpy().tobytes() == (y @ a).cpu().numpy().tobytes()  # persistent CTAs: same bits
+    # the Jacobi diagonal is counted through this schedule's FP32 A'y
+    with np.errstate(divide="ignore"):
+        np.testing.assert_array_equal(cb.jacobi_preconditioner_of_ata(a).cpu().numpy(),
+                                      orc.jacobi(idx, g.index_space_size))
+
+
+@pytest.mark.parametrize("direct", ["0", "1"])
+@pytest.mark.parametrize("rows,masks,mode", [(70_001, SET8, "expanded"), (16385, list(FIXTURES.values()), "reference"),
+                                             (300, SET5, "reference")])
+def test_jacobi_diagonal_both_paths(cuda, orc, monkeypatch, direct, rows, masks, mode):
+    """diag(A'A) from the column counts A'1 plus the repeats' share, and
+    counted directly from G32 (the path of layouts whose A'y items are too
+    long for exact FP32 counts, forced by CAS_DIAG_FROM_G32=1): both equal
+    the oracle's, rows holding a column several times included."""
+    monkeypatch.setenv("CAS_DIAG_FROM_G32", direct)
+    a, pos, g = _build(rows, masks, mode, "blocked", seed=41)
+    idx = orc.group_index(masks, 0 if mode == "reference" else 1, pos.cpu().numpy().view(np.uint64))
+    srt = np.sort(idx.astype(np.int64), axis=1)
+    assert (srt[:, 1:] == srt[:, :-1]).any()  # repeats present
+    with np.errstate(divide="ignore"):
+        np.testing.assert_array_equal(cb.jacobi_preconditioner_of_ata(a).cpu().numpy(),
+                                      orc.jacobi(idx, g.index_space_size))
 
 
 def test_autotuner_times_candidates_and_caches(cuda, monkeypatch):
