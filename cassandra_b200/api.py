@@ -31,6 +31,18 @@ def _ptr(t: torch.Tensor | None) -> C.c_void_p:
     return C.c_void_p(t.data_ptr() if t is not None else 0)
 
 
+def _sync_before_free() -> None:
+    """Waits for the current stream before a handle's device memory goes back.
+    At interpreter exit the torch module may already be torn down; nothing
+    is left to wait for then."""
+    try:
+        cuda = torch.cuda
+        if cuda.is_initialized():
+            cuda.current_stream().synchronize()
+    except (AttributeError, TypeError):  # module attributes already cleared
+        pass
+
+
 def _require_cuda(t: torch.Tensor, name: str) -> None:
     if not t.is_cuda:
         raise ValueError(f"{name} must be a CUDA tensor")
@@ -167,7 +179,7 @@ class MatrixCSR:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            torch.cuda.current_stream().synchronize()
+            _sync_before_free()
             self._lib.cas_csr_destroy(h)
             self._h = None
 
@@ -577,7 +589,7 @@ class MultiStageScoreEstimator:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            torch.cuda.current_stream().synchronize()
+            _sync_before_free()
             self._lib.cas_estimator_destroy(h)
             self._h = None
 
