@@ -58,19 +58,35 @@ cas_status require_device()
 // position record, then the warp walks the 32 positions (broadcast by
 // shuffles) and lane j evaluates slots j, j + 32, ... of the current
 // position, so each CSR row is written as contiguous 128-byte segments.
-// The slot recipes live in shared memory.
+// The slot recipes live in shared memory, and so does the current
+// position's digit board (64 cells, one byte each, written by lanes 0-15 as
+// one word of four cells each), from which every square costs a byte load.
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256) index_kernel(const Instance* __restrict__ g_inst, int k,
-                                                    const uint32_t* __restrict__ tables,
-                                                    const ulonglong2* __restrict__ pos, int64_t n,
-                                                    uint32_t* __restrict__ out)
+// Cells of squares 4j .. 4j+3 as four bytes: each of the four bits of the
+// player's and the opponent's nibble spread to bit 0 of its byte.
+__device__ __forceinline__ uint32_t cell_word(uint32_t p_nib, uint32_t o_nib)
 {
+    const uint32_t sp = (p_nib * 0x00204081u) & 0x01010101u;  // bit i -> bit 8i
+    const uint32_t so = (o_nib * 0x00204081u) & 0x01010101u;
+    return sp | (so << 1);
+}
+
+constexpr int kRowIndexThreads = 256;
+
+__global__ void __launch_bounds__(kRowIndexThreads) index_kernel(const Instance* __restrict__ g_inst, int k,
+                                                                 const uint32_t* __restrict__ tables,
+                                                                 const ulonglong2* __restrict__ pos, int64_t n,
+                                                                 uint32_t* __restrict__ out)
+{
+    __shared__ __align__(16) uint32_t s_board[kRowIndexThreads / 32][16];
     extern __shared__ Instance s_inst[];
     for (int i = threadIdx.x; i < k; i += blockDim.x) s_inst[i] = g_inst[i];
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
+    uint32_t* wboard = s_board[threadIdx.x >> 5];
+    const uint8_t* board = reinterpret_cast<const uint8_t*>(wboard);
     const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
     for (int64_t base = (static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n;
          base += warps * 32) {
@@ -80,10 +96,13 @@ __global__ void __launch_bounds__(256) index_kernel(const Instance* __restrict__
         for (int i = 0; i < cnt; i++) {
             const uint64_t p = __shfl_sync(0xffffffffu, mine.x, i);
             const uint64_t o = __shfl_sync(0xffffffffu, mine.y, i);
-            const uint32_t plo = static_cast<uint32_t>(p), phi = static_cast<uint32_t>(p >> 32);
-            const uint32_t olo = static_cast<uint32_t>(o), ohi = static_cast<uint32_t>(o >> 32);
+            __syncwarp();  // the previous position's board is read
+            if (lane < 16)
+                wboard[lane] = cell_word(static_cast<uint32_t>(p >> (4 * lane)) & 0xFu,
+                                         static_cast<uint32_t>(o >> (4 * lane)) & 0xFu);
+            __syncwarp();
             uint32_t* row = out + (base + i) * k;
-            for (int j = lane; j < k; j += 32) row[j] = eval_slot(s_inst[j], tables, plo, phi, olo, ohi);
+            for (int j = lane; j < k; j += 32) row[j] = eval_slot_board<1>(s_inst[j], tables, board);
         }
     }
 }
@@ -92,7 +111,7 @@ cas_status launch_index(const DevicePatterns& dp, const uint64_t* d_pos, int64_t
                         cudaStream_t stream)
 {
     if (n == 0) return CAS_OK;
-    const int threads = 256;
+    const int threads = kRowIndexThreads;
     const int64_t warps_needed = (n + 31) / 32;
     const int64_t blocks = std::min<int64_t>((warps_needed + 7) / 8, static_cast<int64_t>(sm_count()) * 8);
     const size_t smem = sizeof(Instance) * dp.k;

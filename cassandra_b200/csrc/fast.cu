@@ -51,19 +51,28 @@ unsigned fgrid(int64_t work, int per)
 // ---------------------------------------------------------------------------
 // Indexing into the blocked layout: one thread per row, all patterns.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) fast_index_kernel(const Instance* __restrict__ g_inst, int k,
+constexpr int kIndexThreads = 256;
+constexpr int kIndexBoardBytes = 64 * kIndexThreads;  // one digit board per thread
+
+// A16 of rows [r_begin, r_end): one thread per row, whose 64 cells go to a
+// digit board first, so that every square of every instance costs one
+// shared-memory byte load and a multiply-add.
+__global__ void __launch_bounds__(kIndexThreads) fast_index_kernel(const Instance* __restrict__ g_inst, int k,
                                                          const uint32_t* __restrict__ tables,
                                                          const ulonglong2* __restrict__ pos, FastGeometry g,
                                                          uint16_t* __restrict__ a16, int64_t r_begin, int64_t r_end)
 {
-    extern __shared__ Instance s_inst[];
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    // the digit boards of the CTA's rows, then the instances
+    uint8_t* board = s_raw + threadIdx.x;
+    Instance* s_inst = reinterpret_cast<Instance*>(s_raw + kIndexBoardBytes);
     for (int i = threadIdx.x; i < k; i += blockDim.x) s_inst[i] = g_inst[i];
     __syncthreads();
     for (int64_t r = r_begin + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < r_end;
          r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const ulonglong2 ps = pos[r];
-        const uint32_t plo = static_cast<uint32_t>(ps.x), phi = static_cast<uint32_t>(ps.x >> 32);
-        const uint32_t olo = static_cast<uint32_t>(ps.y), ohi = static_cast<uint32_t>(ps.y >> 32);
+        fill_board<kIndexThreads>(board, static_cast<uint32_t>(ps.x), static_cast<uint32_t>(ps.x >> 32),
+                                  static_cast<uint32_t>(ps.y), static_cast<uint32_t>(ps.y >> 32));
         int64_t b, rb;
         g.locate_row(r, b, rb);
         for (int p = 0; p < g.npat; p++) {
@@ -72,7 +81,7 @@ __global__ void __launch_bounds__(256) fast_index_kernel(const Instance* __restr
             uint32_t v[8];
 #pragma unroll
             for (int s = 0; s < 8; s++)
-                v[s] = s < ns ? eval_slot(s_inst[s0 + s], tables, plo, phi, olo, ohi) - off : 0u;
+                v[s] = s < ns ? eval_slot_board<kIndexThreads>(s_inst[s0 + s], tables, board) - off : 0u;
             uint16_t* dst = a16 + g.seg(b, p) + rb * ns;
             if (ns == 8) {
                 *reinterpret_cast<uint4*>(dst) =
@@ -2239,7 +2248,7 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
             if (chunks) CAS_CUDA(cudaStreamWaitEvent(s, chunks->ready[c], 0));
             if (r1 > r0) {
                 const unsigned grid = fgrid(r1 - r0, threads);
-                { fast_index_kernel<<<grid * 4, threads, sizeof(Instance) * dp.k, s>>>(
+                { fast_index_kernel<<<grid * 4, kIndexThreads, kIndexBoardBytes + sizeof(Instance) * dp.k, s>>>(
                     dp.instances, dp.k, dp.tables, reinterpret_cast<const ulonglong2*>(d_pos), g, f.a16, r0, r1);
                   cas::count_launch(); }
                 CAS_CHECK_LAUNCH();
@@ -2247,7 +2256,7 @@ cas_status fast_build(const DevicePatterns& dp, const PatternSet& ps, const uint
             r0 = std::max(r0, r1);
         }
         if (r0 < rows) {  // rows past the last chunk (all chunks are waited for above)
-            { fast_index_kernel<<<fgrid(rows - r0, threads) * 4, threads, sizeof(Instance) * dp.k, s>>>(
+            { fast_index_kernel<<<fgrid(rows - r0, kIndexThreads) * 4, kIndexThreads, kIndexBoardBytes + sizeof(Instance) * dp.k, s>>>(
                 dp.instances, dp.k, dp.tables, reinterpret_cast<const ulonglong2*>(d_pos), g, f.a16, r0, rows);
               cas::count_launch(); }
             CAS_CHECK_LAUNCH();
