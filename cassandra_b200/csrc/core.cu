@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(kRowIndexThreads) index_kernel(const Instance*
                                          static_cast<uint32_t>(o >> (4 * lane)) & 0xFu);
             __syncwarp();
             uint32_t* row = out + (base + i) * k;
-            for (int j = lane; j < k; j += 32) row[j] = eval_slot_board<1>(s_inst[j], tables, board);
+            for (int j = lane; j < k; j += 32) row[j] = eval_slot_board_all<1>(s_inst[j], tables, board);
         }
     }
 }

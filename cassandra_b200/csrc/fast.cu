@@ -411,6 +411,14 @@ __global__ void fast_count_kernel(FastCols fc, const float* __restrict__ partial
 
 constexpr int kRepeatRounds = 16;  // G32 rounds of one warp's stretch
 
+// One G32 round (4 KB, on a 16-byte boundary) into L2.
+__device__ __forceinline__ void prefetch_round(const uint32_t* round)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(round),
+                 "r"(static_cast<unsigned>(kRound * sizeof(uint32_t)))
+                 : "memory");
+}
+
 // The repeats' share of diag(A'A): a row holding a column m times adds
 // m^2 = m + 2 (1 + 2 + ... + (m - 1)), and the count A'1 holds the m.
 // Equal (column, row) pairs are adjacent in a sorted group and number at
@@ -437,6 +445,7 @@ __global__ void __launch_bounds__(256, 4) fast_repeat_kernel(FastGeometry g, con
         if (r_begin >= n) continue;  // uniform over the warp
         const int64_t r_end = n < r_begin + kRepeatRounds * kRound ? n : r_begin + kRepeatRounds * kRound;
         uint64_t* dcol = diag + g.col_base(b) + g.off[p];
+        if (lane == 0 && r_begin + kRound < r_end) prefetch_round(g32 + seg + r_begin + kRound);
         // the entry before the stretch and the equal entries ending there
         uint32_t carry_last = 0;
         int carry_tail = 0;  // 0: none before
@@ -448,6 +457,9 @@ __global__ void __launch_bounds__(256, 4) fast_repeat_kernel(FastGeometry g, con
                 carry_tail++;
         }
         for (int64_t r0 = r_begin; r0 < r_end; r0 += kRound) {
+            // the round after next into L2 (whole rounds: the segment's room
+            // ends on a round)
+            if (lane == 0 && r0 + 2 * kRound < r_end) prefetch_round(g32 + seg + r0 + 2 * kRound);
             const int64_t lb = r0 + kLaneRun * lane;  // the lane's first sorted position
             const int64_t rem = r_end - lb;
             const int cnt = rem <= 0 ? 0 : (rem >= kLaneRun ? kLaneRun : static_cast<int>(rem));

@@ -71,12 +71,30 @@ __device__ __forceinline__ uint32_t eval_slot(const Instance& in, const uint32_t
                         [&](const uint8_t* sq, int n) { return digits(sq, n, plo, phi, olo, ohi); });
 }
 
-// eval_slot from the row's digit board (fill_board).
+// eval_slot from the row's digit board (fill_board), every kind inlined.
+template <int STRIDE>
+__device__ __forceinline__ uint32_t eval_slot_board_all(const Instance& in, const uint32_t* __restrict__ tables,
+                                                        const uint8_t* board)
+{
+    return combine_slot(in, tables, [&](const uint8_t* sq, int n) { return board_digits<STRIDE>(sq, n, board); });
+}
+
+template <int STRIDE>
+__device__ __noinline__ uint32_t eval_slot_board_other(const Instance& in, const uint32_t* __restrict__ tables,
+                                                       const uint8_t* board)
+{
+    return eval_slot_board_all<STRIDE>(in, tables, board);
+}
+
+// The same for callers that unroll it over a pattern's slots: only the
+// direct kind (every instance of the expanded mode) is inlined, as the other
+// kinds' code would not fit the instruction cache beside it.
 template <int STRIDE>
 __device__ __forceinline__ uint32_t eval_slot_board(const Instance& in, const uint32_t* __restrict__ tables,
                                                     const uint8_t* board)
 {
-    return combine_slot(in, tables, [&](const uint8_t* sq, int n) { return board_digits<STRIDE>(sq, n, board); });
+    if (in.kind == kDirect) return in.offset + board_digits<STRIDE>(in.sq[0], in.n0, board);
+    return eval_slot_board_other<STRIDE>(in, tables, board);
 }
 
 }  // namespace cas
