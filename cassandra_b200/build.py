@@ -74,7 +74,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     newest = max(o.stat().st_mtime for o in objs)
     if force or not LIB.exists() or LIB.stat().st_mtime < newest:
         # cudart is linked statically (nvcc's default), so the library needs
-        # only the driver at run time.
+        # only the CUDA driver at run time.
         cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fopenmp", "-o", str(LIB), *map(str, objs), "-lgomp"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:

@@ -184,7 +184,12 @@ CAS_API cas_status cas_spmv(const cas_csr* a, cas_dtype dtype, const void* d_x, 
  * computed over the transposed copy: deterministic, no atomics. */
 CAS_API cas_status cas_spmv_t(const cas_csr* a, cas_dtype dtype, const void* d_y, void* d_x, void* stream);
 /* 1 / diag(A'A) with a duplicate of multiplicity m counting m^2
- * (JacobiPreconditionerOfATA, Math/MatrixCSR.cpp:21-47); empty columns give inf. */
+ * (JacobiPreconditionerOfATA, Math/MatrixCSR.cpp:21-47); empty columns give inf.
+ * diag(A'A) is exact integers, counted when the matrix is built: on the
+ * blocked layout from the FP32 transposed product of a vector of ones (exact
+ * while every work item holds fewer than 2^24 entries) plus the repeated
+ * (column, row) pairs, else directly from the sorted copy; the environment
+ * variable CAS_DIAG_FROM_G32=1 selects the direct count for every build. */
 CAS_API cas_status cas_jacobi(const cas_csr* a, cas_dtype dtype, void* d_out, void* stream);
 
 /* ------------------------------------------------------------------------ */
