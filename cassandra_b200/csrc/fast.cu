@@ -119,6 +119,7 @@ constexpr int kSortPerThread = 16;                           // items per thread
 constexpr int kSortTile = kSortThreads * kSortPerThread;     // items per tile
 constexpr int kSortWarpItems = 32 * kSortPerThread;          // items a warp ranks per tile
 constexpr uint32_t kNoPend = 0xFFFFFFFFu;
+constexpr int kSortPrefetchPieces = kSortTile * 4 / 4096;  // 4 KB pieces of a tile of 4-byte items
 
 struct SortSmem {
     uint32_t hist[256];     // digit counts of the first pass (counted from the input)
@@ -216,6 +217,21 @@ __device__ void sort_pass(const uint16_t* __restrict__ a16_in, const uint32_t* _
         sm.pend_pos[t] = kNoPend;
     }
     for (int t0 = 0; t0 < n; t0 += kSortTile) {
+        // the next tile's input into L2 while this one is ranked, in 4 KB
+        // pieces rounded up to 16 bytes (inside the group's room: whole
+        // rounds of A16, whole tiles of the scratch slice)
+        if (t < kSortPrefetchPieces) {
+            const int nt = t0 + kSortTile;
+            const int64_t bytes = static_cast<int64_t>(min(kSortTile, n - nt)) * (FROM_A16 ? 2 : 4);
+            const int64_t lo = static_cast<int64_t>(t) * 4096;
+            if (nt < n && lo < bytes) {
+                const char* src = FROM_A16 ? reinterpret_cast<const char*>(a16_in + nt)
+                                           : reinterpret_cast<const char*>(in + nt);
+                const int64_t piece = bytes - lo < 4096 ? bytes - lo : 4096;
+                const unsigned len = static_cast<unsigned>((piece + 15) & ~int64_t(15));
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src + lo), "r"(len) : "memory");
+            }
+        }
         // 1. rank: the warp's items t0 + warp * 512 + 32 k + lane, in item order
         for (int i = lane; i < 256; i += 32) sm.wcnt[warp][i] = 0;
         __syncwarp();
